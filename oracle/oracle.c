@@ -1,0 +1,723 @@
+/*
+ * CPU FP64 oracle for the oap Arnoldi hot path.  TEST INFRASTRUCTURE ONLY:
+ * the tests, the smoke check and the CPU-baseline leg of the benchmark use it
+ * as the checker; the shipped library never links or calls it.
+ *
+ * It restates, in plain C99 with double / double complex arithmetic:
+ *   - the oap::CuProceduresApi operator surface used by the solver
+ *     (oapMatrixCuda/CuProceduresApi.h:45-421), on the reference's matrix
+ *     layout: split re/im planes, row-major, element (column c, row r) at
+ *     c + r * columns (oapMatrix/MatrixAPI.h:33-40); im == NULL means a
+ *     real matrix;
+ *   - the implicitly restarted Arnoldi method of CuHArnoldi
+ *     (ArnoldiPackage/ArnoldiProcedures.cpp:129-519,
+ *     ArnoldiPackage/oapGenericArnoldiApi.h:61-298) in its textbook form:
+ *     classical Gram-Schmidt with one conditional DGKS pass, Schur form of
+ *     the Hessenberg by shifted QR with deflation, exact-shift implicit
+ *     restarts, Sorensen's residual update, Ritz vectors, and a residual
+ *     stopping rule.
+ *
+ * Parity is pinned by the reference's own fixtures (tests/golden): the
+ * Givens QR samples, the Householder / shifted-QR cases, the Schur
+ * diagonals and the known-spectrum matrices.
+ */
+#include <complex.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+typedef double complex cplx;
+
+static inline cplx ld(const double* re, const double* im, size_t i) {
+  return (re ? re[i] : 0.0) + I * (im ? im[i] : 0.0);
+}
+static inline void st(double* re, double* im, size_t i, cplx v) {
+  if (re) re[i] = creal(v);
+  if (im) im[i] = cimag(v);
+}
+
+/* Unitary rotation G = [p q; -conj(q) conj(p)] with p = conj(x)/r,
+ * q = conj(y)/r, r = sqrt(|x|^2 + |y|^2), so that G [x; y] = [r; 0] with r
+ * real and positive.  For real x, y this is the reference's rotation
+ * c = x/r, s = y/r (CuQRProcedures_GR.h:80-101). */
+static void givens(cplx x, cplx y, cplx* p, cplx* q) {
+  double r = hypot(cabs(x), cabs(y));
+  if (r == 0) { *p = 1; *q = 0; return; }
+  *p = conj(x) / r;
+  *q = conj(y) / r;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Operator surface (oapMatrixCuda/CuProceduresApi.h)                        */
+/* ------------------------------------------------------------------------ */
+
+/* C (ocols x orows) = A (inner x orows) * B (ocols x inner).
+ * CuDotProductSpecificProcedures.h:26-141: out[r][c] = sum_k A[r][k] B[k][c]. */
+void orc_dot_product(double* ore, double* oim, const double* are,
+                     const double* aim, const double* bre, const double* bim,
+                     int ocols, int orows, int inner) {
+#pragma omp parallel for schedule(static) if ((long)ocols * orows * inner > 4000000)
+  for (int r = 0; r < orows; ++r) {
+    for (int c = 0; c < ocols; ++c) {
+      cplx acc = 0;
+      for (int k = 0; k < inner; ++k)
+        acc += ld(are, aim, (size_t)r * inner + k) *
+               ld(bre, bim, (size_t)k * ocols + c);
+      st(ore, oim, (size_t)r * ocols + c, acc);
+    }
+  }
+}
+
+/* out (rows x cols) = in^T or in^H; in is cols x rows.
+ * CuTransposeProcedures.h:141-158, CuConjugateTransposeProcedures.h:141-158. */
+void orc_transpose(double* ore, double* oim, const double* ire,
+                   const double* iim, int cols, int rows, int conjugate) {
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c) {
+      cplx v = ld(ire, iim, (size_t)r * cols + c);
+      st(ore, oim, (size_t)c * rows + r, conjugate ? conj(v) : v);
+    }
+}
+
+/* sqrt(sum |x|^2).  CuProceduresApi.cpp:342-345, 765-803. */
+double orc_magnitude(const double* re, const double* im, long len) {
+  double s = 0;
+  for (long i = 0; i < len; ++i) {
+    double a = re ? re[i] : 0, b = im ? im[i] : 0;
+    s += a * a + b * b;
+  }
+  return sqrt(s);
+}
+
+/* CuProceduresApi.cpp:358-389, CuSumProcedures.h:110-141. */
+void orc_sum(const double* re, const double* im, long len, double* sre,
+             double* sim) {
+  double a = 0, b = 0;
+  for (long i = 0; i < len; ++i) {
+    if (re) a += re[i];
+    if (im) b += im[i];
+  }
+  *sre = a;
+  *sim = b;
+}
+
+/* Kronecker product; out is (c0*c1) x (r0*r1).
+ * CuTensorProductProcedures.h:26-42: out[y][x] = P0[y / r1][x / c1] * P1[y % r1][x % c1]. */
+void orc_tensor_product(double* ore, double* oim, const double* p0re,
+                        const double* p0im, int c0, int r0, const double* p1re,
+                        const double* p1im, int c1, int r1) {
+  int oc = c0 * c1, orow = r0 * r1;
+  for (int y = 0; y < orow; ++y)
+    for (int x = 0; x < oc; ++x) {
+      cplx v0 = ld(p0re, p0im, (size_t)(y / r1) * c0 + x / c1);
+      cplx v1 = ld(p1re, p1im, (size_t)(y % r1) * c1 + x % c1);
+      st(ore, oim, (size_t)y * oc + x, v0 * v1);
+    }
+}
+
+/* out = a + sign * b.  CuAdditionProcedures.h:88-107,
+ * CuSubstractionProcedures.h:92-110 (the oracle indexes the whole grid). */
+void orc_add(double* ore, double* oim, const double* are, const double* aim,
+             const double* bre, const double* bim, long len, double sign) {
+  for (long i = 0; i < len; ++i)
+    st(ore, oim, i, ld(are, aim, i) + sign * ld(bre, bim, i));
+}
+
+/* out = in * (re + i im), a complex scale. */
+void orc_scale(double* ore, double* oim, const double* ire, const double* iim,
+               long len, double sre, double sim) {
+  cplx s = sre + I * sim;
+  for (long i = 0; i < len; ++i) st(ore, oim, i, ld(ire, iim, i) * s);
+}
+
+/* CuVectorUtils.h:27-69: V[r][column] = v[r] for r < length (and back). */
+void orc_set_vector(double* Vre, double* Vim, int Vcols, int column,
+                    const double* vre, const double* vim, int length) {
+  for (int r = 0; r < length; ++r)
+    st(Vre, Vim, (size_t)r * Vcols + column, ld(vre, vim, r));
+}
+void orc_get_vector(double* vre, double* vim, int length, const double* Vre,
+                    const double* Vim, int Vcols, int column) {
+  for (int r = 0; r < length; ++r)
+    st(vre, vim, r, ld(Vre, Vim, (size_t)r * Vcols + column));
+}
+
+/* CuSetMatrixProcedures.h:30-97. */
+void orc_set_diagonal(double* re, double* im, int cols, int rows, double dre,
+                      double dim) {
+  for (int r = 0; r < rows; ++r)
+    for (int c = 0; c < cols; ++c)
+      st(re, im, (size_t)r * cols + c, r == c ? dre + I * dim : 0);
+}
+
+/* CuIsUpperTriangularProcedures.h:29-89: every first-subdiagonal entry
+ * within (-tol, tol) in each present plane (the reference's tol is 1e-3). */
+int orc_is_upper_triangular(const double* re, const double* im, int n,
+                            double tol) {
+  for (int c = 0; c + 1 < n; ++c) {
+    size_t i = (size_t)(c + 1) * n + c;
+    if (re && !(-tol < re[i] && re[i] < tol)) return 0;
+    if (im && !(-tol < im[i] && im[i] < tol)) return 0;
+  }
+  return 1;
+}
+
+/* ---- Givens QR, CuQRProcedures_GR.h:38-150 ------------------------------ */
+/* A = Q R with the reference's rotation order: for column fa, rows fb from
+ * the bottom up to fa+1, rotate rows (fa, fb) with
+ *   c = R[fa][fa] / r, s = R[fb][fa] / r, r = sqrt(|R[fa][fa]|^2 + |R[fb][fa]|^2)
+ * (G[fa][fa] = G[fb][fb] = c, G[fa][fb] = s, G[fb][fa] = -s; lines 80-101),
+ * R <- G R, Q <- Q G^T.  The reference skips a rotation when the INPUT entry
+ * A[fb][fa] is within 1e-5 (line 128); the oracle skips it when the CURRENT
+ * entry of R is exactly zero, which agrees on Hessenberg inputs and keeps R
+ * triangular for general ones.  Complex inputs use the unitary rotation
+ * [c s; -conj(s) c] with real c (the reference's complex G is not unitary). */
+void orc_qr_givens(double* Qre, double* Qim, double* Rre, double* Rim,
+                   const double* Are, const double* Aim, int n) {
+  size_t nn = (size_t)n * n;
+  cplx* R = malloc(nn * sizeof(cplx));
+  cplx* Q = malloc(nn * sizeof(cplx));
+  for (size_t i = 0; i < nn; ++i) R[i] = ld(Are, Aim, i);
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) Q[(size_t)r * n + c] = (r == c);
+  for (int fa = 0; fa < n; ++fa) {
+    for (int fb = n - 1; fb > fa; --fb) {
+      cplx x = R[(size_t)fa * n + fa], y = R[(size_t)fb * n + fa];
+      if (y == 0) continue;
+      cplx p, q;
+      givens(x, y, &p, &q);
+      /* rows: R[fa] <- p R[fa] + q R[fb]; R[fb] <- -conj(q) R[fa] + conj(p) R[fb] */
+      for (int j = 0; j < n; ++j) {
+        cplx a = R[(size_t)fa * n + j], b = R[(size_t)fb * n + j];
+        R[(size_t)fa * n + j] = p * a + q * b;
+        R[(size_t)fb * n + j] = -conj(q) * a + conj(p) * b;
+      }
+      R[(size_t)fb * n + fa] = 0;
+      /* Q <- Q G^H: columns fa, fb */
+      for (int i = 0; i < n; ++i) {
+        cplx a = Q[(size_t)i * n + fa], b = Q[(size_t)i * n + fb];
+        Q[(size_t)i * n + fa] = a * conj(p) + b * conj(q);
+        Q[(size_t)i * n + fb] = -a * q + b * p;
+      }
+    }
+  }
+  for (size_t i = 0; i < nn; ++i) {
+    st(Qre, Qim, i, Q[i]);
+    st(Rre, Rim, i, R[i]);
+  }
+  free(R);
+  free(Q);
+}
+
+/* ---- Householder QR, CuQRProcedures_HT.h:63-131 (real) ----------------- */
+/* For k = 0..n-1: v = column k of the current R below row k, with
+ * v[k] += sign(R[k][k]) * ||R[k:, k]|| (sign(0) = +1, line 40), P = I - 2 v v^T / |v|^2,
+ * R <- P R, Q <- Q P.  The reference takes sqrtf of the norm (line 97); the
+ * oracle keeps double. */
+void orc_qr_householder(double* Q, double* R, const double* A, int n) {
+  size_t nn = (size_t)n * n;
+  double* v = malloc(n * sizeof(double));
+  double* tmp = malloc(n * sizeof(double));
+  memcpy(R, A, nn * sizeof(double));
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) Q[(size_t)r * n + c] = (r == c);
+  for (int k = 0; k < n; ++k) {
+    double s = 0;
+    for (int r = k; r < n; ++r) s += R[(size_t)r * n + k] * R[(size_t)r * n + k];
+    for (int r = 0; r < n; ++r) v[r] = r < k ? 0.0 : R[(size_t)r * n + k];
+    double x = R[(size_t)k * n + k];
+    v[k] += (x < 0 ? -1.0 : 1.0) * sqrt(s);
+    double vv = 0;
+    for (int r = 0; r < n; ++r) vv += v[r] * v[r];
+    if (vv == 0) continue;
+    /* R <- (I - 2 v v^T / vv) R */
+    for (int j = 0; j < n; ++j) {
+      double d = 0;
+      for (int r = k; r < n; ++r) d += v[r] * R[(size_t)r * n + j];
+      d *= 2.0 / vv;
+      for (int r = k; r < n; ++r) R[(size_t)r * n + j] -= d * v[r];
+    }
+    /* Q <- Q (I - 2 v v^T / vv) */
+    for (int i = 0; i < n; ++i) {
+      double d = 0;
+      for (int r = k; r < n; ++r) d += Q[(size_t)i * n + r] * v[r];
+      d *= 2.0 / vv;
+      for (int r = k; r < n; ++r) Q[(size_t)i * n + r] -= d * v[r];
+    }
+    (void)tmp;
+  }
+  free(v);
+  free(tmp);
+}
+
+/* ---- Unshifted QR iteration to triangular form ------------------------- */
+/* oapGenericArnoldiApi.h:268-296 (iram_calcTriangularH_Host): repeat at most
+ * `count` times while not is_upper_triangular(H, tol): H = Q R; H <- R Q;
+ * Qacc <- Q Qacc.  Returns the number of iterations performed. */
+int orc_calc_triangular_h(double* Hre, double* Him, double* Qre, double* Qim,
+                          int n, int count, double tol) {
+  size_t nn = (size_t)n * n;
+  double* qr = malloc(nn * 8), *qi = Him ? malloc(nn * 8) : NULL;
+  double* rr = malloc(nn * 8), *ri = Him ? malloc(nn * 8) : NULL;
+  double* ar = malloc(nn * 8), *ai = Him ? malloc(nn * 8) : NULL;
+  orc_set_diagonal(Qre, Qim, n, n, 1, 0);
+  int it = 0;
+  while (it < count && !orc_is_upper_triangular(Hre, Him, n, tol)) {
+    orc_qr_givens(qr, qi, rr, ri, Hre, Him, n);
+    orc_dot_product(Hre, Him, rr, ri, qr, qi, n, n, n);
+    orc_dot_product(ar, ai, qr, qi, Qre, Qim, n, n, n);
+    memcpy(Qre, ar, nn * 8);
+    if (Qim) memcpy(Qim, ai, nn * 8);
+    ++it;
+  }
+  free(qr); free(qi); free(rr); free(ri); free(ar); free(ai);
+  return it;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Dense complex kernels for the solver (column-major small matrices)       */
+/* ------------------------------------------------------------------------ */
+
+/* Small matrices in the solver are column-major: M[i + j*ld]. */
+#define E(M, i, j, ld) (M)[(size_t)(i) + (size_t)(j) * (ld)]
+
+/* H <- G H G^H acting on rows/cols (k, k+1) (columns of H from 0, rows of
+ * the column update rlo..rhi); Z <- Z G^H. */
+static void rot_apply(cplx* H, cplx* Z, int m, int k, cplx p, cplx q,
+                      int rlo, int rhi) {
+  for (int j = 0; j < m; ++j) {
+    cplx a = E(H, k, j, m), b = E(H, k + 1, j, m);
+    E(H, k, j, m) = p * a + q * b;
+    E(H, k + 1, j, m) = -conj(q) * a + conj(p) * b;
+  }
+  for (int i = rlo; i <= rhi; ++i) {
+    cplx a = E(H, i, k, m), b = E(H, i, k + 1, m);
+    E(H, i, k, m) = a * conj(p) + b * conj(q);
+    E(H, i, k + 1, m) = -a * q + b * p;
+  }
+  if (Z)
+    for (int i = 0; i < m; ++i) {
+      cplx a = E(Z, i, k, m), b = E(Z, i, k + 1, m);
+      E(Z, i, k, m) = a * conj(p) + b * conj(q);
+      E(Z, i, k + 1, m) = -a * q + b * p;
+    }
+}
+
+/* One shifted QR step on the active window [l, h] of Hessenberg H (m x m)
+ * by Givens bulge chasing; applied to whole rows/columns so that H stays a
+ * similarity transform of the input and Z accumulates it. */
+static void qr_sweep(cplx* H, cplx* Z, int m, int l, int h, cplx mu) {
+  for (int k = l; k < h; ++k) {
+    cplx x, y;
+    if (k == l) {
+      x = E(H, l, l, m) - mu;
+      y = E(H, l + 1, l, m);
+    } else {
+      x = E(H, k, k - 1, m);
+      y = E(H, k + 1, k - 1, m);
+    }
+    cplx p, q;
+    givens(x, y, &p, &q);
+    int rhi = k + 2 < m - 1 ? k + 2 : m - 1;
+    rot_apply(H, Z, m, k, p, q, 0, rhi);
+    if (k > l) E(H, k + 1, k - 1, m) = 0;
+  }
+}
+
+/* Complex Schur form of an upper Hessenberg matrix: H <- T = Z^H H Z.
+ * Wilkinson shifts, deflation when |H[i][i-1]| <= eps (|H[i-1][i-1]| + |H[i][i]|),
+ * an exceptional shift every 10 stalled sweeps.  Returns 0 on success. */
+int orc_schur(cplx* H, cplx* Z, int m, int maxit) {
+  const double eps = 2.220446049250313e-16;
+  int h = m - 1, its = 0, total = 0;
+  while (h > 0) {
+    int l = h;
+    while (l > 0) {
+      double s = cabs(E(H, l - 1, l - 1, m)) + cabs(E(H, l, l, m));
+      if (s == 0) s = 1e-300;
+      if (cabs(E(H, l, l - 1, m)) <= eps * s) {
+        E(H, l, l - 1, m) = 0;
+        break;
+      }
+      --l;
+    }
+    if (l == h) { --h; its = 0; continue; }
+    if (++total > maxit * m) return 1;
+    cplx a = E(H, h - 1, h - 1, m), b = E(H, h - 1, h, m);
+    cplx c = E(H, h, h - 1, m), d = E(H, h, h, m);
+    cplx mu;
+    if (its > 0 && its % 10 == 0) {
+      mu = d + cabs(c);
+    } else {
+      cplx tr2 = (a + d) / 2.0, disc = csqrt((a - d) * (a - d) / 4.0 + b * c);
+      cplx m1 = tr2 + disc, m2 = tr2 - disc;
+      mu = cabs(m1 - d) < cabs(m2 - d) ? m1 : m2;
+    }
+    qr_sweep(H, Z, m, l, h, mu);
+    ++its;
+  }
+  /* clean strictly-lower part */
+  for (int j = 0; j < m; ++j)
+    for (int i = j + 1; i < m; ++i) E(H, i, j, m) = 0;
+  return 0;
+}
+
+/* Eigenvector of upper-triangular T (m x m) for T[i][i]: back substitution
+ * with u[i] = 1, u[j > i] = 0; then y = Z u normalised to unit 2-norm. */
+static void tri_eigvec(const cplx* T, const cplx* Z, int m, int idx, cplx* y) {
+  const double eps = 2.220446049250313e-16;
+  cplx* u = calloc(m, sizeof(cplx));
+  cplx lam = E(T, idx, idx, m);
+  double tn = 0;
+  for (int i = 0; i < m; ++i) tn = fmax(tn, cabs(E(T, i, i, m)));
+  double small = eps * (tn > 0 ? tn : 1);
+  u[idx] = 1;
+  for (int i = idx - 1; i >= 0; --i) {
+    cplx acc = 0;
+    for (int j = i + 1; j <= idx; ++j) acc += E(T, i, j, m) * u[j];
+    cplx den = E(T, i, i, m) - lam;
+    if (cabs(den) < small) den = small;
+    u[i] = -acc / den;
+  }
+  double nrm = 0;
+  for (int r = 0; r < m; ++r) {
+    cplx acc = 0;
+    for (int j = 0; j <= idx; ++j) acc += E(Z, r, j, m) * u[j];
+    y[r] = acc;
+    nrm += creal(acc) * creal(acc) + cimag(acc) * cimag(acc);
+  }
+  nrm = sqrt(nrm);
+  for (int r = 0; r < m; ++r) y[r] /= nrm;
+  free(u);
+}
+
+/* ---- wanted-set ordering, ArnoldiPackage/ArnoldiUtils.cpp:24-50 -------- */
+enum { ORC_LM = 0, ORC_LR = 1, ORC_LI = 2, ORC_SM = 3, ORC_SR = 4, ORC_SI = 5 };
+
+static double sort_key(cplx v, int which) {
+  switch (which) {
+    case ORC_LM: return -(creal(v) * creal(v) + cimag(v) * cimag(v));
+    case ORC_LR: return -creal(v);
+    case ORC_LI: return -cimag(v);
+    case ORC_SM: return creal(v) * creal(v) + cimag(v) * cimag(v);
+    case ORC_SR: return creal(v);
+    case ORC_SI: return cimag(v);
+  }
+  return 0;
+}
+
+/* Stable order of indices 0..m-1 by the key (insertion sort, m <= few hundred). */
+void orc_sort_order(const double* re, const double* im, int m, int which,
+                    int* order) {
+  for (int i = 0; i < m; ++i) order[i] = i;
+  for (int i = 1; i < m; ++i) {
+    int o = order[i];
+    double k = sort_key(re[o] + I * (im ? im[o] : 0), which);
+    int j = i - 1;
+    while (j >= 0 && sort_key(re[order[j]] + I * (im ? im[order[j]] : 0), which) > k) {
+      order[j + 1] = order[j];
+      --j;
+    }
+    order[j + 1] = o;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Implicitly restarted Arnoldi (textbook FP64)                             */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  int n, is_complex;
+  const double *are, *aim; /* dense operator, row-major n x n */
+} orc_op;
+
+static void op_apply(const orc_op* op, const cplx* x, cplx* y) {
+  int n = op->n;
+#pragma omp parallel for schedule(static) if (n >= 512)
+  for (int r = 0; r < n; ++r) {
+    const double* ar = op->are + (size_t)r * n;
+    const double* ai = op->aim ? op->aim + (size_t)r * n : NULL;
+    double sr = 0, si = 0;
+    if (ai) {
+      for (int c = 0; c < n; ++c) {
+        double xr = creal(x[c]), xi = cimag(x[c]);
+        sr += ar[c] * xr - ai[c] * xi;
+        si += ar[c] * xi + ai[c] * xr;
+      }
+    } else {
+      for (int c = 0; c < n; ++c) {
+        sr += ar[c] * creal(x[c]);
+        si += ar[c] * cimag(x[c]);
+      }
+    }
+    y[r] = sr + I * si;
+  }
+}
+
+static double vnorm(const cplx* x, int n) {
+  double s = 0;
+  for (int i = 0; i < n; ++i) s += creal(x[i]) * creal(x[i]) + cimag(x[i]) * cimag(x[i]);
+  return sqrt(s);
+}
+
+/* h[0..j] = V[:,0..j]^H w ; w -= V h.  V is n x ld column-major (vector-contiguous). */
+static void cgs_pass(const cplx* V, int n, int j, cplx* w, cplx* h) {
+  for (int i = 0; i <= j; ++i) {
+    cplx acc = 0;
+    const cplx* v = V + (size_t)i * n;
+    for (int r = 0; r < n; ++r) acc += conj(v[r]) * w[r];
+    h[i] = acc;
+  }
+  for (int r = 0; r < n; ++r) {
+    cplx acc = 0;
+    for (int i = 0; i <= j; ++i) acc += V[(size_t)i * n + r] * h[i];
+    w[r] -= acc;
+  }
+}
+
+typedef struct {
+  int restarts, matvecs, converged, dgks_passes;
+} orc_stats;
+
+/* Extend the Arnoldi factorization A V_j = V_j H_j + f e_j^T from length
+ * `start` to m (ArnoldiProcedures.cpp:407-461): v = f / ||f||; w = A v;
+ * h = V^H w; f = w - V h; if ||f|| < rho ||h||: s = V^H f; f -= V s; h += s. */
+static int extend(const orc_op* op, cplx* V, cplx* H, cplx* f, int n, int m,
+                  int start, double rho, int real_basis, orc_stats* st) {
+  cplx* w = malloc(n * sizeof(cplx));
+  cplx* h = malloc(m * sizeof(cplx));
+  cplx* s = malloc(m * sizeof(cplx));
+  for (int j = start; j < m; ++j) {
+    double beta = vnorm(f, n);
+    if (j > 0) E(H, j, j - 1, m) = beta;
+    if (beta == 0) { free(w); free(h); free(s); return -1; }
+    cplx* v = V + (size_t)j * n;
+    for (int r = 0; r < n; ++r) v[r] = f[r] / beta;
+    op_apply(op, v, w);
+    st->matvecs++;
+    cgs_pass(V, n, j, w, h);
+    double mf = vnorm(w, n), mh = vnorm(h, j + 1);
+    if (mf < rho * mh) {
+      cgs_pass(V, n, j, w, s);
+      for (int i = 0; i <= j; ++i) h[i] += s[i];
+      st->dgks_passes++;
+    }
+    if (real_basis) {
+      for (int r = 0; r < n; ++r) w[r] = creal(w[r]);
+      for (int i = 0; i <= j; ++i) h[i] = creal(h[i]);
+    }
+    memcpy(f, w, n * sizeof(cplx));
+    for (int i = 0; i <= j; ++i) E(H, i, j, m) = h[i];
+    for (int i = j + 1; i < m; ++i) E(H, i, j, m) = 0;
+  }
+  free(w); free(h); free(s);
+  return 0;
+}
+
+/*
+ * Solve for the k wanted eigenpairs of the dense operator A (n x n, row-major
+ * split re/im; aim == NULL for a real operator) with Krylov dimension m.
+ *
+ *   v0re/v0im : start vector (normalised here), e.g. seeded U[-1, 1]
+ *   which     : 0 LM (SortLargestValues), 1 LR, 2 LI, 3 SM, 4 SR, 5 SI
+ *   tol       : stop when every wanted Ritz estimate ||f|| |e_m^T y| <=
+ *               tol * |theta_1| (theta_1 = the largest-|.| wanted value)
+ * Outputs: eigenvalues (k), Ritz vectors (k x n, vector-contiguous), the
+ * true relative residuals ||A x - theta x|| / (|theta_1| ||x||), stats[4] =
+ * {restarts, matvecs, converged, dgks passes}.
+ * Returns 0 on success, 1 if maxit restarts did not converge, 2 on a
+ * Schur failure, 3 on invalid arguments.
+ */
+int orc_iram(int n, const double* are, const double* aim, int m, int k,
+             int which, double tol, int maxit, double rho, const double* v0re,
+             const double* v0im, double* evre, double* evim, double* xre,
+             double* xim, double* resid, int* stats) {
+  if (n <= 0 || m > n || k <= 0 || k >= m) return 3;
+  orc_op op = {n, aim != NULL, are, aim};
+  int real_basis = (aim == NULL);
+  cplx* V = calloc((size_t)(m + 1) * n, sizeof(cplx));
+  cplx* Vn = calloc((size_t)m * n, sizeof(cplx));
+  cplx* f = calloc(n, sizeof(cplx));
+  cplx* H = calloc((size_t)m * m, sizeof(cplx));
+  cplx* T = calloc((size_t)m * m, sizeof(cplx));
+  cplx* Z = calloc((size_t)m * m, sizeof(cplx));
+  cplx* Q = calloc((size_t)m * m, sizeof(cplx));
+  cplx* Y = calloc((size_t)k * m, sizeof(cplx));
+  double* tre = malloc(m * 8), *tim = malloc(m * 8);
+  int* order = malloc(m * sizeof(int));
+  orc_stats st = {0, 0, 0, 0};
+  int rc = 1;
+
+  for (int r = 0; r < n; ++r) f[r] = v0re[r] + I * (v0im && !real_basis ? v0im[r] : 0);
+  /* executeInit (oapGenericArnoldiApi.h:61-71) is the j = 0 step of extend */
+  double nv = vnorm(f, n);
+  for (int r = 0; r < n; ++r) f[r] /= nv;
+  int start = 0;
+  cplx theta1 = 0;
+  for (int restart = 0; restart <= maxit; ++restart) {
+    if (extend(&op, V, H, f, n, m, start, rho, real_basis, &st) != 0) {
+      rc = 4;
+      break;
+    }
+    /* Ritz values: Schur form of H (ArnoldiProcedures.cpp:341-349) */
+    memcpy(T, H, (size_t)m * m * sizeof(cplx));
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) E(Z, i, j, m) = (i == j);
+    if (orc_schur(T, Z, m, 60) != 0) { rc = 2; break; }
+    for (int i = 0; i < m; ++i) { tre[i] = creal(E(T, i, i, m)); tim[i] = cimag(E(T, i, i, m)); }
+    /* sortPWorstEigens / getWanted (ArnoldiProcedures.cpp:351-398) */
+    orc_sort_order(tre, tim, m, which, order);
+    theta1 = tre[order[0]] + I * tim[order[0]];
+    double scale = cabs(theta1) > 0 ? cabs(theta1) : 1;
+    double beta = vnorm(f, n);
+    int conv = 1;
+    for (int q = 0; q < k; ++q) {
+      /* eigenvector of T for diagonal entry order[q]; need T ordered so the
+       * back substitution only uses the leading block: solve on T directly. */
+      tri_eigvec(T, Z, m, order[q], Y + (size_t)q * m);
+      double est = beta * cabs(Y[(size_t)q * m + m - 1]);
+      if (est > tol * scale) conv = 0;
+    }
+    if (conv) { rc = 0; st.converged = 1; break; }
+    if (restart == maxit) break;
+    st.restarts++;
+    /* exact shifts (oapGenericArnoldiApi.h:186-222): QR steps with the
+     * unwanted Ritz values on the full H; Q accumulates the rotations. */
+    for (int j = 0; j < m; ++j)
+      for (int i = 0; i < m; ++i) E(Q, i, j, m) = (i == j);
+    for (int q = k; q < m; ++q) {
+      cplx mu = tre[order[q]] + I * tim[order[q]];
+      if (real_basis) mu = creal(mu);
+      qr_sweep(H, Q, m, 0, m - 1, mu);
+    }
+    if (real_basis)
+      for (size_t i = 0; i < (size_t)m * m; ++i) { H[i] = creal(H[i]); Q[i] = creal(Q[i]); }
+    /* iram_fVplusfq (oapGenericArnoldiApi.h:73-102), Sorensen's indices:
+     * f_k = (V Q e_{k}) * H[k][k-1] + f * Q[m-1][k-1]  (0-based) */
+    cplx bk = E(H, k, k - 1, m), sk = E(Q, m - 1, k - 1, m);
+    /* V <- V Q[:, 0..k] (ArnoldiProcedures.cpp:509-519) */
+    for (int j = 0; j <= k; ++j) {
+      cplx* dst = Vn + (size_t)j * n;
+      for (int r = 0; r < n; ++r) {
+        cplx acc = 0;
+        for (int i = 0; i < m; ++i) acc += V[(size_t)i * n + r] * E(Q, i, j, m);
+        dst[r] = acc;
+      }
+    }
+    for (int r = 0; r < n; ++r) f[r] = Vn[(size_t)k * n + r] * bk + f[r] * sk;
+    memcpy(V, Vn, (size_t)k * n * sizeof(cplx));
+    for (int j = k; j < m; ++j)
+      for (int i = 0; i < m; ++i) E(H, i, j, m) = 0;
+    for (int i = k; i < m; ++i)
+      for (int j = 0; j < k; ++j) E(H, i, j, m) = 0;
+    start = k;
+  }
+  /* Ritz vectors x_q = V y_q, eigenvalues, true residuals */
+  cplx* x = malloc(n * sizeof(cplx));
+  cplx* ax = malloc(n * sizeof(cplx));
+  double scale = cabs(theta1) > 0 ? cabs(theta1) : 1;
+  for (int q = 0; q < k; ++q) {
+    cplx lam = tre[order[q]] + I * tim[order[q]];
+    for (int r = 0; r < n; ++r) {
+      cplx acc = 0;
+      for (int i = 0; i < m; ++i) acc += V[(size_t)i * n + r] * Y[(size_t)q * m + i];
+      x[r] = acc;
+    }
+    double nx = vnorm(x, n);
+    for (int r = 0; r < n; ++r) x[r] /= nx;
+    op_apply(&op, x, ax);
+    for (int r = 0; r < n; ++r) ax[r] -= lam * x[r];
+    if (resid) resid[q] = vnorm(ax, n) / scale;
+    if (evre) evre[q] = creal(lam);
+    if (evim) evim[q] = cimag(lam);
+    for (int r = 0; r < n; ++r) {
+      if (xre) xre[(size_t)q * n + r] = creal(x[r]);
+      if (xim) xim[(size_t)q * n + r] = cimag(x[r]);
+    }
+  }
+  if (stats) { stats[0] = st.restarts; stats[1] = st.matvecs; stats[2] = st.converged; stats[3] = st.dgks_passes; }
+  free(x); free(ax);
+  free(V); free(Vn); free(f); free(H); free(T); free(Z); free(Q); free(Y);
+  free(tre); free(tim); free(order);
+  return rc;
+}
+
+/* Schur form of a dense (not necessarily Hessenberg) real/complex matrix,
+ * for the schur fixtures: reduce to Hessenberg by Householder, then
+ * orc_schur.  Writes the eigenvalues (diagonal of T). */
+int orc_eigvals_dense(const double* are, const double* aim, int n, double* wre,
+                      double* wim) {
+  cplx* H = malloc((size_t)n * n * sizeof(cplx));
+  for (int r = 0; r < n; ++r)
+    for (int c = 0; c < n; ++c) E(H, r, c, n) = ld(are, aim, (size_t)r * n + c);
+  cplx* v = malloc(n * sizeof(cplx));
+  for (int k = 0; k + 2 < n + 0 && k < n - 2; ++k) {
+    double s = 0;
+    for (int i = k + 1; i < n; ++i) s += cabs(E(H, i, k, n)) * cabs(E(H, i, k, n));
+    double a = sqrt(s);
+    if (a == 0) continue;
+    cplx x0 = E(H, k + 1, k, n);
+    cplx ph = cabs(x0) > 0 ? x0 / cabs(x0) : 1;
+    for (int i = 0; i < n; ++i) v[i] = 0;
+    for (int i = k + 1; i < n; ++i) v[i] = E(H, i, k, n);
+    v[k + 1] += ph * a;
+    double vv = 0;
+    for (int i = k + 1; i < n; ++i) vv += cabs(v[i]) * cabs(v[i]);
+    for (int j = 0; j < n; ++j) {
+      cplx d = 0;
+      for (int i = k + 1; i < n; ++i) d += conj(v[i]) * E(H, i, j, n);
+      d *= 2.0 / vv;
+      for (int i = k + 1; i < n; ++i) E(H, i, j, n) -= d * v[i];
+    }
+    for (int i = 0; i < n; ++i) {
+      cplx d = 0;
+      for (int j = k + 1; j < n; ++j) d += E(H, i, j, n) * v[j];
+      d *= 2.0 / vv;
+      for (int j = k + 1; j < n; ++j) E(H, i, j, n) -= d * conj(v[j]);
+    }
+  }
+  int rc = orc_schur(H, NULL, n, 60);
+  for (int i = 0; i < n; ++i) { wre[i] = creal(E(H, i, i, n)); wim[i] = cimag(E(H, i, i, n)); }
+  free(H); free(v);
+  return rc;
+}
+
+/* Schur of an m x m Hessenberg given split column-major planes (for tests
+ * of the device Schur kernel): T and Z returned as split planes. */
+int orc_schur_split(const double* hre, const double* him, int m, double* tre,
+                    double* tim, double* zre, double* zim) {
+  size_t mm = (size_t)m * m;
+  cplx* H = malloc(mm * sizeof(cplx));
+  cplx* Z = malloc(mm * sizeof(cplx));
+  for (size_t i = 0; i < mm; ++i) H[i] = ld(hre, him, i);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < m; ++i) E(Z, i, j, m) = (i == j);
+  int rc = orc_schur(H, Z, m, 60);
+  for (size_t i = 0; i < mm; ++i) { st(tre, tim, i, H[i]); st(zre, zim, i, Z[i]); }
+  free(H); free(Z);
+  return rc;
+}
+
+/* Dense complex matvec y = A x on the reference layout (for tests). */
+void orc_matvec(int n, const double* are, const double* aim, const double* xre,
+                const double* xim, double* yre, double* yim) {
+  orc_op op = {n, aim != NULL, are, aim};
+  cplx* x = malloc(n * sizeof(cplx));
+  cplx* y = malloc(n * sizeof(cplx));
+  for (int i = 0; i < n; ++i) x[i] = ld(xre, xim, i);
+  op_apply(&op, x, y);
+  for (int i = 0; i < n; ++i) st(yre, yim, i, y[i]);
+  free(x); free(y);
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
