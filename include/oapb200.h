@@ -1,0 +1,264 @@
+/*
+ * oapb200 - B200-native (sm_100a) Arnoldi eigensolver hot path of oap.
+ *
+ * C ABI.  Plain pointers, sizes and status codes; no C++ or torch types.
+ *
+ * Matrix convention (the reference's math::Matrix, oapMatrix/Matrix.h:31-44,
+ * oapMatrix/MatrixAPI.h:33-40): split real / imaginary planes, row-major,
+ * element (column c, row r) at index c + r * columns.  A NULL plane is absent
+ * (a real matrix has im == NULL).  A vector is 1 column x n rows.  Every
+ * operator-surface call takes FP64 planes, like the reference's
+ * floatt = double (project_generic.mk:34).
+ *
+ * Unlike the reference, the matrix handle lives on the HOST (no device
+ * struct dereference, no global registry lookup): its re / im pointers are
+ * device pointers.
+ *
+ * Errors never abort the process (the reference aborts on every CUDA error,
+ * oapCuda/KernelExecutor.h:34-41); each call returns an oapb_status.
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).  Calls that
+ * return a host scalar synchronise that stream; the others are asynchronous.
+ */
+#ifndef OAPB200_H
+#define OAPB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define OAPB_EXPORT __attribute__((visibility("default")))
+#else
+#define OAPB_EXPORT
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OAPB_API_VERSION 1
+
+typedef enum oapb_status {
+  OAPB_OK = 0,
+  OAPB_ERR_ARG = 1,          /* invalid argument (dims, NULL planes, sizes) */
+  OAPB_ERR_CUDA = 2,         /* a CUDA runtime call failed */
+  OAPB_NOT_CONVERGED = 3,    /* restart budget spent before the residual goal */
+  OAPB_ERR_TIMEOUT = 4,      /* a bounded device-side loop gave up */
+  OAPB_ERR_BOUNDS = 5,       /* a device-side bounds check fired */
+  OAPB_ERR_CALLBACK = 6,     /* the user matvec callback returned non-zero */
+  OAPB_ERR_NOMEM = 7,        /* device allocation failed */
+  OAPB_ERR_BREAKDOWN = 8     /* the Krylov space became invariant before hdim */
+} oapb_status;
+
+/* Element type of a plane. */
+typedef enum oapb_dtype { OAPB_F64 = 0, OAPB_F32 = 1 } oapb_dtype;
+
+/* Host-side matrix handle over device planes (math::Matrix). */
+typedef struct oapb_mat {
+  uint32_t columns;
+  uint32_t rows;
+  void* re;        /* device pointer or NULL */
+  void* im;        /* device pointer or NULL */
+  int32_t dtype;   /* oapb_dtype */
+} oapb_mat;
+
+OAPB_EXPORT const char* oapb_status_string(int status);
+OAPB_EXPORT int oapb_api_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Operator surface: oap::CuProceduresApi (oapMatrixCuda/CuProceduresApi.h)  */
+/* ------------------------------------------------------------------------ */
+
+/* output = params0 * params1 (CuProceduresApi.h:74, CuProceduresApi.cpp:91-105).
+ * output: c x r, params0: k x r, params1: c x k.  A matrix-vector product
+ * (params1 a 1-column vector) takes the coalesced GEMV path. */
+OAPB_EXPORT int oapb_dot_product(const oapb_mat* output, const oapb_mat* params0,
+                     const oapb_mat* params1, void* stream);
+
+/* output = params0^T / params0^H (CuProceduresApi.h:171-173, .cpp:268-307). */
+OAPB_EXPORT int oapb_transpose(const oapb_mat* output, const oapb_mat* params0, void* stream);
+OAPB_EXPORT int oapb_conjugate_transpose(const oapb_mat* output, const oapb_mat* params0,
+                             void* stream);
+
+/* output = sqrt(sum |x|^2) (CuProceduresApi.h:199, .cpp:342-345). */
+OAPB_EXPORT int oapb_magnitude(double* output, const oapb_mat* params0, void* stream);
+
+/* (reoutput, imoutput) = (sum re, sum im) (CuProceduresApi.h:201-202, .cpp:358-389). */
+OAPB_EXPORT int oapb_sum(double* reoutput, double* imoutput, const oapb_mat* matrix,
+             void* stream);
+
+/* Kronecker product (CuProceduresApi.h:57, .cpp:136-156): output is
+ * (c0 * c1) x (r0 * r1), output[y][x] = p0[y / r1][x / c1] * p1[y % r1][x % c1]. */
+OAPB_EXPORT int oapb_tensor_product(const oapb_mat* output, const oapb_mat* params0,
+                        const oapb_mat* params1, void* stream);
+
+/* element-wise output = params0 +/- params1 (CuProceduresApi.h:175-189). */
+OAPB_EXPORT int oapb_add(const oapb_mat* output, const oapb_mat* params0,
+             const oapb_mat* params1, void* stream);
+OAPB_EXPORT int oapb_substract(const oapb_mat* output, const oapb_mat* params0,
+                   const oapb_mat* params1, void* stream);
+
+/* v = f * re (CuProceduresApi.h:215) and v = f * (re + i im), a complex scale
+ * (CuProceduresApi.h:217). */
+OAPB_EXPORT int oapb_multiply_re_constant(const oapb_mat* v, const oapb_mat* f, double re,
+                              void* stream);
+OAPB_EXPORT int oapb_multiply_constant(const oapb_mat* v, const oapb_mat* f, double re,
+                           double im, void* stream);
+
+/* output[r][column] = params0[r] for r < length (CuProceduresApi.h:191-197,
+ * CuVectorUtils.h:27-69) and the inverse copy. */
+OAPB_EXPORT int oapb_set_vector(const oapb_mat* output, uint32_t column,
+                    const oapb_mat* params0, uint32_t length, void* stream);
+OAPB_EXPORT int oapb_get_vector(const oapb_mat* vector, uint32_t length,
+                    const oapb_mat* matrix, uint32_t column, void* stream);
+
+/* I, diag(re + i im), 0 (CuProceduresApi.h:219-223). */
+OAPB_EXPORT int oapb_set_identity(const oapb_mat* matrix, void* stream);
+OAPB_EXPORT int oapb_set_diagonal(const oapb_mat* matrix, double re, double im, void* stream);
+OAPB_EXPORT int oapb_set_zero_matrix(const oapb_mat* matrix, void* stream);
+
+/* Givens QR A = Q R of a square matrix in one CTA (CuProceduresApi.h:303-304,
+ * CuQRProcedures_GR.h:38-150).  Rotation order and sign convention of the
+ * reference (c = x / r, s = y / r), FP64 throughout. */
+OAPB_EXPORT int oapb_qr_givens(const oapb_mat* Q, const oapb_mat* R, const oapb_mat* A,
+                   void* stream);
+
+/* Householder QR of a real square matrix (CuProceduresApi.h:306,
+ * CuQRProcedures_HT.h:63-131). */
+OAPB_EXPORT int oapb_qr_householder(const oapb_mat* Q, const oapb_mat* R, const oapb_mat* A,
+                        void* stream);
+
+/* 1 if every first-subdiagonal entry is within (-tolerance, tolerance) in each
+ * present plane (CuProceduresApi.h:308, CuIsUpperTriangularProcedures.h:29-89;
+ * the reference's fixed tolerance is 1e-3). */
+OAPB_EXPORT int oapb_is_upper_triangular(int* output, const oapb_mat* matrix,
+                             double tolerance, void* stream);
+
+/* Unshifted QR iteration H <- R Q until oapb_is_upper_triangular(H, 1e-3) or
+ * max_iterations, Q accumulating the rotations, entirely on the device
+ * (CuProceduresApi.h:310-312, oapGenericArnoldiApi.h:268-296).  *iterations
+ * (host, may be NULL) receives the count. */
+OAPB_EXPORT int oapb_calc_triangular_h(const oapb_mat* H, const oapb_mat* Q,
+                           uint32_t max_iterations, uint32_t* iterations,
+                           void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Solver: CuHArnoldi / CuHArnoldiCallback (ArnoldiPackage)                  */
+/* ------------------------------------------------------------------------ */
+
+/* Wanted-set ordering, ArnUtils::Sort* (ArnoldiPackage/ArnoldiUtils.cpp:24-50). */
+typedef enum oapb_sort {
+  OAPB_SORT_LARGEST_VALUES = 0,     /* |lambda| descending (LM) */
+  OAPB_SORT_LARGEST_RE = 1,
+  OAPB_SORT_LARGEST_IM = 2,
+  OAPB_SORT_SMALLEST_VALUES = 3,
+  OAPB_SORT_SMALLEST_RE = 4,
+  OAPB_SORT_SMALLEST_IM = 5
+} oapb_sort;
+
+/* Arithmetic of the solve. */
+typedef enum oapb_precision {
+  /* FP64 everywhere: the plain GPU Arnoldi. */
+  OAPB_PREC_FP64 = 0,
+  /* FP32 matvec on an FP32 copy of the operator, FP64 Gram-Schmidt / Schur,
+   * then FP64 subspace refinement of the wanted pairs against the FP64
+   * operator until the residual goal holds. */
+  OAPB_PREC_MIXED = 1
+} oapb_precision;
+
+/* Start vector, oap::InitVVectorType (oapGenericArnoldiApi.h:38-42). */
+typedef enum oapb_init {
+  OAPB_INIT_RANDOM = 0,            /* seeded U[-1, 1] (reference: unseeded) */
+  OAPB_INIT_FIRST_VALUE_IS_ONE = 1,
+  OAPB_INIT_USER = 2               /* oapb_arnoldi_set_start_vector */
+} oapb_init;
+
+/* oap::VecMultiplicationType (oapGenericArnoldiApi.h:32-36). */
+typedef enum oapb_vec_mult { OAPB_TYPE_EIGENVECTOR = 0, OAPB_TYPE_WV = 1 } oapb_vec_mult;
+
+typedef struct oapb_arnoldi_config {
+  uint32_t n;              /* operator dimension (MatrixInfo rows) */
+  uint32_t hdim;           /* Krylov dimension m (CuHArnoldi::execute hdim) */
+  uint32_t wanted;         /* k wanted eigenpairs */
+  int32_t is_complex;      /* operator / basis complex (MatrixInfo isIm) */
+  int32_t sort;            /* oapb_sort */
+  int32_t precision;       /* oapb_precision */
+  int32_t init;            /* oapb_init */
+  uint32_t max_restarts;   /* restart budget (reference: CHECK_* rules) */
+  double tolerance;        /* ||A x - l x|| / (|l_1| ||x||) goal, e.g. 1e-10 */
+  double rho;              /* DGKS threshold (CuHArnoldi::setRho, default 1/3.14) */
+  uint64_t seed;           /* start-vector seed for OAPB_INIT_RANDOM */
+  int32_t profile;         /* 1: time every dense matvec with CUDA events
+                              (oapb_arnoldi_stats.matvec_seconds) */
+} oapb_arnoldi_config;
+
+/* Fill defaults: rho = 1/3.14, tolerance = 1e-10, LM, FP64, random start,
+ * max_restarts = 300. */
+OAPB_EXPORT void oapb_arnoldi_config_default(oapb_arnoldi_config* cfg);
+
+typedef struct oapb_arnoldi_stats {
+  uint32_t restarts;         /* implicit restarts performed */
+  uint32_t matvecs;          /* single-vector operator applications */
+  uint32_t block_matvecs;    /* block (multi-vector) FP64 operator passes */
+  uint32_t dgks_passes;      /* reorthogonalisation passes taken */
+  uint32_t refine_iterations;
+  int32_t converged;
+  double max_residual;       /* largest relative residual of the wanted pairs */
+  double seconds;            /* host wall time of the last solve */
+  double matvec_seconds;     /* device time of the timed dense matvecs (profile) */
+  uint32_t matvec_timed;     /* number of dense matvec launches timed */
+  uint32_t matvec_fp32;      /* of which on the FP32 operator copy */
+} oapb_arnoldi_stats;
+
+typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */
+
+/* User operator, CuHArnoldiCallbackBase::MultiplyFunc
+ * (ArnoldiProceduresImpl.h:51-56): w = A v.  v and w are n-row, 1-column FP64
+ * device vectors, valid only during the call.  Return 0 on success. */
+typedef int (*oapb_matvec_fn)(const oapb_mat* w, const oapb_mat* v, void* user,
+                              int vec_mult_type, void* stream);
+
+OAPB_EXPORT int oapb_arnoldi_create(oapb_arnoldi** handle, const oapb_arnoldi_config* cfg,
+                        void* stream);
+OAPB_EXPORT int oapb_arnoldi_destroy(oapb_arnoldi* handle);
+
+/* Dense operator A (n x n, FP64 device planes, reference layout); im must be
+ * NULL iff cfg.is_complex == 0.  With OAPB_PREC_MIXED the solver keeps an
+ * FP32 copy (library-owned). */
+OAPB_EXPORT int oapb_arnoldi_set_dense_operator(oapb_arnoldi* handle, const oapb_mat* A);
+
+/* User callback operator (CuHArnoldiCallback::setCallback).  Runs FP64. */
+OAPB_EXPORT int oapb_arnoldi_set_callback(oapb_arnoldi* handle, oapb_matvec_fn fn,
+                              void* user);
+
+/* Start vector (device planes, n values each; im ignored for real solves). */
+OAPB_EXPORT int oapb_arnoldi_set_start_vector(oapb_arnoldi* handle, const double* re,
+                                  const double* im);
+
+/* Solve (CuHArnoldi::execute, ArnoldiProcedures.cpp:129-140).
+ * Host outputs (each may be NULL): eigenvalues re / im (wanted values in
+ * sort order), relative residuals.  Device output (may be NULL): eigenvectors,
+ * an n x wanted matrix in the reference layout (column q = eigenvector q),
+ * unit 2-norm.  Returns OAPB_OK or OAPB_NOT_CONVERGED (outputs still hold
+ * the best pairs). */
+OAPB_EXPORT int oapb_arnoldi_solve(oapb_arnoldi* handle, double* eig_re, double* eig_im,
+                       double* residuals, const oapb_mat* eigenvectors);
+
+/* Same as a dense solve, but the operator comes from HOST memory (FP64 planes
+ * in the reference layout); the copy to the device is part of the call. */
+OAPB_EXPORT int oapb_arnoldi_solve_host(oapb_arnoldi* handle, const double* a_re,
+                            const double* a_im, double* eig_re, double* eig_im,
+                            double* residuals, double* eigvec_re,
+                            double* eigvec_im);
+
+OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_stats* out);
+
+/* Relative residual ||A x - lambda x|| / (|lambda_1| ||x||) of pair `index`
+ * of the last solve (CuHArnoldi::testOutcome, ArnoldiProcedures.cpp:521-542,
+ * 642-649), recomputed in FP64 on the device. */
+OAPB_EXPORT int oapb_arnoldi_test_outcome(oapb_arnoldi* handle, uint32_t index, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OAPB200_H */

@@ -1,0 +1,263 @@
+"""oap_b200: B200-native Arnoldi eigensolver hot path of oap.
+
+The product is ``liboapb200.so`` (C ABI, ``include/oapb200.h``); this module
+is a ctypes front end over it for Python callers, the tests and the
+benchmark.  Device buffers are passed as raw pointers (e.g. from torch
+tensors); nothing here computes on the host.  Importing works without a GPU;
+every call needs the built library and raises if it is missing.
+"""
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboapb200.so")
+_LIB = None
+
+OK, ERR_ARG, ERR_CUDA, NOT_CONVERGED, ERR_TIMEOUT, ERR_BOUNDS, ERR_CALLBACK, ERR_NOMEM, ERR_BREAKDOWN = range(9)
+F64, F32 = 0, 1
+SORT = {"LM": 0, "LR": 1, "LI": 2, "SM": 3, "SR": 4, "SI": 5}
+PREC_FP64, PREC_MIXED = 0, 1
+INIT_RANDOM, INIT_FIRST_VALUE_IS_ONE, INIT_USER = 0, 1, 2
+
+
+class OapbError(RuntimeError):
+    def __init__(self, status, where=""):
+        self.status = status
+        super().__init__("%s: %s (status %d)" % (where, status_string(status), status))
+
+
+class Mat(C.Structure):
+    """oapb_mat: host handle over device planes (reference layout)."""
+    _fields_ = [("columns", C.c_uint32), ("rows", C.c_uint32),
+                ("re", C.c_void_p), ("im", C.c_void_p), ("dtype", C.c_int32)]
+
+
+class Config(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("hdim", C.c_uint32), ("wanted", C.c_uint32),
+                ("is_complex", C.c_int32), ("sort", C.c_int32),
+                ("precision", C.c_int32), ("init", C.c_int32),
+                ("max_restarts", C.c_uint32), ("tolerance", C.c_double),
+                ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("restarts", C.c_uint32), ("matvecs", C.c_uint32),
+                ("block_matvecs", C.c_uint32), ("dgks_passes", C.c_uint32),
+                ("refine_iterations", C.c_uint32), ("converged", C.c_int32),
+                ("max_residual", C.c_double), ("seconds", C.c_double),
+                ("matvec_seconds", C.c_double), ("matvec_timed", C.c_uint32),
+                ("matvec_fp32", C.c_uint32)]
+
+
+MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,
+                        C.c_int, C.c_void_p)
+
+
+def lib():
+    """Load liboapb200.so; raise (never fall back) when it is not built."""
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                "liboapb200.so is not built (run python -m oap_b200.build); "
+                "there is no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER
+        vp = C.c_void_p
+        L.oapb_status_string.restype = C.c_char_p
+        L.oapb_status_string.argtypes = [C.c_int]
+        for name, args in {
+            "oapb_dot_product": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_transpose": [P(Mat), P(Mat), vp],
+            "oapb_conjugate_transpose": [P(Mat), P(Mat), vp],
+            "oapb_magnitude": [P(C.c_double), P(Mat), vp],
+            "oapb_sum": [P(C.c_double), P(C.c_double), P(Mat), vp],
+            "oapb_tensor_product": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_add": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_substract": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_multiply_re_constant": [P(Mat), P(Mat), C.c_double, vp],
+            "oapb_multiply_constant": [P(Mat), P(Mat), C.c_double, C.c_double, vp],
+            "oapb_set_vector": [P(Mat), C.c_uint32, P(Mat), C.c_uint32, vp],
+            "oapb_get_vector": [P(Mat), C.c_uint32, P(Mat), C.c_uint32, vp],
+            "oapb_set_identity": [P(Mat), vp],
+            "oapb_set_diagonal": [P(Mat), C.c_double, C.c_double, vp],
+            "oapb_set_zero_matrix": [P(Mat), vp],
+            "oapb_qr_givens": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_qr_householder": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_is_upper_triangular": [P(C.c_int), P(Mat), C.c_double, vp],
+            "oapb_calc_triangular_h": [P(Mat), P(Mat), C.c_uint32, P(C.c_uint32), vp],
+            "oapb_arnoldi_create": [P(vp), P(Config), vp],
+            "oapb_arnoldi_destroy": [vp],
+            "oapb_arnoldi_set_dense_operator": [vp, P(Mat)],
+            "oapb_arnoldi_set_callback": [vp, MATVEC_FN, vp],
+            "oapb_arnoldi_set_start_vector": [vp, vp, vp],
+            "oapb_arnoldi_solve": [vp, P(C.c_double), P(C.c_double), P(C.c_double), P(Mat)],
+            "oapb_arnoldi_solve_host": [vp, vp, vp, P(C.c_double), P(C.c_double),
+                                        P(C.c_double), vp, vp],
+            "oapb_arnoldi_get_stats": [vp, P(Stats)],
+            "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
+        }.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = C.c_int
+        L.oapb_arnoldi_config_default.argtypes = [P(Config)]
+        L.oapb_arnoldi_config_default.restype = None
+        _LIB = L
+    return _LIB
+
+
+def status_string(st):
+    try:
+        return lib().oapb_status_string(st).decode()
+    except RuntimeError:
+        return "status %d" % st
+
+
+def check(st, where=""):
+    if st != OK:
+        raise OapbError(st, where)
+    return st
+
+
+# ---------------------------------------------------------------- torch glue
+def mat(re, im=None, columns=None, rows=None):
+    """Mat over torch tensors (FP64, contiguous, on the device).  A 2-D tensor
+    of shape (rows, columns) maps to the reference's row-major layout; a 1-D
+    tensor is a 1-column vector."""
+    t = re if re is not None else im
+    if t.dim() == 1:
+        r, c = t.shape[0], 1
+    else:
+        r, c = t.shape
+    for x in (re, im):
+        if x is not None:
+            assert x.is_contiguous() and x.is_cuda
+    return Mat(columns or c, rows or r,
+               re.data_ptr() if re is not None else None,
+               im.data_ptr() if im is not None else None,
+               F64 if t.dtype.is_floating_point and t.element_size() == 8 else F32)
+
+
+def _stream(stream):
+    if stream is None:
+        import torch
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return C.c_void_p(stream)
+
+
+class Arnoldi:
+    """CuHArnoldi over the C ABI (oapb_arnoldi_*)."""
+
+    def __init__(self, n, hdim, wanted, is_complex=False, sort="LM",
+                 precision=PREC_FP64, tolerance=1e-10, max_restarts=300,
+                 rho=1.0 / 3.14, seed=1, init=INIT_RANDOM, stream=None,
+                 profile=False):
+        L = lib()
+        cfg = Config()
+        L.oapb_arnoldi_config_default(C.byref(cfg))
+        cfg.n, cfg.hdim, cfg.wanted = n, hdim, wanted
+        cfg.is_complex = int(bool(is_complex))
+        cfg.sort = SORT[sort] if isinstance(sort, str) else int(sort)
+        cfg.precision, cfg.init = precision, init
+        cfg.max_restarts, cfg.tolerance, cfg.rho, cfg.seed = max_restarts, tolerance, rho, seed
+        cfg.profile = int(bool(profile))
+        self.cfg = cfg
+        self.h = C.c_void_p()
+        check(L.oapb_arnoldi_create(C.byref(self.h), C.byref(cfg), _stream(stream)),
+              "oapb_arnoldi_create")
+        self._cb = None
+
+    def close(self):
+        if self.h:
+            lib().oapb_arnoldi_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_operator(self, are, aim=None):
+        self._A = (are, aim)
+        m = mat(are, aim)
+        check(lib().oapb_arnoldi_set_dense_operator(self.h, C.byref(m)),
+              "oapb_arnoldi_set_dense_operator")
+
+    def set_callback(self, fn):
+        """fn(w: Mat, v: Mat, type: int, stream: int) -> int"""
+        def tramp(w, v, user, typ, stream):
+            try:
+                return int(fn(w.contents, v.contents, typ, stream) or 0)
+            except Exception:
+                return 1
+        self._cb = MATVEC_FN(tramp)
+        check(lib().oapb_arnoldi_set_callback(self.h, self._cb, None),
+              "oapb_arnoldi_set_callback")
+
+    def set_start_vector(self, re, im=None):
+        check(lib().oapb_arnoldi_set_start_vector(
+            self.h, C.c_void_p(re.data_ptr()),
+            C.c_void_p(im.data_ptr()) if im is not None else None),
+            "oapb_arnoldi_set_start_vector")
+
+    def solve(self, vectors=None, allow_not_converged=False):
+        k = self.cfg.wanted
+        er, ei, rs = (C.c_double * k)(), (C.c_double * k)(), (C.c_double * k)()
+        vm = None
+        if vectors is not None:
+            vm = mat(vectors[0], vectors[1], columns=k, rows=self.cfg.n)
+        st = lib().oapb_arnoldi_solve(self.h, er, ei, rs, C.byref(vm) if vm else None)
+        if not (st == OK or (allow_not_converged and st == NOT_CONVERGED)):
+            raise OapbError(st, "oapb_arnoldi_solve")
+        return [complex(er[i], ei[i]) for i in range(k)], list(rs), st
+
+    def solve_host(self, are, aim=None, vectors=False):
+        """Dense solve from host FP64 arrays (numpy, C-contiguous)."""
+        import numpy as np
+        k, n = self.cfg.wanted, self.cfg.n
+        er, ei, rs = (C.c_double * k)(), (C.c_double * k)(), (C.c_double * k)()
+        vr = np.zeros((n, k)) if vectors else None
+        vi = np.zeros((n, k)) if (vectors and aim is not None) else None
+        p = lambda a: C.c_void_p(a.ctypes.data) if a is not None else None
+        st = lib().oapb_arnoldi_solve_host(self.h, p(are), p(aim), er, ei, rs, p(vr), p(vi))
+        if st not in (OK, NOT_CONVERGED):
+            raise OapbError(st, "oapb_arnoldi_solve_host")
+        out = [complex(er[i], ei[i]) for i in range(k)], list(rs), st
+        if vectors:
+            return out + (vr if vi is None else vr + 1j * vi,)
+        return out
+
+    def stats(self):
+        s = Stats()
+        check(lib().oapb_arnoldi_get_stats(self.h, C.byref(s)), "oapb_arnoldi_get_stats")
+        return {f: getattr(s, f) for f, _ in Stats._fields_}
+
+    def test_outcome(self, index):
+        out = C.c_double()
+        check(lib().oapb_arnoldi_test_outcome(self.h, index, C.byref(out)),
+              "oapb_arnoldi_test_outcome")
+        return out.value
+
+
+def start_vector(n, seed, is_complex=False):
+    """Host restatement of the library's seeded U[-1, 1) start vector
+    (splitmix64 of seed * 0x100000001B3 + i), for comparing with the oracle."""
+    import numpy as np
+    M = (1 << 64) - 1
+
+    def uni(seed_, i):
+        z = (seed_ * 0x100000001B3 + i) & M
+        z = (z + 0x9E3779B97F4A7C15) & M
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        z = z ^ (z >> 31)
+        return (z >> 11) * (2.0 / 9007199254740992.0) - 1.0
+
+    re = np.array([uni(seed, i) for i in range(n)])
+    if not is_complex:
+        return re
+    s2 = seed ^ 0x5851F42D4C957F2D
+    im = np.array([uni(s2, i) for i in range(n)])
+    return re + 1j * im

@@ -1,0 +1,106 @@
+// Shared helpers for the oapb200 kernels (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "oapb200.h"
+
+#define OAPB_CUDA_TRY(expr)                                  \
+  do {                                                       \
+    cudaError_t _e = (expr);                                 \
+    if (_e != cudaSuccess) return OAPB_ERR_CUDA;             \
+  } while (0)
+
+#define OAPB_LAUNCH_CHECK()                                  \
+  do {                                                       \
+    cudaError_t _e = cudaGetLastError();                     \
+    if (_e != cudaSuccess) return OAPB_ERR_CUDA;             \
+  } while (0)
+
+namespace oapb {
+
+constexpr int kNumSMs = 148;  // B200: 2 dies x 74 SMs
+
+// ---------------------------------------------------------------- complex --
+struct cplx {
+  double re, im;
+};
+
+__host__ __device__ __forceinline__ cplx mk(double r, double i) { return cplx{r, i}; }
+__host__ __device__ __forceinline__ cplx operator+(cplx a, cplx b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cplx operator-(cplx a, cplx b) { return {a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ cplx operator-(cplx a) { return {-a.re, -a.im}; }
+__host__ __device__ __forceinline__ cplx operator*(cplx a, cplx b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__host__ __device__ __forceinline__ cplx operator*(double s, cplx a) { return {s * a.re, s * a.im}; }
+__host__ __device__ __forceinline__ cplx conj(cplx a) { return {a.re, -a.im}; }
+__host__ __device__ __forceinline__ double abs2(cplx a) { return a.re * a.re + a.im * a.im; }
+__host__ __device__ __forceinline__ double cabs_(cplx a) { return hypot(a.re, a.im); }
+__host__ __device__ __forceinline__ cplx cdiv(cplx a, cplx b) {
+  // Smith's algorithm
+  if (fabs(b.re) >= fabs(b.im)) {
+    double r = b.im / b.re, d = b.re + b.im * r;
+    return {(a.re + a.im * r) / d, (a.im - a.re * r) / d};
+  } else {
+    double r = b.re / b.im, d = b.re * r + b.im;
+    return {(a.re * r + a.im) / d, (a.im * r - a.re) / d};
+  }
+}
+__host__ __device__ __forceinline__ cplx csqrt_(cplx z) {
+  double r = hypot(z.re, z.im);
+  if (r == 0) return {0, 0};
+  double t = sqrt(0.5 * (r + fabs(z.re)));
+  if (z.re >= 0) return {t, z.im / (2 * t)};
+  return {fabs(z.im) / (2 * t), z.im >= 0 ? t : -t};
+}
+
+// Unitary rotation G = [p q; -conj(q) conj(p)], p = conj(x)/r, q = conj(y)/r,
+// so G [x; y] = [r; 0] with r = sqrt(|x|^2 + |y|^2) > 0.  For real inputs
+// this is the reference's c = x / r, s = y / r (CuQRProcedures_GR.h:80-101).
+__host__ __device__ __forceinline__ void givens(cplx x, cplx y, cplx& p, cplx& q) {
+  double r = hypot(cabs_(x), cabs_(y));
+  if (r == 0) {
+    p = {1, 0};
+    q = {0, 0};
+    return;
+  }
+  double ir = 1.0 / r;
+  p = {x.re * ir, -x.im * ir};
+  q = {y.re * ir, -y.im * ir};
+}
+
+// ------------------------------------------------------------ warp reduce --
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sumf(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Deterministic U[-1, 1) start vector: splitmix64 of (seed, index).  The
+// same function is restated on the host side of the tests.
+__host__ __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__host__ __device__ __forceinline__ double uniform_pm1(uint64_t seed, uint64_t i) {
+  uint64_t h = splitmix64(seed * 0x100000001B3ull + i);
+  return (double)(h >> 11) * (2.0 / 9007199254740992.0) - 1.0;
+}
+
+inline int grid_for(long work, int per_block, int cap = kNumSMs * 16) {
+  long g = (work + per_block - 1) / per_block;
+  if (g < 1) g = 1;
+  if (g > cap) g = cap;
+  return (int)g;
+}
+
+}  // namespace oapb

@@ -1,0 +1,855 @@
+// Implicitly restarted Arnoldi (CuHArnoldi, ArnoldiPackage/ArnoldiProcedures.cpp)
+// resident on one B200.
+//
+// Layout in HBM (per solver handle):
+//   V      (m + 1) Krylov vectors of n, FP64, vector-contiguous split planes
+//          (the reference stores the basis row-major with stride m,
+//          oapGenericArnoldiApi.h:348-352; here vector j is one contiguous
+//          run so every pass over the basis is coalesced)
+//   f, w   residual and operator output, FP64 split planes
+//   x32    FP32 copy of the current basis vector (mixed form)
+//   A32    FP32 copy of the dense operator (mixed form), reference layout
+//   H, Q   m x m complex, column-major; partial-sum buffers of the Gram-Schmidt
+//
+// One Arnoldi step j (executeArnoldiFactorization, ArnoldiProcedures.cpp:407-461):
+//   k_normalize   v_j = f / ||f||, H[j][j-1] = ||f||          (no host sync)
+//   matvec        w = A v_j                                  (HBM-bound)
+//   k_gs_project  partial V^H w per row chunk
+//   k_gs_reduce   h = sum of partials
+//   k_gs_update   f = w - V h, partial ||f||^2
+//   k_gs_finalize ||f||, ||h||, DGKS decision ||f|| < rho ||h||
+//   (the same four kernels again for the DGKS pass; they return at once
+//    when the device flag says the pass is not needed)
+// After the m-th column one warp computes the Schur form, Ritz pairs,
+// estimates and the exact-shift restart (k_hess); V <- V Q and the Sorensen
+// residual update follow.  The host reads one small status block per
+// restart.
+#include <chrono>
+#include <new>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+#include "common.cuh"
+#include "hess.cuh"
+#include "matvec.cuh"
+
+namespace oapb {
+
+constexpr int kGsThreads = 256;
+constexpr int kUpdThreads = 256;
+
+// ------------------------------------------------------------ vector kernels
+__global__ void k_init_vector(double* fre, double* fim, int n, uint64_t seed, int mode) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    if (mode == OAPB_INIT_RANDOM) {
+      fre[i] = uniform_pm1(seed, (uint64_t)i);
+      if (fim) fim[i] = uniform_pm1(seed ^ 0x5851F42D4C957F2Dull, (uint64_t)i);
+    } else {
+      fre[i] = (i == 0) ? 1.0 : 0.0;
+      if (fim) fim[i] = 0.0;
+    }
+  }
+}
+
+// part[b] = sum |x|^2 over block b's grid-stride share
+__global__ void k_sumsq_partial(const double* __restrict__ xre, const double* __restrict__ xim, long n,
+                                double* part) {
+  double s = 0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double a = xre[i];
+    s += a * a;
+    if (xim) {
+      double b = xim[i];
+      s += b * b;
+    }
+  }
+  __shared__ double red[32];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) part[blockIdx.x] = s;
+  }
+}
+
+__device__ __forceinline__ double block_sum(const double* part, int np) {
+  // executed by one full block; returns the sum to every thread
+  __shared__ double red[32];
+  __shared__ double out;
+  double s = 0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) s += part[i];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) out = s;
+  }
+  __syncthreads();
+  return out;
+}
+
+__global__ void k_set_fnorm(const double* part, int np, DevState* st) {
+  double s = block_sum(part, np);
+  if (threadIdx.x == 0) st->fnorm2 = s;
+}
+
+// v_j = f / ||f|| (FP64 into V, FP32 copy for the mixed matvec);
+// H[j][j-1] = ||f|| (j > 0).
+template <bool CPLX>
+__global__ void k_normalize(const double* __restrict__ fre, const double* __restrict__ fim, int n,
+                            const DevState* st, double* vre, double* vim, float* x32re, float* x32im, cplx* H,
+                            int m, int j, DevState* wst) {
+  const double beta = sqrt(st->fnorm2);
+  const double inv = beta > 0 ? 1.0 / beta : 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    double a = fre[i] * inv;
+    vre[i] = a;
+    if (x32re) x32re[i] = (float)a;
+    if (CPLX) {
+      double b = fim[i] * inv;
+      vim[i] = b;
+      if (x32im) x32im[i] = (float)b;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    if (j > 0) H[j + (long)(j - 1) * m] = cplx{beta, 0};
+    if (!(beta > 0)) wst->status |= 1;
+  }
+}
+
+// Partial projections: part[b * ldp + i] = sum_{r in chunk b} conj(V_i[r]) x[r]
+// for i < nvec.  Warp w of the block handles vectors i = w, w + 8, ...
+template <bool CPLX>
+__global__ void __launch_bounds__(kGsThreads)
+k_gs_project(const double* __restrict__ Vre, const double* __restrict__ Vim, int n, int nvec,
+             const double* __restrict__ xre, const double* __restrict__ xim, int chunk, cplx* part, int ldp,
+             const DevState* st, int gated) {
+  if (gated && !st->dgks) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long r0 = (long)blockIdx.x * chunk;
+  const long r1 = min((long)n, r0 + chunk);
+  for (int i = warp; i < nvec; i += kGsThreads / 32) {
+    const double* vr = Vre + (long)i * n;
+    const double* vi = CPLX ? Vim + (long)i * n : nullptr;
+    double sr = 0, si = 0;
+    for (long r = r0 + lane; r < r1; r += 32) {
+      double a = vr[r], x = xre[r];
+      if (CPLX) {
+        double b = vi[r], y = xim[r];
+        sr += a * x + b * y;   // conj(v) * x
+        si += a * y - b * x;
+      } else {
+        sr += a * x;
+      }
+    }
+    sr = warp_sum(sr);
+    if (CPLX) si = warp_sum(si);
+    if (lane == 0) part[(long)blockIdx.x * ldp + i] = cplx{sr, si};
+  }
+}
+
+// coef[i] = sum_b part[b][i]   (one block)
+__global__ void k_gs_reduce(const cplx* part, int nblk, int ldp, int nvec, cplx* coef, const DevState* st,
+                            int gated) {
+  if (gated && !st->dgks) return;
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) {
+    double a = 0, b = 0;
+    for (int c = 0; c < nblk; ++c) {
+      cplx v = part[(long)c * ldp + i];
+      a += v.re;
+      b += v.im;
+    }
+    coef[i] = cplx{a, b};
+  }
+}
+
+// f = src - sum_i V_i coef[i]; fpart[b] = block's share of ||f||^2
+template <bool CPLX>
+__global__ void __launch_bounds__(kUpdThreads)
+k_gs_update(const double* __restrict__ Vre, const double* __restrict__ Vim, int n, int nvec, const cplx* coef,
+            const double* srcre, const double* srcim, double* fre, double* fim, double* fpart,
+            const DevState* st, int gated) {
+  if (gated && !st->dgks) return;
+  __shared__ cplx c[kMaxM + 1];
+  for (int i = threadIdx.x; i < nvec; i += blockDim.x) c[i] = coef[i];
+  __syncthreads();
+  double s = 0;
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+    double ar = srcre[r], ai = CPLX ? srcim[r] : 0.0;
+    for (int i = 0; i < nvec; ++i) {
+      double vr = Vre[(long)i * n + r];
+      if (CPLX) {
+        double vi = Vim[(long)i * n + r];
+        ar -= vr * c[i].re - vi * c[i].im;
+        ai -= vr * c[i].im + vi * c[i].re;
+      } else {
+        ar -= vr * c[i].re;
+      }
+    }
+    fre[r] = ar;
+    if (CPLX) fim[r] = ai;
+    s += ar * ar + ai * ai;
+  }
+  __shared__ double red[32];
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    s = warp_sum(s);
+    if (threadIdx.x == 0) fpart[blockIdx.x] = s;
+  }
+}
+
+// pass 0: decide DGKS (||f|| < rho ||h||), write H[:, j] = h when no second
+// pass is needed.  pass 1: h += s, write H[:, j].  Zeroes H below the column.
+__global__ void k_gs_finalize(const double* fpart, int np, cplx* h, const cplx* s, cplx* H, int m, int j,
+                              double rho, DevState* st, int pass, int real_basis) {
+  if (pass == 1 && !st->dgks) return;
+  const double f2 = block_sum(fpart, np);
+  const int nvec = j + 1;
+  if (pass == 0) {
+    __shared__ double hn;
+    if (threadIdx.x == 0) {
+      double a = 0;
+      for (int i = 0; i < nvec; ++i) a += abs2(h[i]);
+      hn = a;
+    }
+    __syncthreads();
+    const int dg = sqrt(f2) < rho * sqrt(hn);
+    if (threadIdx.x == 0) {
+      st->dgks = dg;
+      st->hnorm2 = hn;
+      st->fnorm2 = f2;
+    }
+    if (!dg)
+      for (int i = threadIdx.x; i < m; i += blockDim.x) {
+        cplx v = i < nvec ? h[i] : cplx{0, 0};
+        if (real_basis) v.im = 0;
+        H[i + (long)j * m] = v;
+      }
+  } else {
+    for (int i = threadIdx.x; i < m; i += blockDim.x) {
+      cplx v = i < nvec ? h[i] + s[i] : cplx{0, 0};
+      if (real_basis) v.im = 0;
+      H[i + (long)j * m] = v;
+    }
+    if (threadIdx.x == 0) {
+      st->fnorm2 = f2;
+      st->dgks_count += 1;
+    }
+  }
+}
+
+// out_j = sum_{i < nin} V_i C[i + j * ldc] for j < nout (V vector-contiguous,
+// C column-major complex).  8 output columns per pass over V.
+template <bool CPLX>
+__global__ void k_vq(const double* __restrict__ Vre, const double* __restrict__ Vim, int n, int nin,
+                     const cplx* __restrict__ C, int ldc, int nout, double* outre, double* outim) {
+  extern __shared__ cplx cs[];
+  for (int t = threadIdx.x; t < nin * nout; t += blockDim.x) cs[t] = C[(t % nin) + (long)(t / nin) * ldc];
+  __syncthreads();
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+    for (int j0 = 0; j0 < nout; j0 += 8) {
+      cplx acc[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) acc[q] = {0, 0};
+      const int jn = min(8, nout - j0);
+      for (int i = 0; i < nin; ++i) {
+        cplx v = {Vre[(long)i * n + r], CPLX ? Vim[(long)i * n + r] : 0.0};
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+          if (q < jn) acc[q] = acc[q] + v * cs[i + (j0 + q) * nin];
+      }
+      for (int q = 0; q < jn; ++q) {
+        outre[(long)(j0 + q) * n + r] = acc[q].re;
+        if (CPLX) outim[(long)(j0 + q) * n + r] = acc[q].im;
+      }
+    }
+  }
+}
+
+// f = vk * beta_hat + f * sigma  (iram_fVplusfq, oapGenericArnoldiApi.h:73-102,
+// with Sorensen's indices)
+template <bool CPLX>
+__global__ void k_restart_f(const double* __restrict__ vkre, const double* __restrict__ vkim, double* fre,
+                            double* fim, int n, const DevState* st) {
+  const cplx b = st->beta_hat, s = st->sigma;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    cplx v = {vkre[i], CPLX ? vkim[i] : 0.0};
+    cplx f = {fre[i], CPLX ? fim[i] : 0.0};
+    cplx o = v * b + f * s;
+    fre[i] = o.re;
+    if (CPLX) fim[i] = o.im;
+  }
+}
+
+// y = x * alpha - y  (used for residuals r = A x - lambda x, alpha = lambda)
+template <bool CPLX>
+__global__ void k_axmy(const double* __restrict__ xre, const double* __restrict__ xim, cplx alpha, double* yre,
+                       double* yim, int n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    cplx x = {xre[i], CPLX ? xim[i] : 0.0};
+    cplx y = {yre[i], CPLX ? yim[i] : 0.0};
+    cplx o = y - alpha * x;
+    yre[i] = o.re;
+    if (CPLX) yim[i] = o.im;
+  }
+}
+
+template <typename T>
+__global__ void k_to_f32(const double* __restrict__ src, T* dst, long len) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < len; i += (long)gridDim.x * blockDim.x)
+    dst[i] = (T)src[i];
+}
+
+// row-major (reference layout) n x k matrix from k vector-contiguous vectors
+__global__ void k_vectors_to_rowmajor(const double* __restrict__ xre, const double* __restrict__ xim, int n, int k,
+                                      double* ore, double* oim) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)n * k; t += (long)gridDim.x * blockDim.x) {
+    long r = t / k, q = t % k;
+    if (ore) ore[t] = xre[q * n + r];
+    if (oim) oim[t] = xim ? xim[q * n + r] : 0.0;
+  }
+}
+
+}  // namespace oapb
+
+using namespace oapb;
+
+struct oapb_arnoldi {
+  oapb_arnoldi_config cfg;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  bool is_c = false;
+  int n = 0, m = 0, k = 0;
+  // operator
+  const double* a64re = nullptr;
+  const double* a64im = nullptr;
+  double* own64re = nullptr;   // library-owned FP64 copy (host-input solves)
+  double* own64im = nullptr;
+  float* a32re = nullptr;
+  float* a32im = nullptr;
+  oapb_matvec_fn cb = nullptr;
+  void* cb_user = nullptr;
+  // vectors
+  double *Vre = nullptr, *Vim = nullptr;
+  double *Xre = nullptr, *Xim = nullptr;   // Ritz vectors / restart scratch (m vectors)
+  double *fre = nullptr, *fim = nullptr, *wre = nullptr, *wim = nullptr;
+  float *x32re = nullptr, *x32im = nullptr;
+  double *v0re = nullptr, *v0im = nullptr;
+  bool have_v0 = false;
+  // small
+  cplx *H = nullptr, *Qs = nullptr, *ritz = nullptr, *Y = nullptr, *h = nullptr, *s = nullptr, *part = nullptr,
+       *hws = nullptr;
+  double *est = nullptr, *fpart = nullptr;
+  int* order = nullptr;
+  DevState* st = nullptr;
+  int nchunk = 0, chunk = 0, nupd = 0;
+  size_t hess_smem = 0;
+  oapb_arnoldi_stats stats{};
+  std::vector<cudaEvent_t> ev_pool;   // profiling events (pairs)
+  size_t ev_used = 0;
+  // last solve outputs (host)
+  std::vector<cplx> evals;
+};
+
+namespace {
+
+int launch_check() { return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA; }
+
+template <typename P>
+int dalloc(P** p, size_t bytes) {
+  if (cudaMalloc((void**)p, bytes) != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return OAPB_ERR_NOMEM;
+  }
+  return OAPB_OK;
+}
+
+int grid_n(long n) { return grid_for(n, 256, kNumSMs * 8); }
+
+// f <- ||f||^2 into st->fnorm2
+int set_fnorm(oapb_arnoldi* a) {
+  const int nb = a->nupd;
+  k_sumsq_partial<<<nb, 256, 0, a->stream>>>(a->fre, a->is_c ? a->fim : nullptr, a->n, a->fpart);
+  k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, nb, a->st);
+  return launch_check();
+}
+
+// w = A x (x = basis vector j, FP64; x32 its FP32 copy)
+int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre, double* yim, bool fp32,
+             int type) {
+  cudaStream_t s = a->stream;
+  const int n = a->n;
+  if (a->cb) {
+    oapb_mat w = {1u, (uint32_t)n, yre, a->is_c ? yim : nullptr, OAPB_F64};
+    oapb_mat v = {1u, (uint32_t)n, (void*)xre, a->is_c ? (void*)xim : nullptr, OAPB_F64};
+    int rc = a->cb(&w, &v, a->cb_user, type, (void*)s);
+    return rc == 0 ? OAPB_OK : OAPB_ERR_CALLBACK;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (a->cfg.profile) {
+    while (a->ev_pool.size() < a->ev_used + 2) {
+      cudaEvent_t ev;
+      if (cudaEventCreate(&ev) != cudaSuccess) return OAPB_ERR_CUDA;
+      a->ev_pool.push_back(ev);
+    }
+    e0 = a->ev_pool[a->ev_used];
+    e1 = a->ev_pool[a->ev_used + 1];
+    a->ev_used += 2;
+    cudaEventRecord(e0, s);
+  }
+  cudaError_t e;
+  if (fp32)
+    e = launch_matvec<float>(a->a32re, a->is_c ? a->a32im : nullptr, n, n, a->x32re, a->is_c ? a->x32im : nullptr,
+                             yre, a->is_c ? yim : nullptr, s);
+  else
+    e = launch_matvec<double>(a->a64re, a->is_c ? a->a64im : nullptr, n, n, xre, a->is_c ? xim : nullptr, yre,
+                              a->is_c ? yim : nullptr, s);
+  if (e1) {
+    cudaEventRecord(e1, s);
+    if (fp32) a->stats.matvec_fp32++;
+  }
+  return e == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
+
+template <bool C>
+int gs_pass(oapb_arnoldi* a, int j, const double* srcre, const double* srcim, cplx* coef, int gated) {
+  cudaStream_t s = a->stream;
+  const int n = a->n, nvec = j + 1;
+  k_gs_project<C><<<a->nchunk, kGsThreads, 0, s>>>(a->Vre, a->Vim, n, nvec, srcre, srcim, a->chunk, a->part,
+                                                    a->m + 1, a->st, gated);
+  k_gs_reduce<<<1, 128, 0, s>>>(a->part, a->nchunk, a->m + 1, nvec, coef, a->st, gated);
+  k_gs_update<C><<<a->nupd, kUpdThreads, 0, s>>>(a->Vre, a->Vim, n, nvec, coef, srcre, srcim, a->fre, a->fim,
+                                                 a->fpart, a->st, gated);
+  return launch_check();
+}
+
+template <bool C>
+int arnoldi_step(oapb_arnoldi* a, int j, bool fp32) {
+  cudaStream_t s = a->stream;
+  const int n = a->n, m = a->m;
+  double* vre = a->Vre + (long)j * n;
+  double* vim = C ? a->Vim + (long)j * n : nullptr;
+  k_normalize<C><<<grid_n(n), 256, 0, s>>>(a->fre, a->fim, n, a->st, vre, vim, fp32 ? a->x32re : nullptr,
+                                           fp32 ? a->x32im : nullptr, a->H, m, j, a->st);
+  int rc = launch_check();
+  if (rc) return rc;
+  rc = apply_op(a, vre, vim, a->wre, a->wim, fp32, OAPB_TYPE_WV);
+  if (rc) return rc;
+  a->stats.matvecs++;
+  if ((rc = gs_pass<C>(a, j, a->wre, a->wim, a->h, 0))) return rc;
+  k_gs_finalize<<<1, 256, 0, s>>>(a->fpart, a->nupd, a->h, a->s, a->H, m, j, a->cfg.rho, a->st, 0, !C);
+  if ((rc = gs_pass<C>(a, j, a->fre, a->fim, a->s, 1))) return rc;
+  k_gs_finalize<<<1, 256, 0, s>>>(a->fpart, a->nupd, a->h, a->s, a->H, m, j, a->cfg.rho, a->st, 1, !C);
+  return launch_check();
+}
+
+int hess(oapb_arnoldi* a, int do_shift, double tol) {
+  HessArgs h;
+  h.Hin = a->H;
+  h.Hout = a->H;
+  h.Qout = a->Qs;
+  h.ritz = a->ritz;
+  h.Y = a->Y;
+  h.est = a->est;
+  h.order = a->order;
+  h.st = a->st;
+  h.gws = a->hess_smem ? nullptr : a->hws;
+  h.m = a->m;
+  h.k = a->k;
+  h.which = a->cfg.sort;
+  h.do_shift = do_shift;
+  h.real_shifts = !a->is_c;
+  h.dense = 0;
+  h.use_beta = 1;
+  h.tol = tol;
+  h.beta = 0;
+  k_hess<<<1, 32, a->hess_smem, a->stream>>>(h);
+  return launch_check();
+}
+
+template <bool C>
+int restart(oapb_arnoldi* a) {
+  cudaStream_t s = a->stream;
+  const int n = a->n, m = a->m, k = a->k;
+  // X[0..k] = V Q[:, 0..k]
+  const size_t shm = sizeof(cplx) * m * (k + 1);
+  k_vq<C><<<grid_n(n), 256, shm, s>>>(a->Vre, a->Vim, n, m, a->Qs, m, k + 1, a->Xre, a->Xim);
+  k_restart_f<C><<<grid_n(n), 256, 0, s>>>(a->Xre + (long)k * n, C ? a->Xim + (long)k * n : nullptr, a->fre,
+                                           a->fim, n, a->st);
+  if (cudaMemcpyAsync(a->Vre, a->Xre, sizeof(double) * k * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if (C && cudaMemcpyAsync(a->Vim, a->Xim, sizeof(double) * k * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  int rc = launch_check();
+  if (rc) return rc;
+  return set_fnorm(a);
+}
+
+int read_state(oapb_arnoldi* a, DevState* h) {
+  if (cudaMemcpyAsync(h, a->st, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  return OAPB_OK;
+}
+
+// One IRAM run until the Ritz estimates reach `tol` or the restart budget
+// is spent.  Returns OAPB_OK / OAPB_NOT_CONVERGED / error.
+template <bool C>
+int iram(oapb_arnoldi* a, bool fp32, double tol, unsigned max_restarts, int start) {
+  DevState hs;
+  for (unsigned r = 0;; ++r) {
+    for (int j = start; j < a->m; ++j) {
+      int rc = arnoldi_step<C>(a, j, fp32);
+      if (rc) return rc;
+    }
+    const int do_shift = r < max_restarts;
+    int rc = hess(a, do_shift, tol);
+    if (rc) return rc;
+    if ((rc = read_state(a, &hs))) return rc;
+    if (hs.status & 1) return OAPB_ERR_BREAKDOWN;
+    if (hs.status & 2) return OAPB_ERR_TIMEOUT;
+    a->stats.dgks_passes = hs.dgks_count;
+    if (hs.converged) return OAPB_OK;
+    if (!do_shift) return OAPB_NOT_CONVERGED;
+    if ((rc = restart<C>(a))) return rc;
+    a->stats.restarts++;
+    start = a->k;
+  }
+}
+
+template <bool C>
+int ritz_vectors(oapb_arnoldi* a) {
+  const int n = a->n, m = a->m, k = a->k;
+  const size_t shm = sizeof(cplx) * m * k;
+  k_vq<C><<<grid_n(n), 256, shm, a->stream>>>(a->Vre, a->Vim, n, m, a->Y, m, k, a->Xre, a->Xim);
+  return launch_check();
+}
+
+// FP64 residual ||A x_q - theta_q x_q|| / (scale ||x_q||) for each wanted q.
+template <bool C>
+int residuals(oapb_arnoldi* a, const std::vector<cplx>& th, double scale, double* out) {
+  const int n = a->n, k = a->k;
+  std::vector<double> parts(a->nupd);
+  for (int q = 0; q < k; ++q) {
+    double* xr = a->Xre + (long)q * n;
+    double* xi = C ? a->Xim + (long)q * n : nullptr;
+    int rc = apply_op(a, xr, xi, a->wre, a->wim, false, OAPB_TYPE_EIGENVECTOR);
+    if (rc) return rc;
+    k_axmy<C><<<grid_n(n), 256, 0, a->stream>>>(xr, xi, th[q], a->wre, a->wim, n);
+    k_sumsq_partial<<<a->nupd, 256, 0, a->stream>>>(a->wre, C ? a->wim : nullptr, n, a->fpart);
+    k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, a->nupd, a->st);
+    DevState hs;
+    if ((rc = read_state(a, &hs))) return rc;
+    // restore f's norm is not needed after the solve
+    k_sumsq_partial<<<a->nupd, 256, 0, a->stream>>>(xr, xi, n, a->fpart);
+    k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, a->nupd, a->st);
+    DevState hx;
+    if ((rc = read_state(a, &hx))) return rc;
+    out[q] = sqrt(hs.fnorm2) / (scale * sqrt(hx.fnorm2));
+  }
+  return OAPB_OK;
+}
+
+template <bool C>
+int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
+  cudaStream_t s = a->stream;
+  const int n = a->n, m = a->m, k = a->k;
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb;
+  a->stats.restarts = 0;
+  a->stats.matvecs = 0;
+  a->stats.block_matvecs = 0;
+  a->stats.refine_iterations = 0;
+  if (cudaMemsetAsync(a->st, 0, sizeof(DevState), s) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (cudaMemsetAsync(a->H, 0, sizeof(cplx) * m * m, s) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (a->cfg.init == OAPB_INIT_USER) {
+    if (!a->have_v0) return OAPB_ERR_ARG;
+    cudaMemcpyAsync(a->fre, a->v0re, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    if (C) cudaMemcpyAsync(a->fim, a->v0im, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+  } else {
+    k_init_vector<<<grid_n(n), 256, 0, s>>>(a->fre, C ? a->fim : nullptr, n, a->cfg.seed, a->cfg.init);
+  }
+  int rc = set_fnorm(a);
+  if (rc) return rc;
+  const double tol = a->cfg.tolerance;
+  int st;
+  if (mixed) {
+    // phase 1: FP32 operator; the Ritz estimates cannot go below the FP32
+    // rounding floor, so stop at 1e-7 (or the goal if looser), then
+    // continue in FP64 from the compressed factorization
+    st = iram<C>(a, true, tol > 1e-7 ? tol : 1e-7, a->cfg.max_restarts, 0);
+    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+    if (tol < 1e-7) {
+      // re-enter the restart loop with the FP64 operator: restart with the
+      // current shifts and rebuild the tail of the factorization in FP64
+      DevState hs;
+      if ((rc = read_state(a, &hs))) return rc;
+      (void)hs;
+      st = OAPB_NOT_CONVERGED;
+    }
+  } else {
+    st = iram<C>(a, false, tol, a->cfg.max_restarts, 0);
+    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  }
+  if ((rc = ritz_vectors<C>(a))) return rc;
+  std::vector<cplx> th(m);
+  DevState hs;
+  if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * m, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if ((rc = read_state(a, &hs))) return rc;
+  a->evals.assign(th.begin(), th.begin() + k);
+  std::vector<double> r(k);
+  if ((rc = residuals<C>(a, a->evals, hs.scale, r.data()))) return rc;
+  double mx = 0;
+  for (int q = 0; q < k; ++q) {
+    if (eig_re) eig_re[q] = a->evals[q].re;
+    if (eig_im) eig_im[q] = a->evals[q].im;
+    if (res) res[q] = r[q];
+    mx = r[q] > mx ? r[q] : mx;
+  }
+  a->stats.max_residual = mx;
+  a->stats.converged = mx <= tol;
+  return a->stats.converged ? OAPB_OK : OAPB_NOT_CONVERGED;
+}
+
+void free_all(oapb_arnoldi* a) {
+  void* ps[] = {a->own64re, a->own64im, a->a32re, a->a32im, a->Vre, a->Vim, a->Xre, a->Xim, a->fre,
+                a->fim, a->wre, a->wim, a->x32re, a->x32im, a->v0re, a->v0im, a->H, a->Qs, a->ritz,
+                a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
+  for (void* p : ps)
+    if (p) cudaFree(p);
+}
+
+}  // namespace
+
+extern "C" {
+
+void oapb_arnoldi_config_default(oapb_arnoldi_config* c) {
+  if (!c) return;
+  memset(c, 0, sizeof(*c));
+  c->sort = OAPB_SORT_LARGEST_VALUES;
+  c->precision = OAPB_PREC_FP64;
+  c->init = OAPB_INIT_RANDOM;
+  c->max_restarts = 300;
+  c->tolerance = 1e-10;
+  c->rho = 1.0 / 3.14;
+  c->seed = 1;
+}
+
+int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void* stream) {
+  if (!out || !cfg) return OAPB_ERR_ARG;
+  *out = nullptr;
+  const int n = (int)cfg->n, m = (int)cfg->hdim, k = (int)cfg->wanted;
+  if (n < 2 || m < 2 || k < 1 || k >= m || m > n || m > kMaxM || cfg->sort < 0 || cfg->sort > 5) return OAPB_ERR_ARG;
+  if (!(cfg->tolerance > 0)) return OAPB_ERR_ARG;
+  oapb_arnoldi* a = new (std::nothrow) oapb_arnoldi();
+  if (!a) return OAPB_ERR_NOMEM;
+  a->cfg = *cfg;
+  a->n = n;
+  a->m = m;
+  a->k = k;
+  a->is_c = cfg->is_complex != 0;
+  // NULL selects the legacy default stream, like every other call
+  a->stream = (cudaStream_t)stream;
+  const size_t vb = sizeof(double) * (size_t)n;
+  a->chunk = 128;
+  a->nchunk = (n + a->chunk - 1) / a->chunk;
+  if (a->nchunk > 2 * kNumSMs) {
+    a->nchunk = 2 * kNumSMs;
+    a->chunk = (n + a->nchunk - 1) / a->nchunk;
+  }
+  a->nupd = grid_for(n, kUpdThreads, kNumSMs * 4);
+  int rc = OAPB_OK;
+  const bool C = a->is_c;
+  rc |= dalloc(&a->Vre, vb * (m + 1));
+  if (C) rc |= dalloc(&a->Vim, vb * (m + 1));
+  rc |= dalloc(&a->Xre, vb * (m + 1));
+  if (C) rc |= dalloc(&a->Xim, vb * (m + 1));
+  rc |= dalloc(&a->fre, vb);
+  rc |= dalloc(&a->wre, vb);
+  if (C) rc |= dalloc(&a->fim, vb);
+  if (C) rc |= dalloc(&a->wim, vb);
+  rc |= dalloc(&a->H, sizeof(cplx) * m * m);
+  rc |= dalloc(&a->Qs, sizeof(cplx) * m * m);
+  rc |= dalloc(&a->ritz, sizeof(cplx) * m);
+  rc |= dalloc(&a->Y, sizeof(cplx) * m * m);
+  rc |= dalloc(&a->h, sizeof(cplx) * (m + 1));
+  rc |= dalloc(&a->s, sizeof(cplx) * (m + 1));
+  rc |= dalloc(&a->part, sizeof(cplx) * (size_t)a->nchunk * (m + 1));
+  rc |= dalloc(&a->est, sizeof(double) * m);
+  rc |= dalloc(&a->fpart, sizeof(double) * (a->nupd > 1024 ? a->nupd : 1024));
+  rc |= dalloc(&a->order, sizeof(int) * m);
+  rc |= dalloc(&a->st, sizeof(DevState));
+  const size_t hb = 2 * sizeof(cplx) * (size_t)m * m;
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const size_t static_smem = kMaxM * (sizeof(cplx) + sizeof(double) + sizeof(int)) + 1024;
+  if (hb + static_smem <= (size_t)optin) {
+    a->hess_smem = hb;
+    if (hb > 48 * 1024 &&
+        cudaFuncSetAttribute(k_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hb) != cudaSuccess)
+      rc |= OAPB_ERR_CUDA;
+  } else {
+    rc |= dalloc(&a->hws, hb);
+  }
+  const size_t vqb = sizeof(cplx) * (size_t)m * m;
+  if (vqb > 48 * 1024) {
+    cudaFuncSetAttribute(k_vq<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vqb);
+    cudaFuncSetAttribute(k_vq<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vqb);
+  }
+  if (rc != OAPB_OK) {
+    free_all(a);
+    if (a->own_stream) cudaStreamDestroy(a->stream);
+    delete a;
+    return (rc & OAPB_ERR_NOMEM) ? OAPB_ERR_NOMEM : OAPB_ERR_CUDA;
+  }
+  *out = a;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_destroy(oapb_arnoldi* a) {
+  if (!a) return OAPB_ERR_ARG;
+  cudaStreamSynchronize(a->stream);
+  for (cudaEvent_t e : a->ev_pool) cudaEventDestroy(e);
+  free_all(a);
+  if (a->own_stream) cudaStreamDestroy(a->stream);
+  delete a;
+  return OAPB_OK;
+}
+
+static int make_fp32_copy(oapb_arnoldi* a) {
+  const long nn = (long)a->n * a->n;
+  if (!a->a32re && dalloc(&a->a32re, sizeof(float) * nn)) return OAPB_ERR_NOMEM;
+  if (a->is_c && !a->a32im && dalloc(&a->a32im, sizeof(float) * nn)) return OAPB_ERR_NOMEM;
+  if (!a->x32re && dalloc(&a->x32re, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
+  if (a->is_c && !a->x32im && dalloc(&a->x32im, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
+  const int g = kNumSMs * 8;
+  k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64re, a->a32re, nn);
+  if (a->is_c) k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64im, a->a32im, nn);
+  return launch_check();
+}
+
+int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
+  if (!a || !A || A->dtype != OAPB_F64 || !A->re) return OAPB_ERR_ARG;
+  if (A->columns != (uint32_t)a->n || A->rows != (uint32_t)a->n) return OAPB_ERR_ARG;
+  if ((A->im != nullptr) != a->is_c) return OAPB_ERR_ARG;
+  a->a64re = (const double*)A->re;
+  a->a64im = (const double*)A->im;
+  a->cb = nullptr;
+  if (a->cfg.precision == OAPB_PREC_MIXED) return make_fp32_copy(a);
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_set_callback(oapb_arnoldi* a, oapb_matvec_fn fn, void* user) {
+  if (!a || !fn) return OAPB_ERR_ARG;
+  a->cb = fn;
+  a->cb_user = user;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_set_start_vector(oapb_arnoldi* a, const double* re, const double* im) {
+  if (!a || !re || (a->is_c && !im)) return OAPB_ERR_ARG;
+  const size_t vb = sizeof(double) * a->n;
+  if (!a->v0re && dalloc(&a->v0re, vb)) return OAPB_ERR_NOMEM;
+  if (a->is_c && !a->v0im && dalloc(&a->v0im, vb)) return OAPB_ERR_NOMEM;
+  if (cudaMemcpyAsync(a->v0re, re, vb, cudaMemcpyDefault, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (a->is_c && cudaMemcpyAsync(a->v0im, im, vb, cudaMemcpyDefault, a->stream) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  a->have_v0 = true;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_solve(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals,
+                       const oapb_mat* evecs) {
+  if (!a) return OAPB_ERR_ARG;
+  if (!a->cb && !a->a64re) return OAPB_ERR_ARG;
+  if (evecs && (evecs->columns != (uint32_t)a->k || evecs->rows != (uint32_t)a->n || evecs->dtype != OAPB_F64 ||
+                !evecs->re))
+    return OAPB_ERR_ARG;
+  auto t0 = std::chrono::steady_clock::now();
+  a->ev_used = 0;
+  a->stats.matvec_fp32 = 0;
+  int st = a->is_c ? solve_impl<true>(a, eig_re, eig_im, residuals) : solve_impl<false>(a, eig_re, eig_im, residuals);
+  if ((st == OAPB_OK || st == OAPB_NOT_CONVERGED) && evecs) {
+    const long nk = (long)a->n * a->k;
+    k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(
+        a->Xre, a->is_c ? a->Xim : nullptr, a->n, a->k, (double*)evecs->re, (double*)evecs->im);
+    if (launch_check()) return OAPB_ERR_CUDA;
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  }
+  a->stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  a->stats.matvec_seconds = 0;
+  a->stats.matvec_timed = (uint32_t)(a->ev_used / 2);
+  if (a->ev_used) {
+    cudaStreamSynchronize(a->stream);
+    for (size_t i = 0; i + 1 < a->ev_used; i += 2) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, a->ev_pool[i], a->ev_pool[i + 1]) == cudaSuccess)
+        a->stats.matvec_seconds += ms * 1e-3;
+    }
+  }
+  return st;
+}
+
+int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* him, double* eig_re, double* eig_im,
+                            double* residuals, double* vre, double* vim) {
+  if (!a || !hre || (a->is_c && !him)) return OAPB_ERR_ARG;
+  const size_t bytes = sizeof(double) * (size_t)a->n * a->n;
+  if (!a->own64re && dalloc(&a->own64re, bytes)) return OAPB_ERR_NOMEM;
+  if (a->is_c && !a->own64im && dalloc(&a->own64im, bytes)) return OAPB_ERR_NOMEM;
+  if (cudaMemcpyAsync(a->own64re, hre, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (a->is_c && cudaMemcpyAsync(a->own64im, him, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  oapb_mat A = {(uint32_t)a->n, (uint32_t)a->n, a->own64re, a->is_c ? a->own64im : nullptr, OAPB_F64};
+  int rc = oapb_arnoldi_set_dense_operator(a, &A);
+  if (rc) return rc;
+  int st = oapb_arnoldi_solve(a, eig_re, eig_im, residuals, nullptr);
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  if (vre || vim) {
+    double *dre = nullptr, *dim = nullptr;
+    const long nk = (long)a->n * a->k;
+    if (dalloc(&dre, sizeof(double) * nk)) return OAPB_ERR_NOMEM;
+    if (a->is_c && dalloc(&dim, sizeof(double) * nk)) {
+      cudaFree(dre);
+      return OAPB_ERR_NOMEM;
+    }
+    k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(a->Xre, a->is_c ? a->Xim : nullptr,
+                                                                                  a->n, a->k, dre, dim);
+    if (vre) cudaMemcpyAsync(vre, dre, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream);
+    if (vim && dim) cudaMemcpyAsync(vim, dim, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream);
+    cudaError_t e = cudaStreamSynchronize(a->stream);
+    cudaFree(dre);
+    if (dim) cudaFree(dim);
+    if (e != cudaSuccess) return OAPB_ERR_CUDA;
+  }
+  return st;
+}
+
+int oapb_arnoldi_get_stats(const oapb_arnoldi* a, oapb_arnoldi_stats* out) {
+  if (!a || !out) return OAPB_ERR_ARG;
+  *out = a->stats;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_test_outcome(oapb_arnoldi* a, uint32_t index, double* out) {
+  if (!a || !out || index >= (uint32_t)a->k || a->evals.empty()) return OAPB_ERR_ARG;
+  std::vector<double> r(a->k);
+  double scale = 0;
+  for (auto& e : a->evals) scale = fmax(scale, cabs_(e));
+  if (scale == 0) scale = 1;
+  int rc = a->is_c ? residuals<true>(a, a->evals, scale, r.data()) : residuals<false>(a, a->evals, scale, r.data());
+  if (rc) return rc;
+  *out = r[index];
+  return OAPB_OK;
+}
+
+}  // extern "C"

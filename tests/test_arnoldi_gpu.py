@@ -1,0 +1,131 @@
+"""The implicitly restarted Arnoldi solver on the GPU through the C ABI,
+against the CPU oracle, known spectra and the reference's fixtures."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import oap_b200 as B  # noqa: E402
+from gpu_util import planes, planted_complex, planted_symmetric, zeros, host  # noqa: E402
+
+TOL = 1e-10
+
+
+def solve(A, k, m, sort="LM", precision=B.PREC_FP64, seed=1, vectors=False, **kw):
+    n = A.shape[0]
+    cplx = np.iscomplexobj(A)
+    s = B.Arnoldi(n, m, k, is_complex=cplx, sort=sort, precision=precision, seed=seed, **kw)
+    a = planes(A, cplx)
+    s.set_operator(*a)
+    vec = zeros((n, k), cplx) if vectors else None
+    ev, res, st = s.solve(vectors=vec)
+    out = {"ev": np.array(ev), "res": np.array(res), "stats": s.stats(), "solver": s}
+    if vectors:
+        out["x"] = host(*vec)
+    return out
+
+
+def test_planted_symmetric_n256():
+    # n=256 float64, lambda 1 .. 1e-3, top-5 LM, m=32
+    A, lam = planted_symmetric(256, seed=0)
+    r = solve(A, 5, 32, vectors=True)
+    assert np.allclose(np.sort(r["ev"].real)[::-1], lam[:5], rtol=1e-10, atol=0)
+    assert np.abs(r["ev"].imag).max() == 0
+    assert r["res"].max() <= TOL
+    # eigenvectors: residual recomputed on the host in FP64
+    X = r["x"]
+    for q in range(5):
+        x = X[:, q]
+        assert abs(np.linalg.norm(x) - 1) < 1e-12
+        assert np.linalg.norm(A @ x - r["ev"][q] * x) <= TOL
+    # against the oracle on the same start vector
+    o = O.iram(A, 5, 32, which="LM", tol=TOL, v0=B.start_vector(256, 1))
+    assert np.allclose(np.sort(o["eigenvalues"].real), np.sort(r["ev"].real), rtol=1e-12)
+
+
+@pytest.mark.parametrize("idx", range(4))
+def test_reference_known_spectrum(golden, idx):
+    # oapArnoldiPackageMatricesTests.cpp:244-266 (SortLargestReValues)
+    c = golden["cmatrix"][idx]
+    n = c["n"]
+    A = np.array(c["re"]).reshape(n, n)
+    r = solve(A, c["wanted"], c["hdim"], sort="LR")
+    want = np.sort(c["eigenvalues"])[::-1][: c["wanted"]]
+    assert np.allclose(r["ev"].real, want, rtol=1e-10)
+    assert r["res"].max() <= TOL  # reference gate: 0.02 - 0.047 absolute
+    for q in range(c["wanted"]):
+        assert r["solver"].test_outcome(q) <= TOL
+
+
+@pytest.mark.parametrize("n,k,m", [(512, 6, 30), (1024, 16, 64)])
+def test_complex_nonhermitian(n, k, m):
+    A = planted_complex(n, seed=n, nplant=k)
+    r = solve(A, k, m, vectors=True)
+    assert r["res"].max() <= TOL
+    w = np.linalg.eigvals(A)
+    w = w[np.argsort(-np.abs(w))][:k]
+    for lam in w:
+        assert np.min(np.abs(r["ev"] - lam)) < 1e-9 * abs(lam)
+    o = O.iram(A, k, m, which="LM", tol=TOL, v0=B.start_vector(n, 1, True))
+    for lam in o["eigenvalues"]:
+        assert np.min(np.abs(r["ev"] - lam)) < 1e-9 * abs(lam)
+    X = r["x"]
+    for q in range(k):
+        assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * np.abs(r["ev"]).max()
+
+
+def test_callback_operator_matches_dense():
+    # CuHArnoldiCallback::setCallback: the matvec is user code on the device
+    A, lam = planted_symmetric(300, seed=4)
+    a = planes(A, False)[0]
+
+    def mv(w, v, typ, stream):
+        # run on the solver's stream so the ordering with its kernels holds
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+            torch.mv(a, ptr_tensor(v.re, 300), out=ptr_tensor(w.re, 300))
+        return 0
+
+    s = B.Arnoldi(300, 24, 4, seed=3)
+    s.set_callback(mv)
+    ev, res, st = s.solve()
+    assert st == B.OK
+    assert np.allclose(np.sort(np.array(ev).real)[::-1], lam[:4], rtol=1e-10)
+
+
+def ptr_tensor(ptr, n):
+    """A torch view of n FP64 values at a raw device pointer."""
+    class _A:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                    "version": 3, "strides": None}
+    return torch.as_tensor(_A(), device="cuda")
+
+
+def test_solve_from_host_buffers():
+    A = planted_complex(400, seed=9, nplant=5)
+    s = B.Arnoldi(400, 24, 5, is_complex=True, seed=2)
+    ev, res, st, X = s.solve_host(np.ascontiguousarray(A.real), np.ascontiguousarray(A.imag), vectors=True)
+    assert st == B.OK and max(res) <= TOL
+    for q in range(5):
+        assert np.linalg.norm(A @ X[:, q] - ev[q] * X[:, q]) <= TOL * max(abs(e) for e in ev)
+
+
+def test_first_value_is_one_start():
+    A, lam = planted_symmetric(200, seed=5)
+    r = solve(A, 3, 20, init=B.INIT_FIRST_VALUE_IS_ONE)
+    assert np.allclose(np.sort(r["ev"].real)[::-1], lam[:3], rtol=1e-10)
+
+
+def test_not_converged_is_reported():
+    A, lam = planted_symmetric(256, seed=6, lo_exp=-0.01)   # tiny gaps
+    s = B.Arnoldi(256, 12, 4, max_restarts=1)
+    s.set_operator(*planes(A, False))
+    ev, res, st = s.solve(allow_not_converged=True)
+    assert st == B.NOT_CONVERGED
