@@ -1,0 +1,394 @@
+"""Benchmark: eigensolves/s at relative residual <= 1e-10 on one B200.
+
+Workload (the single complex non-Hermitian solve): n = 16384 dense complex A
+in split re/im FP64 planes (reference layout), entries N(0, 1/n) (each plane
+N(0, 1/(2n))) plus 4 added on 16 seeded diagonal positions; the 16
+largest-magnitude eigenpairs, Krylov dimension m = 64; an eigensolve counts
+only when every wanted pair has ||A x - l x|| / (|l_1| ||x||) <= 1e-10 in
+FP64 against the FP64 operator.  Synthetic seeded data; A (4 GiB) is far
+larger than L2, so no L2 flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+One JSON line on rank 0.  `value` is the chosen form (FP32 matvec IRAM +
+FP64 refinement) with A resident in HBM; `plain_fp64` is the plain FP64 GPU
+Arnoldi on the same problem; `e2e` runs the C-ABI entry that takes HOST
+buffers (pinned), with the 4 GiB host-to-device copy of A inside every step.
+With N > 1 GPUs every rank solves its own replica (the solve does not shard).
+`--impl reference` times the CPU implementation of the path (the oracle's
+FP64 IRAM) on this host's cores, on a bounded sample of the same workload.
+"""
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N, K_WANTED, M_KRYLOV, NPLANT, SHIFT, TOL = 16384, 16, 64, 16, 4.0, 1e-10
+METRIC = "eigensolves/s at residual≤1e-10: chosen form vs plain FP64 GPU Arnoldi"
+WORKLOAD = "complex non-Hermitian dense A, n=16384, split re/im FP64, N(0,1/n) + 4 on 16 planted diagonal entries; top-16 LM, m=64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--e2e-steps", type=int, default=None)
+    p.add_argument("--plain-steps", type=int, default=None)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--n", type=int, default=N)
+    return p.parse_args()
+
+
+def make_operator(n, seed, device):
+    """Seeded complex A on `device` as two FP64 planes (rows, columns)."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    s = (1.0 / (2.0 * n)) ** 0.5
+    are = torch.randn(n, n, dtype=torch.float64, device=device, generator=g).mul_(s)
+    aim = torch.randn(n, n, dtype=torch.float64, device=device, generator=g).mul_(s)
+    pos = torch.randperm(n, generator=g, device=device)[:NPLANT]
+    are[pos, pos] += SHIFT
+    return are, aim
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        self.f.flush()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            rows = open(self.f.name).read().strip().splitlines()
+        except OSError:
+            rows = []
+        for row in rows:
+            parts = [x.strip() for x in row.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return p["hbm_gbs"], "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """dram bytes per launch of the FP32 matvec from the committed ncu summary."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "ncu_traffic.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allsum(world, x):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# --------------------------------------------------------------- CPU arm --
+def cpu_sample(are_h, aim_h, budget_s, n):
+    """Oracle FP64 IRAM cost on the host: the operator-application count of
+    one solve (oracle IRAM on the same ensemble at n = 2048) times the
+    measured time of the oracle's FP64 complex matvec on the full operator."""
+    import numpy as np
+    import oracle as O
+    rng = np.random.default_rng(5)
+    ns = 2048
+    s = (1.0 / (2.0 * ns)) ** 0.5
+    A_s = rng.normal(scale=s, size=(ns, ns)) + 1j * rng.normal(scale=s, size=(ns, ns))
+    pos = rng.choice(ns, NPLANT, replace=False)
+    A_s[pos, pos] += SHIFT
+    t0 = time.perf_counter()
+    r = O.iram(A_s, K_WANTED, M_KRYLOV, which="LM", tol=TOL, seed=1)
+    t_small = time.perf_counter() - t0
+    applications = r["matvecs"] + K_WANTED  # + the residual check of the k pairs
+    x = np.random.default_rng(1).normal(size=n) + 0j
+    times = []
+    t_start = time.perf_counter()
+    while time.perf_counter() - t_start < budget_s or not times:
+        t0 = time.perf_counter()
+        _oracle_matvec(O, are_h, aim_h, x)
+        times.append(time.perf_counter() - t0)
+        if len(times) >= 200:
+            break
+    t_mv = statistics.median(times)
+    solve_s = applications * t_mv
+    return {"value": 1.0 / solve_s, "unit": "eigensolves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": ("%d oracle FP64 complex matvecs (%.3f s each) on the n=%d operator, scaled by the %d "
+                       "operator applications of one oracle FP64 IRAM solve (counted on the same ensemble "
+                       "at n=2048, %d restarts, %.1f s)") % (len(times), t_mv, n, applications,
+                                                             r["restarts"], t_small),
+            "matvec_seconds": t_mv, "applications": applications}
+
+
+def _oracle_matvec(O, are_h, aim_h, x):
+    """y = A x with the oracle's OpenMP FP64 matvec on split host planes."""
+    import numpy as np
+    lib = O.lib()
+    n = are_h.shape[0]
+    xr = np.ascontiguousarray(x.real)
+    xi = np.ascontiguousarray(x.imag)
+    yr, yi = np.zeros(n), np.zeros(n)
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    lib.orc_matvec(n, P(are_h), P(aim_h), P(xr), P(xi), P(yr), P(yi))
+    return yr + 1j * yi
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    import numpy as np
+    import torch
+    n = args.n
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    are, aim = make_operator(n, 1, dev)
+    are_h = are.cpu().numpy()
+    aim_h = aim.cpu().numpy()
+    del are, aim
+    vals = []
+    base = None
+    for _ in range(args.warmup + args.steps):
+        base = cpu_sample(are_h, aim_h, max(1.0, args.cpu_seconds / max(1, args.steps)), n)
+        vals.append(base["value"])
+    timed = vals[args.warmup:]
+    v = statistics.median(timed)
+    out = {"metric": METRIC, "value": v, "unit": "eigensolves/s", "impl": "reference",
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
+           "data": "synthetic (seeded)",
+           "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
+                      "tolerance": TOL, "parallelism": "replicas"},
+           "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "e2e": {"value": v, "unit": "eigensolves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    out["cpu_baseline"]["value"] = v
+    print(json.dumps(out), flush=True)
+
+
+# --------------------------------------------------------------- GPU arm --
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import oap_b200 as B
+
+    torch.cuda.set_device(local)
+    n = args.n
+    are, aim = make_operator(n, 1 + rank, "cuda")
+    torch.cuda.synchronize()
+
+    def solver(prec):
+        s = B.Arnoldi(n, M_KRYLOV, K_WANTED, is_complex=True, precision=prec, tolerance=TOL,
+                      profile=True, seed=3 + rank)
+        s.set_operator(are, aim)
+        return s
+
+    def timed(s, steps, warm):
+        for _ in range(warm):
+            ev, res, st = s.solve()
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        launches0 = s.stats()["kernel_launches"]
+        mv_s, mv_n, conv = 0.0, 0, 0
+        e0.record()
+        for _ in range(steps):
+            ev, res, st = s.solve(allow_not_converged=True)
+            stt = s.stats()
+            mv_s += stt["matvec_seconds"]
+            mv_n += stt["matvec_fp32"] if prec_of(s) == B.PREC_MIXED else stt["matvec_timed"]
+            conv += int(st == B.OK and max(res) <= TOL)
+        e1.record()
+        torch.cuda.synchronize()
+        barrier(world)
+        ms = e0.elapsed_time(e1)
+        return ms / 1e3, conv, mv_s, mv_n, s.stats()["kernel_launches"] - launches0, stt
+
+    def prec_of(s):
+        return s.cfg.precision
+
+    # chosen form
+    mixed = solver(B.PREC_MIXED)
+    with Clocks(local) as clk:
+        secs, conv, mv_s, mv_n, launches, stt = timed(mixed, args.steps, args.warmup)
+    clocks = clk.summary()
+    secs_max = allmax(world, secs)
+    conv_all = allsum(world, conv)
+    value = conv_all / secs_max
+    # plain FP64 GPU Arnoldi
+    plain = solver(B.PREC_FP64)
+    psteps = args.plain_steps or max(2, args.steps // 2)
+    psecs, pconv, pmv_s, pmv_n, _, pstt = timed(plain, psteps, 1)
+    pvalue = allsum(world, pconv) / allmax(world, psecs)
+    plain.close()
+    # end to end through the host-buffer entry point (pinned host planes)
+    are_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    aim_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+    are_h.copy_(are)
+    aim_h.copy_(aim)
+    e2e_solver = B.Arnoldi(n, M_KRYLOV, K_WANTED, is_complex=True, precision=B.PREC_MIXED,
+                           tolerance=TOL, seed=3 + rank)
+    ar_np, ai_np = are_h.numpy(), aim_h.numpy()
+    esteps = args.e2e_steps or max(2, args.steps // 2)
+    e2e_solver.solve_host(ar_np, ai_np, vectors=True)  # warm-up (allocations)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    econv = 0
+    for _ in range(esteps):
+        ev, res, st, X = e2e_solver.solve_host(ar_np, ai_np, vectors=True)
+        econv += int(st == B.OK and max(res) <= TOL)
+    e1.record()
+    torch.cuda.synchronize()
+    esecs = allmax(world, e0.elapsed_time(e1) / 1e3)
+    e2e_value = allsum(world, econv) / esecs
+    e2e_solver.close()
+
+    # roofline of the dominant kernel: FP32 complex matvec
+    hbm, peak_kind = peaks()
+    alg_bytes = 8.0 * n * n + 16.0 * n
+    per_launch = mv_s / max(1, mv_n)
+    achieved = alg_bytes / per_launch / 1e9
+    traffic = ncu_traffic()
+    roof = {"bound": "hbm", "kernel": "k_matvec<float,complex> (FP32 complex matvec)",
+            "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+            "traffic": (traffic or {}).get("bytes_per_launch"),
+            "launch_ms": per_launch * 1e3, "algorithmic_bytes_per_launch": alg_bytes,
+            "plain_fp64_matvec_GBs": (16.0 * n * n + 32.0 * n) / (pmv_s / max(1, pmv_n)) / 1e9}
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cpu = cpu_sample(ar_np, ai_np, args.cpu_seconds, n)
+    out = {"metric": METRIC, "value": value, "unit": "eigensolves/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs_max * 1e3 / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+           "data": "synthetic (seeded)",
+           "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
+                      "tolerance": TOL, "chosen_form": "FP32 matvec IRAM + FP64 subspace refinement",
+                      "parallelism": "replicas" if world > 1 else "single GPU",
+                      "l2": "inputs (4 GiB FP64 + 2 GiB FP32 operator) exceed L2; no flush"},
+           "converged_steps": conv_all,
+           "plain_fp64": {"value": pvalue, "ms_per_step": allmax(world, psecs) * 1e3 / psteps,
+                          "steps": psteps, "restarts": pstt["restarts"], "matvecs": pstt["matvecs"]},
+           "speedup_vs_plain_fp64": value / pvalue if pvalue else None,
+           "solve": {"restarts": stt["restarts"], "matvecs": stt["matvecs"],
+                     "block_matvecs": stt["block_matvecs"], "refine_iterations": stt["refine_iterations"],
+                     "max_residual": stt["max_residual"]},
+           "e2e": {"value": e2e_value, "unit": "eigensolves/s",
+                   "h2d_bytes_per_step": 2 * 8 * n * n,
+                   "d2h_bytes_per_step": 3 * 8 * K_WANTED + 2 * 8 * n * K_WANTED,
+                   "steps": esteps},
+           "roofline": roof, "clocks": clocks,
+           "gpu_launches": int(launches),
+           "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}}
+    mixed.close()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

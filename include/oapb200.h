@@ -207,6 +207,7 @@ typedef struct oapb_arnoldi_stats {
   double matvec_seconds;     /* device time of the timed dense matvecs (profile) */
   uint32_t matvec_timed;     /* number of dense matvec launches timed */
   uint32_t matvec_fp32;      /* of which on the FP32 operator copy */
+  uint64_t kernel_launches;  /* library kernel launches over the handle's life */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

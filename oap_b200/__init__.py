@@ -47,7 +47,7 @@ class Stats(C.Structure):
                 ("refine_iterations", C.c_uint32), ("converged", C.c_int32),
                 ("max_residual", C.c_double), ("seconds", C.c_double),
                 ("matvec_seconds", C.c_double), ("matvec_timed", C.c_uint32),
-                ("matvec_fp32", C.c_uint32)]
+                ("matvec_fp32", C.c_uint32), ("kernel_launches", C.c_uint64)]
 
 
 MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,

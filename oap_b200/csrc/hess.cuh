@@ -35,6 +35,8 @@ struct DevState {
   int converged;
   int status;       // bit 0: breakdown (||f|| = 0), bit 1: Schur sweep limit
   int dgks_count;
+  int brk;          // the current basis vector replaces a zero residual (H[j][j-1] = 0)
+  int brk_count;
   double scale;     // max |theta| over the wanted set
   double maxest;    // max relative Ritz estimate of the wanted set
   cplx beta_hat;    // H[k][k-1] after the shifts
@@ -51,7 +53,7 @@ struct HessArgs {
   int* order;       // m sort order (indices into diag(T))
   DevState* st;
   cplx* gws;        // global workspace (2 m^2) when shared memory is too small
-  int m, k, which, do_shift, real_shifts, dense, use_beta;
+  int m, k, nvec, which, do_shift, real_shifts, dense, use_beta;
   double tol;
   double beta;      // used when use_beta == 0 (dense mode: residual norms come separately)
 };
@@ -243,9 +245,11 @@ __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
   const double small = 2.220446049250313e-16 * (tnorm > 0 ? tnorm : 1.0);
   const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
 
-  // eigenvectors of the wanted Ritz values and their estimates
+  // eigenvectors of the first nvec Ritz values (the wanted k and optional
+  // guard vectors) and the estimates of the wanted ones
   double maxest = 0;
-  for (int q = 0; q < k; ++q) {
+  const int nvec = a.nvec > k ? (a.nvec < m ? a.nvec : m) : k;
+  for (int q = 0; q < nvec; ++q) {
     const int idx = ord[q];
     const cplx lam = TT_(idx, idx);
     for (int i = lane; i < m; i += 32) u[i] = (i == idx) ? cplx{1, 0} : cplx{0, 0};
@@ -284,7 +288,7 @@ __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
     for (int r = lane; r < m; r += 32) a.Y[(long)q * m + r] = inv * a.Y[(long)q * m + r];
     const double e = beta * cabs_(ylast) * inv / scale;
     if (lane == 0) a.est[q] = e;
-    maxest = fmax(maxest, e);
+    if (q < k) maxest = fmax(maxest, e);
     __syncwarp();
   }
   const int conv = maxest <= a.tol;

@@ -30,6 +30,7 @@
 #include <string.h>
 #include <vector>
 
+#include "block.cuh"
 #include "common.cuh"
 #include "hess.cuh"
 #include "matvec.cuh"
@@ -117,8 +118,90 @@ __global__ void k_normalize(const double* __restrict__ fre, const double* __rest
     }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    if (j > 0) H[j + (long)(j - 1) * m] = cplx{beta, 0};
+    if (j > 0) H[j + (long)(j - 1) * m] = cplx{st->brk ? 0.0 : beta, 0};
     if (!(beta > 0)) wst->status |= 1;
+  }
+}
+
+// Invariant-subspace breakdown at the start of step j (j >= 1): when
+// ||f|| <= 1e-12 ||A v_{j-1}||, f is replaced by a seeded random vector made
+// orthogonal to v_0..v_{j-1} (two modified Gram-Schmidt sweeps) and the step
+// records H[j][j-1] = 0, as ARPACK's getv0 restart does.  One CTA; returns
+// at once when there is no breakdown.
+template <bool CPLX>
+__global__ void __launch_bounds__(1024)
+k_breakdown_fix(const double* __restrict__ Vre, const double* __restrict__ Vim, int n, int j, double* fre,
+                double* fim, DevState* st, uint64_t seed) {
+  const double f2 = st->fnorm2, scale2 = st->hnorm2 + st->fnorm2;
+  if (threadIdx.x == 0) st->brk = 0;
+  if (!(f2 <= 1e-24 * scale2)) return;
+  __shared__ double red[2][32];
+  __shared__ double dot[2];
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    fre[i] = uniform_pm1(seed, (uint64_t)i);
+    if (CPLX) fim[i] = uniform_pm1(seed ^ 0x5851F42D4C957F2Dull, (uint64_t)i);
+  }
+  __syncthreads();
+  for (int sweep = 0; sweep < 2; ++sweep) {
+    for (int v = 0; v < j; ++v) {
+      const double* vr = Vre + (long)v * n;
+      const double* vi = CPLX ? Vim + (long)v * n : nullptr;
+      double sr = 0, si = 0;
+      for (long i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = vr[i], x = fre[i];
+        if (CPLX) {
+          double b = vi[i], y = fim[i];
+          sr += a * x + b * y;
+          si += a * y - b * x;
+        } else {
+          sr += a * x;
+        }
+      }
+      sr = warp_sum(sr);
+      si = warp_sum(si);
+      if ((threadIdx.x & 31) == 0) {
+        red[0][threadIdx.x >> 5] = sr;
+        red[1][threadIdx.x >> 5] = si;
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        double a = threadIdx.x < (blockDim.x >> 5) ? red[0][threadIdx.x] : 0.0;
+        double b = threadIdx.x < (blockDim.x >> 5) ? red[1][threadIdx.x] : 0.0;
+        a = warp_sum(a);
+        b = warp_sum(b);
+        if (threadIdx.x == 0) {
+          dot[0] = a;
+          dot[1] = b;
+        }
+      }
+      __syncthreads();
+      const double cr = dot[0], ci = dot[1];
+      for (long i = threadIdx.x; i < n; i += blockDim.x) {
+        double a = vr[i];
+        if (CPLX) {
+          double b = vi[i];
+          fre[i] -= a * cr - b * ci;
+          fim[i] -= a * ci + b * cr;
+        } else {
+          fre[i] -= a * cr;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  double s2 = 0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s2 += fre[i] * fre[i] + (CPLX ? fim[i] * fim[i] : 0.0);
+  s2 = warp_sum(s2);
+  if ((threadIdx.x & 31) == 0) red[0][threadIdx.x >> 5] = s2;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double a = threadIdx.x < (blockDim.x >> 5) ? red[0][threadIdx.x] : 0.0;
+    a = warp_sum(a);
+    if (threadIdx.x == 0) {
+      st->fnorm2 = a;
+      st->brk = 1;
+      st->brk_count += 1;
+    }
   }
 }
 
@@ -351,6 +434,15 @@ struct oapb_arnoldi {
   int* order = nullptr;
   DevState* st = nullptr;
   int nchunk = 0, chunk = 0, nupd = 0;
+  // block (multi-vector) buffers: X, W, R, E of up to kBmMaxB vectors each
+  double *Bre[4] = {nullptr, nullptr, nullptr, nullptr}, *Bim[4] = {nullptr, nullptr, nullptr, nullptr};
+  cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
+  cplx *britz = nullptr;
+  double *best = nullptr, *bnorm = nullptr;
+  int *border = nullptr, *bstatus = nullptr;
+  DevState* bst = nullptr;
+  int ndot = 0, nnorm = 0;
+  int nvec_hess = 0;
   size_t hess_smem = 0;
   oapb_arnoldi_stats stats{};
   std::vector<cudaEvent_t> ev_pool;   // profiling events (pairs)
@@ -378,7 +470,9 @@ int grid_n(long n) { return grid_for(n, 256, kNumSMs * 8); }
 // f <- ||f||^2 into st->fnorm2
 int set_fnorm(oapb_arnoldi* a) {
   const int nb = a->nupd;
+  ++a->stats.kernel_launches;
   k_sumsq_partial<<<nb, 256, 0, a->stream>>>(a->fre, a->is_c ? a->fim : nullptr, a->n, a->fpart);
+  ++a->stats.kernel_launches;
   k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, nb, a->st);
   return launch_check();
 }
@@ -407,6 +501,7 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
     cudaEventRecord(e0, s);
   }
   cudaError_t e;
+  ++a->stats.kernel_launches;
   if (fp32)
     e = launch_matvec<float>(a->a32re, a->is_c ? a->a32im : nullptr, n, n, a->x32re, a->is_c ? a->x32im : nullptr,
                              yre, a->is_c ? yim : nullptr, s);
@@ -424,9 +519,12 @@ template <bool C>
 int gs_pass(oapb_arnoldi* a, int j, const double* srcre, const double* srcim, cplx* coef, int gated) {
   cudaStream_t s = a->stream;
   const int n = a->n, nvec = j + 1;
+  ++a->stats.kernel_launches;
   k_gs_project<C><<<a->nchunk, kGsThreads, 0, s>>>(a->Vre, a->Vim, n, nvec, srcre, srcim, a->chunk, a->part,
                                                     a->m + 1, a->st, gated);
+  ++a->stats.kernel_launches;
   k_gs_reduce<<<1, 128, 0, s>>>(a->part, a->nchunk, a->m + 1, nvec, coef, a->st, gated);
+  ++a->stats.kernel_launches;
   k_gs_update<C><<<a->nupd, kUpdThreads, 0, s>>>(a->Vre, a->Vim, n, nvec, coef, srcre, srcim, a->fre, a->fim,
                                                  a->fpart, a->st, gated);
   return launch_check();
@@ -438,6 +536,11 @@ int arnoldi_step(oapb_arnoldi* a, int j, bool fp32) {
   const int n = a->n, m = a->m;
   double* vre = a->Vre + (long)j * n;
   double* vim = C ? a->Vim + (long)j * n : nullptr;
+  if (j > 0) ++a->stats.kernel_launches;
+  if (j > 0)
+    k_breakdown_fix<C><<<1, 1024, 0, s>>>(a->Vre, a->Vim, n, j, a->fre, a->fim, a->st,
+                                          a->cfg.seed * 7919ull + (uint64_t)(a->stats.restarts * 1024 + j));
+  ++a->stats.kernel_launches;
   k_normalize<C><<<grid_n(n), 256, 0, s>>>(a->fre, a->fim, n, a->st, vre, vim, fp32 ? a->x32re : nullptr,
                                            fp32 ? a->x32im : nullptr, a->H, m, j, a->st);
   int rc = launch_check();
@@ -446,8 +549,10 @@ int arnoldi_step(oapb_arnoldi* a, int j, bool fp32) {
   if (rc) return rc;
   a->stats.matvecs++;
   if ((rc = gs_pass<C>(a, j, a->wre, a->wim, a->h, 0))) return rc;
+  ++a->stats.kernel_launches;
   k_gs_finalize<<<1, 256, 0, s>>>(a->fpart, a->nupd, a->h, a->s, a->H, m, j, a->cfg.rho, a->st, 0, !C);
   if ((rc = gs_pass<C>(a, j, a->fre, a->fim, a->s, 1))) return rc;
+  ++a->stats.kernel_launches;
   k_gs_finalize<<<1, 256, 0, s>>>(a->fpart, a->nupd, a->h, a->s, a->H, m, j, a->cfg.rho, a->st, 1, !C);
   return launch_check();
 }
@@ -465,6 +570,7 @@ int hess(oapb_arnoldi* a, int do_shift, double tol) {
   h.gws = a->hess_smem ? nullptr : a->hws;
   h.m = a->m;
   h.k = a->k;
+  h.nvec = a->nvec_hess;
   h.which = a->cfg.sort;
   h.do_shift = do_shift;
   h.real_shifts = !a->is_c;
@@ -472,6 +578,7 @@ int hess(oapb_arnoldi* a, int do_shift, double tol) {
   h.use_beta = 1;
   h.tol = tol;
   h.beta = 0;
+  ++a->stats.kernel_launches;
   k_hess<<<1, 32, a->hess_smem, a->stream>>>(h);
   return launch_check();
 }
@@ -482,7 +589,9 @@ int restart(oapb_arnoldi* a) {
   const int n = a->n, m = a->m, k = a->k;
   // X[0..k] = V Q[:, 0..k]
   const size_t shm = sizeof(cplx) * m * (k + 1);
+  ++a->stats.kernel_launches;
   k_vq<C><<<grid_n(n), 256, shm, s>>>(a->Vre, a->Vim, n, m, a->Qs, m, k + 1, a->Xre, a->Xim);
+  ++a->stats.kernel_launches;
   k_restart_f<C><<<grid_n(n), 256, 0, s>>>(a->Xre + (long)k * n, C ? a->Xim + (long)k * n : nullptr, a->fre,
                                            a->fim, n, a->st);
   if (cudaMemcpyAsync(a->Vre, a->Xre, sizeof(double) * k * n, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
@@ -527,34 +636,215 @@ int iram(oapb_arnoldi* a, bool fp32, double tol, unsigned max_restarts, int star
 }
 
 template <bool C>
-int ritz_vectors(oapb_arnoldi* a) {
-  const int n = a->n, m = a->m, k = a->k;
-  const size_t shm = sizeof(cplx) * m * k;
-  k_vq<C><<<grid_n(n), 256, shm, a->stream>>>(a->Vre, a->Vim, n, m, a->Y, m, k, a->Xre, a->Xim);
+int ritz_vectors(oapb_arnoldi* a, int nv) {
+  const int n = a->n, m = a->m;
+  const size_t shm = sizeof(cplx) * m * nv;
+  ++a->stats.kernel_launches;
+  k_vq<C><<<grid_n(n), 256, shm, a->stream>>>(a->Vre, a->Vim, n, m, a->Y, m, nv, a->Xre, a->Xim);
   return launch_check();
 }
 
-// FP64 residual ||A x_q - theta_q x_q|| / (scale ||x_q||) for each wanted q.
+// ---------------------------------------------------------------- blocks --
+int alloc_blocks(oapb_arnoldi* a) {
+  if (a->Bre[0]) return OAPB_OK;
+  const size_t vb = sizeof(double) * (size_t)a->n * kBmMaxB;
+  int rc = OAPB_OK;
+  for (int i = 0; i < 4; ++i) {
+    rc |= dalloc(&a->Bre[i], vb);
+    if (a->is_c) rc |= dalloc(&a->Bim[i], vb);
+  }
+  a->ndot = (a->n + kDotChunk - 1) / kDotChunk;
+  a->nnorm = grid_for(a->n, 256, kNumSMs * 2);
+  const size_t bb = sizeof(cplx) * kBmMaxB * kBmMaxB;
+  rc |= dalloc(&a->bpart, bb * (size_t)a->ndot);
+  rc |= dalloc(&a->G, bb);
+  rc |= dalloc(&a->G2, bb);
+  rc |= dalloc(&a->Rinv, bb);
+  rc |= dalloc(&a->bY, bb);
+  rc |= dalloc(&a->bQ, bb);
+  rc |= dalloc(&a->bH, bb);
+  rc |= dalloc(&a->britz, sizeof(cplx) * kBmMaxB);
+  rc |= dalloc(&a->best, sizeof(double) * kBmMaxB);
+  rc |= dalloc(&a->bnorm, sizeof(double) * kBmMaxB * (size_t)a->nnorm);
+  rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
+  rc |= dalloc(&a->bstatus, sizeof(int));
+  rc |= dalloc(&a->bst, sizeof(DevState));
+  return rc ? OAPB_ERR_NOMEM : OAPB_OK;
+}
+
+// G (b1 x b2, column-major) = X^H Y
 template <bool C>
-int residuals(oapb_arnoldi* a, const std::vector<cplx>& th, double scale, double* out) {
-  const int n = a->n, k = a->k;
-  std::vector<double> parts(a->nupd);
-  for (int q = 0; q < k; ++q) {
-    double* xr = a->Xre + (long)q * n;
-    double* xi = C ? a->Xim + (long)q * n : nullptr;
-    int rc = apply_op(a, xr, xi, a->wre, a->wim, false, OAPB_TYPE_EIGENVECTOR);
+void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, const double* yr, const double* yi,
+                int b2, cplx* G) {
+  ++a->stats.kernel_launches;
+  k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(xr, xi, b1, yr, yi, b2, a->n, a->bpart);
+  ++a->stats.kernel_launches;
+  k_block_reduce<<<grid_for(b1 * b2, 128, 8), 128, 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G);
+}
+
+// W = A X (FP64 operator, b vectors)
+template <bool C>
+int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi) {
+  if (a->cb) {
+    for (int q = 0; q < b; ++q) {
+      int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
+                        C ? wi + (long)q * a->n : nullptr, false, OAPB_TYPE_EIGENVECTOR);
+      if (rc) return rc;
+    }
+    return OAPB_OK;
+  }
+  const long tiles = (a->n + kBmRows - 1) / kBmRows;
+  const int grid = (int)(tiles < kNumSMs * 8 ? tiles : kNumSMs * 8);
+  ++a->stats.kernel_launches;
+  k_block_matvec<C><<<grid, 128, 0, a->stream>>>(a->a64re, a->a64im, a->n, xr, xi, b, wr, wi);
+  a->stats.block_matvecs++;
+  return launch_check();
+}
+
+// host copy of the column norms ||Y_q|| for q < b (synchronises)
+template <bool C>
+int col_norms(oapb_arnoldi* a, const double* yr, const double* yi, int b, double* out) {
+  ++a->stats.kernel_launches;
+  k_colnorm2<C><<<a->nnorm, 256, 0, a->stream>>>(yr, yi, b, a->n, a->bnorm);
+  std::vector<double> h((size_t)b * a->nnorm);
+  if (cudaMemcpyAsync(h.data(), a->bnorm, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, a->stream) !=
+      cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  for (int q = 0; q < b; ++q) {
+    double s = 0;
+    for (int blk = 0; blk < a->nnorm; ++blk) s += h[(size_t)blk * b + q];
+    out[q] = sqrt(s);
+  }
+  return OAPB_OK;
+}
+
+// X <- orthonormal basis of span(Win) by two CholeskyQR passes (Win is kept)
+template <bool C>
+int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* xr, double* xi, double* tr,
+            double* ti) {
+  const double* sr = wr;
+  const double* si = wi;
+  for (int pass = 0; pass < 2; ++pass) {
+    double* dr = pass == 0 ? tr : xr;
+    double* di = pass == 0 ? ti : xi;
+    block_gram<C>(a, sr, si, b, sr, si, b, a->G2);
+    ++a->stats.kernel_launches;
+    k_chol_inv<<<1, 32, 0, a->stream>>>(a->G2, b, a->Rinv, a->bstatus);
+    ++a->stats.kernel_launches;
+    k_block_update<C><<<grid_n(a->n), 256, 0, a->stream>>>(sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr,
+                                                           di);
+    sr = dr;
+    si = di;
+  }
+  return launch_check();
+}
+
+// small dense eigenproblem of the b x b matrix G on one warp (Hessenberg
+// reduction + Schur + eigenvectors of the first nv values in sort order)
+int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
+  HessArgs h;
+  h.Hin = G;
+  h.Hout = a->bH;
+  h.Qout = a->bQ;
+  h.ritz = a->britz;
+  h.Y = a->bY;
+  h.est = a->best;
+  h.order = a->border;
+  h.st = a->bst;
+  h.gws = nullptr;
+  h.m = b;
+  h.k = kk;
+  h.nvec = nv;
+  h.which = a->cfg.sort;
+  h.do_shift = 0;
+  h.real_shifts = 0;
+  h.dense = 1;
+  h.use_beta = 0;
+  h.tol = 0;
+  h.beta = 0;
+  ++a->stats.kernel_launches;
+  k_hess<<<1, 32, 2 * sizeof(cplx) * b * b, a->stream>>>(h);
+  return launch_check();
+}
+
+// FP64 subspace iteration with Rayleigh-Ritz, started from the b vectors in
+// X (orthonormalised here).  Returns OAPB_OK when every wanted pair meets
+// `tol`; the Ritz vectors land in a->Xre / a->Xim and the values in a->evals.
+template <bool C>
+int refine(oapb_arnoldi* a, int b, double tol, unsigned max_it, double* res_out) {
+  const int n = a->n, kk = a->k;
+  double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
+  double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3];
+  if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  int rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei);
+  if (rc) return rc;
+  std::vector<double> norms(kk);
+  std::vector<cplx> th(b);
+  for (unsigned it = 0; it < max_it; ++it) {
+    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi))) return rc;
+    block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
+    ++a->stats.kernel_launches;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
+    if ((rc = small_eig(a, a->G, b, kk, kk))) return rc;
+    ++a->stats.kernel_launches;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
+    if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
+    if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    int hstat = 0;
+    DevState bs;
+    cudaMemcpyAsync(&hstat, a->bstatus, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
+    cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    if (bs.status & 2) return OAPB_ERR_TIMEOUT;
+    double scale = 0;
+    for (int q = 0; q < kk; ++q) scale = fmax(scale, cabs_(th[q]));
+    if (scale == 0) scale = 1;
+    double mx = 0;
+    for (int q = 0; q < kk; ++q) {
+      res_out[q] = norms[q] / scale;
+      mx = fmax(mx, res_out[q]);
+    }
+    a->stats.refine_iterations = it + 1;
+    if (mx <= tol || it + 1 == max_it) {
+      // Ritz vectors x_q = X s_q (unit: X orthonormal, s_q unit)
+      ++a->stats.kernel_launches;
+      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
+                                                          a->Xim);
+      a->evals.assign(th.begin(), th.begin() + kk);
+      if ((rc = launch_check())) return rc;
+      return mx <= tol ? OAPB_OK : OAPB_NOT_CONVERGED;
+    }
+    if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
+  }
+  return OAPB_NOT_CONVERGED;
+}
+
+// FP64 residuals of the k Ritz pairs in a->Xre with values a->evals, one
+// block pass per group of kBmMaxB vectors.
+template <bool C>
+int verify(oapb_arnoldi* a, double scale, double* out) {
+  const int n = a->n, kk = a->k;
+  std::vector<cplx> diag((size_t)kBmMaxB * kBmMaxB);
+  for (int q0 = 0; q0 < kk; q0 += kBmMaxB) {
+    const int b = kk - q0 < kBmMaxB ? kk - q0 : kBmMaxB;
+    const double* xr = a->Xre + (long)q0 * n;
+    const double* xi = C ? a->Xim + (long)q0 * n : nullptr;
+    int rc = block_apply<C>(a, xr, xi, b, a->Bre[1], a->Bim[1]);
     if (rc) return rc;
-    k_axmy<C><<<grid_n(n), 256, 0, a->stream>>>(xr, xi, th[q], a->wre, a->wim, n);
-    k_sumsq_partial<<<a->nupd, 256, 0, a->stream>>>(a->wre, C ? a->wim : nullptr, n, a->fpart);
-    k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, a->nupd, a->st);
-    DevState hs;
-    if ((rc = read_state(a, &hs))) return rc;
-    // restore f's norm is not needed after the solve
-    k_sumsq_partial<<<a->nupd, 256, 0, a->stream>>>(xr, xi, n, a->fpart);
-    k_set_fnorm<<<1, 256, 0, a->stream>>>(a->fpart, a->nupd, a->st);
-    DevState hx;
-    if ((rc = read_state(a, &hx))) return rc;
-    out[q] = sqrt(hs.fnorm2) / (scale * sqrt(hx.fnorm2));
+    for (auto& d : diag) d = cplx{0, 0};
+    for (int q = 0; q < b; ++q) diag[q + q * b] = a->evals[q0 + q];
+    if (cudaMemcpyAsync(a->G, diag.data(), sizeof(cplx) * b * b, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    ++a->stats.kernel_launches;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(xr, xi, b, a->G, b, b, a->Bre[1], a->Bim[1], 1, n,
+                                                        a->Bre[2], a->Bim[2]);
+    std::vector<double> rn(b), xn(b);
+    if ((rc = col_norms<C>(a, a->Bre[2], a->Bim[2], b, rn.data()))) return rc;
+    if ((rc = col_norms<C>(a, xr, xi, b, xn.data()))) return rc;
+    for (int q = 0; q < b; ++q) out[q0 + q] = rn[q] / (scale * (xn[q] > 0 ? xn[q] : 1));
   }
   return OAPB_OK;
 }
@@ -563,11 +853,21 @@ template <bool C>
 int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
   cudaStream_t s = a->stream;
   const int n = a->n, m = a->m, k = a->k;
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb;
+  // mixed form: FP32 IRAM, then FP64 subspace refinement on b = k + guard
+  // vectors (needs the block kernels, b <= kBmMaxB)
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB;
+  int guard = k / 4 > 2 ? k / 4 : 2;
+  if (guard > m - k) guard = m - k;
+  if (k + guard > kBmMaxB) guard = kBmMaxB - k;
+  const int b = mixed ? k + guard : k;
+  a->nvec_hess = b;
   a->stats.restarts = 0;
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
   a->stats.refine_iterations = 0;
+  a->stats.dgks_passes = 0;
+  int rc = alloc_blocks(a);
+  if (rc) return rc;
   if (cudaMemsetAsync(a->st, 0, sizeof(DevState), s) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->H, 0, sizeof(cplx) * m * m, s) != cudaSuccess) return OAPB_ERR_CUDA;
   if (a->cfg.init == OAPB_INIT_USER) {
@@ -575,39 +875,29 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
     cudaMemcpyAsync(a->fre, a->v0re, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     if (C) cudaMemcpyAsync(a->fim, a->v0im, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   } else {
+    ++a->stats.kernel_launches;
     k_init_vector<<<grid_n(n), 256, 0, s>>>(a->fre, C ? a->fim : nullptr, n, a->cfg.seed, a->cfg.init);
   }
-  int rc = set_fnorm(a);
-  if (rc) return rc;
+  if ((rc = set_fnorm(a))) return rc;
   const double tol = a->cfg.tolerance;
-  int st;
-  if (mixed) {
-    // phase 1: FP32 operator; the Ritz estimates cannot go below the FP32
-    // rounding floor, so stop at 1e-7 (or the goal if looser), then
-    // continue in FP64 from the compressed factorization
-    st = iram<C>(a, true, tol > 1e-7 ? tol : 1e-7, a->cfg.max_restarts, 0);
-    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
-    if (tol < 1e-7) {
-      // re-enter the restart loop with the FP64 operator: restart with the
-      // current shifts and rebuild the tail of the factorization in FP64
-      DevState hs;
-      if ((rc = read_state(a, &hs))) return rc;
-      (void)hs;
-      st = OAPB_NOT_CONVERGED;
-    }
-  } else {
-    st = iram<C>(a, false, tol, a->cfg.max_restarts, 0);
-    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
-  }
-  if ((rc = ritz_vectors<C>(a))) return rc;
+  // the FP32 operator floors the Ritz estimates near 1e-7 relative
+  const double tol1 = mixed ? (tol > 1e-7 ? tol : 1e-7) : tol;
+  int st = iram<C>(a, mixed, tol1, a->cfg.max_restarts, 0);
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  if ((rc = ritz_vectors<C>(a, b))) return rc;
   std::vector<cplx> th(m);
   DevState hs;
   if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * m, cudaMemcpyDeviceToHost, s) != cudaSuccess)
     return OAPB_ERR_CUDA;
   if ((rc = read_state(a, &hs))) return rc;
-  a->evals.assign(th.begin(), th.begin() + k);
   std::vector<double> r(k);
-  if ((rc = residuals<C>(a, a->evals, hs.scale, r.data()))) return rc;
+  if (mixed) {
+    st = refine<C>(a, b, tol, 40, r.data());
+    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  } else {
+    a->evals.assign(th.begin(), th.begin() + k);
+    if ((rc = verify<C>(a, hs.scale, r.data()))) return rc;
+  }
   double mx = 0;
   for (int q = 0; q < k; ++q) {
     if (eig_re) eig_re[q] = a->evals[q].re;
@@ -626,6 +916,14 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
+  void* bs[] = {a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+                a->bstatus, a->bst};
+  for (void* p : bs)
+    if (p) cudaFree(p);
+  for (int i = 0; i < 4; ++i) {
+    if (a->Bre[i]) cudaFree(a->Bre[i]);
+    if (a->Bim[i]) cudaFree(a->Bim[i]);
+  }
 }
 
 }  // namespace
@@ -733,8 +1031,12 @@ static int make_fp32_copy(oapb_arnoldi* a) {
   if (!a->x32re && dalloc(&a->x32re, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   if (a->is_c && !a->x32im && dalloc(&a->x32im, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   const int g = kNumSMs * 8;
+  ++a->stats.kernel_launches;
   k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64re, a->a32re, nn);
-  if (a->is_c) k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64im, a->a32im, nn);
+  if (a->is_c) {
+    ++a->stats.kernel_launches;
+    k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64im, a->a32im, nn);
+  }
   return launch_check();
 }
 
@@ -781,6 +1083,7 @@ int oapb_arnoldi_solve(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
   int st = a->is_c ? solve_impl<true>(a, eig_re, eig_im, residuals) : solve_impl<false>(a, eig_re, eig_im, residuals);
   if ((st == OAPB_OK || st == OAPB_NOT_CONVERGED) && evecs) {
     const long nk = (long)a->n * a->k;
+    ++a->stats.kernel_launches;
     k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(
         a->Xre, a->is_c ? a->Xim : nullptr, a->n, a->k, (double*)evecs->re, (double*)evecs->im);
     if (launch_check()) return OAPB_ERR_CUDA;
@@ -822,6 +1125,7 @@ int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* hi
       cudaFree(dre);
       return OAPB_ERR_NOMEM;
     }
+    ++a->stats.kernel_launches;
     k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(a->Xre, a->is_c ? a->Xim : nullptr,
                                                                                   a->n, a->k, dre, dim);
     if (vre) cudaMemcpyAsync(vre, dre, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream);
@@ -846,7 +1150,7 @@ int oapb_arnoldi_test_outcome(oapb_arnoldi* a, uint32_t index, double* out) {
   double scale = 0;
   for (auto& e : a->evals) scale = fmax(scale, cabs_(e));
   if (scale == 0) scale = 1;
-  int rc = a->is_c ? residuals<true>(a, a->evals, scale, r.data()) : residuals<false>(a, a->evals, scale, r.data());
+  int rc = a->is_c ? verify<true>(a, scale, r.data()) : verify<false>(a, scale, r.data());
   if (rc) return rc;
   *out = r[index];
   return OAPB_OK;

@@ -129,3 +129,29 @@ def test_not_converged_is_reported():
     s.set_operator(*planes(A, False))
     ev, res, st = s.solve(allow_not_converged=True)
     assert st == B.NOT_CONVERGED
+
+
+@pytest.mark.parametrize("n", [2048, 4096])
+def test_mixed_precision_reaches_fp64_residual(n):
+    # FP32 operator copy for the Krylov phase, FP64 refinement to 1e-10
+    A = planted_complex(n, seed=n + 1, nplant=8)
+    r = solve(A, 8, 40, precision=B.PREC_MIXED, vectors=True)
+    st = r["stats"]
+    assert st["converged"] == 1 and r["res"].max() <= TOL
+    assert st["matvec_fp32"] == 0 or st["refine_iterations"] >= 1
+    p = solve(A, 8, 40, precision=B.PREC_FP64)
+    for lam in p["ev"]:
+        assert np.min(np.abs(r["ev"] - lam)) < 1e-9 * abs(lam)
+    X = r["x"]
+    for q in range(8):
+        assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * np.abs(r["ev"]).max() * 1.01
+
+
+def test_mixed_precision_real_symmetric():
+    A, lam = planted_symmetric(1024, seed=8, lo_exp=-3.0)
+    # separated top of the spectrum so the refinement converges quickly
+    A = A + 3.0 * np.outer(np.ones(1024), np.ones(1024)) / 1024
+    r = solve(A, 4, 24, precision=B.PREC_MIXED)
+    w = np.sort(np.linalg.eigvalsh(A))[::-1][:4]
+    assert r["res"].max() <= TOL
+    assert np.allclose(np.sort(r["ev"].real)[::-1], w, rtol=1e-10)
