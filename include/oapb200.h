@@ -208,6 +208,11 @@ typedef struct oapb_arnoldi_stats {
   uint32_t matvec_timed;     /* number of dense matvec launches timed */
   uint32_t matvec_fp32;      /* of which on the FP32 operator copy */
   uint64_t kernel_launches;  /* library kernel launches over the handle's life */
+  double block_seconds;      /* device time of the timed FP64 block matvecs (profile) */
+  uint32_t block_timed;
+  uint32_t block_fp32_timed; /* FP32 block matvecs timed (profile) */
+  double block_fp32_seconds;
+  uint32_t block_fp32_width; /* right-hand sides of the FP32 block matvec */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

@@ -19,6 +19,7 @@ F64, F32 = 0, 1
 SORT = {"LM": 0, "LR": 1, "LI": 2, "SM": 3, "SR": 4, "SI": 5}
 PREC_FP64, PREC_MIXED = 0, 1
 INIT_RANDOM, INIT_FIRST_VALUE_IS_ONE, INIT_USER = 0, 1, 2
+TYPE_EIGENVECTOR, TYPE_WV = 0, 1
 
 
 class OapbError(RuntimeError):
@@ -47,7 +48,10 @@ class Stats(C.Structure):
                 ("refine_iterations", C.c_uint32), ("converged", C.c_int32),
                 ("max_residual", C.c_double), ("seconds", C.c_double),
                 ("matvec_seconds", C.c_double), ("matvec_timed", C.c_uint32),
-                ("matvec_fp32", C.c_uint32), ("kernel_launches", C.c_uint64)]
+                ("matvec_fp32", C.c_uint32), ("kernel_launches", C.c_uint64),
+                ("block_seconds", C.c_double), ("block_timed", C.c_uint32),
+                ("block_fp32_timed", C.c_uint32), ("block_fp32_seconds", C.c_double),
+                ("block_fp32_width", C.c_uint32)]
 
 
 MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,

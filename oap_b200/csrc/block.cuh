@@ -3,7 +3,9 @@
 // from HBM once per pass instead of once per vector.
 //
 //   k_block_matvec   W = A X        A row-major split planes (reference
-//                                   layout); X, W vector-contiguous, b <= 32
+//                                   layout, FP64 or FP32); X, W
+//                                   vector-contiguous FP64, b <= 32; split
+//                                   over K, partials summed by k_split_reduce
 //   k_block_dot      part = X^H Y   per row chunk (b1 x b2)
 //   k_block_reduce   G = sum of chunk partials
 //   k_block_update   Out = Base - X C   (C column-major b1 x b2)
@@ -16,95 +18,115 @@
 namespace oapb {
 
 constexpr int kBmRows = 64;   // rows per CTA tile
-constexpr int kBmK = 16;      // k-chunk staged in shared memory
 constexpr int kBmTM = 4;      // rows per thread
 constexpr int kBmTQ = 4;      // right-hand sides per thread
 constexpr int kBmMaxB = 32;
+constexpr int kBmThreads = 128;
 
-// Thread layout: (kBmRows / kBmTM) x (QB / kBmTQ) threads, QB = b rounded up
-// to kBmTQ.  A tile (kBmRows x kBmK complex) and X chunk (kBmK x QB) in
-// shared memory; every thread keeps TM x TQ complex accumulators.
-template <bool CPLX>
-__global__ void __launch_bounds__(128)
-k_block_matvec(const double* __restrict__ Are, const double* __restrict__ Aim, int n,
-               const double* __restrict__ Xre, const double* __restrict__ Xim, int b, double* Wre, double* Wim) {
-  __shared__ double as_re[kBmRows][kBmK + 1];
-  __shared__ double as_im[CPLX ? kBmRows : 1][kBmK + 1];
-  __shared__ double xs_re[kBmK][kBmMaxB];
-  __shared__ double xs_im[kBmK][kBmMaxB];
+// Partial products of W = A X over one K split: CTA (tile, split) computes
+// rows [64 tile, 64 tile + 64) over columns [k0, k1) and writes the FP64
+// partial to Wp[split][q][row].  T is the operator's element type (double
+// for the FP64 pass, float for the FP32 pass; X is converted to T when it is
+// staged); the per-thread accumulators are T.  Thread layout: 16 row groups
+// of kBmTM rows x QB / kBmTQ groups of right-hand sides.
+template <typename T, bool CPLX>
+__global__ void __launch_bounds__(kBmThreads)
+k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, const double* __restrict__ Xre,
+               const double* __restrict__ Xim, int b, int ksplit, double* __restrict__ Wp) {
+  constexpr int BK = 128 / sizeof(T);
+  __shared__ T as_re[kBmRows][BK + 1];
+  __shared__ T as_im[CPLX ? kBmRows : 1][BK + 1];
+  __shared__ T xs_re[BK][kBmMaxB];
+  __shared__ T xs_im[CPLX ? BK : 1][kBmMaxB];
   const int QB = ((b + kBmTQ - 1) / kBmTQ) * kBmTQ;
   const int nqg = QB / kBmTQ;
-  const int nthreads = (kBmRows / kBmTM) * nqg;
   const int t = threadIdx.x;
   const int rg = t % (kBmRows / kBmTM), qg = t / (kBmRows / kBmTM);
-  const bool active = t < nthreads;
-  const long ntiles = (n + kBmRows - 1) / kBmRows;
-  for (long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const long r0 = tile * kBmRows;
-    double accr[kBmTM][kBmTQ], acci[kBmTM][kBmTQ];
+  const bool active = qg < nqg;
+  const long r0 = (long)blockIdx.x * kBmRows;
+  const long kb = (long)blockIdx.y * ksplit;
+  const long ke = min((long)n, kb + ksplit);
+  T accr[kBmTM][kBmTQ], acci[kBmTM][kBmTQ];
 #pragma unroll
-    for (int i = 0; i < kBmTM; ++i)
+  for (int i = 0; i < kBmTM; ++i)
 #pragma unroll
-      for (int q = 0; q < kBmTQ; ++q) accr[i][q] = acci[i][q] = 0;
-    for (int k0 = 0; k0 < n; k0 += kBmK) {
-      __syncthreads();
-      for (int e = t; e < kBmRows * kBmK; e += blockDim.x) {
-        const int rr = e / kBmK, kk = e % kBmK;
-        const long r = r0 + rr, c = k0 + kk;
-        const bool in = r < n && c < n;
-        as_re[rr][kk] = in ? Are[r * n + c] : 0.0;
-        if (CPLX) as_im[rr][kk] = in ? Aim[r * n + c] : 0.0;
-      }
-      for (int e = t; e < kBmK * QB; e += blockDim.x) {
-        const int kk = e % kBmK, q = e / kBmK;
-        const long c = k0 + kk;
-        const bool in = q < b && c < n;
-        xs_re[kk][q] = in ? Xre[(long)q * n + c] : 0.0;
-        xs_im[kk][q] = (in && CPLX) ? Xim[(long)q * n + c] : 0.0;
-      }
-      __syncthreads();
-      if (active) {
+    for (int q = 0; q < kBmTQ; ++q) accr[i][q] = acci[i][q] = 0;
+  for (long k0 = kb; k0 < ke; k0 += BK) {
+    __syncthreads();
 #pragma unroll 4
-        for (int kk = 0; kk < kBmK; ++kk) {
-          double ar[kBmTM], ai[kBmTM], xr[kBmTQ], xi[kBmTQ];
-#pragma unroll
-          for (int i = 0; i < kBmTM; ++i) {
-            ar[i] = as_re[rg * kBmTM + i][kk];
-            ai[i] = CPLX ? as_im[rg * kBmTM + i][kk] : 0.0;
-          }
-#pragma unroll
-          for (int q = 0; q < kBmTQ; ++q) {
-            xr[q] = xs_re[kk][qg * kBmTQ + q];
-            xi[q] = xs_im[kk][qg * kBmTQ + q];
-          }
-#pragma unroll
-          for (int i = 0; i < kBmTM; ++i)
-#pragma unroll
-            for (int q = 0; q < kBmTQ; ++q) {
-              accr[i][q] = fma(ar[i], xr[q], accr[i][q]);
-              acci[i][q] = fma(ar[i], xi[q], acci[i][q]);
-              if (CPLX) {
-                accr[i][q] = fma(-ai[i], xi[q], accr[i][q]);
-                acci[i][q] = fma(ai[i], xr[q], acci[i][q]);
-              }
-            }
-        }
-      }
+    for (int e = t; e < kBmRows * BK; e += kBmThreads) {
+      const int rr = e / BK, kk = e % BK;
+      const long r = r0 + rr, c = k0 + kk;
+      const bool in = r < n && c < ke;
+      as_re[rr][kk] = in ? __ldcs(Are + r * n + c) : T(0);
+      if (CPLX) as_im[rr][kk] = in ? __ldcs(Aim + r * n + c) : T(0);
     }
+    for (int e = t; e < BK * QB; e += kBmThreads) {
+      const int kk = e % BK, q = e / BK;
+      const long c = k0 + kk;
+      const bool in = q < b && c < ke;
+      xs_re[kk][q] = in ? (T)Xre[(long)q * n + c] : T(0);
+      if (CPLX) xs_im[kk][q] = in ? (T)Xim[(long)q * n + c] : T(0);
+    }
+    __syncthreads();
     if (active) {
+#pragma unroll 8
+      for (int kk = 0; kk < BK; ++kk) {
+        T ar[kBmTM], ai[kBmTM], xr[kBmTQ], xi[kBmTQ];
 #pragma unroll
-      for (int i = 0; i < kBmTM; ++i) {
-        const long r = r0 + rg * kBmTM + i;
+        for (int i = 0; i < kBmTM; ++i) {
+          ar[i] = as_re[rg * kBmTM + i][kk];
+          ai[i] = CPLX ? as_im[rg * kBmTM + i][kk] : T(0);
+        }
 #pragma unroll
         for (int q = 0; q < kBmTQ; ++q) {
-          const int qq = qg * kBmTQ + q;
-          if (r < n && qq < b) {
-            Wre[(long)qq * n + r] = accr[i][q];
-            if (CPLX) Wim[(long)qq * n + r] = acci[i][q];
+          xr[q] = xs_re[kk][qg * kBmTQ + q];
+          xi[q] = CPLX ? xs_im[kk][qg * kBmTQ + q] : T(0);
+        }
+#pragma unroll
+        for (int i = 0; i < kBmTM; ++i)
+#pragma unroll
+          for (int q = 0; q < kBmTQ; ++q) {
+            accr[i][q] = fma(ar[i], xr[q], accr[i][q]);
+            if (CPLX) {
+              acci[i][q] = fma(ar[i], xi[q], acci[i][q]);
+              accr[i][q] = fma(-ai[i], xi[q], accr[i][q]);
+              acci[i][q] = fma(ai[i], xr[q], acci[i][q]);
+            }
           }
+      }
+    }
+  }
+  if (active) {
+    double* wr = Wp + (long)blockIdx.y * 2 * b * n;
+    double* wi = wr + (long)b * n;
+#pragma unroll
+    for (int i = 0; i < kBmTM; ++i) {
+      const long r = r0 + rg * kBmTM + i;
+#pragma unroll
+      for (int q = 0; q < kBmTQ; ++q) {
+        const int qq = qg * kBmTQ + q;
+        if (r < n && qq < b) {
+          wr[(long)qq * n + r] = (double)accr[i][q];
+          if (CPLX) wi[(long)qq * n + r] = (double)acci[i][q];
         }
       }
     }
+  }
+}
+
+// W[q][r] = sum over splits of Wp[s][q][r]
+template <bool CPLX>
+__global__ void k_split_reduce(const double* __restrict__ Wp, int nsplit, int b, int n, double* Wre, double* Wim) {
+  const long len = (long)b * n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    double a = 0, c = 0;
+    for (int s = 0; s < nsplit; ++s) {
+      a += Wp[(long)s * 2 * len + e];
+      if (CPLX) c += Wp[(long)s * 2 * len + len + e];
+    }
+    Wre[e] = a;
+    if (CPLX) Wim[e] = c;
   }
 }
 

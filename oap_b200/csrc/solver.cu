@@ -443,10 +443,14 @@ struct oapb_arnoldi {
   DevState* bst = nullptr;
   int ndot = 0, nnorm = 0;
   int nvec_hess = 0;
+  double* Wp = nullptr;   // split-K partials of the block matvec
+  int nsplit = 1, ksplit = 0;
   size_t hess_smem = 0;
   oapb_arnoldi_stats stats{};
   std::vector<cudaEvent_t> ev_pool;   // profiling events (pairs)
   size_t ev_used = 0;
+  std::vector<int> ev_kind;           // per pair: 0 matvec, 1 block matvec; +2 if FP32
+  std::vector<int> ev_b;
   // last solve outputs (host)
   std::vector<cplx> evals;
 };
@@ -466,6 +470,30 @@ int dalloc(P** p, size_t bytes) {
 }
 
 int grid_n(long n) { return grid_for(n, 256, kNumSMs * 8); }
+
+// Profiling: an event pair around one launch on the solver stream.
+// kind 0: single-vector dense matvec, 1: block matvec
+struct Timed {
+  cudaEvent_t e0, e1;
+  int kind, fp32, b;
+};
+
+bool prof_begin(oapb_arnoldi* a, Timed& t) {
+  if (!a->cfg.profile) return false;
+  while (a->ev_pool.size() < a->ev_used + 2) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return false;
+    a->ev_pool.push_back(ev);
+  }
+  t.e0 = a->ev_pool[a->ev_used];
+  t.e1 = a->ev_pool[a->ev_used + 1];
+  a->ev_used += 2;
+  a->ev_kind.push_back(t.kind + 2 * t.fp32);
+  a->ev_b.push_back(t.b);
+  cudaEventRecord(t.e0, a->stream);
+  return true;
+}
+void prof_end(oapb_arnoldi* a, Timed& t) { cudaEventRecord(t.e1, a->stream); }
 
 // f <- ||f||^2 into st->fnorm2
 int set_fnorm(oapb_arnoldi* a) {
@@ -488,18 +516,8 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
     int rc = a->cb(&w, &v, a->cb_user, type, (void*)s);
     return rc == 0 ? OAPB_OK : OAPB_ERR_CALLBACK;
   }
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (a->cfg.profile) {
-    while (a->ev_pool.size() < a->ev_used + 2) {
-      cudaEvent_t ev;
-      if (cudaEventCreate(&ev) != cudaSuccess) return OAPB_ERR_CUDA;
-      a->ev_pool.push_back(ev);
-    }
-    e0 = a->ev_pool[a->ev_used];
-    e1 = a->ev_pool[a->ev_used + 1];
-    a->ev_used += 2;
-    cudaEventRecord(e0, s);
-  }
+  Timed tm{nullptr, nullptr, 0, fp32 ? 1 : 0, 1};
+  const bool prof = prof_begin(a, tm);
   cudaError_t e;
   ++a->stats.kernel_launches;
   if (fp32)
@@ -508,10 +526,8 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
   else
     e = launch_matvec<double>(a->a64re, a->is_c ? a->a64im : nullptr, n, n, xre, a->is_c ? xim : nullptr, yre,
                               a->is_c ? yim : nullptr, s);
-  if (e1) {
-    cudaEventRecord(e1, s);
-    if (fp32) a->stats.matvec_fp32++;
-  }
+  if (prof) prof_end(a, tm);
+  if (fp32) a->stats.matvec_fp32++;
   return e == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 
@@ -654,6 +670,17 @@ int alloc_blocks(oapb_arnoldi* a) {
     if (a->is_c) rc |= dalloc(&a->Bim[i], vb);
   }
   a->ndot = (a->n + kDotChunk - 1) / kDotChunk;
+  {
+    const long tiles = (a->n + kBmRows - 1) / kBmRows;
+    long sp = (6L * kNumSMs + tiles - 1) / tiles;
+    if (sp < 1) sp = 1;
+    if (sp > 8) sp = 8;
+    long ks = (a->n + sp - 1) / sp;
+    ks = ((ks + 31) / 32) * 32;
+    a->ksplit = (int)ks;
+    a->nsplit = (int)((a->n + ks - 1) / ks);
+    rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
+  }
   a->nnorm = grid_for(a->n, 256, kNumSMs * 2);
   const size_t bb = sizeof(cplx) * kBmMaxB * kBmMaxB;
   rc |= dalloc(&a->bpart, bb * (size_t)a->ndot);
@@ -677,14 +704,16 @@ template <bool C>
 void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, const double* yr, const double* yi,
                 int b2, cplx* G) {
   ++a->stats.kernel_launches;
+  a->stats.kernel_launches += 2;
   k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(xr, xi, b1, yr, yi, b2, a->n, a->bpart);
   ++a->stats.kernel_launches;
   k_block_reduce<<<grid_for(b1 * b2, 128, 8), 128, 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G);
 }
 
-// W = A X (FP64 operator, b vectors)
+// W = A X (b vectors); FP32 operator copy when fp32, else FP64
 template <bool C>
-int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi) {
+int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
+                bool fp32 = false) {
   if (a->cb) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
@@ -693,10 +722,19 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     }
     return OAPB_OK;
   }
-  const long tiles = (a->n + kBmRows - 1) / kBmRows;
-  const int grid = (int)(tiles < kNumSMs * 8 ? tiles : kNumSMs * 8);
-  ++a->stats.kernel_launches;
-  k_block_matvec<C><<<grid, 128, 0, a->stream>>>(a->a64re, a->a64im, a->n, xr, xi, b, wr, wi);
+  const int tiles = (a->n + kBmRows - 1) / kBmRows;
+  dim3 grid(tiles, a->nsplit);
+  a->stats.kernel_launches += 2;
+  Timed tm{nullptr, nullptr, 1, fp32 ? 1 : 0, b};
+  const bool prof = prof_begin(a, tm);
+  if (fp32)
+    k_block_matvec<float, C><<<grid, kBmThreads, 0, a->stream>>>(a->a32re, a->a32im, a->n, xr, xi, b, a->ksplit,
+                                                                a->Wp);
+  else
+    k_block_matvec<double, C><<<grid, kBmThreads, 0, a->stream>>>(a->a64re, a->a64im, a->n, xr, xi, b, a->ksplit,
+                                                                 a->Wp);
+  if (prof) prof_end(a, tm);
+  k_split_reduce<C><<<grid_n((long)b * a->n), 256, 0, a->stream>>>(a->Wp, a->nsplit, b, a->n, wr, wi);
   a->stats.block_matvecs++;
   return launch_check();
 }
@@ -730,6 +768,7 @@ int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* 
     double* di = pass == 0 ? ti : xi;
     block_gram<C>(a, sr, si, b, sr, si, b, a->G2);
     ++a->stats.kernel_launches;
+    a->stats.kernel_launches += 4;
     k_chol_inv<<<1, 32, 0, a->stream>>>(a->G2, b, a->Rinv, a->bstatus);
     ++a->stats.kernel_launches;
     k_block_update<C><<<grid_n(a->n), 256, 0, a->stream>>>(sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr,
@@ -768,34 +807,39 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
   return launch_check();
 }
 
-// FP64 subspace iteration with Rayleigh-Ritz, started from the b vectors in
-// X (orthonormalised here).  Returns OAPB_OK when every wanted pair meets
-// `tol`; the Ritz vectors land in a->Xre / a->Xim and the values in a->evals.
+constexpr int kSlow = 100;   // subspace(): convergence too slow for the iteration budget
+
+// Block subspace iteration with Rayleigh-Ritz on b vectors:
+//   W = A X; G = X^H W; R = W - X G; G = S diag(theta) S^-1;
+//   residual_q = ||R s_q|| / (max |theta| ||s_q||);  X <- orth(W)
+// The start block is a->Xre (orthonormalised here) or, with from_bx, the
+// current block buffer.  fp32 selects the FP32 operator copy; that phase
+// stops at `tol` or when the residuals stop falling (the FP32 floor).
+// Returns OAPB_OK (goal met: Ritz vectors in a->Xre, values in a->evals),
+// kSlow when the observed rate cannot reach the goal within the budget,
+// OAPB_NOT_CONVERGED or an error.
 template <bool C>
-int refine(oapb_arnoldi* a, int b, double tol, unsigned max_it, double* res_out) {
+int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, double* res_out, bool from_bx) {
   const int n = a->n, kk = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
   double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3];
   if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-  int rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei);
-  if (rc) return rc;
-  std::vector<double> norms(kk);
+  int rc = OAPB_OK;
+  if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei))) return rc;
+  std::vector<double> norms(kk), hist;
   std::vector<cplx> th(b);
   for (unsigned it = 0; it < max_it; ++it) {
-    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi))) return rc;
+    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
     block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
-    ++a->stats.kernel_launches;
+    a->stats.kernel_launches += 5;
     k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
     if ((rc = small_eig(a, a->G, b, kk, kk))) return rc;
-    ++a->stats.kernel_launches;
     k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
     if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
     if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
-    int hstat = 0;
     DevState bs;
-    cudaMemcpyAsync(&hstat, a->bstatus, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
     cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
     if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
     if (bs.status & 2) return OAPB_ERR_TIMEOUT;
@@ -807,15 +851,31 @@ int refine(oapb_arnoldi* a, int b, double tol, unsigned max_it, double* res_out)
       res_out[q] = norms[q] / scale;
       mx = fmax(mx, res_out[q]);
     }
-    a->stats.refine_iterations = it + 1;
-    if (mx <= tol || it + 1 == max_it) {
-      // Ritz vectors x_q = X s_q (unit: X orthonormal, s_q unit)
-      ++a->stats.kernel_launches;
+    hist.push_back(mx);
+    a->stats.refine_iterations++;
+    const bool done = mx <= tol;
+    bool stop = done;
+    if (!done && hist.size() >= 4) {
+      const double r0 = hist[hist.size() - 3], r1 = mx;
+      const double rate = (r0 > 0 && r1 > 0) ? sqrt(r1 / r0) : 1.0;
+      if (fp32 && mx < 1e-4 && rate > 0.6) stop = true;  // FP32 floor reached
+      if (!stop) {
+        const double need = rate < 1.0 ? log(tol / mx) / log(rate) : 1e30;
+        if (rate > 0.85 || need > (double)(max_it - it - 1)) return kSlow;
+      }
+    }
+    if (stop || it + 1 == max_it) {
+      if (fp32 && !done) {
+        // hand the current block to the next phase: X <- orth(W)
+        if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
+        return OAPB_OK;
+      }
+      a->stats.kernel_launches += 1;
       k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
                                                           a->Xim);
       a->evals.assign(th.begin(), th.begin() + kk);
       if ((rc = launch_check())) return rc;
-      return mx <= tol ? OAPB_OK : OAPB_NOT_CONVERGED;
+      return done ? OAPB_OK : OAPB_NOT_CONVERGED;
     }
     if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
   }
@@ -849,25 +909,19 @@ int verify(oapb_arnoldi* a, double scale, double* out) {
   return OAPB_OK;
 }
 
+__global__ void k_init_block(double* xre, double* xim, int b, int n, uint64_t seed) {
+  const long len = (long)b * n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    xre[e] = uniform_pm1(seed ^ 0xA0761D6478BD642Full, (uint64_t)e);
+    if (xim) xim[e] = uniform_pm1(seed ^ 0xE7037ED1A0B428DBull, (uint64_t)e);
+  }
+}
+
+// Fresh start of the Krylov factorization: f = start vector, H = 0.
 template <bool C>
-int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
+int iram_start(oapb_arnoldi* a) {
   cudaStream_t s = a->stream;
-  const int n = a->n, m = a->m, k = a->k;
-  // mixed form: FP32 IRAM, then FP64 subspace refinement on b = k + guard
-  // vectors (needs the block kernels, b <= kBmMaxB)
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB;
-  int guard = k / 4 > 2 ? k / 4 : 2;
-  if (guard > m - k) guard = m - k;
-  if (k + guard > kBmMaxB) guard = kBmMaxB - k;
-  const int b = mixed ? k + guard : k;
-  a->nvec_hess = b;
-  a->stats.restarts = 0;
-  a->stats.matvecs = 0;
-  a->stats.block_matvecs = 0;
-  a->stats.refine_iterations = 0;
-  a->stats.dgks_passes = 0;
-  int rc = alloc_blocks(a);
-  if (rc) return rc;
+  const int n = a->n, m = a->m;
   if (cudaMemsetAsync(a->st, 0, sizeof(DevState), s) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->H, 0, sizeof(cplx) * m * m, s) != cudaSuccess) return OAPB_ERR_CUDA;
   if (a->cfg.init == OAPB_INIT_USER) {
@@ -875,29 +929,82 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
     cudaMemcpyAsync(a->fre, a->v0re, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     if (C) cudaMemcpyAsync(a->fim, a->v0im, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
   } else {
-    ++a->stats.kernel_launches;
+    a->stats.kernel_launches++;
     k_init_vector<<<grid_n(n), 256, 0, s>>>(a->fre, C ? a->fim : nullptr, n, a->cfg.seed, a->cfg.init);
   }
-  if ((rc = set_fnorm(a))) return rc;
-  const double tol = a->cfg.tolerance;
-  // the FP32 operator floors the Ritz estimates near 1e-7 relative
-  const double tol1 = mixed ? (tol > 1e-7 ? tol : 1e-7) : tol;
-  int st = iram<C>(a, mixed, tol1, a->cfg.max_restarts, 0);
+  return set_fnorm(a);
+}
+
+// The plain FP64 GPU Arnoldi: IRAM to the goal, Ritz vectors, FP64
+// verification of every wanted pair in one block pass.
+template <bool C>
+int solve_plain(oapb_arnoldi* a, double* r) {
+  a->nvec_hess = a->k;
+  int rc = iram_start<C>(a);
+  if (rc) return rc;
+  int st = iram<C>(a, false, a->cfg.tolerance, a->cfg.max_restarts, 0);
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
-  if ((rc = ritz_vectors<C>(a, b))) return rc;
-  std::vector<cplx> th(m);
+  if ((rc = ritz_vectors<C>(a, a->k))) return rc;
+  std::vector<cplx> th(a->m);
   DevState hs;
-  if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * m, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+  if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * a->m, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
     return OAPB_ERR_CUDA;
   if ((rc = read_state(a, &hs))) return rc;
-  std::vector<double> r(k);
-  if (mixed) {
-    st = refine<C>(a, b, tol, 40, r.data());
-    if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
-  } else {
-    a->evals.assign(th.begin(), th.begin() + k);
-    if ((rc = verify<C>(a, hs.scale, r.data()))) return rc;
+  a->evals.assign(th.begin(), th.begin() + a->k);
+  return verify<C>(a, hs.scale, r);
+}
+
+// The mixed form: (1) FP32 block subspace iteration from a seeded random
+// block down to the FP32 floor, (2) FP64 block subspace iteration to the
+// goal.  When the spectrum makes subspace iteration too slow, (3) FP32 IRAM
+// followed by the FP64 refinement of its Ritz vectors, and finally (4) the
+// plain FP64 IRAM.
+template <bool C>
+int solve_mixed(oapb_arnoldi* a, double* r) {
+  const int n = a->n, m = a->m, k = a->k;
+  const double tol = a->cfg.tolerance;
+  int b = k + (k / 2 > 4 ? k / 2 : 4);
+  if (b > kBmMaxB) b = kBmMaxB;
+  if (b > n) b = n;
+  a->stats.kernel_launches++;
+  k_init_block<<<grid_n((long)b * n), 256, 0, a->stream>>>(a->Xre, C ? a->Xim : nullptr, b, n, a->cfg.seed);
+  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r, false);
+  if (st == OAPB_OK) {
+    st = subspace<C>(a, b, false, tol, 30, r, true);
+    if (st == OAPB_OK) return OAPB_OK;
   }
+  if (st != OAPB_OK && st != kSlow && st != OAPB_NOT_CONVERGED) return st;
+  // (3) Krylov phase on the FP32 operator
+  int bi = k + (m - k < 4 ? m - k : 4);
+  if (bi > kBmMaxB) bi = kBmMaxB;
+  a->nvec_hess = bi;
+  int rc = iram_start<C>(a);
+  if (rc) return rc;
+  st = iram<C>(a, true, tol > 1e-7 ? tol : 1e-7, a->cfg.max_restarts, 0);
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  if ((rc = ritz_vectors<C>(a, bi))) return rc;
+  st = subspace<C>(a, bi, false, tol, 40, r, false);
+  if (st == OAPB_OK) return OAPB_OK;
+  if (st != kSlow && st != OAPB_NOT_CONVERGED) return st;
+  // (4)
+  return solve_plain<C>(a, r);
+}
+
+template <bool C>
+int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
+  const int k = a->k;
+  // the mixed form needs the dense operator and the block kernels (k <= 32)
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB && a->a32re;
+  a->stats.restarts = 0;
+  a->stats.matvecs = 0;
+  a->stats.block_matvecs = 0;
+  a->stats.refine_iterations = 0;
+  a->stats.dgks_passes = 0;
+  int rc = alloc_blocks(a);
+  if (rc) return rc;
+  std::vector<double> r(k);
+  int st = mixed ? solve_mixed<C>(a, r.data()) : solve_plain<C>(a, r.data());
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   double mx = 0;
   for (int q = 0; q < k; ++q) {
     if (eig_re) eig_re[q] = a->evals[q].re;
@@ -906,7 +1013,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
     mx = r[q] > mx ? r[q] : mx;
   }
   a->stats.max_residual = mx;
-  a->stats.converged = mx <= tol;
+  a->stats.converged = mx <= a->cfg.tolerance;
   return a->stats.converged ? OAPB_OK : OAPB_NOT_CONVERGED;
 }
 
@@ -916,7 +1023,7 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->Wp, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);
@@ -969,8 +1076,9 @@ int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void
   const bool C = a->is_c;
   rc |= dalloc(&a->Vre, vb * (m + 1));
   if (C) rc |= dalloc(&a->Vim, vb * (m + 1));
-  rc |= dalloc(&a->Xre, vb * (m + 1));
-  if (C) rc |= dalloc(&a->Xim, vb * (m + 1));
+  const int nx = (m + 1) > kBmMaxB ? (m + 1) : kBmMaxB;  // Ritz / start blocks
+  rc |= dalloc(&a->Xre, vb * nx);
+  if (C) rc |= dalloc(&a->Xim, vb * nx);
   rc |= dalloc(&a->fre, vb);
   rc |= dalloc(&a->wre, vb);
   if (C) rc |= dalloc(&a->fim, vb);
@@ -1091,15 +1199,32 @@ int oapb_arnoldi_solve(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
   }
   a->stats.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   a->stats.matvec_seconds = 0;
-  a->stats.matvec_timed = (uint32_t)(a->ev_used / 2);
+  a->stats.matvec_timed = 0;
+  a->stats.block_seconds = 0;
+  a->stats.block_timed = 0;
+  a->stats.block_fp32_seconds = 0;
+  a->stats.block_fp32_timed = 0;
   if (a->ev_used) {
     cudaStreamSynchronize(a->stream);
     for (size_t i = 0; i + 1 < a->ev_used; i += 2) {
       float ms = 0;
-      if (cudaEventElapsedTime(&ms, a->ev_pool[i], a->ev_pool[i + 1]) == cudaSuccess)
+      if (cudaEventElapsedTime(&ms, a->ev_pool[i], a->ev_pool[i + 1]) != cudaSuccess) continue;
+      const int kind = a->ev_kind[i / 2];
+      if (kind == 0 || kind == 2) {
         a->stats.matvec_seconds += ms * 1e-3;
+        a->stats.matvec_timed++;
+      } else if (kind == 1) {
+        a->stats.block_seconds += ms * 1e-3;
+        a->stats.block_timed++;
+      } else {
+        a->stats.block_fp32_seconds += ms * 1e-3;
+        a->stats.block_fp32_timed++;
+        a->stats.block_fp32_width = a->ev_b[i / 2];
+      }
     }
   }
+  a->ev_kind.clear();
+  a->ev_b.clear();
   return st;
 }
 

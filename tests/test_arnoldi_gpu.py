@@ -86,18 +86,23 @@ def test_callback_operator_matches_dense():
     # CuHArnoldiCallback::setCallback: the matvec is user code on the device
     A, lam = planted_symmetric(300, seed=4)
     a = planes(A, False)[0]
+    calls = []
 
     def mv(w, v, typ, stream):
         # run on the solver's stream so the ordering with its kernels holds
         with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
             torch.mv(a, ptr_tensor(v.re, 300), out=ptr_tensor(w.re, 300))
+        calls.append(typ)
         return 0
 
-    s = B.Arnoldi(300, 24, 4, seed=3)
+    s = B.Arnoldi(300, 32, 5, seed=3)
     s.set_callback(mv)
     ev, res, st = s.solve()
     assert st == B.OK
-    assert np.allclose(np.sort(np.array(ev).real)[::-1], lam[:4], rtol=1e-10)
+    assert B.TYPE_WV in calls and B.TYPE_EIGENVECTOR in calls
+    assert np.allclose(np.sort(np.array(ev).real)[::-1], lam[:5], rtol=1e-10)
+    d = solve(A, 5, 32, seed=3)
+    assert np.allclose(np.sort(np.array(ev).real), np.sort(d["ev"].real), rtol=1e-12)
 
 
 def ptr_tensor(ptr, n):
@@ -147,11 +152,18 @@ def test_mixed_precision_reaches_fp64_residual(n):
         assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * np.abs(r["ev"]).max() * 1.01
 
 
-def test_mixed_precision_real_symmetric():
-    A, lam = planted_symmetric(1024, seed=8, lo_exp=-3.0)
-    # separated top of the spectrum so the refinement converges quickly
-    A = A + 3.0 * np.outer(np.ones(1024), np.ones(1024)) / 1024
-    r = solve(A, 4, 24, precision=B.PREC_MIXED)
-    w = np.sort(np.linalg.eigvalsh(A))[::-1][:4]
+@pytest.mark.parametrize("gap", ["separated", "clustered"])
+def test_mixed_precision_real_symmetric(gap):
+    # separated: 4 eigenvalues well above the rest; clustered: the geometric
+    # 1 .. 1e-3 spectrum, where the refinement must hand over to the FP64
+    # Krylov restarts
+    n = 1024
+    rng = np.random.default_rng(8)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    lam = 10.0 ** (-3.0 * np.arange(n) / (n - 1))
+    if gap == "separated":
+        lam[:4] = [8.0, 7.0, 6.0, 5.0]
+    A = (Q * lam) @ Q.T
+    r = solve(A, 4, 32, precision=B.PREC_MIXED)
     assert r["res"].max() <= TOL
-    assert np.allclose(np.sort(r["ev"].real)[::-1], w, rtol=1e-10)
+    assert np.allclose(np.sort(r["ev"].real)[::-1], np.sort(lam)[::-1][:4], rtol=1e-10)

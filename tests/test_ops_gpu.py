@@ -73,8 +73,8 @@ def test_magnitude_and_sum():
 def test_tensor_product():
     P0, P1 = rng.normal(size=(3, 4)), rng.normal(size=(5, 2))
     o = zeros((15, 8), False)
-    run(L.oapb_tensor_product, C.byref(B.mat(*o)), C.byref(B.mat(*planes(P0))),
-        C.byref(B.mat(*planes(P1))), S)
+    p0, p1 = planes(P0), planes(P1)   # keep the device buffers alive
+    run(L.oapb_tensor_product, C.byref(B.mat(*o)), C.byref(B.mat(*p0)), C.byref(B.mat(*p1)), S)
     assert np.array_equal(host(*o), O.tensor_product(P0, P1))
 
 
@@ -157,10 +157,12 @@ def test_is_upper_triangular():
     T = np.triu(rng.normal(size=(9, 9)))
     T[4, 3] = 5e-4
     out = C.c_int()
-    run(L.oapb_is_upper_triangular, C.byref(out), C.byref(B.mat(*planes(T))), 1e-3, S)
+    t = planes(T)
+    run(L.oapb_is_upper_triangular, C.byref(out), C.byref(B.mat(*t)), 1e-3, S)
     assert out.value == 1 == int(O.is_upper_triangular(T))
     T[4, 3] = 2e-3
-    run(L.oapb_is_upper_triangular, C.byref(out), C.byref(B.mat(*planes(T))), 1e-3, S)
+    t = planes(T)
+    run(L.oapb_is_upper_triangular, C.byref(out), C.byref(B.mat(*t)), 1e-3, S)
     assert out.value == 0 == int(O.is_upper_triangular(T))
 
 
