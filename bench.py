@@ -47,6 +47,10 @@ def parse():
     p.add_argument("--plain-steps", type=int, default=None)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--n", type=int, default=N)
+    p.add_argument("--quick", action="store_true",
+                   help="profiling run: time one form only, no plain / e2e / CPU legs")
+    p.add_argument("--form", default="mixed", choices=["mixed", "plain"],
+                   help="form timed by --quick")
     return p.parse_args()
 
 
@@ -294,6 +298,15 @@ def run_ours(args, world, rank, local):
         ms = e0.elapsed_time(e1)
         return ms / 1e3, conv, prof, s.stats()["kernel_launches"] - launches0, stt
 
+    if args.quick:
+        s_q = solver(B.PREC_MIXED if args.form == "mixed" else B.PREC_FP64)
+        secs, conv, prof, launches, stt = timed(s_q, args.steps, args.warmup)
+        if rank == 0:
+            print(json.dumps({"quick": True, "form": args.form, "n": n, "steps": args.steps,
+                              "seconds": secs, "converged": conv, "launches": launches, "profile": prof,
+                              "stats": stt}), flush=True)
+        s_q.close()
+        return
     # chosen form
     mixed = solver(B.PREC_MIXED)
     with Clocks(local) as clk:

@@ -194,7 +194,8 @@ class Arnoldi:
         def tramp(w, v, user, typ, stream):
             try:
                 return int(fn(w.contents, v.contents, typ, stream) or 0)
-            except Exception:
+            except Exception as e:  # reported by solve()
+                self._cb_error = e
                 return 1
         self._cb = MATVEC_FN(tramp)
         check(lib().oapb_arnoldi_set_callback(self.h, self._cb, None),
@@ -212,7 +213,10 @@ class Arnoldi:
         vm = None
         if vectors is not None:
             vm = mat(vectors[0], vectors[1], columns=k, rows=self.cfg.n)
+        self._cb_error = None
         st = lib().oapb_arnoldi_solve(self.h, er, ei, rs, C.byref(vm) if vm else None)
+        if st == ERR_CALLBACK and self._cb_error is not None:
+            raise OapbError(st, "oapb_arnoldi_solve") from self._cb_error
         if not (st == OK or (allow_not_converged and st == NOT_CONVERGED)):
             raise OapbError(st, "oapb_arnoldi_solve")
         return [complex(er[i], ei[i]) for i in range(k)], list(rs), st

@@ -14,75 +14,130 @@
 #pragma once
 
 #include "common.cuh"
+#include "matvec.cuh"
 
 namespace oapb {
 
-constexpr int kBmRows = 64;   // rows per CTA tile
+constexpr int kBmRows = 128;  // rows per CTA tile
 constexpr int kBmTM = 4;      // rows per thread
 constexpr int kBmTQ = 4;      // right-hand sides per thread
 constexpr int kBmMaxB = 32;
-constexpr int kBmThreads = 128;
+constexpr int kBmThreads = 256;
+
+__device__ __forceinline__ void mkvec(const float (&t)[4], float4& v) { v = make_float4(t[0], t[1], t[2], t[3]); }
+__device__ __forceinline__ void mkvec(const double (&t)[2], double2& v) { v = make_double2(t[0], t[1]); }
+
+template <typename T>
+struct Quad;  // four consecutive T in shared memory
+template <>
+struct Quad<float> {
+  __device__ static __forceinline__ void ld(const float* p, float (&v)[4]) {
+    float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  }
+};
+template <>
+struct Quad<double> {
+  __device__ static __forceinline__ void ld(const double* p, double (&v)[4]) {
+    double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+  }
+};
 
 // Partial products of W = A X over one K split: CTA (tile, split) computes
-// rows [64 tile, 64 tile + 64) over columns [k0, k1) and writes the FP64
-// partial to Wp[split][q][row].  T is the operator's element type (double
-// for the FP64 pass, float for the FP32 pass; X is converted to T when it is
-// staged); the per-thread accumulators are T.  Thread layout: 16 row groups
-// of kBmTM rows x QB / kBmTQ groups of right-hand sides.
+// rows [128 tile, 128 tile + 128) over columns [k0, k1) and writes the FP64
+// partial to Wp[split][plane][q][row].  T is the operator's element type
+// (double for the FP64 pass, float for the FP32 pass; X is converted to T
+// when it is staged); the per-thread accumulators are T.
+//
+// A tiles are read with 16-byte coalesced loads (8 lanes per 128-byte row
+// segment), prefetched into registers one tile ahead, and stored transposed
+// ([k][row]) in shared memory with the row index XOR-swizzled by the
+// 16-byte column group, so both the transposing stores and the 4-row vector
+// reads are free of bank conflicts.  Thread (rg, qg) owns rows 4 rg .. 4 rg + 3
+// and right-hand sides 4 qg .. 4 qg + 3: per k it reads 4 + 4 A values and
+// 4 + 4 X values (broadcast across the warp) for 16 complex FMAs.
 template <typename T, bool CPLX>
 __global__ void __launch_bounds__(kBmThreads)
 k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, const double* __restrict__ Xre,
-               const double* __restrict__ Xim, int b, int ksplit, double* __restrict__ Wp) {
-  constexpr int BK = 128 / sizeof(T);
-  __shared__ T as_re[kBmRows][BK + 1];
-  __shared__ T as_im[CPLX ? kBmRows : 1][BK + 1];
-  __shared__ T xs_re[BK][kBmMaxB];
-  __shared__ T xs_im[CPLX ? BK : 1][kBmMaxB];
+               const double* __restrict__ Xim, int b, int ksplit, double* __restrict__ Wp, int vec_ok) {
+  using V = typename Vec16<T>::type;
+  constexpr int VW = Vec16<T>::N;            // T per 16-byte vector
+  constexpr int BK = 128 / sizeof(T);        // k per tile: one 128-byte row segment
+  constexpr int VPR = BK / VW;               // vectors per row segment (8)
+  constexpr int NV = kBmRows * VPR / kBmThreads;  // vectors per thread per plane (4)
+  constexpr int NP = CPLX ? 2 : 1;
+  __shared__ __align__(16) T As[NP][BK][kBmRows];
+  __shared__ __align__(16) T Xs[NP][BK][kBmMaxB];
   const int QB = ((b + kBmTQ - 1) / kBmTQ) * kBmTQ;
-  const int nqg = QB / kBmTQ;
   const int t = threadIdx.x;
   const int rg = t % (kBmRows / kBmTM), qg = t / (kBmRows / kBmTM);
-  const bool active = qg < nqg;
+  const bool active = qg * kBmTQ < QB;
   const long r0 = (long)blockIdx.x * kBmRows;
   const long kb = (long)blockIdx.y * ksplit;
   const long ke = min((long)n, kb + ksplit);
+  const T* planes[2] = {Are, Aim};
+  const bool full_rows = r0 + kBmRows <= n;
+
+  V pre[NP][NV];
+  auto fetch = [&](long k0) {
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        const int c = t + i * kBmThreads;
+        const int row = c / VPR, kq = c % VPR;
+        const long r = r0 + row, col = k0 + (long)kq * VW;
+        if (vec_ok && (full_rows || r < n) && col + VW <= ke) {
+          pre[p][i] = __ldcs(reinterpret_cast<const V*>(planes[p] + r * n + col));
+        } else {
+          T tmp[VW];
+#pragma unroll
+          for (int e = 0; e < VW; ++e) tmp[e] = (r < n && col + e < ke) ? planes[p][r * n + col + e] : T(0);
+          mkvec(tmp, pre[p][i]);
+        }
+      }
+  };
+
   T accr[kBmTM][kBmTQ], acci[kBmTM][kBmTQ];
 #pragma unroll
   for (int i = 0; i < kBmTM; ++i)
 #pragma unroll
     for (int q = 0; q < kBmTQ; ++q) accr[i][q] = acci[i][q] = 0;
+
+  if (kb < ke) fetch(kb);
   for (long k0 = kb; k0 < ke; k0 += BK) {
     __syncthreads();
-#pragma unroll 4
-    for (int e = t; e < kBmRows * BK; e += kBmThreads) {
-      const int rr = e / BK, kk = e % BK;
-      const long r = r0 + rr, c = k0 + kk;
-      const bool in = r < n && c < ke;
-      as_re[rr][kk] = in ? __ldcs(Are + r * n + c) : T(0);
-      if (CPLX) as_im[rr][kk] = in ? __ldcs(Aim + r * n + c) : T(0);
-    }
+    // registers -> shared (transposed, swizzled)
+#pragma unroll
+    for (int p = 0; p < NP; ++p)
+#pragma unroll
+      for (int i = 0; i < NV; ++i) {
+        const int c = t + i * kBmThreads;
+        const int row = c / VPR, kq = c % VPR;
+        const int prow = row ^ ((kq & 7) << 2);
+        const T* v = reinterpret_cast<const T*>(&pre[p][i]);
+#pragma unroll
+        for (int e = 0; e < VW; ++e) As[p][kq * VW + e][prow] = v[e];
+      }
     for (int e = t; e < BK * QB; e += kBmThreads) {
       const int kk = e % BK, q = e / BK;
       const long c = k0 + kk;
       const bool in = q < b && c < ke;
-      xs_re[kk][q] = in ? (T)Xre[(long)q * n + c] : T(0);
-      if (CPLX) xs_im[kk][q] = in ? (T)Xim[(long)q * n + c] : T(0);
+      Xs[0][kk][q] = in ? (T)Xre[(long)q * n + c] : T(0);
+      if (CPLX) Xs[NP - 1][kk][q] = in ? (T)Xim[(long)q * n + c] : T(0);
     }
     __syncthreads();
+    if (k0 + BK < ke) fetch(k0 + BK);  // next tile in flight during the math
     if (active) {
-#pragma unroll 8
+#pragma unroll 4
       for (int kk = 0; kk < BK; ++kk) {
-        T ar[kBmTM], ai[kBmTM], xr[kBmTQ], xi[kBmTQ];
-#pragma unroll
-        for (int i = 0; i < kBmTM; ++i) {
-          ar[i] = as_re[rg * kBmTM + i][kk];
-          ai[i] = CPLX ? as_im[rg * kBmTM + i][kk] : T(0);
-        }
-#pragma unroll
-        for (int q = 0; q < kBmTQ; ++q) {
-          xr[q] = xs_re[kk][qg * kBmTQ + q];
-          xi[q] = CPLX ? xs_im[kk][qg * kBmTQ + q] : T(0);
-        }
+        const int prow = (rg * kBmTM) ^ (((kk / VW) & 7) << 2);
+        T ar[4], ai[4], xr[4], xi[4];
+        Quad<T>::ld(&As[0][kk][prow], ar);
+        if (CPLX) Quad<T>::ld(&As[NP - 1][kk][prow], ai);
+        Quad<T>::ld(&Xs[0][kk][qg * kBmTQ], xr);
+        if (CPLX) Quad<T>::ld(&Xs[NP - 1][kk][qg * kBmTQ], xi);
 #pragma unroll
         for (int i = 0; i < kBmTM; ++i)
 #pragma unroll

@@ -727,12 +727,15 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   a->stats.kernel_launches += 2;
   Timed tm{nullptr, nullptr, 1, fp32 ? 1 : 0, b};
   const bool prof = prof_begin(a, tm);
+  const uintptr_t al = fp32 ? ((uintptr_t)a->a32re | (uintptr_t)(C ? (const void*)a->a32im : nullptr))
+                            : ((uintptr_t)a->a64re | (uintptr_t)(C ? (const void*)a->a64im : nullptr));
+  const int vec_ok = (al % 16 == 0) && (a->n % 4 == 0);
   if (fp32)
     k_block_matvec<float, C><<<grid, kBmThreads, 0, a->stream>>>(a->a32re, a->a32im, a->n, xr, xi, b, a->ksplit,
-                                                                a->Wp);
+                                                                a->Wp, vec_ok);
   else
     k_block_matvec<double, C><<<grid, kBmThreads, 0, a->stream>>>(a->a64re, a->a64im, a->n, xr, xi, b, a->ksplit,
-                                                                 a->Wp);
+                                                                 a->Wp, vec_ok);
   if (prof) prof_end(a, tm);
   k_split_reduce<C><<<grid_n((long)b * a->n), 256, 0, a->stream>>>(a->Wp, a->nsplit, b, a->n, wr, wi);
   a->stats.block_matvecs++;

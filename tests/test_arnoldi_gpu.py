@@ -90,7 +90,8 @@ def test_callback_operator_matches_dense():
 
     def mv(w, v, typ, stream):
         # run on the solver's stream so the ordering with its kernels holds
-        with torch.cuda.stream(torch.cuda.ExternalStream(stream)):
+        st = torch.cuda.ExternalStream(stream) if stream else torch.cuda.default_stream()
+        with torch.cuda.stream(st):
             torch.mv(a, ptr_tensor(v.re, 300), out=ptr_tensor(w.re, 300))
         calls.append(typ)
         return 0
