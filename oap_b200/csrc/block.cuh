@@ -68,7 +68,7 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
   constexpr int NV = kBmRows * VPR / kBmThreads;  // vectors per thread per plane (4)
   constexpr int NP = CPLX ? 2 : 1;
   __shared__ __align__(16) T As[NP][BK][kBmRows];
-  __shared__ __align__(16) T Xs[NP][BK][kBmMaxB];
+  __shared__ __align__(16) T Xs[NP][kBmMaxB][BK + 1];
   const int QB = ((b + kBmTQ - 1) / kBmTQ) * kBmTQ;
   const int t = threadIdx.x;
   const int rg = t % (kBmRows / kBmTM), qg = t / (kBmRows / kBmTM);
@@ -124,8 +124,8 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
       const int kk = e % BK, q = e / BK;
       const long c = k0 + kk;
       const bool in = q < b && c < ke;
-      Xs[0][kk][q] = in ? (T)Xre[(long)q * n + c] : T(0);
-      if (CPLX) Xs[NP - 1][kk][q] = in ? (T)Xim[(long)q * n + c] : T(0);
+      Xs[0][q][kk] = in ? (T)Xre[(long)q * n + c] : T(0);
+      if (CPLX) Xs[NP - 1][q][kk] = in ? (T)Xim[(long)q * n + c] : T(0);
     }
     __syncthreads();
     if (k0 + BK < ke) fetch(k0 + BK);  // next tile in flight during the math
@@ -136,8 +136,11 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
         T ar[4], ai[4], xr[4], xi[4];
         Quad<T>::ld(&As[0][kk][prow], ar);
         if (CPLX) Quad<T>::ld(&As[NP - 1][kk][prow], ai);
-        Quad<T>::ld(&Xs[0][kk][qg * kBmTQ], xr);
-        if (CPLX) Quad<T>::ld(&Xs[NP - 1][kk][qg * kBmTQ], xi);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {   // same address across the warp: broadcast
+          xr[q] = Xs[0][qg * kBmTQ + q][kk];
+          if (CPLX) xi[q] = Xs[NP - 1][qg * kBmTQ + q][kk];
+        }
 #pragma unroll
         for (int i = 0; i < kBmTM; ++i)
 #pragma unroll
@@ -186,44 +189,74 @@ __global__ void k_split_reduce(const double* __restrict__ Wp, int nsplit, int b,
 }
 
 constexpr int kDotChunk = 32;
+constexpr int kDotBlocks = 2 * kNumSMs;
 
-// part[blk][i + j * b1] = sum_{r in chunk} conj(X_i[r]) Y_j[r]
+// part[blk][i + j * b1] = sum over the block's row chunks of conj(X_i[r]) Y_j[r]
+// (chunks blk, blk + gridDim.x, ...; every thread owns up to 4 entries)
 template <bool CPLX>
-__global__ void k_block_dot(const double* __restrict__ Xre, const double* __restrict__ Xim, int b1,
-                            const double* __restrict__ Yre, const double* __restrict__ Yim, int b2, int n,
-                            cplx* part) {
-  __shared__ double xr[kBmMaxB][kDotChunk], xi[kBmMaxB][kDotChunk];
-  __shared__ double yr[kBmMaxB][kDotChunk], yi[kBmMaxB][kDotChunk];
-  const long r0 = (long)blockIdx.x * kDotChunk;
-  for (int e = threadIdx.x; e < kBmMaxB * kDotChunk; e += blockDim.x) {
-    const int q = e / kDotChunk, rr = e % kDotChunk;
-    const long r = r0 + rr;
-    const bool in = r < n;
-    xr[q][rr] = (in && q < b1) ? Xre[(long)q * n + r] : 0.0;
-    xi[q][rr] = (in && q < b1 && CPLX) ? Xim[(long)q * n + r] : 0.0;
-    yr[q][rr] = (in && q < b2) ? Yre[(long)q * n + r] : 0.0;
-    yi[q][rr] = (in && q < b2 && CPLX) ? Yim[(long)q * n + r] : 0.0;
-  }
-  __syncthreads();
-  for (int p = threadIdx.x; p < b1 * b2; p += blockDim.x) {
-    const int i = p % b1, j = p / b1;
-    double sr = 0, si = 0;
-    for (int rr = 0; rr < kDotChunk; ++rr) {
-      const double a = xr[i][rr], bb = xi[i][rr], c = yr[j][rr], d = yi[j][rr];
-      sr += a * c + bb * d;
-      si += a * d - bb * c;
+__global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xre, const double* __restrict__ Xim,
+                                                   int b1, const double* __restrict__ Yre,
+                                                   const double* __restrict__ Yim, int b2, int n, cplx* part) {
+  __shared__ double xr[kBmMaxB][kDotChunk + 1], xi[kBmMaxB][kDotChunk + 1];
+  __shared__ double yr[kBmMaxB][kDotChunk + 1], yi[kBmMaxB][kDotChunk + 1];
+  const int cnt = b1 * b2;
+  double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
+  const long nchunks = (n + kDotChunk - 1) / kDotChunk;
+  for (long ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
+    const long r0 = ch * kDotChunk;
+    __syncthreads();
+    for (int e = threadIdx.x; e < kBmMaxB * kDotChunk; e += blockDim.x) {
+      const int q = e / kDotChunk, rr = e % kDotChunk;
+      const long r = r0 + rr;
+      const bool in = r < n;
+      xr[q][rr] = (in && q < b1) ? Xre[(long)q * n + r] : 0.0;
+      xi[q][rr] = (in && q < b1 && CPLX) ? Xim[(long)q * n + r] : 0.0;
+      yr[q][rr] = (in && q < b2) ? Yre[(long)q * n + r] : 0.0;
+      yi[q][rr] = (in && q < b2 && CPLX) ? Yim[(long)q * n + r] : 0.0;
     }
-    part[(long)blockIdx.x * b1 * b2 + p] = cplx{sr, si};
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int p = threadIdx.x + u * 256;
+      if (p < cnt) {
+        const int i = p % b1, j = p / b1;
+        double sr = 0, si = 0;
+#pragma unroll 8
+        for (int rr = 0; rr < kDotChunk; ++rr) {
+          const double a = xr[i][rr], bb = xi[i][rr], c = yr[j][rr], d = yi[j][rr];
+          sr += a * c + bb * d;
+          si += a * d - bb * c;
+        }
+        ar[u] += sr;
+        ai[u] += si;
+      }
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int p = threadIdx.x + u * 256;
+    if (p < cnt) part[(long)blockIdx.x * cnt + p] = cplx{ar[u], ai[u]};
   }
 }
 
-__global__ void k_block_reduce(const cplx* part, int nblk, int cnt, cplx* out) {
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < cnt; p += gridDim.x * blockDim.x) {
-    double a = 0, b = 0;
-    for (int c = 0; c < nblk; ++c) {
+// out[p] = sum_c part[c][p]: 32 entries per block along x, chunks split over y
+__global__ void __launch_bounds__(256) k_block_reduce(const cplx* part, int nblk, int cnt, cplx* out) {
+  __shared__ double sr[8][33], si[8][33];
+  const int p = blockIdx.x * 32 + threadIdx.x;
+  double a = 0, b = 0;
+  if (p < cnt)
+    for (int c = threadIdx.y; c < nblk; c += 8) {
       cplx v = part[(long)c * cnt + p];
       a += v.re;
       b += v.im;
+    }
+  sr[threadIdx.y][threadIdx.x] = a;
+  si[threadIdx.y][threadIdx.x] = b;
+  __syncthreads();
+  if (threadIdx.y == 0 && p < cnt) {
+    for (int y = 1; y < 8; ++y) {
+      a += sr[y][threadIdx.x];
+      b += si[y][threadIdx.x];
     }
     out[p] = cplx{a, b};
   }
@@ -283,37 +316,35 @@ __global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restr
 // One warp: Cholesky G = R^H R of a b x b Hermitian positive definite matrix
 // (column-major), then Rinv = R^-1 (upper triangular).  status bit 2 when a
 // pivot is not positive.
-__global__ void k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
+__global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
   __shared__ cplx R[kBmMaxB * kBmMaxB];
   __shared__ cplx Ri[kBmMaxB * kBmMaxB];
+  __shared__ double rd[kBmMaxB];   // 1 / R[j][j]
   const int lane = threadIdx.x;
   for (int e = lane; e < b * b; e += 32) {
-    R[e] = cplx{0, 0};
+    R[e] = G[e];   // upper triangle is overwritten by R, the rest unused
     Ri[e] = cplx{0, 0};
   }
   __syncwarp();
-  // R[i][j] (i <= j) column-major at i + j b
+  // column j: R[i][j] = (G[i][j] - sum_{p<i} conj(R[p][i]) R[p][j]) / R[i][i]
   for (int j = 0; j < b; ++j) {
-    // R[i][j] = (G[i][j] - sum_{p<i} conj(R[p][i]) R[p][j]) / R[i][i], i < j
     for (int i = 0; i < j; ++i) {
       cplx acc = {0, 0};
       for (int p = lane; p < i; p += 32) acc = acc + conj(R[p + i * b]) * R[p + j * b];
       acc.re = warp_sum(acc.re);
       acc.im = warp_sum(acc.im);
-      if (lane == 0) R[i + j * b] = cdiv(G[i + j * b] - acc, R[i + i * b]);
+      if (lane == 0) R[i + j * b] = rd[i] * (R[i + j * b] - acc);
       __syncwarp();
     }
     double d = 0;
     for (int p = lane; p < j; p += 32) d += abs2(R[p + j * b]);
     d = warp_sum(d);
-    const double piv = G[j + j * b].re - d;
+    const double piv = R[j + j * b].re - d;
     if (lane == 0) {
-      if (!(piv > 0)) {
-        atomicOr(status, 4);
-        R[j + j * b] = cplx{1e-300, 0};
-      } else {
-        R[j + j * b] = cplx{sqrt(piv), 0};
-      }
+      double rjj = piv > 0 ? sqrt(piv) : 1e-300;
+      if (!(piv > 0)) atomicOr(status, 4);
+      R[j + j * b] = cplx{rjj, 0};
+      rd[j] = 1.0 / rjj;
     }
     __syncwarp();
   }
@@ -322,7 +353,7 @@ __global__ void k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
     for (int i = j; i >= 0; --i) {
       cplx acc = (i == j) ? cplx{1, 0} : cplx{0, 0};
       for (int p = i + 1; p <= j; ++p) acc = acc - R[i + p * b] * Ri[p + j * b];
-      Ri[i + j * b] = cdiv(acc, R[i + i * b]);
+      Ri[i + j * b] = rd[i] * acc;
     }
   }
   __syncwarp();

@@ -59,14 +59,23 @@ __host__ __device__ __forceinline__ cplx csqrt_(cplx z) {
 // Unitary rotation G = [p q; -conj(q) conj(p)], p = conj(x)/r, q = conj(y)/r,
 // so G [x; y] = [r; 0] with r = sqrt(|x|^2 + |y|^2) > 0.  For real inputs
 // this is the reference's c = x / r, s = y / r (CuQRProcedures_GR.h:80-101).
-__host__ __device__ __forceinline__ void givens(cplx x, cplx y, cplx& p, cplx& q) {
-  double r = hypot(cabs_(x), cabs_(y));
-  if (r == 0) {
+__device__ __forceinline__ void givens(cplx x, cplx y, cplx& p, cplx& q) {
+  double r2 = x.re * x.re + x.im * x.im + y.re * y.re + y.im * y.im;
+  if (r2 == 0) {
     p = {1, 0};
     q = {0, 0};
     return;
   }
-  double ir = 1.0 / r;
+  double s = 1.0;
+  if (!(r2 < 1e300) || r2 < 1e-290) {
+    // rescale by the largest component so the sum of squares stays finite
+    s = fmax(fmax(fabs(x.re), fabs(x.im)), fmax(fabs(y.re), fabs(y.im)));
+    const double is = 1.0 / s;
+    x = is * x;
+    y = is * y;
+    r2 = x.re * x.re + x.im * x.im + y.re * y.re + y.im * y.im;
+  }
+  const double ir = rsqrt(r2);  // 1 / r of the (rescaled) pair
   p = {x.re * ir, -x.im * ir};
   q = {y.re * ir, -y.im * ir};
 }

@@ -112,11 +112,14 @@ __device__ void warp_sweep(cplx* T, cplx* Z, int m, int l, int h, cplx mu, int l
   }
 }
 
+// |re| + |im| (LAPACK's CABS1): the deflation test only needs a norm-equivalent
+__device__ __forceinline__ double cabs1(cplx a) { return fabs(a.re) + fabs(a.im); }
+
 __device__ __forceinline__ bool negligible(const cplx* T, int m, int l) {
   const double eps = 2.220446049250313e-16;
-  double s = cabs_(TT_(l - 1, l - 1)) + cabs_(TT_(l, l));
+  double s = cabs1(TT_(l - 1, l - 1)) + cabs1(TT_(l, l));
   if (s == 0) s = 1e-300;
-  return cabs_(TT_(l, l - 1)) <= eps * s;
+  return cabs1(TT_(l, l - 1)) <= eps * s;
 }
 
 // Householder reduction of dense T to Hessenberg form, Z accumulating.

@@ -670,6 +670,7 @@ int alloc_blocks(oapb_arnoldi* a) {
     if (a->is_c) rc |= dalloc(&a->Bim[i], vb);
   }
   a->ndot = (a->n + kDotChunk - 1) / kDotChunk;
+  if (a->ndot > kDotBlocks) a->ndot = kDotBlocks;
   {
     const long tiles = (a->n + kBmRows - 1) / kBmRows;
     long sp = (6L * kNumSMs + tiles - 1) / tiles;
