@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
 // out[p] = sum_c part[c][p]: 32 entries per block along x, chunks split over y
 __global__ void __launch_bounds__(256) k_block_reduce(const cplx* part, int nblk, int cnt, cplx* out) {
   __shared__ double sr[8][33], si[8][33];
+  if (blockDim.x != 32 || blockDim.y != 8) return;  // the layout below assumes 32 x 8
   const int p = blockIdx.x * 32 + threadIdx.x;
   double a = 0, b = 0;
   if (p < cnt)

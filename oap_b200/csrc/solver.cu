@@ -704,11 +704,9 @@ int alloc_blocks(oapb_arnoldi* a) {
 template <bool C>
 void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, const double* yr, const double* yi,
                 int b2, cplx* G) {
-  ++a->stats.kernel_launches;
   a->stats.kernel_launches += 2;
   k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(xr, xi, b1, yr, yi, b2, a->n, a->bpart);
-  ++a->stats.kernel_launches;
-  k_block_reduce<<<grid_for(b1 * b2, 128, 8), 128, 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G);
+  k_block_reduce<<<(b1 * b2 + 31) / 32, dim3(32, 8), 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G);
 }
 
 // W = A X (b vectors); FP32 operator copy when fp32, else FP64
