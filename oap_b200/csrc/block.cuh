@@ -79,7 +79,20 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
   const T* planes[2] = {Are, Aim};
   const bool full_rows = r0 + kBmRows <= n;
 
+  constexpr int NX = (BK * kBmMaxB + kBmThreads - 1) / kBmThreads;  // X values per thread per plane
   V pre[NP][NV];
+  T xpre[NP][NX];
+  auto fetch_x = [&](long k0) {
+#pragma unroll
+    for (int u = 0; u < NX; ++u) {
+      const int e = t + u * kBmThreads;
+      const int kk = e % BK, q = e / BK;
+      const long c = k0 + kk;
+      const bool in = q < b && c < ke;
+      xpre[0][u] = in ? (T)Xre[(long)q * n + c] : T(0);
+      if (CPLX) xpre[NP - 1][u] = in ? (T)Xim[(long)q * n + c] : T(0);
+    }
+  };
   auto fetch = [&](long k0) {
 #pragma unroll
     for (int p = 0; p < NP; ++p)
@@ -105,7 +118,10 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
 #pragma unroll
     for (int q = 0; q < kBmTQ; ++q) accr[i][q] = acci[i][q] = 0;
 
-  if (kb < ke) fetch(kb);
+  if (kb < ke) {
+    fetch(kb);
+    fetch_x(kb);
+  }
   for (long k0 = kb; k0 < ke; k0 += BK) {
     __syncthreads();
     // registers -> shared (transposed, swizzled)
@@ -120,15 +136,20 @@ k_block_matvec(const T* __restrict__ Are, const T* __restrict__ Aim, int n, cons
 #pragma unroll
         for (int e = 0; e < VW; ++e) As[p][kq * VW + e][prow] = v[e];
       }
-    for (int e = t; e < BK * QB; e += kBmThreads) {
+#pragma unroll
+    for (int u = 0; u < NX; ++u) {
+      const int e = t + u * kBmThreads;
       const int kk = e % BK, q = e / BK;
-      const long c = k0 + kk;
-      const bool in = q < b && c < ke;
-      Xs[0][q][kk] = in ? (T)Xre[(long)q * n + c] : T(0);
-      if (CPLX) Xs[NP - 1][q][kk] = in ? (T)Xim[(long)q * n + c] : T(0);
+      if (q < kBmMaxB) {
+        Xs[0][q][kk] = xpre[0][u];
+        if (CPLX) Xs[NP - 1][q][kk] = xpre[NP - 1][u];
+      }
     }
     __syncthreads();
-    if (k0 + BK < ke) fetch(k0 + BK);  // next tile in flight during the math
+    if (k0 + BK < ke) {  // next tiles in flight during the math
+      fetch(k0 + BK);
+      fetch_x(k0 + BK);
+    }
     if (active) {
 #pragma unroll 4
       for (int kk = 0; kk < BK; ++kk) {

@@ -831,8 +831,17 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei))) return rc;
   std::vector<double> norms(kk), hist;
   std::vector<cplx> th(b);
+  // In the FP32 phase the first Rayleigh-Ritz checks carry no decision:
+  // from a random block the wanted directions need several powers before
+  // the residuals mean anything, so check from iteration 5 on, every
+  // second iteration.
   for (unsigned it = 0; it < max_it; ++it) {
     if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
+    const bool check = !fp32 || from_bx || (it >= 5 && (it % 2 == 1)) || it + 1 == max_it;
+    if (!check) {
+      if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
+      continue;
+    }
     block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
     a->stats.kernel_launches += 5;
     k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
