@@ -263,6 +263,47 @@ OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_
  * 642-649), recomputed in FP64 on the device. */
 OAPB_EXPORT int oapb_arnoldi_test_outcome(oapb_arnoldi* handle, uint32_t index, double* out);
 
+/* ------------------------------------------------------------------------ */
+/* Batched solver: many independent small problems in one persistent launch */
+/* ------------------------------------------------------------------------ */
+
+/* One problem of a batch (device planes in the reference layout). */
+typedef struct oapb_batch_problem {
+  uint32_t n;            /* 2 <= n <= 2048, n > wanted */
+  const double* re;      /* device, n x n */
+  const double* im;      /* device, or NULL for a real problem */
+  double* eigvec_re;     /* device, n x wanted (column q = eigenvector q), or NULL */
+  double* eigvec_im;     /* device, or NULL */
+} oapb_batch_problem;
+
+typedef struct oapb_batch_stats {
+  uint32_t problems;
+  uint32_t converged;
+  uint64_t matvecs;      /* over all problems, including the residual checks */
+  uint64_t restarts;
+  uint32_t ctas;         /* resident CTAs of the persistent launch */
+  double seconds;        /* host wall time of the call */
+} oapb_batch_stats;
+
+/* Solve `count` independent eigenproblems (IEigenCalculator::calculate,
+ * oap2dt3dDevice/IEigenCalculator.cpp:56-70, called once per problem in the
+ * reference) with one persistent kernel: each CTA takes the next problem
+ * from a queue ordered by decreasing n and runs the full restart loop on the
+ * device.  cfg: hdim caps the Krylov dimension (m_i = min(n_i, hdim),
+ * hdim <= 32), wanted, sort, tolerance, max_restarts, rho, seed; n,
+ * is_complex, precision and init are ignored (complex iff im != NULL,
+ * FP64, seeded random start).  `problems` is a HOST array.  Host outputs:
+ * eig_re / eig_im / residuals (count x wanted, row i = problem i in sort
+ * order), status (count, oapb_status per problem).  Synchronises `stream`.
+ * Returns OAPB_OK when every problem converged, OAPB_NOT_CONVERGED when some
+ * did not (see status), or an error. */
+OAPB_EXPORT int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg,
+                                           const oapb_batch_problem* problems,
+                                           uint32_t count, double* eig_re,
+                                           double* eig_im, double* residuals,
+                                           int32_t* status,
+                                           oapb_batch_stats* stats, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

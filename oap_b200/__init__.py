@@ -54,6 +54,17 @@ class Stats(C.Structure):
                 ("block_fp32_width", C.c_uint32)]
 
 
+class BatchProblem(C.Structure):
+    _fields_ = [("n", C.c_uint32), ("re", C.c_void_p), ("im", C.c_void_p),
+                ("eigvec_re", C.c_void_p), ("eigvec_im", C.c_void_p)]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("problems", C.c_uint32), ("converged", C.c_uint32),
+                ("matvecs", C.c_uint64), ("restarts", C.c_uint64),
+                ("ctas", C.c_uint32), ("seconds", C.c_double)]
+
+
 MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,
                         C.c_int, C.c_void_p)
 
@@ -101,6 +112,9 @@ def lib():
                                         P(C.c_double), vp, vp],
             "oapb_arnoldi_get_stats": [vp, P(Stats)],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
+            "oapb_arnoldi_solve_batched": [P(Config), P(BatchProblem), C.c_uint32,
+                                           P(C.c_double), P(C.c_double), P(C.c_double),
+                                           P(C.c_int32), P(BatchStats), vp],
         }.items():
             fn = getattr(L, name)
             fn.argtypes = args
@@ -269,3 +283,39 @@ def start_vector(n, seed, is_complex=False):
     s2 = seed ^ 0x5851F42D4C957F2D
     im = np.array([uni(s2, i) for i in range(n)])
     return re + 1j * im
+
+
+def solve_batched(mats, wanted, hdim=24, sort="LM", tolerance=1e-10, max_restarts=300,
+                  rho=1.0 / 3.14, seed=1, vectors=None, stream=None):
+    """Batched solve of independent problems.  mats: list of (re, im) device
+    tensors (im None for real problems); vectors: optional list of (vre, vim)
+    device tensors of shape (n, wanted).  Returns (eigenvalues [count x
+    wanted] complex, residuals, status per problem, stats dict, rc)."""
+    import numpy as np
+    L = lib()
+    cfg = Config()
+    L.oapb_arnoldi_config_default(C.byref(cfg))
+    cfg.hdim, cfg.wanted = hdim, wanted
+    cfg.sort = SORT[sort] if isinstance(sort, str) else int(sort)
+    cfg.tolerance, cfg.max_restarts, cfg.rho, cfg.seed = tolerance, max_restarts, rho, seed
+    cnt = len(mats)
+    probs = (BatchProblem * cnt)()
+    for i, (re, im) in enumerate(mats):
+        probs[i].n = re.shape[0]
+        probs[i].re = re.data_ptr()
+        probs[i].im = im.data_ptr() if im is not None else None
+        if vectors is not None:
+            vr, vi = vectors[i]
+            probs[i].eigvec_re = vr.data_ptr()
+            probs[i].eigvec_im = vi.data_ptr() if vi is not None else None
+    er = np.zeros((cnt, wanted))
+    ei = np.zeros((cnt, wanted))
+    rs = np.zeros((cnt, wanted))
+    st = np.zeros(cnt, dtype=np.int32)
+    stats = BatchStats()
+    P = lambda a, t=C.c_double: a.ctypes.data_as(C.POINTER(t))
+    rc = L.oapb_arnoldi_solve_batched(C.byref(cfg), probs, cnt, P(er), P(ei), P(rs),
+                                      P(st, C.c_int32), C.byref(stats), _stream(stream))
+    if rc not in (OK, NOT_CONVERGED):
+        raise OapbError(rc, "oapb_arnoldi_solve_batched")
+    return (er + 1j * ei, rs, st, {f: getattr(stats, f) for f, _ in BatchStats._fields_}, rc)

@@ -74,7 +74,7 @@ __device__ __forceinline__ double sort_key(cplx v, int which) {
 
 // One single-shift QR sweep on the active window [l, h] of Hessenberg T,
 // applied to whole rows / columns; Z <- Z G^H for every rotation.
-__device__ void warp_sweep(cplx* T, cplx* Z, int m, int l, int h, cplx mu, int lane) {
+static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int l, int h, cplx mu, int lane) {
   for (int k = l; k < h; ++k) {
     cplx x, y;
     if (k == l) {
@@ -123,7 +123,7 @@ __device__ __forceinline__ bool negligible(const cplx* T, int m, int l) {
 }
 
 // Householder reduction of dense T to Hessenberg form, Z accumulating.
-__device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lane) {
+static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lane) {
   for (int k = 0; k + 2 < m; ++k) {
     double s = 0;
     for (int i = k + 1 + lane; i < m; i += 32) s += abs2(TT_(i, k));
@@ -170,7 +170,7 @@ __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lane) {
 }
 
 // Complex Schur form in place; returns false when the sweep budget ran out.
-__device__ bool warp_schur(cplx* T, cplx* Z, int m, int lane) {
+static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int lane) {
   int h = m - 1, its = 0, total = 0;
   while (h > 0) {
     int l = h;
@@ -202,16 +202,13 @@ __device__ bool warp_schur(cplx* T, cplx* Z, int m, int lane) {
   return true;
 }
 
-__global__ void __launch_bounds__(32) k_hess(HessArgs a) {
-  extern __shared__ cplx sws[];
-  __shared__ cplx u[kMaxM];
-  __shared__ double key[kMaxM];
-  __shared__ int ord[kMaxM];
-  const int lane = threadIdx.x;
+// The body of k_hess for one warp (lane = 0..31 of the calling warp), with
+// its workspaces passed in: T, Z (m x m each), u (m), key (m), ord (m).
+// Callable from any kernel by one full warp; the outputs in `a` may point
+// to shared or global memory.
+static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, double* key, int* ord, int lane) {
   const int m = a.m, k = a.k;
   const long mm = (long)m * m;
-  cplx* T = a.gws ? a.gws : sws;
-  cplx* Z = T + mm;
   DevState* st = a.st;
 
   for (long i = lane; i < mm; i += 32) {
@@ -336,6 +333,15 @@ __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
     a.Hout[i] = (r < k && c < k) ? T[i] : cplx{0, 0};
     a.Qout[i] = Z[i];
   }
+}
+
+static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
+  extern __shared__ cplx sws[];
+  __shared__ cplx u[kMaxM];
+  __shared__ double key[kMaxM];
+  __shared__ int ord[kMaxM];
+  cplx* T = a.gws ? a.gws : sws;
+  hess_core(a, T, T + (long)a.m * a.m, u, key, ord, threadIdx.x);
 }
 
 #undef TT_
