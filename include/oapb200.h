@@ -264,6 +264,19 @@ OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_
 OAPB_EXPORT int oapb_arnoldi_test_outcome(oapb_arnoldi* handle, uint32_t index, double* out);
 
 /* ------------------------------------------------------------------------ */
+/* Gram operator build                                                      */
+/* ------------------------------------------------------------------------ */
+
+/* A = X X^T for X (rows x cols, FP32, row-major: rows = samples, cols =
+ * pixels), replacing SquareMatrixApi::getDeviceMatrix's dotProduct(out, X,
+ * X^T) (oapMatrixCuda/SquareMatrixApi.cpp:143-156, RecToSquareApi.cpp:57-69).
+ * Split-BF16 on the tensor cores (tcgen05): x = hi + lo, A = hi hi^T +
+ * hi lo^T + lo hi^T accumulated in FP32.  A: device rows x rows FP32; A64:
+ * optional device FP64 copy (NULL to skip).  Synchronises `stream`. */
+OAPB_EXPORT int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols,
+                                float* A, double* A64, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Batched solver: many independent small problems in one persistent launch */
 /* ------------------------------------------------------------------------ */
 

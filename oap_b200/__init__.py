@@ -112,6 +112,7 @@ def lib():
                                         P(C.c_double), vp, vp],
             "oapb_arnoldi_get_stats": [vp, P(Stats)],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
+            "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_solve_batched": [P(Config), P(BatchProblem), C.c_uint32,
                                            P(C.c_double), P(C.c_double), P(C.c_double),
                                            P(C.c_int32), P(BatchStats), vp],
@@ -319,3 +320,17 @@ def solve_batched(mats, wanted, hdim=24, sort="LM", tolerance=1e-10, max_restart
     if rc not in (OK, NOT_CONVERGED):
         raise OapbError(rc, "oapb_arnoldi_solve_batched")
     return (er + 1j * ei, rs, st, {f: getattr(stats, f) for f, _ in BatchStats._fields_}, rc)
+
+
+def gram_build(X, fp64=False, stream=None):
+    """A = X X^T (split-BF16 tensor-core GEMM) for a row-major FP32 CUDA
+    tensor X (rows x cols).  Returns (A float32, A64 float64 or None)."""
+    import torch
+    assert X.is_cuda and X.dtype == torch.float32 and X.is_contiguous()
+    rows, cols = X.shape
+    A = torch.empty((rows, rows), dtype=torch.float32, device=X.device)
+    A64 = torch.empty((rows, rows), dtype=torch.float64, device=X.device) if fp64 else None
+    check(lib().oapb_gram_build(C.c_void_p(X.data_ptr()), rows, cols, C.c_void_p(A.data_ptr()),
+                                C.c_void_p(A64.data_ptr()) if fp64 else None, _stream(stream)),
+          "oapb_gram_build")
+    return A, A64
