@@ -122,6 +122,16 @@ OAPB_EXPORT int oapb_set_zero_matrix(const oapb_mat* matrix, void* stream);
 OAPB_EXPORT int oapb_qr_givens(const oapb_mat* Q, const oapb_mat* R, const oapb_mat* A,
                    void* stream);
 
+/* Givens QR that allocates no device memory.  No counterpart in the
+ * reference: it exists for callers that cannot allocate (a stream capture
+ * that forbids allocations, allocator hooks, fixed memory budgets).  Same
+ * results as oapb_qr_givens; the workspace is a static 512 KiB device array
+ * of the library, so n <= 128 (OAPB_ERR_ARG beyond).  The first call on a
+ * device resolves the array's address and should precede any stream
+ * capture; calls that overlap on the GPU share the array and race. */
+OAPB_EXPORT int oapb_qr_givens_noalloc(const oapb_mat* Q, const oapb_mat* R,
+                                       const oapb_mat* A, void* stream);
+
 /* Householder QR of a real square matrix (CuProceduresApi.h:306,
  * CuQRProcedures_HT.h:63-131). */
 OAPB_EXPORT int oapb_qr_householder(const oapb_mat* Q, const oapb_mat* R, const oapb_mat* A,

@@ -100,6 +100,7 @@ def lib():
             "oapb_set_zero_matrix": [P(Mat), vp],
             "oapb_qr_givens": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_qr_householder": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_qr_givens_noalloc": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_is_upper_triangular": [P(C.c_int), P(Mat), C.c_double, vp],
             "oapb_calc_triangular_h": [P(Mat), P(Mat), C.c_uint32, P(C.c_uint32), vp],
             "oapb_arnoldi_create": [P(vp), P(Config), vp],
