@@ -810,6 +810,7 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
 }
 
 constexpr int kSlow = 100;   // subspace(): convergence too slow for the iteration budget
+constexpr int kMixedMinN = 8192;
 
 // Block subspace iteration with Rayleigh-Ritz on b vectors:
 //   W = A X; G = X^H W; R = W - X G; G = S diag(theta) S^-1;
@@ -1004,8 +1005,12 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
 template <bool C>
 int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
   const int k = a->k;
-  // the mixed form needs the dense operator and the block kernels (k <= 32)
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB && a->a32re;
+  // The mixed form needs the dense operator and the block kernels (k <= 32),
+  // and pays off only when the operator pass is HBM-bound: below n = 8192
+  // (at most 1 GiB of complex FP64 operator) a pass is a few tens of
+  // microseconds and the single-vector FP64 restart loop is faster.
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB && a->a32re &&
+                     a->n >= kMixedMinN;
   a->stats.restarts = 0;
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
