@@ -199,6 +199,9 @@ typedef struct oapb_arnoldi_config {
   uint64_t seed;           /* start-vector seed for OAPB_INIT_RANDOM */
   int32_t profile;         /* 1: time every dense matvec with CUDA events
                               (oapb_arnoldi_stats.matvec_seconds) */
+  int32_t fallback_random; /* 1: when a solve from a user start vector does
+                              not reach the goal within max_restarts, solve
+                              again from the seeded random start */
 } oapb_arnoldi_config;
 
 /* Fill defaults: rho = 1/3.14, tolerance = 1e-10, LM, FP64, random start,
@@ -223,6 +226,7 @@ typedef struct oapb_arnoldi_stats {
   uint32_t block_fp32_timed; /* FP32 block matvecs timed (profile) */
   double block_fp32_seconds;
   uint32_t block_fp32_width; /* right-hand sides of the FP32 block matvec */
+  uint32_t fallbacks;        /* solves restarted from the random start */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */
@@ -249,6 +253,15 @@ OAPB_EXPORT int oapb_arnoldi_set_callback(oapb_arnoldi* handle, oapb_matvec_fn f
 /* Start vector (device planes, n values each; im ignored for real solves). */
 OAPB_EXPORT int oapb_arnoldi_set_start_vector(oapb_arnoldi* handle, const double* re,
                                   const double* im);
+
+/* Shift filter for the user start vector: before the first Arnoldi step
+ * the start vector becomes prod_i (A - shifts[i] I) v0 (host array, up to
+ * 64 shifts; count 0 clears).  With shifts near the unwanted eigenvalues
+ * closest to the wanted set this damps exactly the directions a restart
+ * would damp (the learned shift set of a warm start). */
+OAPB_EXPORT int oapb_arnoldi_set_start_shifts(oapb_arnoldi* handle,
+                                              const double* shifts,
+                                              uint32_t count);
 
 /* Solve (CuHArnoldi::execute, ArnoldiProcedures.cpp:129-140).
  * Host outputs (each may be NULL): eigenvalues re / im (wanted values in
@@ -326,6 +339,40 @@ OAPB_EXPORT int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg,
                                            double* eig_im, double* residuals,
                                            int32_t* status,
                                            oapb_batch_stats* stats, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Learned warm start: parametric operators and the BF16 network            */
+/* ------------------------------------------------------------------------ */
+
+/* out[p] = A0 + sum_i theta[p * nparams + i] B[i] for p < count (all device
+ * FP64, n x n; B is a HOST array of nparams device pointers, nparams <= 32). */
+OAPB_EXPORT int oapb_param_operators(const double* A0, const double* const* B,
+                                     uint32_t nparams, const double* theta,
+                                     uint32_t count, uint32_t n, double* out,
+                                     void* stream);
+
+/* Dense network sizes[0] -> ... -> sizes[nlayers], tanh hidden layers, linear
+ * output; BF16 weights / activations, FP32 accumulation, FP32 master weights
+ * with Adam.  Nearest reference analogue: oapNeuralDevice/oapNetwork.h:27-124
+ * and the generic propagation of oapNeuralHost/oapGenericNeuralApi.h:195-360. */
+typedef struct oapb_mlp oapb_mlp;
+OAPB_EXPORT int oapb_mlp_create(oapb_mlp** handle, const uint32_t* sizes,
+                                uint32_t nlayers, uint64_t seed);
+OAPB_EXPORT int oapb_mlp_destroy(oapb_mlp* handle);
+OAPB_EXPORT uint64_t oapb_mlp_num_params(const oapb_mlp* handle);
+/* y (device FP32, batch x out) = net(x) (device FP32, batch x in) */
+OAPB_EXPORT int oapb_mlp_forward(oapb_mlp* handle, const float* x, uint32_t batch,
+                                 float* y, void* stream);
+/* Forward + backward of 1/(2 batch) sum (y - target)^2; gradients stay in
+ * the handle (packing: all weight matrices [out x in] in layer order, then
+ * all biases); *loss (host, may be NULL) receives the loss. */
+OAPB_EXPORT int oapb_mlp_backward(oapb_mlp* handle, const float* x,
+                                  const float* target, uint32_t batch,
+                                  double* loss, void* stream);
+OAPB_EXPORT int oapb_mlp_adam_step(oapb_mlp* handle, float lr, void* stream);
+/* which 0: parameters, 1: gradients -> dst (host or device FP32) */
+OAPB_EXPORT int oapb_mlp_copy(oapb_mlp* handle, int which, float* dst, void* stream);
+OAPB_EXPORT int oapb_mlp_set_params(oapb_mlp* handle, const float* src, void* stream);
 
 #ifdef __cplusplus
 }

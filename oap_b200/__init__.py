@@ -39,7 +39,8 @@ class Config(C.Structure):
                 ("is_complex", C.c_int32), ("sort", C.c_int32),
                 ("precision", C.c_int32), ("init", C.c_int32),
                 ("max_restarts", C.c_uint32), ("tolerance", C.c_double),
-                ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32)]
+                ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32),
+                ("fallback_random", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -51,7 +52,7 @@ class Stats(C.Structure):
                 ("matvec_fp32", C.c_uint32), ("kernel_launches", C.c_uint64),
                 ("block_seconds", C.c_double), ("block_timed", C.c_uint32),
                 ("block_fp32_timed", C.c_uint32), ("block_fp32_seconds", C.c_double),
-                ("block_fp32_width", C.c_uint32)]
+                ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32)]
 
 
 class BatchProblem(C.Structure):
@@ -114,6 +115,15 @@ def lib():
             "oapb_arnoldi_get_stats": [vp, P(Stats)],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
+            "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
+            "oapb_param_operators": [vp, P(vp), C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp],
+            "oapb_mlp_create": [P(vp), P(C.c_uint32), C.c_uint32, C.c_uint64],
+            "oapb_mlp_destroy": [vp],
+            "oapb_mlp_forward": [vp, vp, C.c_uint32, vp, vp],
+            "oapb_mlp_backward": [vp, vp, vp, C.c_uint32, P(C.c_double), vp],
+            "oapb_mlp_adam_step": [vp, C.c_float, vp],
+            "oapb_mlp_copy": [vp, C.c_int, vp, vp],
+            "oapb_mlp_set_params": [vp, vp, vp],
             "oapb_arnoldi_solve_batched": [P(Config), P(BatchProblem), C.c_uint32,
                                            P(C.c_double), P(C.c_double), P(C.c_double),
                                            P(C.c_int32), P(BatchStats), vp],
@@ -121,6 +131,8 @@ def lib():
             fn = getattr(L, name)
             fn.argtypes = args
             fn.restype = C.c_int
+        L.oapb_mlp_num_params.argtypes = [vp]
+        L.oapb_mlp_num_params.restype = C.c_uint64
         L.oapb_arnoldi_config_default.argtypes = [P(Config)]
         L.oapb_arnoldi_config_default.restype = None
         _LIB = L
@@ -172,7 +184,7 @@ class Arnoldi:
     def __init__(self, n, hdim, wanted, is_complex=False, sort="LM",
                  precision=PREC_FP64, tolerance=1e-10, max_restarts=300,
                  rho=1.0 / 3.14, seed=1, init=INIT_RANDOM, stream=None,
-                 profile=False):
+                 profile=False, fallback_random=False):
         L = lib()
         cfg = Config()
         L.oapb_arnoldi_config_default(C.byref(cfg))
@@ -182,6 +194,7 @@ class Arnoldi:
         cfg.precision, cfg.init = precision, init
         cfg.max_restarts, cfg.tolerance, cfg.rho, cfg.seed = max_restarts, tolerance, rho, seed
         cfg.profile = int(bool(profile))
+        cfg.fallback_random = int(bool(fallback_random))
         self.cfg = cfg
         self.h = C.c_void_p()
         check(L.oapb_arnoldi_create(C.byref(self.h), C.byref(cfg), _stream(stream)),
@@ -216,6 +229,11 @@ class Arnoldi:
         self._cb = MATVEC_FN(tramp)
         check(lib().oapb_arnoldi_set_callback(self.h, self._cb, None),
               "oapb_arnoldi_set_callback")
+
+    def set_start_shifts(self, shifts):
+        arr = (C.c_double * max(1, len(shifts)))(*[float(x) for x in shifts])
+        check(lib().oapb_arnoldi_set_start_shifts(self.h, arr, len(shifts)),
+              "oapb_arnoldi_set_start_shifts")
 
     def set_start_vector(self, re, im=None):
         check(lib().oapb_arnoldi_set_start_vector(

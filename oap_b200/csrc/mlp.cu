@@ -1,0 +1,407 @@
+// Warm-start network and parametric operators.
+//
+// 1. oapb_param_operators: A(theta_p) = A0 + sum_i theta_p[i] B_i for a batch
+//    of parameter vectors (each basis element read once, written P times).
+// 2. A dense MLP (tanh hidden layers, linear output) with BF16 weights and
+//    activations and FP32 accumulation: forward, backward (data and weight
+//    gradients) and an Adam step on FP32 master weights, all on the device.
+//    The network maps an operator's parameters theta to a warm-start vector
+//    and a shift set for the Arnoldi method.  Nearest reference analogue:
+//    the generic forward / back-propagation of the neural library
+//    (oapNeuralHost/oapGenericNeuralApi.h:195-360) over CuProceduresApi ops
+//    (dotProduct, tensorProduct, sum).
+//
+// Every layer product is one kernel: C[M x N] = sum_k A(m, k) B(n, k) with
+// strided BF16 operands (the forward product, the data gradient and the
+// weight gradient differ only in strides), 32 x 32 output tiles, FP32
+// accumulation, optional bias + tanh epilogue and a BF16 copy of the output.
+#include <cuda_bf16.h>
+#include <math.h>
+
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+
+namespace oapb {
+
+// ------------------------------------------------------ parametric operator
+__global__ void k_param_operators(const double* __restrict__ A0, const double* const* __restrict__ Bs, int nparams,
+                                  const double* __restrict__ theta, int P, long nn, double* __restrict__ out) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < nn; e += (long)gridDim.x * blockDim.x) {
+    double base = A0[e];
+    double b[32];
+    for (int i = 0; i < nparams; ++i) b[i] = Bs[i][e];
+    for (int p = 0; p < P; ++p) {
+      double v = base;
+      for (int i = 0; i < nparams; ++i) v += theta[(long)p * nparams + i] * b[i];
+      out[(long)p * nn + e] = v;
+    }
+  }
+}
+
+// ------------------------------------------------------------ layer GEMM --
+constexpr int kLT = 32;  // output tile
+constexpr int kLK = 16;  // k chunk
+
+// C[m][n] (ldc) = sum_k A[m*sam + k*sak] * B[n*sbn + k*sbk]   (+ bias[n], tanh)
+template <bool BIAS_TANH>
+__global__ void __launch_bounds__(256) k_layer_gemm(const __nv_bfloat16* __restrict__ A, long sam, long sak,
+                                                    const __nv_bfloat16* __restrict__ Bm, long sbn, long sbk, int M,
+                                                    int N, int K, const float* __restrict__ bias, float* C,
+                                                    __nv_bfloat16* Cb, int ldc) {
+  __shared__ float As[kLK][kLT + 1];
+  __shared__ float Bsm[kLK][kLT + 1];
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // 16 x 16 threads, 2 x 2 outputs each
+  const int m0 = blockIdx.y * kLT, n0 = blockIdx.x * kLT;
+  float acc[2][2] = {{0, 0}, {0, 0}};
+  for (int k0 = 0; k0 < K; k0 += kLK) {
+    for (int e = threadIdx.x; e < kLK * kLT; e += 256) {
+      const int kk = e / kLT, j = e % kLT;
+      const int m = m0 + j, n = n0 + j, k = k0 + kk;
+      As[kk][j] = (m < M && k < K) ? __bfloat162float(A[m * sam + k * sak]) : 0.f;
+      Bsm[kk][j] = (n < N && k < K) ? __bfloat162float(Bm[n * sbn + k * sbk]) : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < kLK; ++kk) {
+      const float a0 = As[kk][ty * 2], a1 = As[kk][ty * 2 + 1];
+      const float b0 = Bsm[kk][tx * 2], b1 = Bsm[kk][tx * 2 + 1];
+      acc[0][0] = fmaf(a0, b0, acc[0][0]);
+      acc[0][1] = fmaf(a0, b1, acc[0][1]);
+      acc[1][0] = fmaf(a1, b0, acc[1][0]);
+      acc[1][1] = fmaf(a1, b1, acc[1][1]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const int m = m0 + ty * 2 + i, n = n0 + tx * 2 + j;
+      if (m < M && n < N) {
+        float v = acc[i][j];
+        if (BIAS_TANH) v = tanhf(v + bias[n]);
+        if (C) C[(long)m * ldc + n] = v;
+        if (Cb) Cb[(long)m * ldc + n] = __float2bfloat16_rn(v);
+      }
+    }
+}
+
+// y = out + bias (output layer without activation), in place, + BF16 copy
+__global__ void k_add_bias(float* Y, const float* bias, int B, int N, __nv_bfloat16* Yb) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < (long)B * N; e += (long)gridDim.x * blockDim.x) {
+    const float v = Y[e] + bias[e % N];
+    Y[e] = v;
+    if (Yb) Yb[e] = __float2bfloat16_rn(v);
+  }
+}
+
+// dY = (Y - T) / B (BF16 for the backward products); loss partial sums
+__global__ void k_mse_grad(const float* Y, const float* T, int B, long len, __nv_bfloat16* dYb, float* dYf,
+                           double* loss) {
+  double s = 0;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    const float d = Y[e] - T[e];
+    s += (double)d * d;
+    const float g = d / (float)B;
+    dYb[e] = __float2bfloat16_rn(g);
+    if (dYf) dYf[e] = g;
+  }
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) atomicAdd(loss, 0.5 * s / B);
+}
+
+// dZ = dH * (1 - h^2)  (tanh), BF16 out
+__global__ void k_tanh_grad(const float* dH, const float* H, long len, __nv_bfloat16* dZb, float* dZf) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    const float h = H[e];
+    const float g = dH[e] * (1.f - h * h);
+    dZb[e] = __float2bfloat16_rn(g);
+    if (dZf) dZf[e] = g;
+  }
+}
+
+// db[n] = sum_b dZ[b][n]
+__global__ void k_bias_grad(const float* dZ, int B, int N, float* db) {
+  for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+    float s = 0;
+    for (int b = 0; b < B; ++b) s += dZ[(long)b * N + n];
+    db[n] = s;
+  }
+}
+
+// Adam on FP32 masters; BF16 working copy refreshed
+__global__ void k_adam(float* w, const float* g, float* m1, float* m2, long len, float lr, float b1, float b2,
+                       float eps, float c1, float c2, __nv_bfloat16* wb) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    const float gg = g[e];
+    const float a = b1 * m1[e] + (1.f - b1) * gg;
+    const float v = b2 * m2[e] + (1.f - b2) * gg * gg;
+    m1[e] = a;
+    m2[e] = v;
+    const float nw = w[e] - lr * (a / c1) / (sqrtf(v / c2) + eps);
+    w[e] = nw;
+    if (wb) wb[e] = __float2bfloat16_rn(nw);
+  }
+}
+
+__global__ void k_to_bf16(const float* x, long len, __nv_bfloat16* y) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x)
+    y[e] = __float2bfloat16_rn(x[e]);
+}
+
+__global__ void k_init_uniform(float* w, long len, float scale, uint64_t seed) {
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x)
+    w[e] = (float)(scale * uniform_pm1(seed, (uint64_t)e));
+}
+
+}  // namespace oapb
+
+using namespace oapb;
+
+struct oapb_mlp {
+  int nl = 0;                 // layers
+  std::vector<int> sz;        // nl + 1 sizes
+  std::vector<long> woff, boff;
+  long nparam = 0;
+  float *w = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;  // FP32 [all weights | all biases]
+  __nv_bfloat16* wb = nullptr;                                     // BF16 copy of the weights
+  int step = 0;
+  // activations for the last forward (capacity batch)
+  int cap = 0;
+  std::vector<float*> hf;              // FP32 activations per layer output (nl)
+  std::vector<__nv_bfloat16*> hb;      // BF16 activations: input + per layer
+  float *dA = nullptr, *dB2 = nullptr; // FP32 gradient scratch (cap x max size)
+  __nv_bfloat16 *dAb = nullptr;
+  double* loss = nullptr;
+};
+
+namespace {
+
+int g_mlp_free_acts(oapb_mlp* h) {
+  for (auto p : h->hf) cudaFree(p);
+  for (auto p : h->hb) cudaFree(p);
+  h->hf.clear();
+  h->hb.clear();
+  if (h->dA) cudaFree(h->dA);
+  if (h->dB2) cudaFree(h->dB2);
+  if (h->dAb) cudaFree(h->dAb);
+  h->dA = h->dB2 = nullptr;
+  h->dAb = nullptr;
+  h->cap = 0;
+  return OAPB_OK;
+}
+
+int ensure_acts(oapb_mlp* h, int batch) {
+  if (batch <= h->cap) return OAPB_OK;
+  g_mlp_free_acts(h);
+  int mx = 0;
+  for (int s : h->sz) mx = s > mx ? s : mx;
+  h->hb.resize(h->nl + 1, nullptr);
+  h->hf.resize(h->nl, nullptr);
+  for (int l = 0; l <= h->nl; ++l)
+    if (cudaMalloc(&h->hb[l], sizeof(__nv_bfloat16) * (size_t)batch * h->sz[l]) != cudaSuccess) return OAPB_ERR_NOMEM;
+  for (int l = 0; l < h->nl; ++l)
+    if (cudaMalloc(&h->hf[l], sizeof(float) * (size_t)batch * h->sz[l + 1]) != cudaSuccess) return OAPB_ERR_NOMEM;
+  if (cudaMalloc(&h->dA, sizeof(float) * (size_t)batch * mx) != cudaSuccess ||
+      cudaMalloc(&h->dB2, sizeof(float) * (size_t)batch * mx) != cudaSuccess ||
+      cudaMalloc(&h->dAb, sizeof(__nv_bfloat16) * (size_t)batch * mx) != cudaSuccess)
+    return OAPB_ERR_NOMEM;
+  h->cap = batch;
+  return OAPB_OK;
+}
+
+void layer_gemm(bool bias_tanh, const __nv_bfloat16* A, long sam, long sak, const __nv_bfloat16* Bm, long sbn, long sbk,
+                int M, int N, int K, const float* bias, float* C, __nv_bfloat16* Cb, int ldc, cudaStream_t s) {
+  dim3 grid((N + kLT - 1) / kLT, (M + kLT - 1) / kLT);
+  if (bias_tanh)
+    k_layer_gemm<true><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, C, Cb, ldc);
+  else
+    k_layer_gemm<false><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, C, Cb, ldc);
+}
+
+int forward_impl(oapb_mlp* h, const float* x, int B, cudaStream_t s) {
+  int rc = ensure_acts(h, B);
+  if (rc) return rc;
+  const long n0 = (long)B * h->sz[0];
+  k_to_bf16<<<grid_for(n0, 256), 256, 0, s>>>(x, n0, h->hb[0]);
+  for (int l = 0; l < h->nl; ++l) {
+    const int in = h->sz[l], out = h->sz[l + 1];
+    const bool last = l + 1 == h->nl;
+    const __nv_bfloat16* W = h->wb + h->woff[l];
+    const float* bias = h->w + h->boff[l];
+    layer_gemm(!last, h->hb[l], in, 1, W, in, 1, B, out, in, bias, h->hf[l], last ? nullptr : h->hb[l + 1], out, s);
+    if (last) k_add_bias<<<grid_for((long)B * out, 256), 256, 0, s>>>(h->hf[l], bias, B, out, h->hb[l + 1]);
+  }
+  return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oapb_param_operators(const double* A0, const double* const* B, uint32_t nparams, const double* theta,
+                         uint32_t count, uint32_t n, double* out, void* stream) {
+  if (!A0 || !B || !theta || !out || nparams == 0 || nparams > 32 || count == 0 || n == 0) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const double** dB = nullptr;
+  if (cudaMallocAsync((void**)&dB, sizeof(double*) * nparams, s) != cudaSuccess) return OAPB_ERR_NOMEM;
+  int rc = OAPB_OK;
+  if (cudaMemcpyAsync(dB, B, sizeof(double*) * nparams, cudaMemcpyHostToDevice, s) != cudaSuccess) rc = OAPB_ERR_CUDA;
+  if (!rc) {
+    const long nn = (long)n * n;
+    k_param_operators<<<grid_for(nn, 256, kNumSMs * 8), 256, 0, s>>>(A0, dB, (int)nparams, theta, (int)count, nn,
+                                                                      out);
+    if (cudaGetLastError() != cudaSuccess) rc = OAPB_ERR_CUDA;
+  }
+  cudaFreeAsync(dB, s);
+  return rc;
+}
+
+int oapb_mlp_create(oapb_mlp** out, const uint32_t* sizes, uint32_t nlayers, uint64_t seed) {
+  if (!out || !sizes || nlayers < 1 || nlayers > 8) return OAPB_ERR_ARG;
+  oapb_mlp* h = new (std::nothrow) oapb_mlp();
+  if (!h) return OAPB_ERR_NOMEM;
+  h->nl = (int)nlayers;
+  for (uint32_t i = 0; i <= nlayers; ++i) {
+    if (sizes[i] == 0) {
+      delete h;
+      return OAPB_ERR_ARG;
+    }
+    h->sz.push_back((int)sizes[i]);
+  }
+  long off = 0;
+  for (int l = 0; l < h->nl; ++l) {
+    h->woff.push_back(off);
+    off += (long)h->sz[l] * h->sz[l + 1];
+  }
+  const long nw = off;
+  for (int l = 0; l < h->nl; ++l) {
+    h->boff.push_back(off);
+    off += h->sz[l + 1];
+  }
+  h->nparam = off;
+  const size_t fb = sizeof(float) * (size_t)off;
+  if (cudaMalloc(&h->w, fb) != cudaSuccess || cudaMalloc(&h->g, fb) != cudaSuccess ||
+      cudaMalloc(&h->m1, fb) != cudaSuccess || cudaMalloc(&h->m2, fb) != cudaSuccess ||
+      cudaMalloc(&h->wb, sizeof(__nv_bfloat16) * (size_t)off) != cudaSuccess ||
+      cudaMalloc(&h->loss, sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    delete h;
+    return OAPB_ERR_NOMEM;
+  }
+  cudaMemset(h->m1, 0, fb);
+  cudaMemset(h->m2, 0, fb);
+  cudaMemset(h->g, 0, fb);
+  // uniform(-1/sqrt(fan_in), 1/sqrt(fan_in)) weights, zero biases
+  for (int l = 0; l < h->nl; ++l) {
+    const long len = (long)h->sz[l] * h->sz[l + 1];
+    k_init_uniform<<<grid_for(len, 256), 256>>>(h->w + h->woff[l], len, 1.0f / sqrtf((float)h->sz[l]),
+                                                 seed * 1315423911ull + l);
+  }
+  cudaMemset(h->w + nw, 0, sizeof(float) * (size_t)(off - nw));
+  k_to_bf16<<<grid_for(off, 256), 256>>>(h->w, off, h->wb);
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    delete h;
+    return OAPB_ERR_CUDA;
+  }
+  *out = h;
+  return OAPB_OK;
+}
+
+int oapb_mlp_destroy(oapb_mlp* h) {
+  if (!h) return OAPB_ERR_ARG;
+  cudaDeviceSynchronize();
+  g_mlp_free_acts(h);
+  cudaFree(h->w);
+  cudaFree(h->g);
+  cudaFree(h->m1);
+  cudaFree(h->m2);
+  cudaFree(h->wb);
+  cudaFree(h->loss);
+  delete h;
+  return OAPB_OK;
+}
+
+uint64_t oapb_mlp_num_params(const oapb_mlp* h) { return h ? (uint64_t)h->nparam : 0; }
+
+int oapb_mlp_forward(oapb_mlp* h, const float* x, uint32_t batch, float* y, void* stream) {
+  if (!h || !x || batch == 0) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = forward_impl(h, x, (int)batch, s);
+  if (rc) return rc;
+  if (y && cudaMemcpyAsync(y, h->hf[h->nl - 1], sizeof(float) * (size_t)batch * h->sz[h->nl],
+                           cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  return OAPB_OK;
+}
+
+// Forward + backward of loss = 1/(2B) sum (y - target)^2; gradients (FP32,
+// same packing as the parameters) stay in the handle.  *loss_out (host,
+// may be NULL) receives the loss (synchronises the stream).
+int oapb_mlp_backward(oapb_mlp* h, const float* x, const float* target, uint32_t batch, double* loss_out,
+                      void* stream) {
+  if (!h || !x || !target || batch == 0) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int B = (int)batch;
+  int rc = forward_impl(h, x, B, s);
+  if (rc) return rc;
+  if (cudaMemsetAsync(h->loss, 0, sizeof(double), s) != cudaSuccess) return OAPB_ERR_CUDA;
+  const int L = h->nl;
+  const long lenY = (long)B * h->sz[L];
+  // dY of the output layer into dAb (BF16) / dA (FP32)
+  k_mse_grad<<<grid_for(lenY, 256), 256, 0, s>>>(h->hf[L - 1], target, B, lenY, h->dAb, h->dA, h->loss);
+  for (int l = L - 1; l >= 0; --l) {
+    const int in = h->sz[l], out = h->sz[l + 1];
+    // dZ (B x out) in dAb / dA; weight gradient dW[o][i] = sum_b dZ[b][o] X[b][i]
+    layer_gemm(false, h->dAb, 1, out, h->hb[l], 1, in, out, in, B, nullptr, h->g + h->woff[l], nullptr, in, s);
+    k_bias_grad<<<grid_for(out, 256), 256, 0, s>>>(h->dA, B, out, h->g + h->boff[l]);
+    if (l == 0) break;
+    // data gradient dX[b][i] = sum_o dZ[b][o] W[o][i], then through tanh
+    const __nv_bfloat16* W = h->wb + h->woff[l];
+    layer_gemm(false, h->dAb, out, 1, W, 1, in, B, in, out, nullptr, h->dB2, nullptr, in, s);
+    k_tanh_grad<<<grid_for((long)B * in, 256), 256, 0, s>>>(h->dB2, h->hf[l - 1], (long)B * in, h->dAb, h->dA);
+  }
+  if (cudaGetLastError() != cudaSuccess) return OAPB_ERR_CUDA;
+  if (loss_out) {
+    if (cudaMemcpyAsync(loss_out, h->loss, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+  }
+  return OAPB_OK;
+}
+
+int oapb_mlp_adam_step(oapb_mlp* h, float lr, void* stream) {
+  if (!h || !(lr > 0)) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  h->step += 1;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - powf(b1, (float)h->step), c2 = 1.f - powf(b2, (float)h->step);
+  k_adam<<<grid_for(h->nparam, 256), 256, 0, s>>>(h->w, h->g, h->m1, h->m2, h->nparam, lr, b1, b2, 1e-8f, c1, c2,
+                                                   h->wb);
+  return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
+
+// which: 0 parameters (FP32 masters), 1 gradients; dst/src device or host
+int oapb_mlp_copy(oapb_mlp* h, int which, float* dst, void* stream) {
+  if (!h || !dst || which < 0 || which > 1) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(dst, which ? h->g : h->w, sizeof(float) * (size_t)h->nparam, cudaMemcpyDefault, s) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  return OAPB_OK;
+}
+
+int oapb_mlp_set_params(oapb_mlp* h, const float* src, void* stream) {
+  if (!h || !src) return OAPB_ERR_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(h->w, src, sizeof(float) * (size_t)h->nparam, cudaMemcpyDefault, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  k_to_bf16<<<grid_for(h->nparam, 256), 256, 0, s>>>(h->w, h->nparam, h->wb);
+  if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return OAPB_ERR_CUDA;
+  return OAPB_OK;
+}
+
+}  // extern "C"

@@ -427,6 +427,7 @@ struct oapb_arnoldi {
   float *x32re = nullptr, *x32im = nullptr;
   double *v0re = nullptr, *v0im = nullptr;
   bool have_v0 = false;
+  std::vector<double> start_shifts;
   // small
   cplx *H = nullptr, *Qs = nullptr, *ritz = nullptr, *Y = nullptr, *h = nullptr, *s = nullptr, *part = nullptr,
        *hws = nullptr;
@@ -929,20 +930,39 @@ __global__ void k_init_block(double* xre, double* xim, int b, int n, uint64_t se
   }
 }
 
+// f = w - s f (start-vector shift filter)
+template <bool CPLX>
+__global__ void k_shift_filter(const double* __restrict__ wre, const double* __restrict__ wim, double s, double* fre,
+                               double* fim, int n) {
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    fre[i] = wre[i] - s * fre[i];
+    if (CPLX) fim[i] = wim[i] - s * fim[i];
+  }
+}
+
 // Fresh start of the Krylov factorization: f = start vector, H = 0.
 template <bool C>
-int iram_start(oapb_arnoldi* a) {
+int iram_start(oapb_arnoldi* a, bool user_start = true) {
   cudaStream_t s = a->stream;
   const int n = a->n, m = a->m;
   if (cudaMemsetAsync(a->st, 0, sizeof(DevState), s) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->H, 0, sizeof(cplx) * m * m, s) != cudaSuccess) return OAPB_ERR_CUDA;
-  if (a->cfg.init == OAPB_INIT_USER) {
+  if (a->cfg.init == OAPB_INIT_USER && user_start) {
     if (!a->have_v0) return OAPB_ERR_ARG;
     cudaMemcpyAsync(a->fre, a->v0re, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
     if (C) cudaMemcpyAsync(a->fim, a->v0im, sizeof(double) * n, cudaMemcpyDeviceToDevice, s);
+    // shift filter: f <- prod_i (A - s_i I) f
+    for (double sh : a->start_shifts) {
+      int rc = apply_op(a, a->fre, C ? a->fim : nullptr, a->wre, C ? a->wim : nullptr, false, OAPB_TYPE_WV);
+      if (rc) return rc;
+      a->stats.matvecs++;
+      a->stats.kernel_launches++;
+      k_shift_filter<C><<<grid_n(n), 256, 0, s>>>(a->wre, a->wim, sh, a->fre, a->fim, n);
+    }
   } else {
     a->stats.kernel_launches++;
-    k_init_vector<<<grid_n(n), 256, 0, s>>>(a->fre, C ? a->fim : nullptr, n, a->cfg.seed, a->cfg.init);
+    const int mode = a->cfg.init == OAPB_INIT_USER ? OAPB_INIT_RANDOM : a->cfg.init;
+    k_init_vector<<<grid_n(n), 256, 0, s>>>(a->fre, C ? a->fim : nullptr, n, a->cfg.seed, mode);
   }
   return set_fnorm(a);
 }
@@ -955,6 +975,12 @@ int solve_plain(oapb_arnoldi* a, double* r) {
   int rc = iram_start<C>(a);
   if (rc) return rc;
   int st = iram<C>(a, false, a->cfg.tolerance, a->cfg.max_restarts, 0);
+  if (st == OAPB_NOT_CONVERGED && a->cfg.init == OAPB_INIT_USER && a->cfg.fallback_random) {
+    // the warm start did not reach the goal: the random-start method decides
+    a->stats.fallbacks++;
+    if ((rc = iram_start<C>(a, false))) return rc;
+    st = iram<C>(a, false, a->cfg.tolerance, a->cfg.max_restarts, 0);
+  }
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   if ((rc = ritz_vectors<C>(a, a->k))) return rc;
   std::vector<cplx> th(a->m);
@@ -1016,6 +1042,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
   a->stats.block_matvecs = 0;
   a->stats.refine_iterations = 0;
   a->stats.dgks_passes = 0;
+  a->stats.fallbacks = 0;
   int rc = alloc_blocks(a);
   if (rc) return rc;
   std::vector<double> r(k);
@@ -1191,6 +1218,12 @@ int oapb_arnoldi_set_start_vector(oapb_arnoldi* a, const double* re, const doubl
   if (a->is_c && cudaMemcpyAsync(a->v0im, im, vb, cudaMemcpyDefault, a->stream) != cudaSuccess)
     return OAPB_ERR_CUDA;
   a->have_v0 = true;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_set_start_shifts(oapb_arnoldi* a, const double* shifts, uint32_t count) {
+  if (!a || count > 64 || (count && !shifts)) return OAPB_ERR_ARG;
+  a->start_shifts.assign(shifts, shifts + count);
   return OAPB_OK;
 }
 

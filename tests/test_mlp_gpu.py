@@ -1,0 +1,97 @@
+"""Warm-start network kernels (BF16, FP32 accumulation) against the CPU
+oracle, training, and the learned warm start on a parameterised operator."""
+import numpy as np
+import pytest
+
+from oracle import mlp as M
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+if not torch.cuda.is_available():
+    pytest.skip("needs a CUDA device", allow_module_level=True)
+
+import oap_b200 as B  # noqa: E402
+from oap_b200 import warmstart as W  # noqa: E402
+
+
+def test_forward_and_gradients_match_oracle():
+    sizes = [16, 64, 48, 40]
+    net = W.Net(sizes, seed=3)
+    rng = np.random.default_rng(1)
+    x = rng.uniform(-1, 1, size=(24, 16)).astype(np.float32)
+    t = rng.normal(size=(24, 40)).astype(np.float32)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    y = net.forward(xd).cpu().numpy()
+    p = net.params()
+    hf, _ = M.forward(p, sizes, x)
+    assert np.abs(y - hf[-1]).max() <= 1e-3 * max(1.0, np.abs(hf[-1]).max())
+    loss = net.backward(xd, td)
+    g = net.grads()
+    lo, go = M.loss_and_grads(p, sizes, x, t)
+    assert abs(loss - lo) <= 1e-4 * lo
+    rel = np.linalg.norm(g - go) / np.linalg.norm(go)
+    assert rel < 1e-3, rel
+    assert np.allclose(g, go, rtol=2e-2, atol=2e-3 * np.abs(go).max())
+
+
+def test_training_reduces_loss():
+    sizes = [16, 64, 64, 8]
+    net = W.Net(sizes, seed=5)
+    rng = np.random.default_rng(2)
+    X = rng.uniform(-1, 1, size=(2048, 16)).astype(np.float32)
+    A = rng.normal(size=(16, 8)) / 4
+    T = np.sin(X @ A).astype(np.float32)
+    Xd, Td = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+    losses = net.train(Xd, Td, epochs=20, batch=128, lr=3e-3)
+    assert losses[-1] < 0.1 * losses[0]
+
+
+def test_param_operators_match_definition():
+    fam = W.ParamFamily(n=96, nparams=5, seed=2)
+    theta = torch.rand(7, 5, dtype=torch.float64, device="cuda") * 2 - 1
+    ops = fam.operators(theta)
+    for p in range(7):
+        ref = fam.A0 + sum(theta[p, i] * fam.B[i] for i in range(5))
+        assert torch.allclose(ops[p], ref, rtol=0, atol=1e-14)
+
+
+def test_learned_warm_start_on_parametric_family():
+    n, k = 256, 8
+    fam = W.ParamFamily(n=n, nparams=16, seed=4)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(9)
+    th_train = torch.rand(1536, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    th_test = torch.rand(12, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    T, evs, st = W.make_targets(fam, th_train, wanted=k, nshift=8, chunk=512)
+    assert (st == B.OK).all()
+    net = W.Net([16, 256, 256, n + 8], seed=1)
+    X = th_train.float().contiguous()
+    Td = torch.from_numpy(T).cuda()
+    losses = net.train(X, Td, epochs=60, batch=128, lr=2e-3)
+    assert losses[-1] < 0.5 * losses[0]
+    pred = net.forward(th_test.float().contiguous())
+    ops = fam.operators(th_test)
+    mv_warm = mv_rand = 0
+    overlap_pred, overlap_rand = [], []
+    u_rand = torch.randn(n, dtype=torch.float64, device="cuda", generator=g)
+    for i in range(th_test.shape[0]):
+        A = ops[i].contiguous()
+        ev_w, res_w, st_w, s_w = W.solve_from_prediction(A, pred[i], n, wanted=k, hdim=24)
+        ev_r, res_r, st_r, s_r = W.solve_random(A, n, wanted=k, hdim=24)
+        # the plain method judges both: every pair at the residual goal
+        assert st_w == B.OK and max(res_w) <= 1e-10
+        assert st_r == B.OK and max(res_r) <= 1e-10
+        assert np.allclose(np.sort(np.array(ev_w).real), np.sort(np.array(ev_r).real), rtol=1e-9)
+        mv_warm += s_w["matvecs"]
+        mv_rand += s_r["matvecs"]
+        # overlap of the predicted start vector with the wanted subspace
+        w, V = torch.linalg.eigh(A)
+        Xk = V[:, -k:]
+        v = pred[i, :n].double()
+        overlap_pred.append(float(torch.linalg.norm(Xk.T @ v) / torch.linalg.norm(v)))
+        overlap_rand.append(float(torch.linalg.norm(Xk.T @ u_rand) / torch.linalg.norm(u_rand)))
+    print("warm-start matvecs", mv_warm, "random-start matvecs", mv_rand,
+          "mean overlap pred", np.mean(overlap_pred), "random", np.mean(overlap_rand))
+    # the network has learned the wanted subspace far beyond chance
+    assert np.mean(overlap_pred) > 3 * np.mean(overlap_rand)
