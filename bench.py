@@ -51,7 +51,9 @@ def parse():
                    help="profiling run: time one form only, no plain / e2e / CPU legs")
     p.add_argument("--form", default="mixed", choices=["mixed", "plain"],
                    help="form timed by --quick")
-    p.add_argument("--config", default="single", choices=["single", "batched", "gram"],
+    p.add_argument("--train", type=int, default=20000, help="warm-start training solves")
+    p.add_argument("--held-out", type=int, default=48, help="warm-start evaluation solves")
+    p.add_argument("--config", default="single", choices=["single", "batched", "gram", "warmstart"],
                    help="single: the n=16384 complex solve (default line); batched: 2048 uneven "
                         "complex problems n in [32, 512], top-4, hdim=min(n, 24)")
     p.add_argument("--batch", type=int, default=2048)
@@ -557,6 +559,67 @@ def run_gram(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
+def run_warmstart(args, world, rank, local):
+    """Learned warm start on A(theta) = A0 + sum_i theta_i B_i (n = 2048 real
+    symmetric, 16 parameters): training targets from plain FP64 IRAM solves
+    (batched), network 16 -> 256 -> 256 -> 2048 + 8 trained on the GPU,
+    then held-out solves from the prediction vs from a random start."""
+    import numpy as np
+    import torch
+    import oap_b200 as B
+    from oap_b200 import warmstart as W
+    torch.cuda.set_device(local)
+    n, k, hdim = 2048, 8, 24
+    fam = W.ParamFamily(n=n, nparams=16, seed=31 + rank)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(77 + rank)
+    th_train = torch.rand(args.train, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    th_test = torch.rand(args.held_out, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    t0 = time.perf_counter()
+    T, evs, st = W.make_targets(fam, th_train, wanted=k, nshift=8, chunk=256)
+    torch.cuda.synchronize()
+    t_data = time.perf_counter() - t0
+    net = W.Net([16, 256, 256, n + 8], seed=1)
+    t0 = time.perf_counter()
+    losses = net.train(th_train.float().contiguous(), torch.from_numpy(T).cuda(), epochs=40, batch=256, lr=2e-3)
+    torch.cuda.synchronize()
+    t_train = time.perf_counter() - t0
+    ops = fam.operators(th_test)
+    res = {"warm": {"matvecs": 0, "restarts": 0, "seconds": 0.0, "fallbacks": 0, "converged": 0},
+           "random": {"matvecs": 0, "restarts": 0, "seconds": 0.0, "converged": 0}}
+    for i in range(th_test.shape[0]):
+        A = ops[i].contiguous()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        pred = net.forward(th_test[i:i + 1].float().contiguous())[0]
+        ev, r, stw, s_w = W.solve_from_prediction(A, pred, n, wanted=k, hdim=hdim)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        ev, r2, str_, s_r = W.solve_random(A, n, wanted=k, hdim=hdim)
+        torch.cuda.synchronize()
+        t3 = time.perf_counter()
+        for key, s_, st_, rr, dt in (("warm", s_w, stw, r, t2 - t1), ("random", s_r, str_, r2, t3 - t2)):
+            res[key]["matvecs"] += s_["matvecs"]
+            res[key]["restarts"] += s_["restarts"]
+            res[key]["seconds"] += dt
+            res[key]["converged"] += int(st_ == B.OK and max(rr) <= TOL)
+        res["warm"]["fallbacks"] += s_w["fallbacks"]
+    m = th_test.shape[0]
+    for key in res:
+        for f in ("matvecs", "restarts", "seconds"):
+            res[key][f + "_per_solve"] = res[key][f] / m
+    out = {"config": {"workload": "A(theta) = A0 + sum theta_i B_i, n=2048 real symmetric, 16 params, top-8 LR, "
+                                  "hdim 24; network 16-256-256-2056 BF16",
+                      "training_solves": args.train, "held_out": m},
+           "training": {"data_seconds": t_data, "train_seconds": t_train, "loss_first": losses[0],
+                        "loss_last": losses[-1], "plain_solves_converged": int((st == B.OK).sum())},
+           "held_out": res,
+           "speedup_time": res["random"]["seconds"] / res["warm"]["seconds"] if res["warm"]["seconds"] else None,
+           "matvec_ratio": res["random"]["matvecs"] / max(1, res["warm"]["matvecs"])}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -567,6 +630,8 @@ def main():
             run_batched(args, world, rank, local)
         elif args.config == "gram":
             run_gram(args, world, rank, local)
+        elif args.config == "warmstart":
+            run_warmstart(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
