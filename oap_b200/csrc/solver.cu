@@ -763,12 +763,12 @@ int col_norms(oapb_arnoldi* a, const double* yr, const double* yi, int b, double
 // X <- orthonormal basis of span(Win) by two CholeskyQR passes (Win is kept)
 template <bool C>
 int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* xr, double* xi, double* tr,
-            double* ti) {
+            double* ti, int passes = 2) {
   const double* sr = wr;
   const double* si = wi;
-  for (int pass = 0; pass < 2; ++pass) {
-    double* dr = pass == 0 ? tr : xr;
-    double* di = pass == 0 ? ti : xi;
+  for (int pass = 0; pass < passes; ++pass) {
+    double* dr = pass + 1 < passes ? tr : xr;
+    double* di = pass + 1 < passes ? ti : xi;
     block_gram<C>(a, sr, si, b, sr, si, b, a->G2);
     ++a->stats.kernel_launches;
     a->stats.kernel_launches += 4;
@@ -822,16 +822,24 @@ constexpr int kMixedMinN = 8192;
 // Returns OAPB_OK (goal met: Ritz vectors in a->Xre, values in a->evals),
 // kSlow when the observed rate cannot reach the goal within the budget,
 // OAPB_NOT_CONVERGED or an error.
+// fp32 phase: one CholeskyQR pass per iteration (the FP32 operator's
+// rounding dominates), hand-over of the first `b_next` Ritz vectors in
+// a->Xre; the observed per-iteration contraction goes to *rate_out.
+// FP64 phase: two passes; the first `skip` iterations carry no check.
 template <bool C>
-int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, double* res_out, bool from_bx) {
+int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, double* res_out, bool from_bx,
+             int b_next = 0, double* rate_out = nullptr, int skip = 0) {
+  const int passes = fp32 ? 1 : 2;
   const int n = a->n, kk = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
   double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3];
   if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   int rc = OAPB_OK;
-  if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei))) return rc;
+  if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei, 2))) return rc;
+  const int nv = (fp32 && b_next > kk) ? b_next : kk;
   std::vector<double> norms(kk), hist;
+  std::vector<int> hist_it;
   std::vector<cplx> th(b);
   // In the FP32 phase the first Rayleigh-Ritz checks carry no decision:
   // from a random block the wanted directions need several powers before
@@ -839,15 +847,16 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   // second iteration.
   for (unsigned it = 0; it < max_it; ++it) {
     if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
-    const bool check = !fp32 || from_bx || (it >= 5 && (it % 2 == 1)) || it + 1 == max_it;
+    const bool check = fp32 ? ((it >= 5 && (it % 2 == 1)) || it + 1 == max_it)
+                            : ((int)it >= skip || it + 1 == max_it);
     if (!check) {
-      if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
+      if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
       continue;
     }
     block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
     a->stats.kernel_launches += 5;
     k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
-    if ((rc = small_eig(a, a->G, b, kk, kk))) return rc;
+    if ((rc = small_eig(a, a->G, b, kk, nv))) return rc;
     k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
     if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
     if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
@@ -865,23 +874,35 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       mx = fmax(mx, res_out[q]);
     }
     hist.push_back(mx);
+    hist_it.push_back((int)it);
     a->stats.refine_iterations++;
     const bool done = mx <= tol;
     bool stop = done;
-    if (!done && hist.size() >= 4) {
-      const double r0 = hist[hist.size() - 3], r1 = mx;
-      const double rate = (r0 > 0 && r1 > 0) ? sqrt(r1 / r0) : 1.0;
-      if (fp32 && mx < 1e-4 && rate > 0.6) stop = true;  // FP32 floor reached
+    if (!done && hist.size() >= 3) {
+      const size_t h = hist.size();
+      const double r0 = hist[h - 3], r1 = mx;
+      const int span = hist_it[h - 1] - hist_it[h - 3];
+      const double rate = (r0 > 0 && r1 > 0 && span > 0) ? pow(r1 / r0, 1.0 / span) : 1.0;  // per iteration
+      if (rate_out) *rate_out = rate;
+      if (fp32 && mx < 1e-4 && rate > 0.75) stop = true;  // FP32 floor reached
       if (!stop) {
         const double need = rate < 1.0 ? log(tol / mx) / log(rate) : 1e30;
-        if (rate > 0.85 || need > (double)(max_it - it - 1)) return kSlow;
+        if (rate > 0.92 || need > (double)(max_it - it - 1)) return kSlow;
       }
     }
     if (stop || it + 1 == max_it) {
-      if (fp32 && !done) {
-        // hand the current block to the next phase: X <- orth(W)
-        if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
-        return OAPB_OK;
+      if (fp32) {  // the FP32 operator's residuals are not the goal: always hand over
+        // hand the first b_next Ritz vectors X s_q to the FP64 phase
+        const int bn = b_next > kk ? b_next : b;
+        a->stats.kernel_launches += 1;
+        if (bn == b) {
+          if ((rc = cholqr2<C>(a, W, Wi, b, a->Xre, a->Xim, E, Ei, 1))) return rc;
+        } else {
+          k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n,
+                                                              a->Xre, a->Xim);
+        }
+        if (res_out) *res_out = mx;
+        return launch_check();
       }
       a->stats.kernel_launches += 1;
       k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
@@ -890,7 +911,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       if ((rc = launch_check())) return rc;
       return done ? OAPB_OK : OAPB_NOT_CONVERGED;
     }
-    if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei))) return rc;
+    if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
   }
   return OAPB_NOT_CONVERGED;
 }
@@ -1001,14 +1022,22 @@ template <bool C>
 int solve_mixed(oapb_arnoldi* a, double* r) {
   const int n = a->n, m = a->m, k = a->k;
   const double tol = a->cfg.tolerance;
-  int b = k + (k / 2 > 4 ? k / 2 : 4);
+  // FP32 phase on k + 4 vectors, FP64 phase on the first k + 2 Ritz vectors
+  int b = k + 4;
   if (b > kBmMaxB) b = kBmMaxB;
   if (b > n) b = n;
+  int b64 = k + 2 < b ? k + 2 : b;
   a->stats.kernel_launches++;
   k_init_block<<<grid_n((long)b * n), 256, 0, a->stream>>>(a->Xre, C ? a->Xim : nullptr, b, n, a->cfg.seed);
-  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r, false);
+  double rate = 0.5, floor1 = 1e-6;
+  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, &floor1, false, b64, &rate);
   if (st == OAPB_OK) {
-    st = subspace<C>(a, b, false, tol, 30, r, true);
+    // the FP32 phase measured the contraction per iteration: the FP64 phase
+    // cannot meet the goal before about log(tol / floor) / log(rate) passes
+    int skip = 0;
+    if (rate > 0 && rate < 0.9 && floor1 > tol) skip = (int)(log(tol / floor1) / log(rate)) - 2;
+    if (skip < 0) skip = 0;
+    st = subspace<C>(a, b64, false, tol, 30, r, false, 0, nullptr, skip);
     if (st == OAPB_OK) return OAPB_OK;
   }
   if (st != OAPB_OK && st != kSlow && st != OAPB_NOT_CONVERGED) return st;
