@@ -828,7 +828,7 @@ constexpr int kMixedMinN = 8192;
 // FP64 phase: two passes; the first `skip` iterations carry no check.
 template <bool C>
 int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, double* res_out, bool from_bx,
-             int b_next = 0, double* rate_out = nullptr, int skip = 0) {
+             int b_next = 0, double* rate_out = nullptr, int skip = 0, double* floor_out = nullptr) {
   const int passes = fp32 ? 1 : 2;
   const int n = a->n, kk = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
@@ -901,7 +901,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
           k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n,
                                                               a->Xre, a->Xim);
         }
-        if (res_out) *res_out = mx;
+        if (floor_out) *floor_out = mx;
         return launch_check();
       }
       a->stats.kernel_launches += 1;
@@ -1030,7 +1030,8 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   a->stats.kernel_launches++;
   k_init_block<<<grid_n((long)b * n), 256, 0, a->stream>>>(a->Xre, C ? a->Xim : nullptr, b, n, a->cfg.seed);
   double rate = 0.5, floor1 = 1e-6;
-  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, &floor1, false, b64, &rate);
+  std::vector<double> r1(k);
+  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r1.data(), false, b64, &rate, 0, &floor1);
   if (st == OAPB_OK) {
     // the FP32 phase measured the contraction per iteration: the FP64 phase
     // cannot meet the goal before about log(tol / floor) / log(rate) passes
