@@ -883,7 +883,8 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       const double r0 = hist[h - 3], r1 = mx;
       const int span = hist_it[h - 1] - hist_it[h - 3];
       const double rate = (r0 > 0 && r1 > 0 && span > 0) ? pow(r1 / r0, 1.0 / span) : 1.0;  // per iteration
-      if (rate_out) *rate_out = rate;
+      // the contraction of the iteration, not the stagnation at the FP32 floor
+      if (rate_out && (*rate_out <= 0 || rate < *rate_out)) *rate_out = rate;
       if (fp32 && mx < 1e-4 && rate > 0.75) stop = true;  // FP32 floor reached
       if (!stop) {
         const double need = rate < 1.0 ? log(tol / mx) / log(rate) : 1e30;
@@ -1029,15 +1030,16 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   int b64 = k + 2 < b ? k + 2 : b;
   a->stats.kernel_launches++;
   k_init_block<<<grid_n((long)b * n), 256, 0, a->stream>>>(a->Xre, C ? a->Xim : nullptr, b, n, a->cfg.seed);
-  double rate = 0.5, floor1 = 1e-6;
+  double rate = 0.0, floor1 = 1e-6;
   std::vector<double> r1(k);
   int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r1.data(), false, b64, &rate, 0, &floor1);
   if (st == OAPB_OK) {
     // the FP32 phase measured the contraction per iteration: the FP64 phase
     // cannot meet the goal before about log(tol / floor) / log(rate) passes
     int skip = 0;
-    if (rate > 0 && rate < 0.9 && floor1 > tol) skip = (int)(log(tol / floor1) / log(rate)) - 2;
+    if (rate > 0 && rate < 0.9 && floor1 > tol) skip = (int)(log(tol / floor1) / log(rate)) - 1;
     if (skip < 0) skip = 0;
+    if (skip > 12) skip = 12;
     st = subspace<C>(a, b64, false, tol, 30, r, false, 0, nullptr, skip);
     if (st == OAPB_OK) return OAPB_OK;
   }
