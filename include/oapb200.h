@@ -202,10 +202,13 @@ typedef struct oapb_arnoldi_config {
   int32_t fallback_random; /* 1: when a solve from a user start vector does
                               not reach the goal within max_restarts, solve
                               again from the seeded random start */
+  int32_t tensor_cores;    /* mixed form: 1 (default) runs the FP32-class
+                              block passes on the tensor cores (split BF16),
+                              0 on the CUDA cores in FP32 */
 } oapb_arnoldi_config;
 
 /* Fill defaults: rho = 1/3.14, tolerance = 1e-10, LM, FP64, random start,
- * max_restarts = 300. */
+ * max_restarts = 300, tensor_cores = 1. */
 OAPB_EXPORT void oapb_arnoldi_config_default(oapb_arnoldi_config* cfg);
 
 typedef struct oapb_arnoldi_stats {
@@ -280,6 +283,16 @@ OAPB_EXPORT int oapb_arnoldi_solve_host(oapb_arnoldi* handle, const double* a_re
                             double* eigvec_im);
 
 OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_stats* out);
+
+/* W = A X for b <= 32 vectors (device FP64 planes, vector q at offset q n)
+ * with the handle's dense operator: precision OAPB_PREC_FP64 reads the FP64
+ * operator; OAPB_PREC_MIXED the FP32-class copy of the mixed form (tensor
+ * cores when cfg.tensor_cores, else CUDA-core FP32).  The block pass of the
+ * solver, exposed for multiple right-hand sides and for verification. */
+OAPB_EXPORT int oapb_arnoldi_apply_block(oapb_arnoldi* handle, const double* x_re,
+                                         const double* x_im, uint32_t b,
+                                         double* w_re, double* w_im,
+                                         int32_t precision);
 
 /* Relative residual ||A x - lambda x|| / (|lambda_1| ||x||) of pair `index`
  * of the last solve (CuHArnoldi::testOutcome, ArnoldiProcedures.cpp:521-542,

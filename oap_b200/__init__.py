@@ -40,7 +40,7 @@ class Config(C.Structure):
                 ("precision", C.c_int32), ("init", C.c_int32),
                 ("max_restarts", C.c_uint32), ("tolerance", C.c_double),
                 ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32),
-                ("fallback_random", C.c_int32)]
+                ("fallback_random", C.c_int32), ("tensor_cores", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -116,6 +116,7 @@ def lib():
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
+            "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
             "oapb_param_operators": [vp, P(vp), C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp],
             "oapb_mlp_create": [P(vp), P(C.c_uint32), C.c_uint32, C.c_uint64],
             "oapb_mlp_destroy": [vp],
@@ -184,7 +185,7 @@ class Arnoldi:
     def __init__(self, n, hdim, wanted, is_complex=False, sort="LM",
                  precision=PREC_FP64, tolerance=1e-10, max_restarts=300,
                  rho=1.0 / 3.14, seed=1, init=INIT_RANDOM, stream=None,
-                 profile=False, fallback_random=False):
+                 profile=False, fallback_random=False, tensor_cores=True):
         L = lib()
         cfg = Config()
         L.oapb_arnoldi_config_default(C.byref(cfg))
@@ -195,6 +196,7 @@ class Arnoldi:
         cfg.max_restarts, cfg.tolerance, cfg.rho, cfg.seed = max_restarts, tolerance, rho, seed
         cfg.profile = int(bool(profile))
         cfg.fallback_random = int(bool(fallback_random))
+        cfg.tensor_cores = int(bool(tensor_cores))
         self.cfg = cfg
         self.h = C.c_void_p()
         check(L.oapb_arnoldi_create(C.byref(self.h), C.byref(cfg), _stream(stream)),
@@ -270,6 +272,17 @@ class Arnoldi:
         if vectors:
             return out + (vr if vi is None else vr + 1j * vi,)
         return out
+
+    def apply_block(self, xre, xim=None, precision=PREC_FP64):
+        """W = A X for X given as (b, n) device FP64 tensors."""
+        import torch
+        b = xre.shape[0]
+        wre = torch.empty_like(xre)
+        wim = torch.empty_like(xim) if xim is not None else None
+        p = lambda t: C.c_void_p(t.data_ptr()) if t is not None else None
+        check(lib().oapb_arnoldi_apply_block(self.h, p(xre), p(xim), b, p(wre), p(wim), precision),
+              "oapb_arnoldi_apply_block")
+        return wre, wim
 
     def stats(self):
         s = Stats()

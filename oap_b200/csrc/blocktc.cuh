@@ -1,0 +1,27 @@
+// Host interface of the tensor-core block operator pass (blocktc.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+namespace oapb {
+
+// Operator stored as BF16 hi / lo planes, n x kp (kp = n rounded up to 64,
+// zero-padded columns); aih / ail are NULL for a real operator.
+struct BtcOperator {
+  const __nv_bfloat16 *arh, *arl, *aih, *ail;
+  int n, kp;
+};
+
+// hi / lo BF16 planes of one FP64 operator plane
+int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
+
+// Split-K partials Wp[split][plane][q][row] of W = A X for b <= 32 vectors
+// (X vector-contiguous FP64); ksplit % 64 == 0; xbh / xbl hold 64 x kp BF16
+// each; *err receives timeout bits.
+int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* Wp,
+                           int nsplit, int ksplit, __nv_bfloat16* xbh, __nv_bfloat16* xbl, int* err,
+                           cudaStream_t s);
+
+}  // namespace oapb

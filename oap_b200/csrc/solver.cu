@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "block.cuh"
+#include "blocktc.cuh"
 #include "common.cuh"
 #include "hess.cuh"
 #include "matvec.cuh"
@@ -446,6 +447,12 @@ struct oapb_arnoldi {
   int nvec_hess = 0;
   double* Wp = nullptr;   // split-K partials of the block matvec
   int nsplit = 1, ksplit = 0;
+  // tensor-core FP32-class block pass: BF16 hi / lo operator planes
+  __nv_bfloat16* abf = nullptr;   // 4 planes (2 for a real operator) of n x kp
+  __nv_bfloat16* xbf = nullptr;   // B operand scratch, 2 x 64 x kp
+  int kp = 0;
+  int* tcerr = nullptr;
+  bool have_tc = false;
   size_t hess_smem = 0;
   oapb_arnoldi_stats stats{};
   std::vector<cudaEvent_t> ev_pool;   // profiling events (pairs)
@@ -678,7 +685,7 @@ int alloc_blocks(oapb_arnoldi* a) {
     if (sp < 1) sp = 1;
     if (sp > 8) sp = 8;
     long ks = (a->n + sp - 1) / sp;
-    ks = ((ks + 31) / 32) * 32;
+    ks = ((ks + 63) / 64) * 64;  // a multiple of the 64-wide tensor-core K chunk
     a->ksplit = (int)ks;
     a->nsplit = (int)((a->n + ks - 1) / ks);
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
@@ -727,6 +734,18 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   a->stats.kernel_launches += 2;
   Timed tm{nullptr, nullptr, 1, fp32 ? 1 : 0, b};
   const bool prof = prof_begin(a, tm);
+  if (fp32 && a->have_tc && a->cfg.tensor_cores) {
+    BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
+                   C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
+    const int nsp = (a->kp + a->ksplit - 1) / a->ksplit;
+    int rc = launch_block_matvec_tc(op, xr, xi, b, a->Wp, nsp, a->ksplit, a->xbf, a->xbf + 64 * (size_t)a->kp,
+                                    a->tcerr, a->stream);
+    if (prof) prof_end(a, tm);
+    if (rc) return rc;
+    k_split_reduce<C><<<grid_n((long)b * a->n), 256, 0, a->stream>>>(a->Wp, nsp, b, a->n, wr, wi);
+    a->stats.block_matvecs++;
+    return launch_check();
+  }
   const uintptr_t al = fp32 ? ((uintptr_t)a->a32re | (uintptr_t)(C ? (const void*)a->a32im : nullptr))
                             : ((uintptr_t)a->a64re | (uintptr_t)(C ? (const void*)a->a64im : nullptr));
   const int vec_ok = (al % 16 == 0) && (a->n % 4 == 0);
@@ -862,9 +881,11 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
     DevState bs;
+    int tcerr = 0;
     cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
+    if (a->tcerr) cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
     if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-    if (bs.status & 2) return OAPB_ERR_TIMEOUT;
+    if ((bs.status & 2) || tcerr) return OAPB_ERR_TIMEOUT;
     double scale = 0;
     for (int q = 0; q < kk; ++q) scale = fmax(scale, cabs_(th[q]));
     if (scale == 0) scale = 1;
@@ -1098,7 +1119,7 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->Wp, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);
@@ -1122,6 +1143,7 @@ void oapb_arnoldi_config_default(oapb_arnoldi_config* c) {
   c->tolerance = 1e-10;
   c->rho = 1.0 / 3.14;
   c->seed = 1;
+  c->tensor_cores = 1;
 }
 
 int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void* stream) {
@@ -1214,6 +1236,20 @@ static int make_fp32_copy(oapb_arnoldi* a) {
   if (!a->x32re && dalloc(&a->x32re, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   if (a->is_c && !a->x32im && dalloc(&a->x32im, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   const int g = kNumSMs * 8;
+  if (a->cfg.tensor_cores) {
+    a->kp = (a->n + 63) / 64 * 64;
+    const size_t plane = (size_t)a->n * a->kp;
+    const int np = a->is_c ? 4 : 2;
+    if (!a->abf && dalloc(&a->abf, sizeof(__nv_bfloat16) * plane * np)) return OAPB_ERR_NOMEM;
+    if (!a->xbf && dalloc(&a->xbf, sizeof(__nv_bfloat16) * 2 * 64 * (size_t)a->kp)) return OAPB_ERR_NOMEM;
+    if (!a->tcerr && dalloc(&a->tcerr, sizeof(int))) return OAPB_ERR_NOMEM;
+    cudaMemsetAsync(a->tcerr, 0, sizeof(int), a->stream);
+    a->stats.kernel_launches += np / 2;
+    if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream)) return OAPB_ERR_CUDA;
+    if (a->is_c && split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream))
+      return OAPB_ERR_CUDA;
+    a->have_tc = true;
+  }
   ++a->stats.kernel_launches;
   k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64re, a->a32re, nn);
   if (a->is_c) {
@@ -1342,6 +1378,24 @@ int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* hi
     if (e != cudaSuccess) return OAPB_ERR_CUDA;
   }
   return st;
+}
+
+int oapb_arnoldi_apply_block(oapb_arnoldi* a, const double* xre, const double* xim, uint32_t b, double* wre,
+                             double* wim, int32_t precision) {
+  if (!a || !xre || !wre || b == 0 || b > (uint32_t)kBmMaxB || a->cb || !a->a64re) return OAPB_ERR_ARG;
+  if (a->is_c && (!xim || !wim)) return OAPB_ERR_ARG;
+  const bool fp32 = precision == OAPB_PREC_MIXED;
+  if (fp32 && !a->a32re) return OAPB_ERR_ARG;
+  int rc = alloc_blocks(a);
+  if (rc) return rc;
+  rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32)
+               : block_apply<false>(a, xre, nullptr, (int)b, wre, nullptr, fp32);
+  if (rc) return rc;
+  int tcerr = 0;
+  if (a->tcerr && cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  return tcerr ? OAPB_ERR_TIMEOUT : OAPB_OK;
 }
 
 int oapb_arnoldi_get_stats(const oapb_arnoldi* a, oapb_arnoldi_stats* out) {

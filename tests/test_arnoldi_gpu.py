@@ -172,3 +172,28 @@ def test_mixed_precision_real_symmetric(gap):
     assert st == B.OK and max(res) <= TOL
     want = torch.sort(lam, descending=True).values[:4].cpu().numpy()
     assert np.allclose(np.sort(np.array(ev).real)[::-1], want, rtol=1e-10)
+
+
+@pytest.mark.parametrize("cplx", [True, False])
+@pytest.mark.parametrize("n,b", [(1024, 20), (1000, 7), (8192, 18)])
+def test_block_pass_precisions(cplx, n, b):
+    # FP64 block pass vs the FP64 oracle product, the FP32 (CUDA-core) and
+    # split-BF16 tensor-core passes within their precision
+    g = torch.Generator(device="cuda")
+    g.manual_seed(n + b)
+    are = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    aim = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5 if cplx else None
+    xr = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g)
+    xi = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g) if cplx else None
+    A = are if not cplx else torch.complex(are, aim)
+    X = xr if not cplx else torch.complex(xr, xi)
+    ref = (A @ X.T).T
+    scale = (A.abs() @ X.abs().T).T
+    for prec, tc, tol in ((B.PREC_FP64, True, 1e-13), (B.PREC_MIXED, False, 2e-6), (B.PREC_MIXED, True, 1e-4)):
+        s = B.Arnoldi(n, 16, 4, is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=tc)
+        s.set_operator(are, aim)
+        wr, wi = s.apply_block(xr, xi, precision=prec)
+        W = wr if not cplx else torch.complex(wr, wi)
+        err = ((W - ref).abs() / scale).max().item()
+        assert err <= tol, (prec, tc, err)
+        s.close()
