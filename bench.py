@@ -51,6 +51,8 @@ def parse():
                    help="profiling run: time one form only, no plain / e2e / CPU legs")
     p.add_argument("--form", default="mixed", choices=["mixed", "plain"],
                    help="form timed by --quick")
+    p.add_argument("--no-tc", action="store_true",
+                   help="FP32 block passes on CUDA cores instead of the split-BF16 tensor-core pass")
     p.add_argument("--train", type=int, default=20000, help="warm-start training solves")
     p.add_argument("--held-out", type=int, default=48, help="warm-start evaluation solves")
     p.add_argument("--config", default="single", choices=["single", "batched", "gram", "warmstart"],
@@ -277,7 +279,7 @@ def run_ours(args, world, rank, local):
 
     def solver(prec):
         s = B.Arnoldi(n, M_KRYLOV, K_WANTED, is_complex=True, precision=prec, tolerance=TOL,
-                      profile=True, seed=3 + rank)
+                      profile=True, seed=3 + rank, tensor_cores=not args.no_tc)
         s.set_operator(are, aim)
         return s
 

@@ -1,0 +1,259 @@
+// FP64 block operator pass W = A X on the FP64 tensor cores.
+//
+// Each iteration stages a 128 x 16 tile of every operator plane and the
+// 16-wide slice of X in shared memory (cp.async, four stages).  Warp w owns
+// operator rows 16 w .. 16 w + 15 of the tile and all N output columns:
+//   complex: B1 = [X_re | X_im] (N = 2 b columns), B2 = [-X_im | X_re], so
+//            C = A_re B1 + A_im B2 = [W_re | W_im] in one accumulator;
+//   real:    C = A_re X (N = b).
+// Both products run as mma.sync.m16n8k4.f64 over n-tiles of 8 columns with
+// FP64 accumulation (the same rounding class as the FP64 CUDA-core pass).
+// B2 is not stored: its fragment is read from the B1 row of the permuted
+// column, negated where the column is an X_im column.
+//
+// Shared layout per stage:
+//   A plane: 128 rows x 128 bytes, 16-byte chunk c of row r at chunk
+//            c ^ (r & 7) (fragment reads and cp.async writes conflict-free);
+//   X:       NT x 8 rows (B1 columns) x 20 doubles (row stride = 4 mod 16
+//            doubles, so a B fragment read is two wavefronts); rows beyond N
+//            are zero and never written.
+#include "blockdmma.cuh"
+#include "common.cuh"
+
+namespace oapb {
+
+constexpr int kDmM = 128;        // operator rows per tile
+constexpr int kDmK = 16;         // columns per iteration
+constexpr int kDmStages = 4;
+constexpr int kDmThreads = 256;  // 8 warps x 16 rows
+constexpr int kDmXStride = 20;   // doubles per staged X row
+constexpr int kDmMaxNT = 8;      // n-tiles (N <= 64)
+
+__host__ __device__ inline size_t dmma_stage_doubles(int np, int nt) {
+  return (size_t)np * kDmM * kDmK + (size_t)nt * 8 * kDmXStride;
+}
+
+__device__ __forceinline__ void cp_async16_zfill(uint32_t saddr, const void* g, int bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(saddr), "l"(g), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void dcommit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void dwait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
+  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
+               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+               : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// first iteration of CTA c
+__host__ __device__ inline long dm_begin(long c, long total, int G) { return c * total / G; }
+// CTA owning iteration it: the largest c with dm_begin(c) <= it
+__host__ __device__ inline long dm_owner(long it, long total, int G) { return ((it + 1) * G + total - 1) / total - 1; }
+
+struct DmArgs {
+  const double* are;
+  const double* aim;
+  const double* xr;
+  const double* xi;
+  double* ws;
+  int n, b, N, NT;
+  long tiles, kchunks, total;
+  int slots;
+};
+
+template <bool CPLX>
+__global__ void __launch_bounds__(kDmThreads, 1) k_block_matvec_dmma(DmArgs g) {
+  constexpr int NP = CPLX ? 2 : 1;
+  extern __shared__ __align__(128) double dsm[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int gq = lane >> 2, tq = lane & 3;  // fragment group / thread-in-group
+  const int n = g.n, b = g.b, N = g.N, NT = g.NT;
+  const size_t stage_d = dmma_stage_doubles(NP, NT);
+  const long it0 = dm_begin(blockIdx.x, g.total, gridDim.x);
+  const long it1 = dm_begin(blockIdx.x + 1, g.total, gridDim.x);
+  const long first_tile = it0 / g.kchunks;
+
+  // zero the X pad rows of every stage once (cp.async never writes them)
+  for (int s = 0; s < kDmStages; ++s) {
+    double* xs = dsm + s * stage_d + (size_t)NP * kDmM * kDmK;
+    for (int e = tid; e < (NT * 8 - N) * kDmXStride; e += kDmThreads) xs[N * kDmXStride + e] = 0.0;
+  }
+
+  auto load = [&](long it, int stage) {
+    const long tile = it / g.kchunks;
+    const long k0 = (it % g.kchunks) * kDmK;
+    double* base = dsm + stage * stage_d;
+    const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(base);
+    // operator planes: 128 rows x 8 chunks per plane
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      const double* pl = p == 0 ? g.are : g.aim;
+#pragma unroll
+      for (int u = 0; u < kDmM * 8 / kDmThreads; ++u) {
+        const int e = tid + u * kDmThreads;
+        const int r = e >> 3, ch = e & 7;
+        const long row = tile * kDmM + r, col = k0 + 2 * ch;
+        const bool ok = row < n && col < n;
+        const double* src = ok ? pl + row * n + col : pl;
+        const uint32_t dst = sbase + (uint32_t)((p * kDmM * kDmK + r * kDmK + ((ch ^ (r & 7)) << 1)) * 8);
+        cp_async16_zfill(dst, src, ok ? 16 : 0);
+      }
+    }
+    // X slice: N rows x 8 chunks
+    const uint32_t xbase = sbase + (uint32_t)(NP * kDmM * kDmK * 8);
+    for (int e = tid; e < N * 8; e += kDmThreads) {
+      const int r = e >> 3, ch = e & 7;
+      const long col = k0 + 2 * ch;
+      const double* pl = (CPLX && r >= b) ? g.xi + (long)(r - b) * n : g.xr + (long)r * n;
+      const bool ok = col < n;
+      cp_async16_zfill(xbase + (uint32_t)((r * kDmXStride + 2 * ch) * 8), ok ? pl + col : pl, ok ? 16 : 0);
+    }
+  };
+
+  // per-lane B1 row (n-tile j column j*8+gq) and B2 row / sign
+  int r1[kDmMaxNT], r2[kDmMaxNT];
+  double sg[kDmMaxNT];
+#pragma unroll
+  for (int j = 0; j < kDmMaxNT; ++j) {
+    const int c = j * 8 + gq;
+    r1[j] = c;
+    if (CPLX && c < 2 * b) {
+      r2[j] = c < b ? c + b : c - b;
+      sg[j] = c < b ? -1.0 : 1.0;
+    } else {
+      r2[j] = c;
+      sg[j] = 1.0;
+    }
+  }
+
+  double acc[kDmMaxNT][4];
+#pragma unroll
+  for (int j = 0; j < kDmMaxNT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+
+  auto flush = [&](long tile) {
+    const int slot = (int)(tile - first_tile);
+    double* out = g.ws + ((size_t)blockIdx.x * g.slots + slot) * (size_t)NP * b * kDmM;
+#pragma unroll
+    for (int j = 0; j < kDmMaxNT; ++j) {
+      if (j < NT) {
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int row = warp * 16 + gq + (e >> 1) * 8;
+          const int col = j * 8 + 2 * tq + (e & 1);
+          if (col < N) {
+            const int plane = col < b ? 0 : 1;
+            const int q = col - plane * b;
+            out[((size_t)plane * b + q) * kDmM + row] = acc[j][e];
+          }
+          acc[j][e] = 0.0;
+        }
+      }
+    }
+  };
+
+#pragma unroll
+  for (int s = 0; s < kDmStages - 1; ++s) {
+    if (it0 + s < it1) load(it0 + s, s);
+    dcommit();
+  }
+  for (long it = it0; it < it1; ++it) {
+    dwait<kDmStages - 2>();
+    __syncthreads();
+    {
+      const long nx = it + kDmStages - 1;
+      if (nx < it1) load(nx, (int)((nx - it0) % kDmStages));
+      dcommit();
+    }
+    const double* base = dsm + (size_t)((it - it0) % kDmStages) * stage_d;
+    const double* xs = base + (size_t)NP * kDmM * kDmK;
+    const int ra = warp * 16 + gq;  // ra & 7 == gq
+#pragma unroll
+    for (int k4 = 0; k4 < kDmK / 4; ++k4) {
+      const int kk = k4 * 4 + tq;
+      const int off = ((((kk >> 1) ^ gq)) << 1) | (kk & 1);
+      const double ar0 = base[ra * kDmK + off], ar1 = base[(ra + 8) * kDmK + off];
+      double ai0 = 0.0, ai1 = 0.0;
+      if (CPLX) {
+        ai0 = base[kDmM * kDmK + ra * kDmK + off];
+        ai1 = base[kDmM * kDmK + (ra + 8) * kDmK + off];
+      }
+#pragma unroll
+      for (int j = 0; j < kDmMaxNT; ++j) {
+        if (j < NT) {
+          dmma(acc[j], ar0, ar1, xs[r1[j] * kDmXStride + kk]);
+          if (CPLX) dmma(acc[j], ai0, ai1, sg[j] * xs[r2[j] * kDmXStride + kk]);
+        }
+      }
+    }
+    if ((it + 1) % g.kchunks == 0 || it + 1 == it1) flush(it / g.kchunks);
+  }
+  dwait<0>();
+}
+
+// W[plane][q][row] = sum over the CTAs that touched the row's tile
+template <bool CPLX>
+__global__ void k_dmma_reduce(DmArgs g, int G, double* wr, double* wi) {
+  constexpr int NP = CPLX ? 2 : 1;
+  const long total_e = (long)NP * g.b * g.n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total_e; e += (long)gridDim.x * blockDim.x) {
+    const int row = (int)(e % g.n);
+    const long pq = e / g.n;
+    const int q = (int)(pq % g.b), plane = (int)(pq / g.b);
+    const long tile = row / kDmM;
+    const long ilo = tile * g.kchunks;
+    const long ihi = min(g.total, ilo + g.kchunks) - 1;
+    const long c0 = dm_owner(ilo, g.total, G), c1 = dm_owner(ihi, g.total, G);
+    double s = 0.0;
+    for (long c = c0; c <= c1; ++c) {
+      const long slot = tile - dm_begin(c, g.total, G) / g.kchunks;
+      s += g.ws[((size_t)c * g.slots + slot) * (size_t)NP * g.b * kDmM + ((size_t)plane * g.b + q) * kDmM +
+                row % kDmM];
+    }
+    (plane == 0 ? wr : wi)[(long)q * g.n + row] = s;
+  }
+}
+
+bool dmma_plan(int n, DmmaPlan* p) {
+  if (n < 2 || n % 2) return false;
+  p->tiles = (n + kDmM - 1) / kDmM;
+  p->kchunks = (n + kDmK - 1) / kDmK;
+  p->total = p->tiles * p->kchunks;
+  long G = kNumSMs;  // one CTA per SM (four stages of up to 42 KB)
+  if (G > p->total) G = p->total;
+  p->grid = (int)G;
+  // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
+  const long share = (p->total + G - 1) / G;
+  p->slots = (int)((share + p->kchunks - 1) / p->kchunks + 1);
+  return true;
+}
+
+size_t dmma_workspace(const DmmaPlan& p) { return (size_t)p.grid * p.slots * 2 * 32 * kDmM; }
+
+int launch_block_matvec_dmma(const double* Are, const double* Aim, int n, const double* xr, const double* xi,
+                             int b, double* wr, double* wi, const DmmaPlan& p, double* ws, cudaStream_t s) {
+  const bool cplx = Aim != nullptr;
+  if (b < 1 || b > 32 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
+  DmArgs g{Are, Aim, xr, xi, ws, n, b, cplx ? 2 * b : b, 0, p.tiles, p.kchunks, p.total, p.slots};
+  g.NT = (g.N + 7) / 8;
+  const size_t smem = dmma_stage_doubles(cplx ? 2 : 1, g.NT) * kDmStages * sizeof(double);
+  const int rgrid = grid_for((long)(cplx ? 2 : 1) * b * n, 256, kNumSMs * 4);
+  if (cplx) {
+    if (cudaFuncSetAttribute(k_block_matvec_dmma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return OAPB_ERR_CUDA;
+    k_block_matvec_dmma<true><<<p.grid, kDmThreads, smem, s>>>(g);
+    k_dmma_reduce<true><<<rgrid, 256, 0, s>>>(g, p.grid, wr, wi);
+  } else {
+    if (cudaFuncSetAttribute(k_block_matvec_dmma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return OAPB_ERR_CUDA;
+    k_block_matvec_dmma<false><<<p.grid, kDmThreads, smem, s>>>(g);
+    k_dmma_reduce<false><<<rgrid, 256, 0, s>>>(g, p.grid, wr, nullptr);
+  }
+  return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
+
+}  // namespace oapb

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "block.cuh"
+#include "blockdmma.cuh"
 #include "blocktc.cuh"
 #include "common.cuh"
 #include "hess.cuh"
@@ -446,6 +447,9 @@ struct oapb_arnoldi {
   int ndot = 0, nnorm = 0;
   int nvec_hess = 0;
   double* Wp = nullptr;   // split-K partials of the block matvec
+  double* wdm = nullptr;  // stream-K partials of the FP64 tensor-core pass
+  DmmaPlan dplan{};
+  bool have_dmma = false;
   int nsplit = 1, ksplit = 0;
   // tensor-core FP32-class block pass: BF16 hi / lo operator planes
   __nv_bfloat16* abf = nullptr;   // 4 planes (2 for a real operator) of n x kp
@@ -690,6 +694,10 @@ int alloc_blocks(oapb_arnoldi* a) {
     a->nsplit = (int)((a->n + ks - 1) / ks);
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
   }
+  if (!a->cb && dmma_plan(a->n, &a->dplan)) {
+    rc |= dalloc(&a->wdm, sizeof(double) * dmma_workspace(a->dplan));
+    a->have_dmma = true;
+  }
   a->nnorm = grid_for(a->n, 256, kNumSMs * 2);
   const size_t bb = sizeof(cplx) * kBmMaxB * kBmMaxB;
   rc |= dalloc(&a->bpart, bb * (size_t)a->ndot);
@@ -745,6 +753,18 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     k_split_reduce<C><<<grid_n((long)b * a->n), 256, 0, a->stream>>>(a->Wp, nsp, b, a->n, wr, wi);
     a->stats.block_matvecs++;
     return launch_check();
+  }
+  if (!fp32 && a->have_dmma && a->cfg.tensor_cores) {
+    const uintptr_t al64 = (uintptr_t)a->a64re | (uintptr_t)(C ? (const void*)a->a64im : nullptr) | (uintptr_t)xr |
+                           (uintptr_t)(C ? (const void*)xi : nullptr);
+    if (al64 % 16 == 0) {
+      int rc = launch_block_matvec_dmma(a->a64re, C ? a->a64im : nullptr, a->n, xr, xi, b, wr, wi, a->dplan, a->wdm,
+                                        a->stream);
+      if (prof) prof_end(a, tm);
+      if (rc) return rc;
+      a->stats.block_matvecs++;
+      return launch_check();
+    }
   }
   const uintptr_t al = fp32 ? ((uintptr_t)a->a32re | (uintptr_t)(C ? (const void*)a->a32im : nullptr))
                             : ((uintptr_t)a->a64re | (uintptr_t)(C ? (const void*)a->a64im : nullptr));
@@ -1119,7 +1139,7 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);

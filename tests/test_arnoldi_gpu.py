@@ -175,9 +175,10 @@ def test_mixed_precision_real_symmetric(gap):
 
 
 @pytest.mark.parametrize("cplx", [True, False])
-@pytest.mark.parametrize("n,b", [(1024, 20), (1000, 7), (8192, 18)])
+@pytest.mark.parametrize("n,b", [(1024, 20), (1000, 7), (8192, 18), (999, 5), (130, 32), (2, 1)])
 def test_block_pass_precisions(cplx, n, b):
-    # FP64 block pass vs the FP64 oracle product, the FP32 (CUDA-core) and
+    # FP64 block passes (DMMA tensor cores and CUDA cores; odd n takes the
+    # CUDA-core pass) vs the FP64 torch product, the FP32 (CUDA-core) and
     # split-BF16 tensor-core passes within their precision
     g = torch.Generator(device="cuda")
     g.manual_seed(n + b)
@@ -189,8 +190,9 @@ def test_block_pass_precisions(cplx, n, b):
     X = xr if not cplx else torch.complex(xr, xi)
     ref = (A @ X.T).T
     scale = (A.abs() @ X.abs().T).T
-    for prec, tc, tol in ((B.PREC_FP64, True, 1e-13), (B.PREC_MIXED, False, 2e-6), (B.PREC_MIXED, True, 1e-4)):
-        s = B.Arnoldi(n, 16, 4, is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=tc)
+    for prec, tc, tol in ((B.PREC_FP64, True, 1e-13), (B.PREC_FP64, False, 1e-13), (B.PREC_MIXED, False, 2e-6),
+                          (B.PREC_MIXED, True, 1e-4)):
+        s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=tc)
         s.set_operator(are, aim)
         wr, wi = s.apply_block(xr, xi, precision=prec)
         W = wr if not cplx else torch.complex(wr, wi)
