@@ -1,7 +1,8 @@
 // FP64 block operator pass W = A X on the FP64 tensor cores.
 //
-// Each iteration stages a 128 x 16 tile of every operator plane and the
-// 16-wide slice of X in shared memory (cp.async, four stages).  Warp w owns
+// Each iteration stages a 128 x 8 tile of every operator plane and the
+// 8-wide slice of X in shared memory (cp.async, four stages; two CTAs per SM
+// up to 48 output columns).  Warp w owns
 // operator rows 16 w .. 16 w + 15 of the tile and all N output columns:
 //   complex: B1 = [X_re | X_im] (N = 2 b columns), B2 = [-X_im | X_re], so
 //            C = A_re B1 + A_im B2 = [W_re | W_im] in one accumulator;
@@ -12,22 +13,22 @@
 // column, negated where the column is an X_im column.
 //
 // Shared layout per stage:
-//   A plane: 128 rows x 128 bytes, 16-byte chunk c of row r at chunk
-//            c ^ (r & 7) (fragment reads and cp.async writes conflict-free);
-//   X:       NT x 8 rows (B1 columns) x 20 doubles (row stride = 4 mod 16
-//            doubles, so a B fragment read is two wavefronts); rows beyond N
-//            are zero and never written.
+//   A plane: 128 rows x 64 bytes, 16-byte chunk c of row r at chunk
+//            c ^ ((r >> 1) & 3) (a fragment read is two wavefronts, the
+//            minimum for 256 bytes);
+//   X:       NT x 8 rows (B1 columns) x 12 doubles (row stride 12: a B
+//            fragment read is two wavefronts); rows beyond N are zero and
+//            never written.
 #include "blockdmma.cuh"
 #include "common.cuh"
 
 namespace oapb {
 
 constexpr int kDmM = 128;        // operator rows per tile
-constexpr int kDmK = 16;         // columns per iteration
+constexpr int kDmK = 8;          // columns per iteration
 constexpr int kDmStages = 4;
 constexpr int kDmThreads = 256;  // 8 warps x 16 rows
-constexpr int kDmXStride = 20;   // doubles per staged X row
-constexpr int kDmMaxNT = 8;      // n-tiles (N <= 64)
+constexpr int kDmXStride = 12;   // doubles per staged X row
 
 __host__ __device__ inline size_t dmma_stage_doubles(int np, int nt) {
   return (size_t)np * kDmM * kDmK + (size_t)nt * 8 * kDmXStride;
@@ -64,13 +65,16 @@ struct DmArgs {
   int slots;
 };
 
-template <bool CPLX>
-__global__ void __launch_bounds__(kDmThreads, 1) k_block_matvec_dmma(DmArgs g) {
+// 16-byte chunk c (0..3) of operator row r inside a staged plane, in doubles
+__device__ __forceinline__ int dm_aoff(int r, int c) { return r * kDmK + ((c ^ ((r >> 1) & 3)) << 1); }
+
+template <bool CPLX, int NT>
+__global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_dmma(DmArgs g) {
   constexpr int NP = CPLX ? 2 : 1;
   extern __shared__ __align__(128) double dsm[];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int gq = lane >> 2, tq = lane & 3;  // fragment group / thread-in-group
-  const int n = g.n, b = g.b, N = g.N, NT = g.NT;
+  const int n = g.n, b = g.b, N = g.N;
   const size_t stage_d = dmma_stage_doubles(NP, NT);
   const long it0 = dm_begin(blockIdx.x, g.total, gridDim.x);
   const long it1 = dm_begin(blockIdx.x + 1, g.total, gridDim.x);
@@ -87,25 +91,25 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_block_matvec_dmma(DmArgs g) {
     const long k0 = (it % g.kchunks) * kDmK;
     double* base = dsm + stage * stage_d;
     const uint32_t sbase = (uint32_t)__cvta_generic_to_shared(base);
-    // operator planes: 128 rows x 8 chunks per plane
+    // operator planes: 128 rows x 4 chunks per plane
 #pragma unroll
     for (int p = 0; p < NP; ++p) {
       const double* pl = p == 0 ? g.are : g.aim;
 #pragma unroll
-      for (int u = 0; u < kDmM * 8 / kDmThreads; ++u) {
+      for (int u = 0; u < kDmM * (kDmK / 2) / kDmThreads; ++u) {
         const int e = tid + u * kDmThreads;
-        const int r = e >> 3, ch = e & 7;
+        const int r = e >> 2, ch = e & 3;
         const long row = tile * kDmM + r, col = k0 + 2 * ch;
         const bool ok = row < n && col < n;
         const double* src = ok ? pl + row * n + col : pl;
-        const uint32_t dst = sbase + (uint32_t)((p * kDmM * kDmK + r * kDmK + ((ch ^ (r & 7)) << 1)) * 8);
+        const uint32_t dst = sbase + (uint32_t)((p * kDmM * kDmK + dm_aoff(r, ch)) * 8);
         cp_async16_zfill(dst, src, ok ? 16 : 0);
       }
     }
-    // X slice: N rows x 8 chunks
+    // X slice: N rows x 4 chunks
     const uint32_t xbase = sbase + (uint32_t)(NP * kDmM * kDmK * 8);
-    for (int e = tid; e < N * 8; e += kDmThreads) {
-      const int r = e >> 3, ch = e & 7;
+    for (int e = tid; e < N * (kDmK / 2); e += kDmThreads) {
+      const int r = e >> 2, ch = e & 3;
       const long col = k0 + 2 * ch;
       const double* pl = (CPLX && r >= b) ? g.xi + (long)(r - b) * n : g.xr + (long)r * n;
       const bool ok = col < n;
@@ -113,43 +117,40 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_block_matvec_dmma(DmArgs g) {
     }
   };
 
-  // per-lane B1 row (n-tile j column j*8+gq) and B2 row / sign
-  int r1[kDmMaxNT], r2[kDmMaxNT];
-  double sg[kDmMaxNT];
+  // per-lane B2 row / sign of n-tile j (B1 row is the column j * 8 + gq)
+  int r2[NT];
+  double sg[NT];
 #pragma unroll
-  for (int j = 0; j < kDmMaxNT; ++j) {
+  for (int j = 0; j < NT; ++j) {
     const int c = j * 8 + gq;
-    r1[j] = c;
     if (CPLX && c < 2 * b) {
-      r2[j] = c < b ? c + b : c - b;
+      r2[j] = (c < b ? c + b : c - b) * kDmXStride;
       sg[j] = c < b ? -1.0 : 1.0;
     } else {
-      r2[j] = c;
+      r2[j] = c * kDmXStride;
       sg[j] = 1.0;
     }
   }
 
-  double acc[kDmMaxNT][4];
+  double acc[NT][4];
 #pragma unroll
-  for (int j = 0; j < kDmMaxNT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
+  for (int j = 0; j < NT; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0;
 
   auto flush = [&](long tile) {
     const int slot = (int)(tile - first_tile);
     double* out = g.ws + ((size_t)blockIdx.x * g.slots + slot) * (size_t)NP * b * kDmM;
 #pragma unroll
-    for (int j = 0; j < kDmMaxNT; ++j) {
-      if (j < NT) {
+    for (int j = 0; j < NT; ++j) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int row = warp * 16 + gq + (e >> 1) * 8;
-          const int col = j * 8 + 2 * tq + (e & 1);
-          if (col < N) {
-            const int plane = col < b ? 0 : 1;
-            const int q = col - plane * b;
-            out[((size_t)plane * b + q) * kDmM + row] = acc[j][e];
-          }
-          acc[j][e] = 0.0;
+      for (int e = 0; e < 4; ++e) {
+        const int row = warp * 16 + gq + (e >> 1) * 8;
+        const int col = j * 8 + 2 * tq + (e & 1);
+        if (col < N) {
+          const int plane = col < b ? 0 : 1;
+          const int q = col - plane * b;
+          out[((size_t)plane * b + q) * kDmM + row] = acc[j][e];
         }
+        acc[j][e] = 0.0;
       }
     }
   };
@@ -169,23 +170,28 @@ __global__ void __launch_bounds__(kDmThreads, 1) k_block_matvec_dmma(DmArgs g) {
     }
     const double* base = dsm + (size_t)((it - it0) % kDmStages) * stage_d;
     const double* xs = base + (size_t)NP * kDmM * kDmK;
-    const int ra = warp * 16 + gq;  // ra & 7 == gq
+    const int ra = warp * 16 + gq;  // rows ra and ra + 8 share the swizzle
 #pragma unroll
     for (int k4 = 0; k4 < kDmK / 4; ++k4) {
       const int kk = k4 * 4 + tq;
-      const int off = ((((kk >> 1) ^ gq)) << 1) | (kk & 1);
-      const double ar0 = base[ra * kDmK + off], ar1 = base[(ra + 8) * kDmK + off];
+      const int off = dm_aoff(ra, kk >> 1) + (kk & 1);
+      const double ar0 = base[off], ar1 = base[off + 8 * kDmK];
       double ai0 = 0.0, ai1 = 0.0;
       if (CPLX) {
-        ai0 = base[kDmM * kDmK + ra * kDmK + off];
-        ai1 = base[kDmM * kDmK + (ra + 8) * kDmK + off];
+        ai0 = base[kDmM * kDmK + off];
+        ai1 = base[kDmM * kDmK + off + 8 * kDmK];
+      }
+      double b1[NT], b2[NT];
+#pragma unroll
+      for (int j = 0; j < NT; ++j) {
+        b1[j] = xs[(j * 8 + gq) * kDmXStride + kk];
+        if (CPLX) b2[j] = sg[j] * xs[r2[j] + kk];
       }
 #pragma unroll
-      for (int j = 0; j < kDmMaxNT; ++j) {
-        if (j < NT) {
-          dmma(acc[j], ar0, ar1, xs[r1[j] * kDmXStride + kk]);
-          if (CPLX) dmma(acc[j], ai0, ai1, sg[j] * xs[r2[j] * kDmXStride + kk]);
-        }
+      for (int j = 0; j < NT; ++j) dmma(acc[j], ar0, ar1, b1[j]);
+      if (CPLX) {
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma(acc[j], ai0, ai1, b2[j]);
       }
     }
     if ((it + 1) % g.kchunks == 0 || it + 1 == it1) flush(it / g.kchunks);
@@ -216,44 +222,85 @@ __global__ void k_dmma_reduce(DmArgs g, int G, double* wr, double* wi) {
   }
 }
 
+// grid of `ctas` CTAs over the iterations of an n x n operator
+static DmmaPlan dmma_grid(int n, long ctas) {
+  DmmaPlan p;
+  p.n = n;
+  p.tiles = (n + kDmM - 1) / kDmM;
+  p.kchunks = (n + kDmK - 1) / kDmK;
+  p.total = p.tiles * p.kchunks;
+  const long G = ctas < p.total ? ctas : p.total;
+  p.grid = (int)G;
+  // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
+  const long share = (p.total + G - 1) / G;
+  p.slots = (int)((share + p.kchunks - 1) / p.kchunks + 1);
+  return p;
+}
+
 bool dmma_plan(int n, DmmaPlan* p) {
   if (n < 2 || n % 2) return false;
-  p->tiles = (n + kDmM - 1) / kDmM;
-  p->kchunks = (n + kDmK - 1) / kDmK;
-  p->total = p->tiles * p->kchunks;
-  long G = kNumSMs;  // one CTA per SM (four stages of up to 42 KB)
-  if (G > p->total) G = p->total;
-  p->grid = (int)G;
-  // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
-  const long share = (p->total + G - 1) / G;
-  p->slots = (int)((share + p->kchunks - 1) / p->kchunks + 1);
+  *p = dmma_grid(n, kNumSMs);
   return true;
 }
 
-size_t dmma_workspace(const DmmaPlan& p) { return (size_t)p.grid * p.slots * 2 * 32 * kDmM; }
+// workspace for either occupancy (one or two CTAs per SM)
+size_t dmma_workspace(const DmmaPlan& p) {
+  size_t best = 0;
+  for (long occ = 1; occ <= 2; ++occ) {
+    const DmmaPlan q = dmma_grid(p.n, kNumSMs * occ);
+    const size_t need = (size_t)q.grid * q.slots * 2 * 32 * kDmM;
+    if (need > best) best = need;
+  }
+  return best;
+}
+
+template <bool CPLX, int NT>
+static int dmma_launch(const DmArgs& g0, int n, double* wr, double* wi, cudaStream_t s) {
+  auto kern = k_block_matvec_dmma<CPLX, NT>;
+  const size_t smem = dmma_stage_doubles(CPLX ? 2 : 1, NT) * kDmStages * sizeof(double);
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  int occ = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kDmThreads, smem) != cudaSuccess || occ < 1)
+    return OAPB_ERR_CUDA;
+  if (occ > 2) occ = 2;
+  const DmmaPlan p = dmma_grid(n, (long)kNumSMs * occ);
+  DmArgs g = g0;
+  g.tiles = p.tiles;
+  g.kchunks = p.kchunks;
+  g.total = p.total;
+  g.slots = p.slots;
+  kern<<<p.grid, kDmThreads, smem, s>>>(g);
+  const int rgrid = grid_for((long)(CPLX ? 2 : 1) * g.b * n, 256, kNumSMs * 4);
+  k_dmma_reduce<CPLX><<<rgrid, 256, 0, s>>>(g, p.grid, wr, wi);
+  return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
 
 int launch_block_matvec_dmma(const double* Are, const double* Aim, int n, const double* xr, const double* xi,
                              int b, double* wr, double* wi, const DmmaPlan& p, double* ws, cudaStream_t s) {
   const bool cplx = Aim != nullptr;
   if (b < 1 || b > 32 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
-  DmArgs g{Are, Aim, xr, xi, ws, n, b, cplx ? 2 * b : b, 0, p.tiles, p.kchunks, p.total, p.slots};
+  (void)p;
+  DmArgs g{Are, Aim, xr, xi, ws, n, b, cplx ? 2 * b : b, 0, 0, 0, 0, 0};
   g.NT = (g.N + 7) / 8;
-  const size_t smem = dmma_stage_doubles(cplx ? 2 : 1, g.NT) * kDmStages * sizeof(double);
-  const int rgrid = grid_for((long)(cplx ? 2 : 1) * b * n, 256, kNumSMs * 4);
   if (cplx) {
-    if (cudaFuncSetAttribute(k_block_matvec_dmma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return OAPB_ERR_CUDA;
-    k_block_matvec_dmma<true><<<p.grid, kDmThreads, smem, s>>>(g);
-    k_dmma_reduce<true><<<rgrid, 256, 0, s>>>(g, p.grid, wr, wi);
-  } else {
-    if (cudaFuncSetAttribute(k_block_matvec_dmma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return OAPB_ERR_CUDA;
-    k_block_matvec_dmma<false><<<p.grid, kDmThreads, smem, s>>>(g);
-    k_dmma_reduce<false><<<rgrid, 256, 0, s>>>(g, p.grid, wr, nullptr);
+    switch (g.NT) {
+      case 1: return dmma_launch<true, 1>(g, n, wr, wi, s);
+      case 2: return dmma_launch<true, 2>(g, n, wr, wi, s);
+      case 3: return dmma_launch<true, 3>(g, n, wr, wi, s);
+      case 4: return dmma_launch<true, 4>(g, n, wr, wi, s);
+      case 5: return dmma_launch<true, 5>(g, n, wr, wi, s);
+      case 6: return dmma_launch<true, 6>(g, n, wr, wi, s);
+      case 7: return dmma_launch<true, 7>(g, n, wr, wi, s);
+      default: return dmma_launch<true, 8>(g, n, wr, wi, s);
+    }
   }
-  return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+  switch (g.NT) {
+    case 1: return dmma_launch<false, 1>(g, n, wr, nullptr, s);
+    case 2: return dmma_launch<false, 2>(g, n, wr, nullptr, s);
+    case 3: return dmma_launch<false, 3>(g, n, wr, nullptr, s);
+    default: return dmma_launch<false, 4>(g, n, wr, nullptr, s);
+  }
 }
 
 }  // namespace oapb

@@ -14,6 +14,7 @@
 namespace oapb {
 
 struct DmmaPlan {
+  int n;
   long tiles, kchunks, total;   // iterations = tiles x kchunks
   int grid;                     // CTAs
   int slots;                    // partial slots per CTA (tiles one CTA can touch)
@@ -23,11 +24,12 @@ struct DmmaPlan {
 // apply (n odd: rows of A are not 16-byte aligned).
 bool dmma_plan(int n, DmmaPlan* p);
 
-// Doubles of partial workspace the plan needs for b <= 32 vectors.
+// Doubles of partial workspace for b <= 32 vectors at either occupancy.
 size_t dmma_workspace(const DmmaPlan& p);
 
 // W (planes wr / wi, vector q at offset q n) = A X; X planes likewise.
-// Are / Aim / X / W 16-byte aligned.  ws: dmma_workspace() doubles.
+// Are / Aim / X 16-byte aligned.  ws: dmma_workspace() doubles.  The grid
+// is re-planned per launch for the occupancy of the n-tile count.
 int launch_block_matvec_dmma(const double* Are, const double* Aim, int n, const double* xr, const double* xi,
                              int b, double* wr, double* wi, const DmmaPlan& p, double* ws, cudaStream_t s);
 
