@@ -70,7 +70,9 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 __host__ __device__ inline size_t batch_smem_bytes(int nmax, int m) {
   size_t b = 0;
   b += 6 * (size_t)nmax * sizeof(double);  // x, w, f (re / im)
-  b += 5 * (size_t)m * m * sizeof(cplx);   // H, T, Z, Q, Y
+  b += 3 * (size_t)m * m * sizeof(cplx);   // H, Q, Y
+  b += (2 * (size_t)m + 2) * sizeof(cplx); // Q tail: rotation list while Q is hess_core scratch
+  b += 2 * (size_t)hess_ld(m) * m * sizeof(cplx);  // T, Z
   b += 4 * (size_t)(m + 1) * sizeof(cplx); // ritz, h, s, u
   b += 2 * (size_t)(m + 1) * sizeof(double) + 64 * sizeof(double);
   b += 2 * (size_t)(m + 1) * sizeof(int) + sizeof(DevState) + 16 * 16;
@@ -92,9 +94,9 @@ __device__ BatchSmem carve(char* base, int nmax, int m) {
   S.fr = (double*)take(sizeof(double) * nmax);
   S.fi = (double*)take(sizeof(double) * nmax);
   S.H = (cplx*)take(sizeof(cplx) * m * m);
-  S.T = (cplx*)take(sizeof(cplx) * m * m);
-  S.Z = (cplx*)take(sizeof(cplx) * m * m);
-  S.Q = (cplx*)take(sizeof(cplx) * m * m);
+  S.T = (cplx*)take(sizeof(cplx) * hess_ld(m) * m);
+  S.Z = (cplx*)take(sizeof(cplx) * hess_ld(m) * m);
+  S.Q = (cplx*)take(sizeof(cplx) * ((size_t)m * m + 2 * m + 2));
   S.Y = (cplx*)take(sizeof(cplx) * m * m);
   S.ritz = (cplx*)take(sizeof(cplx) * (m + 1));
   S.h = (cplx*)take(sizeof(cplx) * (m + 1));
@@ -326,7 +328,9 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
       h.use_beta = 1;
       h.tol = A.tol;
       h.beta = 0;
-      hess_core(h, S.T, S.Z, S.u, S.key, S.ord, lane);
+      // Q is written only at the end of hess_core: until then it is the
+      // rotation list and eigenvector scratch (2 m + 2 + m k <= m^2 + 2 m + 2)
+      hess_core(h, S.T, S.Z, S.u, S.key, S.ord, S.Q, lane);
     }
     __syncthreads();
     if (S.st->status & 2) {

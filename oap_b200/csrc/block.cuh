@@ -336,50 +336,57 @@ __global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restr
 }
 
 // One warp: Cholesky G = R^H R of a b x b Hermitian positive definite matrix
-// (column-major), then Rinv = R^-1 (upper triangular).  status bit 2 when a
-// pivot is not positive.
+// (column-major, b <= 32), then Rinv = R^-1 (upper triangular).  status bit
+// 2 when a pivot is not positive.
+// Right-looking factorization with lane j owning column j: per step k the
+// lanes scale row k and update their own trailing column entries, reading
+// row k by broadcast; shared arrays use an odd leading dimension, so the
+// per-lane column accesses are conflict-free.  The inverse is one back
+// substitution per lane (column j of R^-1).
 __global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
-  __shared__ cplx R[kBmMaxB * kBmMaxB];
-  __shared__ cplx Ri[kBmMaxB * kBmMaxB];
+  constexpr int LD = kBmMaxB + 1;
+  __shared__ cplx R[kBmMaxB * LD];
+  __shared__ cplx X[kBmMaxB * LD];
   __shared__ double rd[kBmMaxB];   // 1 / R[j][j]
   const int lane = threadIdx.x;
-  for (int e = lane; e < b * b; e += 32) {
-    R[e] = G[e];   // upper triangle is overwritten by R, the rest unused
-    Ri[e] = cplx{0, 0};
-  }
+  const int j = lane;
+  const bool own = j < b;
+  for (int e = lane; e < b * b; e += 32) R[e % b + (e / b) * LD] = G[e];
   __syncwarp();
-  // column j: R[i][j] = (G[i][j] - sum_{p<i} conj(R[p][i]) R[p][j]) / R[i][i]
-  for (int j = 0; j < b; ++j) {
-    for (int i = 0; i < j; ++i) {
-      cplx acc = {0, 0};
-      for (int p = lane; p < i; p += 32) acc = acc + conj(R[p + i * b]) * R[p + j * b];
-      acc.re = warp_sum(acc.re);
-      acc.im = warp_sum(acc.im);
-      if (lane == 0) R[i + j * b] = rd[i] * (R[i + j * b] - acc);
-      __syncwarp();
+  for (int k = 0; k < b; ++k) {
+    const double piv = R[k + k * LD].re;
+    const double rkk = piv > 0 ? sqrt(piv) : 1e-300;
+    const double inv = 1.0 / rkk;
+    if (lane == 0 && !(piv > 0)) atomicOr(status, 4);
+    cplx rkj = {0, 0};
+    if (own && j >= k) {
+      rkj = (j == k) ? cplx{rkk, 0} : inv * R[k + j * LD];
+      R[k + j * LD] = rkj;
     }
-    double d = 0;
-    for (int p = lane; p < j; p += 32) d += abs2(R[p + j * b]);
-    d = warp_sum(d);
-    const double piv = R[j + j * b].re - d;
-    if (lane == 0) {
-      double rjj = piv > 0 ? sqrt(piv) : 1e-300;
-      if (!(piv > 0)) atomicOr(status, 4);
-      R[j + j * b] = cplx{rjj, 0};
-      rd[j] = 1.0 / rjj;
-    }
+    if (lane == k) rd[k] = inv;
+    __syncwarp();
+    if (own && j > k)
+      for (int i = k + 1; i <= j; ++i) R[i + j * LD] = R[i + j * LD] - conj(R[k + i * LD]) * rkj;
     __syncwarp();
   }
-  // inverse of upper-triangular R: column j of Ri solves R x = e_j
-  for (int j = lane; j < b; j += 32) {
-    for (int i = j; i >= 0; --i) {
-      cplx acc = (i == j) ? cplx{1, 0} : cplx{0, 0};
-      for (int p = i + 1; p <= j; ++p) acc = acc - R[i + p * b] * Ri[p + j * b];
-      Ri[i + j * b] = rd[i] * acc;
+  // column j of R^-1: x_j = 1 / R[j][j]; x_i = -(sum_{p>i} R[i][p] x_p) / R[i][i]
+  for (int i = b - 1; i >= 0; --i) {
+    cplx a0 = {0, 0}, a1 = {0, 0};
+    if (own && i < j) {
+      int p = i + 1;
+      for (; p + 1 <= j; p += 2) {
+        a0 = a0 + R[i + p * LD] * X[p + j * LD];
+        a1 = a1 + R[i + (p + 1) * LD] * X[p + 1 + j * LD];
+      }
+      if (p <= j) a0 = a0 + R[i + p * LD] * X[p + j * LD];
     }
+    if (own && i <= j) X[i + j * LD] = (i == j) ? cplx{rd[i], 0} : (-rd[i]) * (a0 + a1);
   }
   __syncwarp();
-  for (int e = lane; e < b * b; e += 32) Rinv[e] = Ri[e];
+  for (int e = lane; e < b * b; e += 32) {
+    const int r = e % b, c = e / b;
+    Rinv[e] = r <= c ? X[r + c * LD] : cplx{0, 0};
+  }
 }
 
 }  // namespace oapb

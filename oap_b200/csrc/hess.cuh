@@ -18,6 +18,16 @@
 // With `dense` set the input is a general matrix, first reduced to
 // Hessenberg form by Householder reflectors accumulated into Z.
 //
+// Work layout (one warp): T and Z are column-major with an odd leading
+// dimension hess_ld(m), so a lane-per-column access (row rotations) and a
+// lane-per-row access (column rotations) are both free of bank conflicts.
+// A QR sweep costs two warp syncs per rotation: the row rotation runs one
+// lane per column, the column rotation one lane per row, and the lanes that
+// produce the next bulge pair hand it to the warp by shuffle.  Rotations on
+// Z are deferred to the end of the sweep (each lane then applies the whole
+// sequence to its rows).  The eigenvector back substitutions run one lane
+// per eigenvector (T read by broadcast).
+//
 // Every loop is bounded (30 m sweeps for the Schur form); hitting the bound
 // sets bit 1 of DevState::status and the kernel returns.
 #pragma once
@@ -52,14 +62,23 @@ struct HessArgs {
   double* est;      // k relative Ritz estimates
   int* order;       // m sort order (indices into diag(T))
   DevState* st;
-  cplx* gws;        // global workspace (2 m^2) when shared memory is too small
+  cplx* gws;        // global workspace (hess_ws_cplx(m)) when shared memory is too small
   int m, k, nvec, which, do_shift, real_shifts, dense, use_beta;
   double tol;
   double beta;      // used when use_beta == 0 (dense mode: residual norms come separately)
 };
 
-#define TT_(i, j) T[(i) + (long)(j) * m]
-#define ZZ_(i, j) Z[(i) + (long)(j) * m]
+// leading dimension of the T / Z work arrays (odd)
+__host__ __device__ __forceinline__ int hess_ld(int m) { return m | 1; }
+// scratch (rotation list and eigenvector columns), in cplx
+__host__ __device__ __forceinline__ size_t hess_scratch_cplx(int m) { return (size_t)m * 32 + 2 * (size_t)m + 2; }
+// whole k_hess workspace: T, Z and the scratch
+__host__ __device__ __forceinline__ size_t hess_ws_cplx(int m) {
+  return 2 * (size_t)hess_ld(m) * m + hess_scratch_cplx(m);
+}
+
+#define TT_(i, j) T[(i) + (j) * ld]
+#define ZZ_(i, j) Z[(i) + (j) * ld]
 
 __device__ __forceinline__ double sort_key(cplx v, int which) {
   switch (which) {
@@ -72,58 +91,86 @@ __device__ __forceinline__ double sort_key(cplx v, int which) {
   }
 }
 
-// One single-shift QR sweep on the active window [l, h] of Hessenberg T,
-// applied to whole rows / columns; Z <- Z G^H for every rotation.
-static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int l, int h, cplx mu, int lane) {
-  for (int k = l; k < h; ++k) {
-    cplx x, y;
-    if (k == l) {
-      x = TT_(l, l) - mu;
-      y = TT_(l + 1, l);
-    } else {
-      x = TT_(k, k - 1);
-      y = TT_(k + 1, k - 1);
-    }
-    cplx p, q;
-    givens(x, y, p, q);
-    __syncwarp();
-    const int j0 = k > 0 ? k - 1 : 0;
-    for (int j = j0 + lane; j < m; j += 32) {
-      cplx a = TT_(k, j), b = TT_(k + 1, j);
-      TT_(k, j) = p * a + q * b;
-      TT_(k + 1, j) = (-conj(q)) * a + conj(p) * b;
-    }
-    __syncwarp();
-    const int ihi = (k + 2 < h) ? k + 2 : h;
-    for (int i = lane; i <= ihi; i += 32) {
-      cplx a = TT_(i, k), b = TT_(i, k + 1);
-      TT_(i, k) = a * conj(p) + b * conj(q);
-      TT_(i, k + 1) = (-a) * q + b * p;
-    }
-    if (Z)
-      for (int i = lane; i < m; i += 32) {
-        cplx a = ZZ_(i, k), b = ZZ_(i, k + 1);
-        ZZ_(i, k) = a * conj(p) + b * conj(q);
-        ZZ_(i, k + 1) = (-a) * q + b * p;
-      }
-    __syncwarp();
-    if (k > l && lane == 0) TT_(k + 1, k - 1) = cplx{0, 0};
-    __syncwarp();
-  }
-}
-
 // |re| + |im| (LAPACK's CABS1): the deflation test only needs a norm-equivalent
 __device__ __forceinline__ double cabs1(cplx a) { return fabs(a.re) + fabs(a.im); }
 
-__device__ __forceinline__ bool negligible(const cplx* T, int m, int l) {
+__device__ __forceinline__ bool negligible(const cplx* T, int ld, int l) {
   const double eps = 2.220446049250313e-16;
   double s = cabs1(TT_(l - 1, l - 1)) + cabs1(TT_(l, l));
   if (s == 0) s = 1e-300;
   return cabs1(TT_(l, l - 1)) <= eps * s;
 }
 
+__device__ __forceinline__ cplx shfl_c(cplx v, int src) {
+  return cplx{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
+
+// The largest l in [1, h] with T[l][l-1] negligible, else 0 (all lanes).
+static __device__ int find_split(const cplx* T, int ld, int h, int lane) {
+  for (int base = h; base >= 1; base -= 32) {
+    const int l = base - lane;
+    const bool f = l >= 1 && negligible(T, ld, l);
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (bal) return base - (__ffs(bal) - 1);
+  }
+  return 0;
+}
+
+// One single-shift QR sweep on the active window [l, h] of Hessenberg T,
+// applied to whole rows / columns of T; Z <- Z G_l^H ... G_{h-1}^H at the end
+// of the sweep.  rot: 2 m cplx of scratch.
+static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int ld, int l, int h, cplx mu, cplx* rot, int lane) {
+  cplx x = TT_(l, l) - mu, y = TT_(l + 1, l);
+  for (int k = l; k < h; ++k) {
+    cplx p, q;
+    givens(x, y, p, q);
+    if (lane == 0) {
+      rot[2 * k] = p;
+      rot[2 * k + 1] = q;
+    }
+    // rows k, k+1 (one lane per column)
+    const int j0 = k > l ? k - 1 : k;
+    for (int j = j0 + lane; j < m; j += 32) {
+      const cplx a = TT_(k, j), b = TT_(k + 1, j);
+      TT_(k, j) = p * a + q * b;
+      TT_(k + 1, j) = (k > l && j == k - 1) ? cplx{0, 0} : (-conj(q)) * a + conj(p) * b;
+    }
+    __syncwarp();
+    // columns k, k+1 (one lane per row); rows k+1 and k+2 of column k are
+    // the next bulge pair
+    const int ihi = (k + 2 < h) ? k + 2 : h;
+    cplx xn = {0, 0}, yn = {0, 0};
+    for (int i = lane; i <= ihi; i += 32) {
+      const cplx a = TT_(i, k), b = TT_(i, k + 1);
+      const cplx na = a * conj(p) + b * conj(q);
+      TT_(i, k) = na;
+      TT_(i, k + 1) = (-a) * q + b * p;
+      if (i == k + 1) xn = na;
+      if (i == k + 2) yn = na;
+    }
+    if (k + 1 < h) {
+      x = shfl_c(xn, (k + 1) & 31);
+      y = shfl_c(yn, (k + 2) & 31);
+    }
+    __syncwarp();
+  }
+  if (Z) {
+    for (int i = lane; i < m; i += 32) {
+      cplx c = ZZ_(i, l);
+      for (int k = l; k < h; ++k) {
+        const cplx p = rot[2 * k], q = rot[2 * k + 1];
+        const cplx z1 = ZZ_(i, k + 1);
+        ZZ_(i, k) = c * conj(p) + z1 * conj(q);
+        c = (-c) * q + z1 * p;
+      }
+      ZZ_(i, h) = c;
+    }
+    __syncwarp();
+  }
+}
+
 // Householder reduction of dense T to Hessenberg form, Z accumulating.
-static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lane) {
+static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int ld, int lane) {
   for (int k = 0; k + 2 < m; ++k) {
     double s = 0;
     for (int i = k + 1 + lane; i < m; i += 32) s += abs2(TT_(i, k));
@@ -141,24 +188,35 @@ static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lan
     for (int i = k + 1 + lane; i < m; i += 32) vv += abs2(v[i]);
     vv = warp_sum(vv);
     const double f = 2.0 / vv;
-    // T <- P T : column j
+    // T <- P T : column j (two partial sums break the dependency chain)
     for (int j = lane; j < m; j += 32) {
-      cplx d = {0, 0};
-      for (int i = k + 1; i < m; ++i) d = d + conj(v[i]) * TT_(i, j);
-      d = f * d;
-      for (int i = k + 1; i < m; ++i) TT_(i, j) = TT_(i, j) - d * v[i];
+      cplx d0 = {0, 0}, d1 = {0, 0};
+      int i = k + 1;
+      for (; i + 1 < m; i += 2) {
+        d0 = d0 + conj(v[i]) * TT_(i, j);
+        d1 = d1 + conj(v[i + 1]) * TT_(i + 1, j);
+      }
+      if (i < m) d0 = d0 + conj(v[i]) * TT_(i, j);
+      const cplx d = f * (d0 + d1);
+      for (i = k + 1; i < m; ++i) TT_(i, j) = TT_(i, j) - d * v[i];
     }
     __syncwarp();
     // T <- T P, Z <- Z P : row i
     for (int i = lane; i < m; i += 32) {
-      cplx d = {0, 0}, e = {0, 0};
-      for (int j = k + 1; j < m; ++j) {
-        d = d + TT_(i, j) * v[j];
-        e = e + ZZ_(i, j) * v[j];
+      cplx d0 = {0, 0}, d1 = {0, 0}, e0 = {0, 0}, e1 = {0, 0};
+      int j = k + 1;
+      for (; j + 1 < m; j += 2) {
+        d0 = d0 + TT_(i, j) * v[j];
+        d1 = d1 + TT_(i, j + 1) * v[j + 1];
+        e0 = e0 + ZZ_(i, j) * v[j];
+        e1 = e1 + ZZ_(i, j + 1) * v[j + 1];
       }
-      d = f * d;
-      e = f * e;
-      for (int j = k + 1; j < m; ++j) {
+      if (j < m) {
+        d0 = d0 + TT_(i, j) * v[j];
+        e0 = e0 + ZZ_(i, j) * v[j];
+      }
+      const cplx d = f * (d0 + d1), e = f * (e0 + e1);
+      for (j = k + 1; j < m; ++j) {
         TT_(i, j) = TT_(i, j) - d * conj(v[j]);
         ZZ_(i, j) = ZZ_(i, j) - e * conj(v[j]);
       }
@@ -170,12 +228,10 @@ static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int lan
 }
 
 // Complex Schur form in place; returns false when the sweep budget ran out.
-static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int lane) {
+static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int ld, cplx* rot, int lane) {
   int h = m - 1, its = 0, total = 0;
   while (h > 0) {
-    int l = h;
-    while (l > 0 && !negligible(T, m, l)) --l;
-    __syncwarp();
+    const int l = find_split(T, ld, h, lane);
     if (l > 0 && lane == 0) TT_(l, l - 1) = cplx{0, 0};
     __syncwarp();
     if (l == h) {
@@ -195,29 +251,113 @@ static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int lane) {
       cplx m1 = tr2 + disc, m2 = tr2 - disc;
       mu = cabs_(m1 - d) < cabs_(m2 - d) ? m1 : m2;
     }
-    warp_sweep(T, Z, m, l, h, mu, lane);
+    warp_sweep(T, Z, m, ld, l, h, mu, rot, lane);
     ++its;
   }
   __syncwarp();
   return true;
 }
 
+// Eigenvectors y_q = Z u_q (q < nvec) of the upper triangular T for the
+// diagonal entries ord[q]: u by back substitution, one lane per eigenvector
+// (columns of U in the scratch, stride min(32, nvec)); Y = Z U one lane per
+// row.  Returns max over q < k of the relative estimates beta |y_q[m-1]| /
+// (scale ||y_q||).
+static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int ld, const int* ord, int nvec, int k,
+                                      double small, double beta, double scale, cplx* U, cplx* Y, double* est,
+                                      int lane) {
+  double maxest = 0;
+  const int W = nvec < 32 ? nvec : 32;
+  for (int q0 = 0; q0 < nvec; q0 += 32) {
+    const int q = q0 + lane;
+    const bool act = lane < W && q < nvec;
+    const int idx = act ? ord[q] : 0;
+    const cplx lam = TT_(idx, idx);
+    if (lane < W)
+      for (int i = 0; i < m; ++i) U[i * W + lane] = (act && i == idx) ? cplx{1, 0} : cplx{0, 0};
+    for (int i = m - 2; i >= 0; --i) {
+      cplx a0 = {0, 0}, a1 = {0, 0};
+      if (lane < W) {
+        int j = i + 1;
+        for (; j + 1 < m; j += 2) {
+          a0 = a0 + TT_(i, j) * U[j * W + lane];
+          a1 = a1 + TT_(i, j + 1) * U[(j + 1) * W + lane];
+        }
+        if (j < m) a0 = a0 + TT_(i, j) * U[j * W + lane];
+      }
+      if (act && i < idx) {
+        cplx den = TT_(i, i) - lam;
+        if (cabs_(den) < small) den = cplx{small, 0};
+        const cplx ui = -cdiv(a0 + a1, den);
+        U[i * W + lane] = ui;
+        if (cabs_(ui) > 1e150)  // rescale this column to avoid overflow
+          for (int j = i; j <= idx; ++j) U[j * W + lane] = 1e-150 * U[j * W + lane];
+      }
+    }
+    __syncwarp();
+    // Y[:, q] = Z U[:, q], one lane per row; normalise; estimate
+    const int nq = (nvec - q0) < W ? (nvec - q0) : W;
+    for (int c = 0; c < nq; ++c) {
+      const int qq = q0 + c;
+      cplx yv[kMaxM / 32];
+      double nrm = 0;
+      cplx ylast = {0, 0};
+#pragma unroll
+      for (int t = 0; t < kMaxM / 32; ++t) {
+        const int r = lane + 32 * t;
+        yv[t] = cplx{0, 0};
+        if (r < m) {
+          cplx s0 = {0, 0}, s1 = {0, 0};
+          int j = 0;
+          for (; j + 1 < m; j += 2) {
+            s0 = s0 + ZZ_(r, j) * U[j * W + c];
+            s1 = s1 + ZZ_(r, j + 1) * U[(j + 1) * W + c];
+          }
+          if (j < m) s0 = s0 + ZZ_(r, j) * U[j * W + c];
+          yv[t] = s0 + s1;
+          nrm += abs2(yv[t]);
+          if (r == m - 1) ylast = yv[t];
+        }
+      }
+      nrm = sqrt(warp_sum(nrm));
+      ylast.re = warp_sum(ylast.re);
+      ylast.im = warp_sum(ylast.im);
+      const double inv = nrm > 0 ? 1.0 / nrm : 0.0;
+#pragma unroll
+      for (int t = 0; t < kMaxM / 32; ++t) {
+        const int r = lane + 32 * t;
+        if (r < m) Y[(long)qq * m + r] = inv * yv[t];
+      }
+      const double e = beta * cabs_(ylast) * inv / scale;
+      if (lane == 0) est[qq] = e;
+      if (qq < k) maxest = fmax(maxest, e);
+    }
+    __syncwarp();
+  }
+  return maxest;
+}
+
 // The body of k_hess for one warp (lane = 0..31 of the calling warp), with
-// its workspaces passed in: T, Z (m x m each), u (m), key (m), ord (m).
-// Callable from any kernel by one full warp; the outputs in `a` may point
-// to shared or global memory.
-static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, double* key, int* ord, int lane) {
-  const int m = a.m, k = a.k;
+// its workspaces passed in: T, Z (leading dimension hess_ld(m), m columns
+// each), u (m), key (m), ord (m), scratch (hess_scratch_cplx(m)).  Callable
+// from any kernel by one full warp; the outputs in `a` may point to shared
+// or global memory.
+static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, double* key, int* ord, cplx* scratch,
+                                 int lane) {
+  const int m = a.m, k = a.k, ld = hess_ld(m);
   const long mm = (long)m * m;
   DevState* st = a.st;
+  cplx* rot = scratch;           // 2 m
+  cplx* U = scratch + 2 * m + 2; // m x 32
 
   for (long i = lane; i < mm; i += 32) {
-    T[i] = a.Hin[i];
-    Z[i] = (i % m == i / m) ? cplx{1, 0} : cplx{0, 0};
+    const int r = (int)(i % m), c = (int)(i / m);
+    TT_(r, c) = a.Hin[i];
+    ZZ_(r, c) = (r == c) ? cplx{1, 0} : cplx{0, 0};
   }
   __syncwarp();
-  if (a.dense) warp_hessenberg(T, Z, u, m, lane);
-  if (!warp_schur(T, Z, m, lane)) {
+  if (a.dense) warp_hessenberg(T, Z, u, m, ld, lane);
+  if (!warp_schur(T, Z, m, ld, rot, lane)) {
     if (lane == 0) { st->status |= 2; st->converged = 0; }
     return;
   }
@@ -241,56 +381,16 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   for (int q = 0; q < k; ++q) scale = fmax(scale, cabs_(TT_(ord[q], ord[q])));
   if (scale == 0) scale = 1;
   double tnorm = 0;
-  for (int i = 0; i < m; ++i) tnorm = fmax(tnorm, cabs_(TT_(i, i)));
+  for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, cabs_(TT_(i, i)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
   const double small = 2.220446049250313e-16 * (tnorm > 0 ? tnorm : 1.0);
   const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
 
   // eigenvectors of the first nvec Ritz values (the wanted k and optional
   // guard vectors) and the estimates of the wanted ones
-  double maxest = 0;
   const int nvec = a.nvec > k ? (a.nvec < m ? a.nvec : m) : k;
-  for (int q = 0; q < nvec; ++q) {
-    const int idx = ord[q];
-    const cplx lam = TT_(idx, idx);
-    for (int i = lane; i < m; i += 32) u[i] = (i == idx) ? cplx{1, 0} : cplx{0, 0};
-    __syncwarp();
-    for (int i = idx - 1; i >= 0; --i) {
-      cplx acc = {0, 0};
-      for (int j = i + 1 + lane; j <= idx; j += 32) acc = acc + TT_(i, j) * u[j];
-      acc.re = warp_sum(acc.re);
-      acc.im = warp_sum(acc.im);
-      cplx den = TT_(i, i) - lam;
-      if (cabs_(den) < small) den = cplx{small, 0};
-      if (lane == 0) {
-        cplx ui = -cdiv(acc, den);
-        u[i] = ui;
-      }
-      __syncwarp();
-      if (cabs_(u[i]) > 1e150) {  // rescale to avoid overflow
-        for (int j = i + lane; j <= idx; j += 32) u[j] = 1e-150 * u[j];
-        __syncwarp();
-      }
-    }
-    double nrm = 0;
-    cplx ylast = {0, 0};
-    for (int r = lane; r < m; r += 32) {
-      cplx y = {0, 0};
-      for (int j = 0; j <= idx; ++j) y = y + ZZ_(r, j) * u[j];
-      a.Y[(long)q * m + r] = y;
-      nrm += abs2(y);
-      if (r == m - 1) ylast = y;
-    }
-    nrm = sqrt(warp_sum(nrm));
-    ylast.re = warp_sum(ylast.re);
-    ylast.im = warp_sum(ylast.im);
-    __syncwarp();
-    const double inv = nrm > 0 ? 1.0 / nrm : 0.0;
-    for (int r = lane; r < m; r += 32) a.Y[(long)q * m + r] = inv * a.Y[(long)q * m + r];
-    const double e = beta * cabs_(ylast) * inv / scale;
-    if (lane == 0) a.est[q] = e;
-    if (q < k) maxest = fmax(maxest, e);
-    __syncwarp();
-  }
+  const double maxest = warp_eigvecs(T, Z, m, ld, ord, nvec, k, small, beta, scale, U, a.Y, a.est, lane);
   const int conv = maxest <= a.tol;
   if (lane == 0) {
     st->converged = conv;
@@ -305,8 +405,9 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   for (int q = lane; q < m; q += 32) u[q] = TT_(ord[q], ord[q]);
   __syncwarp();
   for (long i = lane; i < mm; i += 32) {
-    T[i] = a.Hin[i];
-    Z[i] = (i % m == i / m) ? cplx{1, 0} : cplx{0, 0};
+    const int r = (int)(i % m), c = (int)(i / m);
+    TT_(r, c) = a.Hin[i];
+    ZZ_(r, c) = (r == c) ? cplx{1, 0} : cplx{0, 0};
   }
   __syncwarp();
   for (int q = k; q < m; ++q) {
@@ -314,12 +415,10 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
     if (a.real_shifts) mu.im = 0;
     int hb = m - 1;
     while (hb > 0) {
-      int l = hb;
-      while (l > 0 && !negligible(T, m, l)) --l;
-      __syncwarp();
+      const int l = find_split(T, ld, hb, lane);
       if (l > 0 && lane == 0) TT_(l, l - 1) = cplx{0, 0};
       __syncwarp();
-      if (l < hb) warp_sweep(T, Z, m, l, hb, mu, lane);
+      if (l < hb) warp_sweep(T, Z, m, ld, l, hb, mu, rot, lane);
       hb = l - 1;
     }
   }
@@ -329,19 +428,21 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
     st->sigma = ZZ_(m - 1, k - 1);
   }
   for (long i = lane; i < mm; i += 32) {
-    const int r = i % m, c = i / m;
-    a.Hout[i] = (r < k && c < k) ? T[i] : cplx{0, 0};
-    a.Qout[i] = Z[i];
+    const int r = (int)(i % m), c = (int)(i / m);
+    a.Hout[i] = (r < k && c < k) ? TT_(r, c) : cplx{0, 0};
+    a.Qout[i] = ZZ_(r, c);
   }
 }
 
+// dynamic shared memory (or a.gws): T, Z, scratch
 static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
   extern __shared__ cplx sws[];
   __shared__ cplx u[kMaxM];
   __shared__ double key[kMaxM];
   __shared__ int ord[kMaxM];
   cplx* T = a.gws ? a.gws : sws;
-  hess_core(a, T, T + (long)a.m * a.m, u, key, ord, threadIdx.x);
+  const size_t tz = (size_t)hess_ld(a.m) * a.m;
+  hess_core(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x);
 }
 
 #undef TT_

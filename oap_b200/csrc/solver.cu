@@ -24,6 +24,7 @@
 // estimates and the exact-shift restart (k_hess); V <- V Q and the Sorensen
 // residual update follow.  The host reads one small status block per
 // restart.
+#include <algorithm>
 #include <chrono>
 #include <new>
 #include <stdio.h>
@@ -845,7 +846,7 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
   h.tol = 0;
   h.beta = 0;
   ++a->stats.kernel_launches;
-  k_hess<<<1, 32, 2 * sizeof(cplx) * b * b, a->stream>>>(h);
+  k_hess<<<1, 32, sizeof(cplx) * hess_ws_cplx(b), a->stream>>>(h);
   return launch_check();
 }
 
@@ -1211,18 +1212,22 @@ int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void
   rc |= dalloc(&a->fpart, sizeof(double) * (a->nupd > 1024 ? a->nupd : 1024));
   rc |= dalloc(&a->order, sizeof(int) * m);
   rc |= dalloc(&a->st, sizeof(DevState));
-  const size_t hb = 2 * sizeof(cplx) * (size_t)m * m;
+  const size_t hb = sizeof(cplx) * hess_ws_cplx(m);
+  const size_t hb_block = sizeof(cplx) * hess_ws_cplx(kBmMaxB);  // small_eig of the block methods
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   const size_t static_smem = kMaxM * (sizeof(cplx) + sizeof(double) + sizeof(int)) + 1024;
   if (hb + static_smem <= (size_t)optin) {
     a->hess_smem = hb;
-    if (hb > 48 * 1024 &&
-        cudaFuncSetAttribute(k_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hb) != cudaSuccess)
-      rc |= OAPB_ERR_CUDA;
   } else {
     rc |= dalloc(&a->hws, hb);
+  }
+  {
+    const size_t attr = std::max(a->hess_smem, hb_block);
+    if (attr > 48 * 1024 &&
+        cudaFuncSetAttribute(k_hess, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)attr) != cudaSuccess)
+      rc |= OAPB_ERR_CUDA;
   }
   const size_t vqb = sizeof(cplx) * (size_t)m * m;
   if (vqb > 48 * 1024) {
