@@ -21,6 +21,7 @@
 //            never written.
 #include "blockdmma.cuh"
 #include "common.cuh"
+#include "streamk.cuh"
 
 namespace oapb {
 
@@ -49,11 +50,6 @@ __device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, doubl
                : "d"(a0), "d"(a1), "d"(b0));
 }
 
-// first iteration of CTA c
-__host__ __device__ inline long dm_begin(long c, long total, int G) { return c * total / G; }
-// CTA owning iteration it: the largest c with dm_begin(c) <= it
-__host__ __device__ inline long dm_owner(long it, long total, int G) { return ((it + 1) * G + total - 1) / total - 1; }
-
 struct DmArgs {
   const double* are;
   const double* aim;
@@ -76,8 +72,8 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
   const int gq = lane >> 2, tq = lane & 3;  // fragment group / thread-in-group
   const int n = g.n, b = g.b, N = g.N;
   const size_t stage_d = dmma_stage_doubles(NP, NT);
-  const long it0 = dm_begin(blockIdx.x, g.total, gridDim.x);
-  const long it1 = dm_begin(blockIdx.x + 1, g.total, gridDim.x);
+  const long it0 = sk_begin(blockIdx.x, g.total, gridDim.x);
+  const long it1 = sk_begin(blockIdx.x + 1, g.total, gridDim.x);
   const long first_tile = it0 / g.kchunks;
 
   // zero the X pad rows of every stage once (cp.async never writes them)
@@ -199,41 +195,16 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
   dwait<0>();
 }
 
-// W[plane][q][row] = sum over the CTAs that touched the row's tile
-template <bool CPLX>
-__global__ void k_dmma_reduce(DmArgs g, int G, double* wr, double* wi) {
-  constexpr int NP = CPLX ? 2 : 1;
-  const long total_e = (long)NP * g.b * g.n;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total_e; e += (long)gridDim.x * blockDim.x) {
-    const int row = (int)(e % g.n);
-    const long pq = e / g.n;
-    const int q = (int)(pq % g.b), plane = (int)(pq / g.b);
-    const long tile = row / kDmM;
-    const long ilo = tile * g.kchunks;
-    const long ihi = min(g.total, ilo + g.kchunks) - 1;
-    const long c0 = dm_owner(ilo, g.total, G), c1 = dm_owner(ihi, g.total, G);
-    double s = 0.0;
-    for (long c = c0; c <= c1; ++c) {
-      const long slot = tile - dm_begin(c, g.total, G) / g.kchunks;
-      s += g.ws[((size_t)c * g.slots + slot) * (size_t)NP * g.b * kDmM + ((size_t)plane * g.b + q) * kDmM +
-                row % kDmM];
-    }
-    (plane == 0 ? wr : wi)[(long)q * g.n + row] = s;
-  }
-}
-
 // grid of `ctas` CTAs over the iterations of an n x n operator
 static DmmaPlan dmma_grid(int n, long ctas) {
+  const SkGrid k = sk_grid((n + kDmM - 1) / kDmM, (n + kDmK - 1) / kDmK, ctas);
   DmmaPlan p;
   p.n = n;
-  p.tiles = (n + kDmM - 1) / kDmM;
-  p.kchunks = (n + kDmK - 1) / kDmK;
-  p.total = p.tiles * p.kchunks;
-  const long G = ctas < p.total ? ctas : p.total;
-  p.grid = (int)G;
-  // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
-  const long share = (p.total + G - 1) / G;
-  p.slots = (int)((share + p.kchunks - 1) / p.kchunks + 1);
+  p.tiles = k.tiles;
+  p.kchunks = k.kchunks;
+  p.total = k.total;
+  p.grid = k.grid;
+  p.slots = k.slots;
   return p;
 }
 
@@ -271,8 +242,8 @@ static int dmma_launch(const DmArgs& g0, int n, double* wr, double* wi, cudaStre
   g.total = p.total;
   g.slots = p.slots;
   kern<<<p.grid, kDmThreads, smem, s>>>(g);
-  const int rgrid = grid_for((long)(CPLX ? 2 : 1) * g.b * n, 256, kNumSMs * 4);
-  k_dmma_reduce<CPLX><<<rgrid, 256, 0, s>>>(g, p.grid, wr, wi);
+  const SkGrid sg{p.tiles, p.kchunks, p.total, p.grid, p.slots};
+  launch_sk_reduce<CPLX>(g.ws, sg, n, g.b, wr, wi, s);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 

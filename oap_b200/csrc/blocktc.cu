@@ -5,26 +5,51 @@
 // lo = bf16(a - hi): 2 x 2 bytes per element, the footprint of FP32) and X
 // is split the same way into B = [X_re | X_im] (N = 2 QB columns, QB = b
 // rounded up to 8; real operators use B = [X] only).  Per 64-wide K chunk
-// the CTA accumulates in tensor memory
+// of a 128-row tile the CTA accumulates in tensor memory
 //     D1 += Ar_hi B_hi^T + Ar_hi B_lo^T + Ar_lo B_hi^T
 //     D2 += Ai_hi B_hi^T + Ai_hi B_lo^T + Ai_lo B_hi^T
-// (tcgen05.mma kind::f16, M = 128, both operands K-major in 128-byte
-// swizzled shared memory filled by cp.async, two stages), and the epilogue
-// forms W_re = D1[:, :QB] - D2[:, QB:], W_im = D1[:, QB:] + D2[:, :QB] as
-// FP64 split-K partials (summed by k_split_reduce).  The pass is HBM-bound:
-// 8 n^2 bytes of operator per pass, read once.
+// (tcgen05.mma kind::f16, M = 128, both operands K-major, 128-byte
+// swizzle), and the epilogue forms W_re = D1[:, :QB] - D2[:, QB:],
+// W_im = D1[:, QB:] + D2[:, :QB] in FP64.
+//
+// The kernel is persistent and stream-K scheduled (streamk.cuh): one CTA
+// per SM walks an equal share of the (tile, K chunk) iterations.  Warps are
+// specialised:
+//   warp 0      TMA producer: per stage one cp.async.bulk.tensor load per
+//               operator plane and per B plane, completion counted on the
+//               stage's `full` mbarrier;
+//   warp 1      MMA issuer (one lane) and TMEM owner; tcgen05.commit frees
+//               the stage (`empty`) and, at the end of a tile segment,
+//               hands the accumulator to the epilogue (`accf`);
+//   warps 2-5   epilogue: TMEM -> registers -> FP64 tile partial, then
+//               release the accumulator (`acce`).
+// Two accumulator buffers in TMEM let the epilogue of one segment overlap
+// the MMAs of the next.  A segment is at most kBtcSub K chunks of one tile;
+// the epilogue writes the first segment of a tile and adds the others in
+// FP64.  The pass is HBM-bound: 8 n^2 bytes of operator per
+// pass (complex), read once.  Every wait is bounded; a timeout sets *err.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
 #include <vector>
 
 #include "blocktc.cuh"
 #include "common.cuh"
+#include "streamk.cuh"
 #include "tc.cuh"
 
 namespace oapb {
 
 constexpr int kBtcM = 128;
 constexpr int kBtcK = 64;
-constexpr int kBtcThreads = 128;
+constexpr int kBtcThreads = 192;
 constexpr uint64_t kBtcWaitNs = 2000000000ull;
+constexpr size_t kBtcSmemBudget = 220 * 1024;
+// K chunks accumulated in FP32 (TMEM) before the epilogue adds the
+// sub-partial in FP64: 2048 columns, which keeps the FP32 accumulation
+// error of a pass independent of n.
+constexpr int kBtcSub = 32;
 
 // X (FP64 planes, b vectors of n) -> B operand hi / lo (rows: q for re,
 // QB + q for im; K = n padded to kp), zero rows / columns beyond b / n
@@ -72,37 +97,72 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(tc::smem_u32(bar)) : "memory");
+}
+// 2-D tiled TMA load (no multicast) into this CTA's shared memory
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+          "r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(tc::smem_u32(bar))
+      : "memory");
+}
+
 struct BtcArgs {
-  const __nv_bfloat16 *arh, *arl, *aih, *ail;  // operator planes, n x kp
-  const __nv_bfloat16 *bh, *bl;                // B operand, N x kp
-  int n, kp, b, QB, N, ksplit;                 // N = QB (real) or 2 QB (complex)
-  double* Wp;                                  // nsplit x 2 x b x n partials
+  CUtensorMap tm[6];  // ar_hi, ar_lo, ai_hi, ai_lo, b_hi, b_lo
+  double* ws;         // stream-K tile partials
   int* err;
+  SkGrid grid;
+  int n, b, QB, N, stages;
+  uint32_t stage_bytes;
 };
 
+// wait for `parity` of `bar`; gives up after the time limit or when another
+// role has already given up (*abort set)
+__device__ __forceinline__ bool btc_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
+  const uint64_t t0 = tc::globaltimer();
+  while (!tc::mbar_try_wait(bar, parity)) {
+    if (*abort || tc::globaltimer() - t0 > kBtcWaitNs) {
+      *abort = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
 template <bool CPLX>
-__global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(BtcArgs g) {
+__global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid_constant__ BtcArgs g) {
   extern __shared__ __align__(1024) uint8_t bsm_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  constexpr int kMaxStages = 4;
+  __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], accf[2], acce[2], done;
   __shared__ uint32_t tmem_slot;
-  __shared__ int abort_flag;
+  __shared__ volatile int abort_flag;
   constexpr int NA = CPLX ? 4 : 2;  // operator tiles per stage
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* sm = (uint8_t*)(((uintptr_t)bsm_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = tc::smem_u32(sm);
-  const int N = g.N;
+  const int N = g.N, S = g.stages;
   const uint32_t a_tile = kBtcM * 128, b_tile = (uint32_t)N * 128;
-  const uint32_t stage_bytes = ((NA * a_tile + 2 * b_tile) + 1023) & ~1023u;
-  const long i0 = (long)blockIdx.x * kBtcM;
-  const long kb = (long)blockIdx.y * g.ksplit;
-  const long ke = min((long)g.kp, kb + g.ksplit);
-  const int niter = (int)((ke - kb) / kBtcK);
-  const __nv_bfloat16* ap[4] = {g.arh, g.arl, g.aih, g.ail};
+  const long total = g.grid.total, kch = g.grid.kchunks;
+  const long it0 = sk_begin(blockIdx.x, total, gridDim.x), it1 = sk_begin(blockIdx.x + 1, total, gridDim.x);
+  const long first_tile = it0 / kch;
 
-  if (warp == 0) tc::tmem_alloc(&tmem_slot, 128);
+  if (warp == 1) tc::tmem_alloc(&tmem_slot, 256);
   if (tid == 0) {
-    tc::mbar_init(&bar[0], 1);
-    tc::mbar_init(&bar[1], 1);
+    for (int i = 0; i < S; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&accf[i], 1);
+      tc::mbar_init(&acce[i], 4);
+    }
+    tc::mbar_init(&done, 1);
     tc::fence_mbar_init();
     abort_flag = 0;
   }
@@ -110,116 +170,158 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(BtcArgs g) {
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  const uint32_t idesc = tc::idesc_bf16_f32(kBtcM, N);
 
-  auto load_stage = [&](int it, int s) {
-    const uint32_t st = sbase + s * stage_bytes;
-    const long k0 = kb + (long)it * kBtcK;
-    for (int c = tid; c < NA * kBtcM * 8; c += kBtcThreads) {
-      const int part = c / (kBtcM * 8), q = c % (kBtcM * 8);
-      const int r = q >> 3, ch = q & 7;
-      const long row = i0 + r;
-      const __nv_bfloat16* src = ap[part] + (row < g.n ? row : 0) * (long)g.kp + k0 + ch * 8;
-      tc::cp_async16(st + part * a_tile + tc::sw128(r, ch), src);
-    }
-    for (int c = tid; c < 2 * N * 8; c += kBtcThreads) {
-      const int part = c / (N * 8), q = c % (N * 8);
-      const int r = q >> 3, ch = q & 7;
-      const __nv_bfloat16* src = (part ? g.bl : g.bh) + (long)r * g.kp + k0 + ch * 8;
-      tc::cp_async16(st + NA * a_tile + part * b_tile + tc::sw128(r, ch), src);
-    }
-    tc::cp_async_commit();
-  };
-
-  bool ok = niter > 0;
-  if (ok) load_stage(0, 0);
-  for (int it = 0; ok && it < niter; ++it) {
-    const int s = it & 1;
-    if (it + 1 < niter) {
-      const int s1 = (it + 1) & 1;
-      if (it >= 1 && !tc::mbar_wait(&bar[s1], ((it - 1) >> 1) & 1, kBtcWaitNs)) atomicOr(&abort_flag, 1);
-      __syncthreads();
-      if (abort_flag) {
-        ok = false;
-        break;
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer --
+    if (lane == 0) {
+      const uint32_t tx = NA * a_tile + 2 * b_tile;
+      long it = it0;
+      for (; it < it1; ++it) {
+        const long i = it - it0;
+        const int s = (int)(i % S);
+        if (i >= S && !btc_wait(&empty[s], (uint32_t)((i / S - 1) & 1), &abort_flag)) break;
+        const uint32_t st = sbase + s * g.stage_bytes;
+        const int x = (int)((it % kch) * kBtcK), y = (int)((it / kch) * kBtcM);
+        mbar_expect_tx(&full[s], tx);
+#pragma unroll
+        for (int p = 0; p < NA; ++p) tma_load_2d(st + p * a_tile, &g.tm[p], x, y, &full[s]);
+        tma_load_2d(st + NA * a_tile, &g.tm[4], x, 0, &full[s]);
+        tma_load_2d(st + NA * a_tile + b_tile, &g.tm[5], x, 0, &full[s]);
       }
-      load_stage(it + 1, s1);
-      tc::cp_async_wait<1>();
-    } else {
-      tc::cp_async_wait<0>();
+      // no copy may still be landing in shared memory when the CTA exits:
+      // wait for the last stage loads issued (already consumed normally)
+      for (long j = (it - S > it0 ? it - S : it0); j < it; ++j) {
+        const long i = j - it0;
+        tc::mbar_wait(&full[i % S], (uint32_t)((i / S) & 1), kBtcWaitNs);
+      }
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 1) {
+    // --------------------------------------------------------------- MMA --
+    if (lane == 0) {
+      const uint32_t idesc = tc::idesc_bf16_f32(kBtcM, N);
+      long seg = 0;
+      bool ok = true;
+      for (long it = it0; ok && it < it1; ++it) {
+        const long i = it - it0;
+        const int s = (int)(i % S);
+        const long kc = it % kch;
+        const bool seg_first = it == it0 || kc % kBtcSub == 0;
+        const int buf = (int)(seg & 1);
+        if (seg_first && seg >= 2 && !btc_wait(&acce[buf], (uint32_t)((seg / 2 - 1) & 1), &abort_flag)) break;
+        if (!btc_wait(&full[s], (uint32_t)((i / S) & 1), &abort_flag)) break;
+        tc::tc_fence_after();
+        const uint32_t st = sbase + s * g.stage_bytes;
+        const uint64_t bh = tc::sdesc_k_sw128(st + NA * a_tile), bl = tc::sdesc_k_sw128(st + NA * a_tile + b_tile);
+#pragma unroll
+        for (int kk = 0; kk < kBtcK / 16; ++kk) {
+          const uint64_t off = (uint64_t)(kk * 32) >> 4;
+          const uint32_t acc0 = (seg_first && kk == 0) ? 0u : 1u;
+#pragma unroll
+          for (int p = 0; p < NA / 2; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
+            const uint64_t ah = tc::sdesc_k_sw128(st + (2 * p) * a_tile) + off;
+            const uint64_t al = tc::sdesc_k_sw128(st + (2 * p + 1) * a_tile) + off;
+            const uint32_t d = tmem + buf * 128 + p * 64;
+            tc::mma_bf16(d, ah, bh + off, idesc, acc0);
+            tc::mma_bf16(d, ah, bl + off, idesc, 1u);
+            tc::mma_bf16(d, al, bh + off, idesc, 1u);
+          }
+        }
+        tc::commit(&empty[s]);
+        if (it + 1 == it1 || (kc + 1) % kBtcSub == 0 || kc + 1 == kch) {
+          tc::commit(&accf[buf]);
+          ++seg;
+        }
+      }
+      // every MMA issued so far has completed once `done` flips
+      tc::commit(&done);
+      if (!tc::mbar_wait(&done, 0, kBtcWaitNs)) abort_flag = 1;
+    }
+  } else {
+    // ---------------------------------------------------------- epilogue --
+    const int wq = warp & 3;  // TMEM lane quarter of this warp
+    const int row = wq * 32 + lane;
+    long seg = 0;
+    for (long it = it0; it < it1; ++seg) {
+      const long tile = it / kch, kc = it % kch;
+      long kc_end = (kc / kBtcSub + 1) * kBtcSub;
+      if (kc_end > kch) kc_end = kch;
+      const long end = min(it1, tile * kch + kc_end);
+      const bool add = !(it == it0 || kc == 0);  // not the first segment of this tile in this CTA
+      it = end;
+      const int buf = (int)(seg & 1);
+      if (!btc_wait(&accf[buf], (uint32_t)((seg / 2) & 1), &abort_flag)) break;
       tc::tc_fence_after();
-      const uint32_t st = sbase + s * stage_bytes;
-      const uint64_t bh = tc::sdesc_k_sw128(st + NA * a_tile), bl = tc::sdesc_k_sw128(st + NA * a_tile + b_tile);
+      const uint32_t tl = tmem + ((uint32_t)(wq * 32) << 16) + buf * 128;
+      float d1[64], d2[64];
 #pragma unroll
-      for (int kk = 0; kk < kBtcK / 16; ++kk) {
-        const uint64_t off = (uint64_t)(kk * 32) >> 4;
-        const uint32_t first = (it > 0 || kk > 0) ? 1u : 0u;
+      for (int c = 0; c < 4; ++c) {
+        if (c * 16 < N) {
+          float v[16];
+          tmem_ld16(tl + c * 16, v);
 #pragma unroll
-        for (int p = 0; p < NA / 2; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
-          const uint64_t ah = tc::sdesc_k_sw128(st + (2 * p) * a_tile) + off;
-          const uint64_t al = tc::sdesc_k_sw128(st + (2 * p + 1) * a_tile) + off;
-          const uint32_t d = tmem + p * 64;
-          tc::mma_bf16(d, ah, bh + off, idesc, first);
-          tc::mma_bf16(d, ah, bl + off, idesc, 1u);
-          tc::mma_bf16(d, al, bh + off, idesc, 1u);
+          for (int j = 0; j < 16; ++j) d1[c * 16 + j] = v[j];
+          if (CPLX) {
+            tmem_ld16(tl + 64 + c * 16, v);
+#pragma unroll
+            for (int j = 0; j < 16; ++j) d2[c * 16 + j] = v[j];
+          }
         }
       }
-      tc::commit(&bar[s]);
-    }
-  }
-  if (ok) {
-    const int last = niter - 1;
-    if (!tc::mbar_wait(&bar[last & 1], (last >> 1) & 1, kBtcWaitNs)) atomicOr(&abort_flag, 2);
-  }
-  tc::cp_async_wait<0>();
-  __syncthreads();
-  tc::tc_fence_after();
-  if (ok && !abort_flag) {
-    const long row = i0 + warp * 32 + lane;
-    const uint32_t tl = tmem + ((uint32_t)(warp * 32) << 16);
-    float d1[64], d2[64];
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      float v[16];
-      if (c * 16 < N) {
-        tmem_ld16(tl + c * 16, v);
-#pragma unroll
-        for (int j = 0; j < 16; ++j) d1[c * 16 + j] = v[j];
-        if (CPLX) {
-          tmem_ld16(tl + 64 + c * 16, v);
-#pragma unroll
-          for (int j = 0; j < 16; ++j) d2[c * 16 + j] = v[j];
-        }
-      }
-    }
-    if (row < g.n) {
-      double* wr = g.Wp + (long)blockIdx.y * 2 * g.b * g.n;
-      double* wi = wr + (long)g.b * g.n;
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&acce[buf]);
+      constexpr int NP = CPLX ? 2 : 1;
+      double* out = g.ws + ((size_t)blockIdx.x * g.grid.slots + (tile - first_tile)) * (size_t)NP * g.b * kSkRows;
       for (int q = 0; q < g.b; ++q) {
+        double* o1 = out + (size_t)q * kSkRows + row;
+        const double v1 = CPLX ? (double)d1[q] - (double)d2[g.QB + q] : (double)d1[q];
+        *o1 = add ? *o1 + v1 : v1;
         if (CPLX) {
-          wr[(long)q * g.n + row] = (double)d1[q] - (double)d2[g.QB + q];
-          wi[(long)q * g.n + row] = (double)d1[g.QB + q] + (double)d2[q];
-        } else {
-          wr[(long)q * g.n + row] = (double)d1[q];
+          double* o2 = out + ((size_t)g.b + q) * kSkRows + row;
+          const double v2 = (double)d1[g.QB + q] + (double)d2[q];
+          *o2 = add ? *o2 + v2 : v2;
         }
       }
     }
-  } else if (tid == 0) {
-    atomicOr(g.err, abort_flag | (ok ? 0 : 4));
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 128);
+  if (abort_flag && tid == 0) atomicOr(g.err, 1);
+  if (warp == 1) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, 256);
+  }
 }
 
-size_t block_tc_smem(int N, bool cplx) {
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+// BF16 row-major plane (rows x kp, row stride kp), box 64 x box_rows, 128-byte swizzle
+static bool make_tmap(CUtensorMap* m, const __nv_bfloat16* base, int kp, int rows, int box_rows) {
+  auto enc = tmap_encoder();
+  if (!enc || ((uintptr_t)base % 16) || kp % kBtcK) return false;
+  cuuint64_t dims[2] = {(cuuint64_t)kp, (cuuint64_t)rows};
+  cuuint64_t strides[1] = {(cuuint64_t)kp * sizeof(__nv_bfloat16)};
+  cuuint32_t box[2] = {(cuuint32_t)kBtcK, (cuuint32_t)box_rows};
+  cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+static size_t btc_stage_bytes(int N, bool cplx) {
   const int NA = cplx ? 4 : 2;
-  const size_t stage = ((size_t)(NA * kBtcM * 128 + 2 * N * 128) + 1023) & ~(size_t)1023;
-  return 2 * stage + 1024;
+  return ((size_t)(NA * kBtcM * 128 + 2 * N * 128) + 1023) & ~(size_t)1023;
 }
 
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s) {
@@ -227,31 +329,45 @@ int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 
-// W partials (nsplit x 2 x b x n) of A X on the tensor cores; xbh / xbl:
-// scratch for the split block (2 x 64 x kp BF16 each).
-int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* Wp,
-                           int nsplit, int ksplit, __nv_bfloat16* xbh, __nv_bfloat16* xbl, int* err,
+static SkGrid btc_grid(int n, int kp) { return sk_grid((n + kBtcM - 1) / kBtcM, kp / kBtcK, kNumSMs); }
+
+size_t btc_workspace(int n, int kp) { return sk_workspace(btc_grid(n, kp)); }
+
+int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
+                           double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
                            cudaStream_t s) {
   const bool cplx = op.aih != nullptr;
-  if (b < 1 || b > 32 || ksplit % kBtcK != 0) return OAPB_ERR_ARG;
+  if (b < 1 || b > 32 || op.kp % kBtcK != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
   k_split_block_bf16<<<kNumSMs * 4, 256, 0, s>>>(xr, cplx ? xi : nullptr, b, QB, N, op.n, op.kp, xbh, xbl);
-  const size_t smem = block_tc_smem(N, cplx);
-  BtcArgs g{op.arh, op.arl, op.aih, op.ail, xbh, xbl, op.n, op.kp, b, QB, N, ksplit, Wp, err};
-  dim3 grid((op.n + kBtcM - 1) / kBtcM, nsplit);
-  if (cplx) {
-    if (cudaFuncSetAttribute(k_block_matvec_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return OAPB_ERR_CUDA;
-    k_block_matvec_tc<true><<<grid, kBtcThreads, smem, s>>>(g);
-  } else {
-    if (cudaFuncSetAttribute(k_block_matvec_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
-      return OAPB_ERR_CUDA;
-    k_block_matvec_tc<false><<<grid, kBtcThreads, smem, s>>>(g);
-  }
+  BtcArgs g;
+  const __nv_bfloat16* planes[4] = {op.arh, op.arl, cplx ? op.aih : op.arh, cplx ? op.ail : op.arl};
+  for (int p = 0; p < 4; ++p)
+    if (!make_tmap(&g.tm[p], planes[p], op.kp, op.n, kBtcM)) return OAPB_ERR_CUDA;
+  if (!make_tmap(&g.tm[4], xbh, op.kp, N, N) || !make_tmap(&g.tm[5], xbl, op.kp, N, N)) return OAPB_ERR_CUDA;
+  g.ws = ws;
+  g.err = err;
+  g.grid = btc_grid(op.n, op.kp);
+  g.n = op.n;
+  g.b = b;
+  g.QB = QB;
+  g.N = N;
+  const size_t stage = btc_stage_bytes(N, cplx);
+  g.stage_bytes = (uint32_t)stage;
+  g.stages = (int)(kBtcSmemBudget / stage);
+  if (g.stages > 4) g.stages = 4;
+  if (g.stages < 2) return OAPB_ERR_ARG;
+  const size_t smem = g.stages * stage + 1024;
+  auto kern = cplx ? k_block_matvec_tc<true> : k_block_matvec_tc<false>;
+  if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  kern<<<g.grid.grid, kBtcThreads, smem, s>>>(g);
+  if (cplx)
+    launch_sk_reduce<true>(ws, g.grid, op.n, b, wr, wi, s);
+  else
+    launch_sk_reduce<false>(ws, g.grid, op.n, b, wr, nullptr, s);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 

@@ -17,11 +17,14 @@ struct BtcOperator {
 // hi / lo BF16 planes of one FP64 operator plane
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s);
 
-// Split-K partials Wp[split][plane][q][row] of W = A X for b <= 32 vectors
-// (X vector-contiguous FP64); ksplit % 64 == 0; xbh / xbl hold 64 x kp BF16
-// each; *err receives timeout bits.
-int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* Wp,
-                           int nsplit, int ksplit, __nv_bfloat16* xbh, __nv_bfloat16* xbl, int* err,
+// Doubles of stream-K partial workspace for an n x n operator (b <= 32).
+size_t btc_workspace(int n, int kp);
+
+// W (planes wr / wi, vector q at offset q n) = A X for b <= 32 vectors (X
+// vector-contiguous FP64).  xbh / xbl hold 64 x kp BF16 each (the split
+// block); ws: btc_workspace() doubles; *err receives timeout bits.
+int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
+                           double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
                            cudaStream_t s);
 
 }  // namespace oapb

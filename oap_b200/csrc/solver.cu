@@ -448,7 +448,7 @@ struct oapb_arnoldi {
   int ndot = 0, nnorm = 0;
   int nvec_hess = 0;
   double* Wp = nullptr;   // split-K partials of the block matvec
-  double* wdm = nullptr;  // stream-K partials of the FP64 tensor-core pass
+  double* wdm = nullptr;  // stream-K partials of the tensor-core passes
   DmmaPlan dplan{};
   bool have_dmma = false;
   int nsplit = 1, ksplit = 0;
@@ -695,9 +695,13 @@ int alloc_blocks(oapb_arnoldi* a) {
     a->nsplit = (int)((a->n + ks - 1) / ks);
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
   }
-  if (!a->cb && dmma_plan(a->n, &a->dplan)) {
-    rc |= dalloc(&a->wdm, sizeof(double) * dmma_workspace(a->dplan));
-    a->have_dmma = true;
+  if (!a->cb) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
+    size_t need = btc_workspace(a->n, (a->n + 63) / 64 * 64);
+    if (dmma_plan(a->n, &a->dplan)) {
+      need = std::max(need, dmma_workspace(a->dplan));
+      a->have_dmma = true;
+    }
+    rc |= dalloc(&a->wdm, sizeof(double) * need);
   }
   a->nnorm = grid_for(a->n, 256, kNumSMs * 2);
   const size_t bb = sizeof(cplx) * kBmMaxB * kBmMaxB;
@@ -746,12 +750,10 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   if (fp32 && a->have_tc && a->cfg.tensor_cores) {
     BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
                    C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
-    const int nsp = (a->kp + a->ksplit - 1) / a->ksplit;
-    int rc = launch_block_matvec_tc(op, xr, xi, b, a->Wp, nsp, a->ksplit, a->xbf, a->xbf + 64 * (size_t)a->kp,
+    int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
                                     a->tcerr, a->stream);
     if (prof) prof_end(a, tm);
     if (rc) return rc;
-    k_split_reduce<C><<<grid_n((long)b * a->n), 256, 0, a->stream>>>(a->Wp, nsp, b, a->n, wr, wi);
     a->stats.block_matvecs++;
     return launch_check();
   }

@@ -1,0 +1,74 @@
+// Stream-K decomposition of a block operator pass over 128-row tiles.
+//
+// A pass is tiles x kchunks iterations.  A persistent grid of G CTAs splits
+// the iteration range into G contiguous, equal shares (CTA c owns
+// [sk_begin(c), sk_begin(c + 1))), so every SM gets the same work whatever
+// the tile count.  A CTA writes one FP64 partial per tile it touches into
+// slot (tile - first tile of the CTA); k_sk_reduce sums the partials of a
+// tile in CTA order, so the result is deterministic.
+//
+// Partial layout: ws[((c * slots + slot) * planes * b + plane * b + q) * 128 + row].
+#pragma once
+
+#include "common.cuh"
+
+namespace oapb {
+
+constexpr int kSkRows = 128;
+
+struct SkGrid {
+  long tiles, kchunks, total;
+  int grid, slots;
+};
+
+// first iteration of CTA c
+__host__ __device__ inline long sk_begin(long c, long total, int G) { return c * total / G; }
+// CTA owning iteration it: the largest c with sk_begin(c) <= it
+__host__ __device__ inline long sk_owner(long it, long total, int G) { return ((it + 1) * G + total - 1) / total - 1; }
+
+inline SkGrid sk_grid(long tiles, long kchunks, long ctas) {
+  SkGrid p;
+  p.tiles = tiles;
+  p.kchunks = kchunks;
+  p.total = tiles * kchunks;
+  const long G = ctas < p.total ? ctas : p.total;
+  p.grid = (int)G;
+  // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
+  const long share = (p.total + G - 1) / G;
+  p.slots = (int)((share + p.kchunks - 1) / p.kchunks + 1);
+  return p;
+}
+
+// doubles of partial workspace for b <= 32 vectors, two planes
+inline size_t sk_workspace(const SkGrid& p) { return (size_t)p.grid * p.slots * 2 * 32 * kSkRows; }
+
+// W[plane][q][row] = sum of the partials of the row's tile
+template <bool CPLX>
+__global__ void k_sk_reduce(const double* __restrict__ ws, SkGrid p, int n, int b, double* wr, double* wi) {
+  constexpr int NP = CPLX ? 2 : 1;
+  const long total_e = (long)NP * b * n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total_e; e += (long)gridDim.x * blockDim.x) {
+    const int row = (int)(e % n);
+    const long pq = e / n;
+    const int q = (int)(pq % b), plane = (int)(pq / b);
+    const long tile = row / kSkRows;
+    const long ilo = tile * p.kchunks;
+    const long ihi = min(p.total, ilo + p.kchunks) - 1;
+    const long c0 = sk_owner(ilo, p.total, p.grid), c1 = sk_owner(ihi, p.total, p.grid);
+    double s = 0.0;
+    for (long c = c0; c <= c1; ++c) {
+      const long slot = tile - sk_begin(c, p.total, p.grid) / p.kchunks;
+      s += ws[(((size_t)c * p.slots + slot) * NP * b + (size_t)plane * b + q) * kSkRows + row % kSkRows];
+    }
+    (plane == 0 ? wr : wi)[(long)q * n + row] = s;
+  }
+}
+
+template <bool CPLX>
+inline void launch_sk_reduce(const double* ws, const SkGrid& p, int n, int b, double* wr, double* wi,
+                             cudaStream_t s) {
+  const int rgrid = grid_for((long)(CPLX ? 2 : 1) * b * n, 256, kNumSMs * 4);
+  k_sk_reduce<CPLX><<<rgrid, 256, 0, s>>>(ws, p, n, b, wr, wi);
+}
+
+}  // namespace oapb
