@@ -202,9 +202,13 @@ typedef struct oapb_arnoldi_config {
   int32_t fallback_random; /* 1: when a solve from a user start vector does
                               not reach the goal within max_restarts, solve
                               again from the seeded random start */
-  int32_t tensor_cores;    /* mixed form: 1 (default) runs the FP32-class
-                              block passes on the tensor cores (split BF16),
-                              0 on the CUDA cores in FP32 */
+  int32_t tensor_cores;    /* 1 (default): block operator passes on the
+                              tensor cores (FP32-class passes as split BF16
+                              tcgen05, FP64 passes as DMMA); 0: CUDA cores */
+  int32_t refine;          /* mixed form, complex LM problems: 1 (default)
+                              refines the FP32-phase subspace by FP64
+                              residual + FP32-class Sylvester corrections;
+                              0 runs FP64 subspace iteration instead */
 } oapb_arnoldi_config;
 
 /* Fill defaults: rho = 1/3.14, tolerance = 1e-10, LM, FP64, random start,

@@ -40,7 +40,8 @@ class Config(C.Structure):
                 ("precision", C.c_int32), ("init", C.c_int32),
                 ("max_restarts", C.c_uint32), ("tolerance", C.c_double),
                 ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32),
-                ("fallback_random", C.c_int32), ("tensor_cores", C.c_int32)]
+                ("fallback_random", C.c_int32), ("tensor_cores", C.c_int32),
+                ("refine", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -185,7 +186,7 @@ class Arnoldi:
     def __init__(self, n, hdim, wanted, is_complex=False, sort="LM",
                  precision=PREC_FP64, tolerance=1e-10, max_restarts=300,
                  rho=1.0 / 3.14, seed=1, init=INIT_RANDOM, stream=None,
-                 profile=False, fallback_random=False, tensor_cores=True):
+                 profile=False, fallback_random=False, tensor_cores=True, refine=True):
         L = lib()
         cfg = Config()
         L.oapb_arnoldi_config_default(C.byref(cfg))
@@ -197,6 +198,7 @@ class Arnoldi:
         cfg.profile = int(bool(profile))
         cfg.fallback_random = int(bool(fallback_random))
         cfg.tensor_cores = int(bool(tensor_cores))
+        cfg.refine = int(bool(refine))
         self.cfg = cfg
         self.h = C.c_void_p()
         check(L.oapb_arnoldi_create(C.byref(self.h), C.byref(cfg), _stream(stream)),

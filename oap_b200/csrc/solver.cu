@@ -439,7 +439,9 @@ struct oapb_arnoldi {
   DevState* st = nullptr;
   int nchunk = 0, chunk = 0, nupd = 0;
   // block (multi-vector) buffers: X, W, R, E of up to kBmMaxB vectors each
-  double *Bre[4] = {nullptr, nullptr, nullptr, nullptr}, *Bim[4] = {nullptr, nullptr, nullptr, nullptr};
+  static constexpr int kBlocks = 6;
+  double *Bre[kBlocks] = {}, *Bim[kBlocks] = {};
+  cplx* thinv = nullptr;  // 1 / Ritz values of the refinement (kBmMaxB)
   cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
   cplx *britz = nullptr;
   double *best = nullptr, *bnorm = nullptr;
@@ -678,7 +680,7 @@ int alloc_blocks(oapb_arnoldi* a) {
   if (a->Bre[0]) return OAPB_OK;
   const size_t vb = sizeof(double) * (size_t)a->n * kBmMaxB;
   int rc = OAPB_OK;
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
     rc |= dalloc(&a->Bre[i], vb);
     if (a->is_c) rc |= dalloc(&a->Bim[i], vb);
   }
@@ -713,6 +715,7 @@ int alloc_blocks(oapb_arnoldi* a) {
   rc |= dalloc(&a->bQ, bb);
   rc |= dalloc(&a->bH, bb);
   rc |= dalloc(&a->britz, sizeof(cplx) * kBmMaxB);
+  rc |= dalloc(&a->thinv, sizeof(cplx) * kBmMaxB);
   rc |= dalloc(&a->best, sizeof(double) * kBmMaxB);
   rc |= dalloc(&a->bnorm, sizeof(double) * kBmMaxB * (size_t)a->nnorm);
   rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
@@ -870,7 +873,8 @@ constexpr int kMixedMinN = 8192;
 // FP64 phase: two passes; the first `skip` iterations carry no check.
 template <bool C>
 int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, double* res_out, bool from_bx,
-             int b_next = 0, double* rate_out = nullptr, int skip = 0, double* floor_out = nullptr) {
+             int b_next = 0, double* rate_out = nullptr, int skip = 0, double* floor_out = nullptr,
+             std::vector<cplx>* ritz_out = nullptr) {
   const int passes = fp32 ? 1 : 2;
   const int n = a->n, kk = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
@@ -885,11 +889,14 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   std::vector<cplx> th(b);
   // In the FP32 phase the first Rayleigh-Ritz checks carry no decision:
   // from a random block the wanted directions need several powers before
-  // the residuals mean anything, so check from iteration 5 on, every
-  // second iteration.
+  // the residuals mean anything, so the first check is at iteration 5, the
+  // second two later, and from then on at the iteration the observed
+  // contraction predicts for the goal (each check costs a small dense
+  // eigensolve and a host synchronisation).
+  unsigned next_check = 5;
   for (unsigned it = 0; it < max_it; ++it) {
     if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
-    const bool check = fp32 ? ((it >= 5 && (it % 2 == 1)) || it + 1 == max_it)
+    const bool check = fp32 ? (it >= next_check || it + 1 == max_it)
                             : ((int)it >= skip || it + 1 == max_it);
     if (!check) {
       if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
@@ -922,6 +929,19 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     a->stats.refine_iterations++;
     const bool done = mx <= tol;
     bool stop = done;
+    if (fp32) {
+      unsigned step = 2;
+      const size_t h = hist.size();
+      if (h >= 2 && !done) {
+        const double r2 = pow(mx / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2]));
+        if (r2 > 0 && r2 < 0.9) {
+          const double need = log(tol / mx) / log(r2);
+          step = need < 1 ? 1u : (unsigned)ceil(0.9 * need);
+          if (step > 6) step = 6;
+        }
+      }
+      next_check = it + step;
+    }
     if (!done && hist.size() >= 3) {
       const size_t h = hist.size();
       const double r0 = hist[h - 3], r1 = mx;
@@ -947,6 +967,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
                                                               a->Xre, a->Xim);
         }
         if (floor_out) *floor_out = mx;
+        if (ritz_out) *ritz_out = th;
         return launch_check();
       }
       a->stats.kernel_launches += 1;
@@ -959,6 +980,119 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
   }
   return OAPB_NOT_CONVERGED;
+}
+
+// D_q = (Y_q + E_q) * s_q
+__global__ void k_scale_cols(const double* __restrict__ yr, const double* __restrict__ yi, const double* __restrict__ er,
+                             const double* __restrict__ ei, const cplx* __restrict__ s, int b, int n, double* dr,
+                             double* di) {
+  const long len = (long)b * n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    const cplx v{yr[e] + er[e], yi[e] + ei[e]};
+    const cplx w = v * s[e / n];
+    dr[e] = w.re;
+    di[e] = w.im;
+  }
+}
+
+// Out = X + Y (b vectors)
+__global__ void k_block_add(const double* __restrict__ xr, const double* __restrict__ xi, const double* __restrict__ yr,
+                            const double* __restrict__ yi, int b, int n, double* outr, double* outi) {
+  const long len = (long)b * n;
+  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
+    outr[e] = xr[e] + yr[e];
+    outi[e] = xi[e] + yi[e];
+  }
+}
+
+// FP64-anchored refinement of the wanted invariant subspace (complex
+// operator, largest-magnitude wanted set, p = k vectors from a->Xre).
+// Outer step: W = A X on the FP64 operator, T = X^H W, R = W - X T,
+// Rayleigh-Ritz T S = S Theta; the pairs are accepted when every
+// ||R s_q|| / (max |theta| ||s_q||) <= tol.  Otherwise the correction D
+// (in the Ritz basis X S) of the projected Sylvester equation
+//     P A D - D Theta = -R S,   P = I - X X^H,
+// is computed by the fixed point D <- (P A D + R S) Theta^-1 on the
+// FP32-class operator (contraction about rho = |theta_{k+1}| / |theta_k|)
+// and X <- orth(X S + D).  The outer iteration converges quadratically, so
+// the FP64 operator is applied about twice per solve; the FP32-class
+// operator's rounding enters only through the small correction.
+// Returns OAPB_OK, kSlow (no quadratic progress) or an error.
+template <bool C>
+int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_outer = 3) {
+  const int n = a->n, p = a->k;
+  double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3], *D = a->Bre[4], *Tm = a->Bre[5];
+  double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3], *Di = a->Bim[4], *Tmi = a->Bim[5];
+  if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  int rc = cholqr2<C>(a, a->Xre, a->Xim, p, X, Xi, Tm, Tmi, 2);
+  if (rc) return rc;
+  std::vector<double> norms(p);
+  std::vector<cplx> th(p), thinv(p);
+  double prev = 0;
+  for (int outer = 0; outer < max_outer; ++outer) {
+    if ((rc = block_apply<C>(a, X, Xi, p, W, Wi, false))) return rc;
+    block_gram<C>(a, X, Xi, p, W, Wi, p, a->G);
+    a->stats.kernel_launches += 2;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
+    if ((rc = small_eig(a, a->G, p, p, p))) return rc;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, p, a->bY, p, p, nullptr, nullptr, 0, n, E, Ei);
+    if ((rc = col_norms<C>(a, E, Ei, p, norms.data()))) return rc;
+    DevState bs;
+    int tcerr = 0;
+    cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * p, cudaMemcpyDeviceToHost, a->stream);
+    cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
+    if (a->tcerr) cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    if ((bs.status & 2) || tcerr) return OAPB_ERR_TIMEOUT;
+    a->stats.refine_iterations++;
+    double scale = 0, mx = 0;
+    for (int q = 0; q < p; ++q) scale = fmax(scale, cabs_(th[q]));
+    if (scale == 0) return kSlow;
+    for (int q = 0; q < p; ++q) {
+      res_out[q] = norms[q] / scale;
+      mx = fmax(mx, res_out[q]);
+    }
+    if (mx <= tol) {  // Ritz vectors X S
+      ++a->stats.kernel_launches;
+      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
+                                                          a->Xim);
+      a->evals.assign(th.begin(), th.end());
+      return launch_check();
+    }
+    if (!(mx == mx) || (outer > 0 && mx > 1e-2 * prev)) return kSlow;
+    prev = mx;
+    // inner fixed point on the FP32-class operator
+    for (int q = 0; q < p; ++q) thinv[q] = cdiv(cplx{1, 0}, th[q]);
+    if (cudaMemcpyAsync(a->thinv, thinv.data(), sizeof(cplx) * p, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    // inner iterations for a correction about 100x below the goal; the
+    // observed contraction of non-normal problems is slower than rho
+    const double rho_eff = rho > 0.3 ? rho : 0.3;
+    int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff)) + 2;
+    if (J < 2) J = 2;
+    if (J > 30) J = 30;
+    const long len = (long)p * n;
+    a->stats.kernel_launches++;
+    // D = R S Theta^-1 (Y = 0)
+    if (cudaMemsetAsync(W, 0, sizeof(double) * len, a->stream) != cudaSuccess ||
+        cudaMemsetAsync(Wi, 0, sizeof(double) * len, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
+    for (int j = 0; j < J; ++j) {
+      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true))) return rc;
+      block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
+      a->stats.kernel_launches += 2;
+      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi);
+      k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
+    }
+    // X <- orth(X S + D)
+    a->stats.kernel_launches += 2;
+    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, R, Ri);
+    k_block_add<<<grid_n(len), 256, 0, a->stream>>>(R, Ri, D, Di, p, n, R, Ri);
+    if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 2))) return rc;
+  }
+  return kSlow;
 }
 
 // FP64 residuals of the k Ritz pairs in a->Xre with values a->evals, one
@@ -1076,7 +1210,18 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   k_init_block<<<grid_n((long)b * n), 256, 0, a->stream>>>(a->Xre, C ? a->Xim : nullptr, b, n, a->cfg.seed);
   double rate = 0.0, floor1 = 1e-6;
   std::vector<double> r1(k);
-  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r1.data(), false, b64, &rate, 0, &floor1);
+  std::vector<cplx> th32;
+  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r1.data(), false, b64, &rate, 0, &floor1, &th32);
+  if (st == OAPB_OK && C && a->cfg.sort == 0 && a->cfg.refine && (int)th32.size() > k && cabs_(th32[k - 1]) > 0) {
+    // largest-magnitude wanted set: the correction contracts by |theta_{k+1}| / |theta_k|
+    const double rho = cabs_(th32[k]) / cabs_(th32[k - 1]);
+    if (rho < 0.6) {
+      const int rs = refine<C>(a, tol, rho, r);
+      if (rs == OAPB_OK) return OAPB_OK;
+      if (rs != kSlow) return rs;
+      a->stats.fallbacks++;
+    }
+  }
   if (st == OAPB_OK) {
     // the FP32 phase measured the contraction per iteration: the FP64 phase
     // cannot meet the goal before about log(tol / floor) / log(rate) passes
@@ -1142,11 +1287,11 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);
-  for (int i = 0; i < 4; ++i) {
+  for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
     if (a->Bre[i]) cudaFree(a->Bre[i]);
     if (a->Bim[i]) cudaFree(a->Bim[i]);
   }
@@ -1167,6 +1312,7 @@ void oapb_arnoldi_config_default(oapb_arnoldi_config* c) {
   c->rho = 1.0 / 3.14;
   c->seed = 1;
   c->tensor_cores = 1;
+  c->refine = 1;
 }
 
 int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void* stream) {

@@ -137,14 +137,17 @@ def test_not_converged_is_reported():
     assert st == B.NOT_CONVERGED
 
 
-@pytest.mark.parametrize("n", [8192])
-def test_mixed_precision_reaches_fp64_residual(n):
-    # FP32 operator copy for the Krylov phase, FP64 refinement to 1e-10
+@pytest.mark.parametrize("n,refine", [(8192, True), (8192, False)])
+def test_mixed_precision_reaches_fp64_residual(n, refine):
+    # FP32-class phase, then the FP64-anchored Sylvester refinement (refine)
+    # or FP64 subspace iteration to 1e-10
     A = planted_complex(n, seed=n + 1, nplant=8)
-    r = solve(A, 8, 40, precision=B.PREC_MIXED, vectors=True)
+    r = solve(A, 8, 40, precision=B.PREC_MIXED, vectors=True, refine=refine)
     st = r["stats"]
     assert st["converged"] == 1 and r["res"].max() <= TOL
     assert st["matvec_fp32"] == 0 or st["refine_iterations"] >= 1
+    if refine:  # FP64 operator: about two passes (no fallback to FP64 subspace iteration)
+        assert st["fallbacks"] == 0 and st["block_matvecs"] - st["refine_iterations"] >= 1
     p = solve(A, 8, 40, precision=B.PREC_FP64)
     for lam in p["ev"]:
         assert np.min(np.abs(r["ev"] - lam)) < 1e-9 * abs(lam)
