@@ -10,8 +10,10 @@ larger than L2, so no L2 flush is needed between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-One JSON line on rank 0.  `value` is the chosen form (FP32 matvec IRAM +
-FP64 refinement) with A resident in HBM; `plain_fp64` is the plain FP64 GPU
+One JSON line on rank 0.  `value` is the chosen form (split-BF16 tcgen05
+block subspace iteration, then FP64-anchored refinement: FP64 DMMA residual
+passes and FP32-class Sylvester corrections) with A resident in HBM;
+`plain_fp64` is the plain FP64 GPU
 Arnoldi on the same problem; `e2e` runs the C-ABI entry that takes HOST
 buffers (pinned), with the 4 GiB host-to-device copy of A inside every step.
 With N > 1 GPUs every rank solves its own replica (the solve does not shard).
@@ -357,12 +359,19 @@ def run_ours(args, world, rank, local):
     # time among the timed operator kernels), HBM-bound by design
     hbm, peak_kind = peaks()
     bw = prof["block_fp32_width"] or K_WANTED
+    # algorithmic bytes per pass: the operator once (FP32-class pass: BF16
+    # hi + lo of both planes, 8 n^2; FP64 pass: 16 n^2) plus X in and W out
+    # (FP64 planes, 32 b n); flops 8 b n^2 (complex)
+    fp32_name = ("k_block_matvec_tc<complex> (split-BF16 tcgen05 block pass, %d vectors)" % bw if not args.no_tc
+                 else "k_block_matvec<float,complex> (FP32 CUDA-core block pass, %d vectors)" % bw)
+    fp64_name = ("k_block_matvec_dmma<complex> (FP64 DMMA block pass)" if not args.no_tc
+                 else "k_block_matvec<double,complex> (FP64 CUDA-core block pass)")
     kernels = {
         "k_matvec<float,complex> (FP32 complex matvec)":
             (prof["matvec_seconds"], prof["matvec_timed"], 8.0 * n * n + 16.0 * n, 8.0 * n * n),
-        "k_block_matvec<float,complex> (FP32 block matvec, %d vectors)" % bw:
+        fp32_name:
             (prof["block_fp32_seconds"], prof["block_fp32_timed"], 8.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
-        "k_block_matvec<double,complex> (FP64 block matvec)":
+        fp64_name:
             (prof["block_seconds"], prof["block_timed"], 16.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
     }
     name, (tot, cnt, alg_bytes, flops) = max(kernels.items(), key=lambda kv: kv[1][0])
@@ -387,12 +396,14 @@ def run_ours(args, world, rank, local):
         cpu = cpu_sample(ar_np, ai_np, args.cpu_seconds, n)
     out = {"metric": METRIC, "value": value, "unit": "eigensolves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs_max * 1e3 / args.steps,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3(fp32-class)+f64",
            "data": "synthetic (seeded)",
            "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
-                      "tolerance": TOL, "chosen_form": "FP32 matvec IRAM + FP64 subspace refinement",
+                      "tolerance": TOL,
+                      "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, then FP64-anchored "
+                                      "refinement: FP64 DMMA residual + FP32-class Sylvester corrections"),
                       "parallelism": "replicas" if world > 1 else "single GPU",
-                      "l2": "inputs (4 GiB FP64 + 2 GiB FP32 operator) exceed L2; no flush"},
+                      "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo operator) exceed L2; no flush"},
            "converged_steps": conv_all,
            "plain_fp64": {"value": pvalue, "ms_per_step": allmax(world, psecs) * 1e3 / psteps,
                           "steps": psteps, "restarts": pstt["restarts"], "matvecs": pstt["matvecs"]},
