@@ -7,7 +7,8 @@
 //                                   vector-contiguous FP64, b <= 32; split
 //                                   over K, partials summed by k_split_reduce
 //   k_block_dot      part = X^H Y   per row chunk (b1 x b2)
-//   k_block_reduce   G = sum of chunk partials
+//   k_block_reduce   G = sum of chunk partials (optionally followed by the
+//                    Cholesky inverse in the last block to finish)
 //   k_block_update   Out = Base - X C   (C column-major b1 x b2)
 //   k_colnorm2       per-column ||Y_q||^2 partials
 //   k_chol_inv       one warp: G = R^H R (Cholesky), Rinv = R^-1
@@ -260,81 +261,6 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
   }
 }
 
-// out[p] = sum_c part[c][p]: 32 entries per block along x, chunks split over y
-__global__ void __launch_bounds__(256) k_block_reduce(const cplx* part, int nblk, int cnt, cplx* out) {
-  __shared__ double sr[8][33], si[8][33];
-  if (blockDim.x != 32 || blockDim.y != 8) return;  // the layout below assumes 32 x 8
-  const int p = blockIdx.x * 32 + threadIdx.x;
-  double a = 0, b = 0;
-  if (p < cnt)
-    for (int c = threadIdx.y; c < nblk; c += 8) {
-      cplx v = part[(long)c * cnt + p];
-      a += v.re;
-      b += v.im;
-    }
-  sr[threadIdx.y][threadIdx.x] = a;
-  si[threadIdx.y][threadIdx.x] = b;
-  __syncthreads();
-  if (threadIdx.y == 0 && p < cnt) {
-    for (int y = 1; y < 8; ++y) {
-      a += sr[y][threadIdx.x];
-      b += si[y][threadIdx.x];
-    }
-    out[p] = cplx{a, b};
-  }
-}
-
-// Out_j = Base_j - sum_i X_i C[i + j ldc]  (Base may be null: Out = -X C, or
-// with negate = 0: Out = X C)
-template <bool CPLX>
-__global__ void k_block_update(const double* __restrict__ Xre, const double* __restrict__ Xim, int b1,
-                               const cplx* __restrict__ Cm, int ldc, int b2, const double* Bre, const double* Bim,
-                               int negate, int n, double* Ore, double* Oim) {
-  __shared__ cplx cs[kBmMaxB * kBmMaxB];
-  for (int e = threadIdx.x; e < b1 * b2; e += blockDim.x) cs[e] = Cm[(e % b1) + (long)(e / b1) * ldc];
-  __syncthreads();
-  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
-    cplx xv[kBmMaxB];
-    for (int i = 0; i < b1; ++i) xv[i] = cplx{Xre[(long)i * n + r], CPLX ? Xim[(long)i * n + r] : 0.0};
-    for (int j = 0; j < b2; ++j) {
-      cplx acc = {0, 0};
-      for (int i = 0; i < b1; ++i) acc = acc + xv[i] * cs[i + j * b1];
-      cplx o;
-      if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc;
-      else o = negate ? -acc : acc;
-      Ore[(long)j * n + r] = o.re;
-      if (CPLX) Oim[(long)j * n + r] = o.im;
-    }
-  }
-}
-
-// part[blk * b + q] = sum over the block's rows of |Y_q[r]|^2
-template <bool CPLX>
-__global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restrict__ Yim, int b, int n,
-                           double* part) {
-  __shared__ double red[kBmMaxB][8];
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int q = 0; q < b; ++q) {
-    double s = 0;
-    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
-      double a = Yre[(long)q * n + r];
-      s += a * a;
-      if (CPLX) {
-        double c = Yim[(long)q * n + r];
-        s += c * c;
-      }
-    }
-    s = warp_sum(s);
-    if (lane == 0) red[q][warp] = s;
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < b; q += blockDim.x) {
-    double s = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[q][w];
-    part[(long)blockIdx.x * b + q] = s;
-  }
-}
-
 // One warp: Cholesky G = R^H R of a b x b Hermitian positive definite matrix
 // (column-major, b <= 32), then Rinv = R^-1 (upper triangular).  status bit
 // 2 when a pivot is not positive.
@@ -343,15 +269,25 @@ __global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restr
 // row k by broadcast; shared arrays use an odd leading dimension, so the
 // per-lane column accesses are conflict-free.  The inverse is one back
 // substitution per lane (column j of R^-1).
-__global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
-  constexpr int LD = kBmMaxB + 1;
-  __shared__ cplx R[kBmMaxB * LD];
-  __shared__ cplx X[kBmMaxB * LD];
-  __shared__ double rd[kBmMaxB];   // 1 / R[j][j]
-  const int lane = threadIdx.x;
+constexpr int kCholLD = kBmMaxB + 1;
+struct CholSmem {
+  cplx R[kBmMaxB * kCholLD];
+  cplx X[kBmMaxB * kCholLD];
+  double rd[kBmMaxB];  // 1 / R[j][j]
+};
+
+// one full warp (lane = 0..31); sm in shared memory
+__device__ void warp_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, CholSmem& sm, int lane) {
+  constexpr int LD = kCholLD;
+  cplx* R = sm.R;
+  cplx* X = sm.X;
+  double* rd = sm.rd;
   const int j = lane;
   const bool own = j < b;
-  for (int e = lane; e < b * b; e += 32) R[e % b + (e / b) * LD] = G[e];
+  for (int e = lane; e < b * b; e += 32) {  // L2 loads: G may come from other blocks of the caller
+    const double* gp = reinterpret_cast<const double*>(G + e);
+    R[e % b + (e / b) * LD] = cplx{__ldcg(gp), __ldcg(gp + 1)};
+  }
   __syncwarp();
   for (int k = 0; k < b; ++k) {
     const double piv = R[k + k * LD].re;
@@ -388,5 +324,141 @@ __global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rin
     Rinv[e] = r <= c ? X[r + c * LD] : cplx{0, 0};
   }
 }
+
+__global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
+  __shared__ CholSmem sm;
+  warp_chol_inv(G, b, Rinv, status, sm, threadIdx.x);
+}
+
+// G[p] = sum_c part[c][p] (block order, deterministic): 32 entries per
+// block along x, the partials split over 32 rows of threads, four
+// independent sums per thread.  With Rinv set, the last block to finish
+// (counter *done, reset on exit) forms Rinv = R^-1 of the Cholesky factor
+// G = R^H R on one warp.
+__global__ void __launch_bounds__(1024) k_block_reduce(const cplx* __restrict__ part, int nblk, int cnt, cplx* G,
+                                                       unsigned* done, int b, cplx* Rinv, int* status) {
+  union Smem {
+    struct {
+      double sr[32][33], si[32][33];
+    } r;
+    CholSmem chol;
+  };
+  __shared__ Smem sm;
+  __shared__ bool last;
+  auto& sr = sm.r.sr;
+  auto& si = sm.r.si;
+  if (blockDim.x != 32 || blockDim.y != 32) return;  // the layout below assumes 32 x 32
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int p = blockIdx.x * 32 + tx;
+  double a[4] = {0, 0, 0, 0}, c4[4] = {0, 0, 0, 0};
+  if (p < cnt) {
+    int c = ty;
+    for (; c + 96 < nblk; c += 128) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const cplx v = part[(long)(c + 32 * u) * cnt + p];
+        a[u] += v.re;
+        c4[u] += v.im;
+      }
+    }
+    for (; c < nblk; c += 32) {
+      const cplx v = part[(long)c * cnt + p];
+      a[0] += v.re;
+      c4[0] += v.im;
+    }
+  }
+  sr[ty][tx] = (a[0] + a[1]) + (a[2] + a[3]);
+  si[ty][tx] = (c4[0] + c4[1]) + (c4[2] + c4[3]);
+  __syncthreads();
+  if (ty == 0 && p < cnt) {
+    double x = 0, y = 0;
+    for (int r = 0; r < 32; ++r) {
+      x += sr[r][tx];
+      y += si[r][tx];
+    }
+    G[p] = cplx{x, y};
+  }
+  if (!Rinv) return;
+  __threadfence();
+  __syncthreads();
+  if (tx == 0 && ty == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (ty == 0) {
+    warp_chol_inv(G, b, Rinv, status, sm.chol, tx);
+    if (tx == 0) *done = 0;
+  }
+}
+
+// Out_j = Base_j - sum_i X_i C[i + j ldc]  (Base may be null: Out = -X C, or
+// with negate = 0: Out = X C).  A block stages kUpRows rows of X (all b1
+// vectors) in shared memory; thread (row, g) forms the outputs j = g, g + 4,
+// ... of its row.  Out may alias Base (each element is read and written by
+// one thread) and X (rows are staged before any output is written).
+constexpr int kUpRows = 64;
+constexpr int kUpGroups = 4;  // 256 threads
+template <bool CPLX>
+__global__ void __launch_bounds__(256) k_block_update(const double* __restrict__ Xre, const double* __restrict__ Xim,
+                                                      int b1, const cplx* __restrict__ Cm, int ldc, int b2,
+                                                      const double* Bre, const double* Bim, int negate, int n,
+                                                      double* Ore, double* Oim) {
+  __shared__ cplx cs[kBmMaxB * kBmMaxB];
+  __shared__ double xs_r[kBmMaxB][kUpRows], xs_i[CPLX ? kBmMaxB : 1][kUpRows];
+  for (int e = threadIdx.x; e < b1 * b2; e += blockDim.x) cs[e] = Cm[(e % b1) + (long)(e / b1) * ldc];
+  const int rr = threadIdx.x % kUpRows, g = threadIdx.x / kUpRows;
+  const long nblk = (n + kUpRows - 1) / kUpRows;
+  for (long blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
+    const long r0 = blk * kUpRows;
+    __syncthreads();
+    for (int e = threadIdx.x; e < b1 * kUpRows; e += blockDim.x) {
+      const int i = e / kUpRows, q = e % kUpRows;
+      const long r = r0 + q;
+      xs_r[i][q] = r < n ? Xre[(long)i * n + r] : 0.0;
+      if (CPLX) xs_i[i][q] = r < n ? Xim[(long)i * n + r] : 0.0;
+    }
+    __syncthreads();
+    const long r = r0 + rr;
+    if (r < n) {
+      for (int j = g; j < b2; j += kUpGroups) {
+        cplx acc = {0, 0};
+        for (int i = 0; i < b1; ++i) acc = acc + cplx{xs_r[i][rr], CPLX ? xs_i[i][rr] : 0.0} * cs[i + j * b1];
+        cplx o;
+        if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc;
+        else o = negate ? -acc : acc;
+        Ore[(long)j * n + r] = o.re;
+        if (CPLX) Oim[(long)j * n + r] = o.im;
+      }
+    }
+  }
+}
+
+// part[blk * b + q] = sum over the block's rows of |Y_q[r]|^2
+template <bool CPLX>
+__global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restrict__ Yim, int b, int n,
+                           double* part) {
+  __shared__ double red[kBmMaxB][8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int q = 0; q < b; ++q) {
+    double s = 0;
+    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+      double a = Yre[(long)q * n + r];
+      s += a * a;
+      if (CPLX) {
+        double c = Yim[(long)q * n + r];
+        s += c * c;
+      }
+    }
+    s = warp_sum(s);
+    if (lane == 0) red[q][warp] = s;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < b; q += blockDim.x) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[q][w];
+    part[(long)blockIdx.x * b + q] = s;
+  }
+}
+
 
 }  // namespace oapb

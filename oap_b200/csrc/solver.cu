@@ -448,6 +448,7 @@ struct oapb_arnoldi {
   int *border = nullptr, *bstatus = nullptr;
   DevState* bst = nullptr;
   int ndot = 0, nnorm = 0;
+  unsigned* bdone = nullptr;  // arrival counter of k_block_reduce (self-resetting)
   int nvec_hess = 0;
   double* Wp = nullptr;   // split-K partials of the block matvec
   double* wdm = nullptr;  // stream-K partials of the tensor-core passes
@@ -485,6 +486,8 @@ int dalloc(P** p, size_t bytes) {
 }
 
 int grid_n(long n) { return grid_for(n, 256, kNumSMs * 8); }
+// k_block_update: one block per kUpRows rows
+int grid_up(long n) { return grid_for(n, kUpRows, kNumSMs * 8); }
 
 // Profiling: an event pair around one launch on the solver stream.
 // kind 0: single-vector dense matvec, 1: block matvec
@@ -708,6 +711,8 @@ int alloc_blocks(oapb_arnoldi* a) {
   a->nnorm = grid_for(a->n, 256, kNumSMs * 2);
   const size_t bb = sizeof(cplx) * kBmMaxB * kBmMaxB;
   rc |= dalloc(&a->bpart, bb * (size_t)a->ndot);
+  rc |= dalloc(&a->bdone, sizeof(unsigned));
+  if (a->bdone && cudaMemset(a->bdone, 0, sizeof(unsigned)) != cudaSuccess) rc |= OAPB_ERR_CUDA;
   rc |= dalloc(&a->G, bb);
   rc |= dalloc(&a->G2, bb);
   rc |= dalloc(&a->Rinv, bb);
@@ -730,7 +735,8 @@ void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, con
                 int b2, cplx* G) {
   a->stats.kernel_launches += 2;
   k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(xr, xi, b1, yr, yi, b2, a->n, a->bpart);
-  k_block_reduce<<<(b1 * b2 + 31) / 32, dim3(32, 8), 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G);
+  k_block_reduce<<<(b1 * b2 + 31) / 32, dim3(32, 32), 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G, a->bdone,
+                                                                       0, nullptr, nullptr);
 }
 
 // W = A X (b vectors); FP32 operator copy when fp32, else FP64
@@ -814,12 +820,12 @@ int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* 
   for (int pass = 0; pass < passes; ++pass) {
     double* dr = pass + 1 < passes ? tr : xr;
     double* di = pass + 1 < passes ? ti : xi;
-    block_gram<C>(a, sr, si, b, sr, si, b, a->G2);
-    ++a->stats.kernel_launches;
-    a->stats.kernel_launches += 4;
-    k_chol_inv<<<1, 32, 0, a->stream>>>(a->G2, b, a->Rinv, a->bstatus);
-    ++a->stats.kernel_launches;
-    k_block_update<C><<<grid_n(a->n), 256, 0, a->stream>>>(sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr,
+    // Gram matrix, then (last reduce block) its Cholesky factor and R^-1
+    a->stats.kernel_launches += 3;
+    k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(sr, si, b, sr, si, b, a->n, a->bpart);
+    k_block_reduce<<<(b * b + 31) / 32, dim3(32, 32), 0, a->stream>>>(a->bpart, a->ndot, b * b, a->G2, a->bdone, b,
+                                                                       a->Rinv, a->bstatus);
+    k_block_update<C><<<grid_up(a->n), 256, 0, a->stream>>>(sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr,
                                                            di);
     sr = dr;
     si = di;
@@ -904,9 +910,9 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     }
     block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
     a->stats.kernel_launches += 5;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
     if ((rc = small_eig(a, a->G, b, kk, nv))) return rc;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
     if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
     if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
@@ -963,7 +969,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
         if (bn == b) {
           if ((rc = cholqr2<C>(a, W, Wi, b, a->Xre, a->Xim, E, Ei, 1))) return rc;
         } else {
-          k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n,
+          k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n,
                                                               a->Xre, a->Xim);
         }
         if (floor_out) *floor_out = mx;
@@ -971,7 +977,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
         return launch_check();
       }
       a->stats.kernel_launches += 1;
-      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
+      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
                                                           a->Xim);
       a->evals.assign(th.begin(), th.begin() + kk);
       if ((rc = launch_check())) return rc;
@@ -1034,9 +1040,9 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     if ((rc = block_apply<C>(a, X, Xi, p, W, Wi, false))) return rc;
     block_gram<C>(a, X, Xi, p, W, Wi, p, a->G);
     a->stats.kernel_launches += 2;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
     if ((rc = small_eig(a, a->G, p, p, p))) return rc;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(R, Ri, p, a->bY, p, p, nullptr, nullptr, 0, n, E, Ei);
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, p, a->bY, p, p, nullptr, nullptr, 0, n, E, Ei);
     if ((rc = col_norms<C>(a, E, Ei, p, norms.data()))) return rc;
     DevState bs;
     int tcerr = 0;
@@ -1055,7 +1061,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     }
     if (mx <= tol) {  // Ritz vectors X S
       ++a->stats.kernel_launches;
-      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
+      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
                                                           a->Xim);
       a->evals.assign(th.begin(), th.end());
       return launch_check();
@@ -1079,16 +1085,30 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
         cudaMemsetAsync(Wi, 0, sizeof(double) * len, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
     k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
+    // Components of D inside span(X) do not move the subspace; between
+    // projections they grow at most like |theta_1| / |theta_p| per
+    // iteration, so project when that growth would pass 4x, and last.
+    double tmax = 0, tmin = 1e300;
+    for (int q = 0; q < p; ++q) {
+      tmax = fmax(tmax, cabs_(th[q]));
+      tmin = fmin(tmin, cabs_(th[q]));
+    }
+    const double spread = tmin > 0 ? tmax / tmin : 1e300;
+    int every = spread > 1.0 + 1e-12 ? (int)floor(log(4.0) / log(spread)) : J;
+    if (every < 1) every = 1;
     for (int j = 0; j < J; ++j) {
       if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true))) return rc;
-      block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
-      a->stats.kernel_launches += 2;
-      k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi);
+      if ((j + 1) % every == 0 || j + 1 == J) {
+        block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
+        a->stats.kernel_launches++;
+        k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi);
+      }
+      a->stats.kernel_launches++;
       k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
     }
     // X <- orth(X S + D)
     a->stats.kernel_launches += 2;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, R, Ri);
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, R, Ri);
     k_block_add<<<grid_n(len), 256, 0, a->stream>>>(R, Ri, D, Di, p, n, R, Ri);
     if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 2))) return rc;
   }
@@ -1112,7 +1132,7 @@ int verify(oapb_arnoldi* a, double scale, double* out) {
     if (cudaMemcpyAsync(a->G, diag.data(), sizeof(cplx) * b * b, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
     ++a->stats.kernel_launches;
-    k_block_update<C><<<grid_n(n), 256, 0, a->stream>>>(xr, xi, b, a->G, b, b, a->Bre[1], a->Bim[1], 1, n,
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(xr, xi, b, a->G, b, b, a->Bre[1], a->Bim[1], 1, n,
                                                         a->Bre[2], a->Bim[2]);
     std::vector<double> rn(b), xn(b);
     if ((rc = col_norms<C>(a, a->Bre[2], a->Bim[2], b, rn.data()))) return rc;
@@ -1287,7 +1307,7 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->bdone, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);

@@ -42,33 +42,32 @@ inline SkGrid sk_grid(long tiles, long kchunks, long ctas) {
 // doubles of partial workspace for b <= 32 vectors, two planes
 inline size_t sk_workspace(const SkGrid& p) { return (size_t)p.grid * p.slots * 2 * 32 * kSkRows; }
 
-// W[plane][q][row] = sum of the partials of the row's tile
+// W[plane][q][row] = sum of the partials of the row's tile; block (tile,
+// plane * b + q), one thread per row of the tile
 template <bool CPLX>
-__global__ void k_sk_reduce(const double* __restrict__ ws, SkGrid p, int n, int b, double* wr, double* wi) {
+__global__ void __launch_bounds__(kSkRows) k_sk_reduce(const double* __restrict__ ws, SkGrid p, int n, int b,
+                                                       double* wr, double* wi) {
   constexpr int NP = CPLX ? 2 : 1;
-  const long total_e = (long)NP * b * n;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total_e; e += (long)gridDim.x * blockDim.x) {
-    const int row = (int)(e % n);
-    const long pq = e / n;
-    const int q = (int)(pq % b), plane = (int)(pq / b);
-    const long tile = row / kSkRows;
-    const long ilo = tile * p.kchunks;
-    const long ihi = min(p.total, ilo + p.kchunks) - 1;
-    const long c0 = sk_owner(ilo, p.total, p.grid), c1 = sk_owner(ihi, p.total, p.grid);
-    double s = 0.0;
-    for (long c = c0; c <= c1; ++c) {
-      const long slot = tile - sk_begin(c, p.total, p.grid) / p.kchunks;
-      s += ws[(((size_t)c * p.slots + slot) * NP * b + (size_t)plane * b + q) * kSkRows + row % kSkRows];
-    }
-    (plane == 0 ? wr : wi)[(long)q * n + row] = s;
+  const long tile = blockIdx.x;
+  const int pq = blockIdx.y;
+  const long row = tile * kSkRows + threadIdx.x;
+  if (row >= n) return;
+  const long ilo = tile * p.kchunks;
+  const long ihi = min(p.total, ilo + p.kchunks) - 1;
+  const long c0 = sk_owner(ilo, p.total, p.grid), c1 = sk_owner(ihi, p.total, p.grid);
+  double s = 0.0;
+  for (long c = c0; c <= c1; ++c) {
+    const long slot = tile - sk_begin(c, p.total, p.grid) / p.kchunks;
+    s += ws[(((size_t)c * p.slots + slot) * NP * b + pq) * kSkRows + threadIdx.x];
   }
+  const int q = pq % b, plane = pq / b;
+  (plane == 0 ? wr : wi)[(long)q * n + row] = s;
 }
 
 template <bool CPLX>
 inline void launch_sk_reduce(const double* ws, const SkGrid& p, int n, int b, double* wr, double* wi,
                              cudaStream_t s) {
-  const int rgrid = grid_for((long)(CPLX ? 2 : 1) * b * n, 256, kNumSMs * 4);
-  k_sk_reduce<CPLX><<<rgrid, 256, 0, s>>>(ws, p, n, b, wr, wi);
+  k_sk_reduce<CPLX><<<dim3((unsigned)p.tiles, (CPLX ? 2 : 1) * b), kSkRows, 0, s>>>(ws, p, n, b, wr, wi);
 }
 
 }  // namespace oapb
