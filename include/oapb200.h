@@ -169,9 +169,13 @@ typedef enum oapb_sort {
 typedef enum oapb_precision {
   /* FP64 everywhere: the plain GPU Arnoldi. */
   OAPB_PREC_FP64 = 0,
-  /* FP32 matvec on an FP32 copy of the operator, FP64 Gram-Schmidt / Schur,
-   * then FP64 subspace refinement of the wanted pairs against the FP64
-   * operator until the residual goal holds. */
+  /* The chosen form (dense operators, n >= 8192; below that the FP64 path
+   * is faster and runs): block subspace iteration on an FP32-class copy of
+   * the operator (split-BF16 tensor-core passes, or FP32 CUDA-core passes
+   * with tensor_cores = 0), then FP64-anchored refinement (FP64 residual
+   * passes, FP32-class Sylvester corrections) until the residual goal holds
+   * against the FP64 operator; FP64 subspace iteration, FP32 IRAM and the
+   * plain FP64 IRAM as fall-backs. */
   OAPB_PREC_MIXED = 1
 } oapb_precision;
 

@@ -210,3 +210,87 @@ def iram(a, k, m, which="LM", tol=1e-10, maxit=300, rho=1.0 / 3.14,
 
 def num_threads():
     return lib().orc_num_threads()
+
+
+# --------------------------------------------------------------------------
+# The reference's own host implementation (oracle/_ref/libref.so, built from
+# the reference sources by oracle/ref/build_ref.sh where they are present):
+# used only to check this oracle against the reference's code.
+_REF = None
+
+
+def ref():
+    """ctypes handle of oracle/_ref/libref.so, or None when it is not built."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(_HERE, "_ref", "libref.so")
+        if not os.path.exists(path):
+            return None
+        _REF = C.CDLL(path)
+    return _REF
+
+
+def _planes(a):
+    a = np.asarray(a)
+    re = np.ascontiguousarray(a.real, dtype=np.float64)
+    im = np.ascontiguousarray(a.imag, dtype=np.float64) if np.iscomplexobj(a) else None
+    return re, im
+
+
+def ref_dot_product(a, b):
+    """output = a b by HostProcedures::dotProduct (a: M x K, b: K x N as numpy (rows, cols))."""
+    M, K = a.shape
+    N = b.shape[1]
+    ar, ai = _planes(a)
+    br, bi = _planes(b)
+    cplx = ai is not None or bi is not None
+    if cplx:
+        ai = ai if ai is not None else np.zeros_like(ar)
+        bi = bi if bi is not None else np.zeros_like(br)
+    o_re = np.zeros((M, N))
+    o_im = np.zeros((M, N)) if cplx else None
+    ref().ref_dot_product(M, K, N, _p(ar), _p(ai), _p(br), _p(bi), _p(o_re), _p(o_im))
+    return o_re + 1j * o_im if cplx else o_re
+
+
+def ref_transpose(a):
+    rows, cols = a.shape
+    ar, ai = _planes(a)
+    o_re = np.zeros((cols, rows))
+    o_im = np.zeros((cols, rows)) if ai is not None else None
+    ref().ref_transpose(cols, rows, _p(ar), _p(ai), _p(o_re), _p(o_im))
+    return o_re + 1j * o_im if ai is not None else o_re
+
+
+def ref_substract(a, b):
+    rows, cols = a.shape
+    ar, ai = _planes(a)
+    br, bi = _planes(b)
+    o_re = np.zeros((rows, cols))
+    o_im = np.zeros((rows, cols)) if ai is not None else None
+    ref().ref_substract(cols, rows, _p(ar), _p(ai), _p(br), _p(bi), _p(o_re), _p(o_im))
+    return o_re + 1j * o_im if ai is not None else o_re
+
+
+def ref_sum(a):
+    rows, cols = a.shape
+    ar, ai = _planes(a)
+    sre, sim = C.c_double(), C.c_double()
+    ref().ref_sum(cols, rows, _p(ar), _p(ai), C.byref(sre), C.byref(sim))
+    return sre.value, sim.value
+
+
+def ref_qr_householder(a):
+    n = a.shape[0]
+    q, r = np.zeros((n, n)), np.zeros((n, n))
+    rc = ref().ref_qr_householder(n, _p(np.ascontiguousarray(a, dtype=np.float64)), _p(q), _p(r))
+    if rc:
+        raise ValueError("n * n > 1024")
+    return q, r
+
+
+def ref_set_vector(V, column, x, length):
+    V = np.ascontiguousarray(V, dtype=np.float64).copy()
+    rows, cols = V.shape
+    ref().ref_set_vector(cols, rows, _p(V), column, _p(np.ascontiguousarray(x, dtype=np.float64)), length)
+    return V
