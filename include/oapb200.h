@@ -307,6 +307,44 @@ OAPB_EXPORT int oapb_arnoldi_apply_block(oapb_arnoldi* handle, const double* x_r
  * 642-649), recomputed in FP64 on the device. */
 OAPB_EXPORT int oapb_arnoldi_test_outcome(oapb_arnoldi* handle, uint32_t index, double* out);
 
+/* Checkpoint of the plain FP64 restart loop: the complete m-step Arnoldi
+ * factorization A V = V H + f e_m^T left on the device by the last solve
+ * that ran the plain path (OAPB_PREC_FP64, or the mixed form's last
+ * fall-back), written as one file in the reference's matrix format (the
+ * utils::ByteBuffer of oap::host::SaveMatrix, oapMatrixCpu/oapHostMatrixUtils.cpp:
+ * 1054-1113): a header (1 x 8: format 1, n, m, k, complex, restarts,
+ * matvecs, sort), V (m columns x n rows), H (m x m) and f (1 x n).  This
+ * fills the save / load / stop contract that CuHArnoldiCallbackThread
+ * declares and leaves empty (ArnoldiPackage/ArnoldiProceduresImpl.cpp:59-69).
+ * save: OAPB_ERR_ARG when the handle holds no such factorization.
+ * load: into a handle created with the same n, hdim, wanted and is_complex
+ * (OAPB_ERR_ARG otherwise). */
+OAPB_EXPORT int oapb_arnoldi_save(oapb_arnoldi* handle, const char* path);
+OAPB_EXPORT int oapb_arnoldi_load(oapb_arnoldi* handle, const char* path);
+
+/* Continue the restart loop from the loaded (or last) factorization with a
+ * fresh restart budget, then finish like oapb_arnoldi_solve (same outputs;
+ * the operator must be set).  Interrupting a solve (max_restarts), saving,
+ * loading into a new handle and resuming gives the result of the
+ * uninterrupted solve. */
+OAPB_EXPORT int oapb_arnoldi_resume(oapb_arnoldi* handle, double* eig_re, double* eig_im,
+                                    double* residuals, const oapb_mat* eigenvectors);
+
+/* ------------------------------------------------------------------------ */
+/* Matrix files in the reference's format (oap::host::WriteMatrix /           */
+/* ReadMatrix, oapMatrixCpu/oapHostMatrixUtils.cpp:974-988, 1054-1113)       */
+/* ------------------------------------------------------------------------ */
+
+/* Write device FP64 planes (im may be NULL) as one matrix file. */
+OAPB_EXPORT int oapb_mat_write(const char* path, const oapb_mat* m, void* stream);
+/* Dimensions and planes of the first matrix of a file (outputs may be NULL). */
+OAPB_EXPORT int oapb_mat_read_info(const char* path, uint32_t* columns, uint32_t* rows,
+                                   int32_t* has_re, int32_t* has_im);
+/* Read the first matrix of a file into device FP64 planes of the same
+ * dimensions (a plane absent from the file is zeroed; an imaginary plane
+ * in the file needs dst->im). */
+OAPB_EXPORT int oapb_mat_read(const char* path, const oapb_mat* dst, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Gram operator build                                                      */
 /* ------------------------------------------------------------------------ */

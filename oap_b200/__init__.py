@@ -118,6 +118,12 @@ def lib():
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
             "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
+            "oapb_arnoldi_save": [vp, C.c_char_p],
+            "oapb_arnoldi_load": [vp, C.c_char_p],
+            "oapb_arnoldi_resume": [vp, P(C.c_double), P(C.c_double), P(C.c_double), P(Mat)],
+            "oapb_mat_write": [C.c_char_p, P(Mat), vp],
+            "oapb_mat_read_info": [C.c_char_p, P(C.c_uint32), P(C.c_uint32), P(C.c_int32), P(C.c_int32)],
+            "oapb_mat_read": [C.c_char_p, P(Mat), vp],
             "oapb_param_operators": [vp, P(vp), C.c_uint32, vp, C.c_uint32, C.c_uint32, vp, vp],
             "oapb_mlp_create": [P(vp), P(C.c_uint32), C.c_uint32, C.c_uint64],
             "oapb_mlp_destroy": [vp],
@@ -245,19 +251,29 @@ class Arnoldi:
             C.c_void_p(im.data_ptr()) if im is not None else None),
             "oapb_arnoldi_set_start_vector")
 
-    def solve(self, vectors=None, allow_not_converged=False):
+    def solve(self, vectors=None, allow_not_converged=False, _entry="oapb_arnoldi_solve"):
         k = self.cfg.wanted
         er, ei, rs = (C.c_double * k)(), (C.c_double * k)(), (C.c_double * k)()
         vm = None
         if vectors is not None:
             vm = mat(vectors[0], vectors[1], columns=k, rows=self.cfg.n)
         self._cb_error = None
-        st = lib().oapb_arnoldi_solve(self.h, er, ei, rs, C.byref(vm) if vm else None)
+        st = getattr(lib(), _entry)(self.h, er, ei, rs, C.byref(vm) if vm else None)
         if st == ERR_CALLBACK and self._cb_error is not None:
-            raise OapbError(st, "oapb_arnoldi_solve") from self._cb_error
+            raise OapbError(st, _entry) from self._cb_error
         if not (st == OK or (allow_not_converged and st == NOT_CONVERGED)):
-            raise OapbError(st, "oapb_arnoldi_solve")
+            raise OapbError(st, _entry)
         return [complex(er[i], ei[i]) for i in range(k)], list(rs), st
+
+    def resume(self, vectors=None, allow_not_converged=False):
+        """Continue from the loaded (or last) factorization (oapb_arnoldi_resume)."""
+        return self.solve(vectors, allow_not_converged, _entry="oapb_arnoldi_resume")
+
+    def save(self, path):
+        check(lib().oapb_arnoldi_save(self.h, str(path).encode()), "oapb_arnoldi_save")
+
+    def load(self, path):
+        check(lib().oapb_arnoldi_load(self.h, str(path).encode()), "oapb_arnoldi_load")
 
     def solve_host(self, are, aim=None, vectors=False):
         """Dense solve from host FP64 arrays (numpy, C-contiguous)."""
@@ -368,3 +384,29 @@ def gram_build(X, fp64=False, stream=None):
                                 C.c_void_p(A64.data_ptr()) if fp64 else None, _stream(stream)),
           "oapb_gram_build")
     return A, A64
+
+
+def mat_write(path, re, im=None, stream=None):
+    """Write device FP64 planes (2-D torch tensors, rows x columns) as a matrix
+    file in the reference's format (oapb_mat_write)."""
+    m = mat(re, im)
+    check(lib().oapb_mat_write(str(path).encode(), C.byref(m), _stream(stream)), "oapb_mat_write")
+
+
+def mat_read_info(path):
+    """(columns, rows, has_re, has_im) of the first matrix of a file."""
+    c, r, hr, hi = C.c_uint32(), C.c_uint32(), C.c_int32(), C.c_int32()
+    check(lib().oapb_mat_read_info(str(path).encode(), C.byref(c), C.byref(r), C.byref(hr), C.byref(hi)),
+          "oapb_mat_read_info")
+    return c.value, r.value, bool(hr.value), bool(hi.value)
+
+
+def mat_read(path, device="cuda", stream=None):
+    """Read a matrix file into new device FP64 tensors (re, im or None)."""
+    import torch
+    c, r, hr, hi = mat_read_info(path)
+    re = torch.empty(r, c, dtype=torch.float64, device=device)
+    im = torch.empty(r, c, dtype=torch.float64, device=device) if hi else None
+    m = mat(re, im)
+    check(lib().oapb_mat_read(str(path).encode(), C.byref(m), _stream(stream)), "oapb_mat_read")
+    return re, im

@@ -36,6 +36,7 @@
 #include "blocktc.cuh"
 #include "common.cuh"
 #include "hess.cuh"
+#include "matio.cuh"
 #include "matvec.cuh"
 
 namespace oapb {
@@ -426,6 +427,9 @@ struct oapb_arnoldi {
   // vectors
   double *Vre = nullptr, *Vim = nullptr;
   double *Xre = nullptr, *Xim = nullptr;   // Ritz vectors / restart scratch (m vectors)
+  // the device holds a complete m-step factorization (V, H, f) of the
+  // plain restart loop: after a plain solve, or loaded from a checkpoint
+  bool ckpt_ready = false;
   double *fre = nullptr, *fim = nullptr, *wre = nullptr, *wim = nullptr;
   float *x32re = nullptr, *x32im = nullptr;
   double *v0re = nullptr, *v0im = nullptr;
@@ -1187,6 +1191,23 @@ int iram_start(oapb_arnoldi* a, bool user_start = true) {
   return set_fnorm(a);
 }
 
+// Ritz vectors and FP64 verification after the plain restart loop ended
+// with status st; V, H, f stay a complete factorization (checkpointable).
+template <bool C>
+int finish_plain(oapb_arnoldi* a, int st, double* r) {
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  a->ckpt_ready = true;
+  int rc = ritz_vectors<C>(a, a->k);
+  if (rc) return rc;
+  std::vector<cplx> th(a->m);
+  DevState hs;
+  if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * a->m, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if ((rc = read_state(a, &hs))) return rc;
+  a->evals.assign(th.begin(), th.begin() + a->k);
+  return verify<C>(a, hs.scale, r);
+}
+
 // The plain FP64 GPU Arnoldi: IRAM to the goal, Ritz vectors, FP64
 // verification of every wanted pair in one block pass.
 template <bool C>
@@ -1201,15 +1222,20 @@ int solve_plain(oapb_arnoldi* a, double* r) {
     if ((rc = iram_start<C>(a, false))) return rc;
     st = iram<C>(a, false, a->cfg.tolerance, a->cfg.max_restarts, 0);
   }
-  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
-  if ((rc = ritz_vectors<C>(a, a->k))) return rc;
-  std::vector<cplx> th(a->m);
-  DevState hs;
-  if (cudaMemcpyAsync(th.data(), a->ritz, sizeof(cplx) * a->m, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
-    return OAPB_ERR_CUDA;
-  if ((rc = read_state(a, &hs))) return rc;
-  a->evals.assign(th.begin(), th.begin() + a->k);
-  return verify<C>(a, hs.scale, r);
+  return finish_plain<C>(a, st, r);
+}
+
+// Continue the plain restart loop from the factorization a checkpoint
+// restored (oapb_arnoldi_load): Schur form and shifts of the restored H
+// first, then restarts as in solve_plain, with a fresh restart budget.
+template <bool C>
+int resume_plain(oapb_arnoldi* a, double* r) {
+  a->nvec_hess = a->k;
+  if (cudaMemsetAsync(a->st, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  int rc = set_fnorm(a);
+  if (rc) return rc;
+  const int st = iram<C>(a, false, a->cfg.tolerance, a->cfg.max_restarts, a->m);
+  return finish_plain<C>(a, st, r);
 }
 
 // The mixed form: (1) FP32 block subspace iteration from a seeded random
@@ -1270,7 +1296,7 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
 }
 
 template <bool C>
-int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
+int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, bool resume = false) {
   const int k = a->k;
   // The mixed form needs the dense operator and the block kernels (k <= 32),
   // and pays off only when the operator pass is HBM-bound: below n = 8192
@@ -1278,7 +1304,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
   // microseconds and the single-vector FP64 restart loop is faster.
   const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB && a->a32re &&
                      a->n >= kMixedMinN;
-  a->stats.restarts = 0;
+  if (!resume) a->stats.restarts = 0;  // a resumed solve continues the saved count
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
   a->stats.refine_iterations = 0;
@@ -1287,7 +1313,8 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res) {
   int rc = alloc_blocks(a);
   if (rc) return rc;
   std::vector<double> r(k);
-  int st = mixed ? solve_mixed<C>(a, r.data()) : solve_plain<C>(a, r.data());
+  a->ckpt_ready = false;
+  int st = resume ? resume_plain<C>(a, r.data()) : mixed ? solve_mixed<C>(a, r.data()) : solve_plain<C>(a, r.data());
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   double mx = 0;
   for (int q = 0; q < k; ++q) {
@@ -1488,8 +1515,123 @@ int oapb_arnoldi_set_start_shifts(oapb_arnoldi* a, const double* shifts, uint32_
   return OAPB_OK;
 }
 
+static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals, const oapb_mat* evecs,
+                       bool resume);
+
 int oapb_arnoldi_solve(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals,
                        const oapb_mat* evecs) {
+  return solve_entry(a, eig_re, eig_im, residuals, evecs, false);
+}
+
+int oapb_arnoldi_resume(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals,
+                        const oapb_mat* evecs) {
+  if (!a || !a->ckpt_ready) return OAPB_ERR_ARG;
+  return solve_entry(a, eig_re, eig_im, residuals, evecs, true);
+}
+
+// ------------------------------------------------------------ checkpoint --
+// File: one buffer in the reference's matrix format (matio.cuh) holding four
+// matrices: a header (1 column x 8 rows: format 1, n, m, k, complex,
+// restarts, matvecs, sort), V (m columns x n rows, the reference's basis
+// layout: column j = Krylov vector j), H (m x m, row-major (c, r) = H[r][c])
+// and f (1 column x n rows).
+int oapb_arnoldi_save(oapb_arnoldi* a, const char* path) {
+  if (!a || !path || !a->ckpt_ready) return OAPB_ERR_ARG;
+  const int n = a->n, m = a->m;
+  cudaStream_t s = a->stream;
+  std::vector<double> vre((size_t)n * m), vim(a->is_c ? (size_t)n * m : 0), fre(n), fim(a->is_c ? n : 0);
+  std::vector<cplx> H((size_t)m * m);
+  bool ok = cudaMemcpyAsync(vre.data(), a->Vre, sizeof(double) * n * m, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+            cudaMemcpyAsync(fre.data(), a->fre, sizeof(double) * n, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+            cudaMemcpyAsync(H.data(), a->H, sizeof(cplx) * m * m, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (a->is_c)
+    ok = ok && cudaMemcpyAsync(vim.data(), a->Vim, sizeof(double) * n * m, cudaMemcpyDeviceToHost, s) == cudaSuccess &&
+         cudaMemcpyAsync(fim.data(), a->fim, sizeof(double) * n, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (!ok || cudaStreamSynchronize(s) != cudaSuccess) return OAPB_ERR_CUDA;
+  std::vector<char> payload;
+  HostMat hd;
+  hd.columns = 1;
+  hd.rows = 8;
+  hd.re = {1.0, (double)n, (double)m, (double)a->k, a->is_c ? 1.0 : 0.0, (double)a->stats.restarts,
+           (double)a->stats.matvecs, (double)a->cfg.sort};
+  matio_append(payload, hd);
+  HostMat V;
+  V.columns = m;
+  V.rows = n;
+  V.has_im = a->is_c;
+  V.re.resize((size_t)n * m);
+  if (a->is_c) V.im.resize((size_t)n * m);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < n; ++i) {
+      V.re[(size_t)j + (size_t)i * m] = vre[(size_t)j * n + i];
+      if (a->is_c) V.im[(size_t)j + (size_t)i * m] = vim[(size_t)j * n + i];
+    }
+  matio_append(payload, V);
+  HostMat Hm;
+  Hm.columns = Hm.rows = m;
+  Hm.has_im = true;
+  Hm.re.resize((size_t)m * m);
+  Hm.im.resize((size_t)m * m);
+  for (int c = 0; c < m; ++c)
+    for (int r = 0; r < m; ++r) {
+      Hm.re[(size_t)c + (size_t)r * m] = H[(size_t)r + (size_t)c * m].re;
+      Hm.im[(size_t)c + (size_t)r * m] = H[(size_t)r + (size_t)c * m].im;
+    }
+  matio_append(payload, Hm);
+  HostMat F;
+  F.columns = 1;
+  F.rows = n;
+  F.has_im = a->is_c;
+  F.re = fre;
+  F.im = fim;
+  matio_append(payload, F);
+  return matio_write_file(path, payload);
+}
+
+int oapb_arnoldi_load(oapb_arnoldi* a, const char* path) {
+  if (!a || !path) return OAPB_ERR_ARG;
+  std::vector<char> payload;
+  int rc = matio_read_file(path, &payload);
+  if (rc) return rc;
+  size_t off = 0;
+  HostMat hd, V, Hm, F;
+  if (!matio_parse(payload, off, &hd) || !matio_parse(payload, off, &V) || !matio_parse(payload, off, &Hm) ||
+      !matio_parse(payload, off, &F))
+    return OAPB_ERR_ARG;
+  const int n = a->n, m = a->m;
+  if (hd.re.size() != 8 || hd.re[0] != 1.0 || hd.re[1] != n || hd.re[2] != m || hd.re[3] != a->k ||
+      (hd.re[4] != 0.0) != a->is_c)
+    return OAPB_ERR_ARG;
+  if (V.columns != (uint32_t)m || V.rows != (uint32_t)n || Hm.columns != (uint32_t)m || Hm.rows != (uint32_t)m ||
+      F.columns != 1 || F.rows != (uint32_t)n || !V.has_re || !Hm.has_re || !F.has_re ||
+      (a->is_c && (!V.has_im || !F.has_im)))
+    return OAPB_ERR_ARG;
+  std::vector<double> vre((size_t)n * m), vim(a->is_c ? (size_t)n * m : 0);
+  for (int j = 0; j < m; ++j)
+    for (int i = 0; i < n; ++i) {
+      vre[(size_t)j * n + i] = V.re[(size_t)j + (size_t)i * m];
+      if (a->is_c) vim[(size_t)j * n + i] = V.im[(size_t)j + (size_t)i * m];
+    }
+  std::vector<cplx> H((size_t)m * m);
+  for (int c = 0; c < m; ++c)
+    for (int r = 0; r < m; ++r)
+      H[(size_t)r + (size_t)c * m] =
+          cplx{Hm.re[(size_t)c + (size_t)r * m], Hm.has_im ? Hm.im[(size_t)c + (size_t)r * m] : 0.0};
+  cudaStream_t s = a->stream;
+  bool ok = cudaMemcpyAsync(a->Vre, vre.data(), sizeof(double) * n * m, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(a->fre, F.re.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+            cudaMemcpyAsync(a->H, H.data(), sizeof(cplx) * m * m, cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (a->is_c)
+    ok = ok && cudaMemcpyAsync(a->Vim, vim.data(), sizeof(double) * n * m, cudaMemcpyHostToDevice, s) == cudaSuccess &&
+         cudaMemcpyAsync(a->fim, F.im.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s) == cudaSuccess;
+  if (!ok || cudaStreamSynchronize(s) != cudaSuccess) return OAPB_ERR_CUDA;
+  a->stats.restarts = (uint32_t)hd.re[5];
+  a->ckpt_ready = true;
+  return OAPB_OK;
+}
+
+static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals, const oapb_mat* evecs,
+                       bool resume) {
   if (!a) return OAPB_ERR_ARG;
   if (!a->cb && !a->a64re) return OAPB_ERR_ARG;
   if (evecs && (evecs->columns != (uint32_t)a->k || evecs->rows != (uint32_t)a->n || evecs->dtype != OAPB_F64 ||
@@ -1498,7 +1640,8 @@ int oapb_arnoldi_solve(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
   auto t0 = std::chrono::steady_clock::now();
   a->ev_used = 0;
   a->stats.matvec_fp32 = 0;
-  int st = a->is_c ? solve_impl<true>(a, eig_re, eig_im, residuals) : solve_impl<false>(a, eig_re, eig_im, residuals);
+  int st = a->is_c ? solve_impl<true>(a, eig_re, eig_im, residuals, resume)
+                   : solve_impl<false>(a, eig_re, eig_im, residuals, resume);
   if ((st == OAPB_OK || st == OAPB_NOT_CONVERGED) && evecs) {
     const long nk = (long)a->n * a->k;
     ++a->stats.kernel_launches;

@@ -294,3 +294,13 @@ def ref_set_vector(V, column, x, length):
     rows, cols = V.shape
     ref().ref_set_vector(cols, rows, _p(V), column, _p(np.ascontiguousarray(x, dtype=np.float64)), length)
     return V
+
+
+def ref_write_matrix(path, a):
+    """The reference's oap::host::WriteMatrix of a numpy matrix (rows, columns)."""
+    rows, cols = a.shape
+    ar, ai = _planes(a)
+    rc = ref().ref_write_matrix(str(path).encode(), cols, rows, _p(ar), _p(ai))
+    if rc:
+        raise OSError("WriteMatrix failed")
+

@@ -15,7 +15,7 @@ objs=()
 for dir in oapUtils oapMath oapMatrix oapMatrixCpu; do
   for src in "$REF/$dir"/*.cpp; do
     o="$OBJ/${dir}_$(basename "$src" .cpp).o"
-    if [ ! -f "$o" ] || [ "$src" -nt "$o" ]; then
+    if [ ! -f "$o" ] || [ "$src" -nt "$o" ] || [ "$0" -nt "$o" ]; then
       g++ $FLAGS $INC -w -c "$src" -o "$o"
     fi
     objs+=("$o")

@@ -116,4 +116,17 @@ int ref_set_vector(unsigned columns, unsigned rows, double* v_re, unsigned colum
   return 0;
 }
 
+// oap::host::WriteMatrix: the reference's matrix file
+int ref_write_matrix(const char* path, unsigned columns, unsigned rows, const double* re, const double* im) {
+  math::Matrix* m = make(columns, rows, re, im);
+  const bool ok = oap::host::WriteMatrix(path, m);
+  oap::host::DeleteMatrix(m);
+  return ok ? 0 : 1;
+}
+
+// (oap::host::ReadMatrix is not wrapped: utils::Buffer::increaseReadIdx,
+// oapUtils/Buffer.h:324-327, returns no value from a value-returning
+// function, and g++ compiles the fall-through into a trap, so every read of
+// a matrix file by the reference code ends the process.)
+
 }  // extern "C"
