@@ -261,6 +261,16 @@ OAPB_EXPORT int oapb_arnoldi_set_dense_operator(oapb_arnoldi* handle, const oapb
 OAPB_EXPORT int oapb_arnoldi_set_callback(oapb_arnoldi* handle, oapb_matvec_fn fn,
                               void* user);
 
+/* Implicit Gram operator A = X X^T for FP32 images X (rows = n samples x
+ * cols pixels, row-major, device; 16-byte aligned when cols % 4 == 0):
+ * every operator application runs w = X (X^T v) in two HBM-bound passes
+ * over X, FP64 accumulation, without forming A (the reference application
+ * rebuilds the Gram on every multiplication, oap2dt3dDevice/
+ * MainAPExecutor.cpp:42-127, SquareMatrixApi.cpp:143-181).  Real solves
+ * only; runs the FP64 path.  X must stay valid during solves. */
+OAPB_EXPORT int oapb_arnoldi_set_gram_operator(oapb_arnoldi* handle, const float* X, uint32_t rows,
+                                               uint32_t cols);
+
 /* Start vector (device planes, n values each; im ignored for real solves). */
 OAPB_EXPORT int oapb_arnoldi_set_start_vector(oapb_arnoldi* handle, const double* re,
                                   const double* im);

@@ -118,6 +118,7 @@ def lib():
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
             "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
+            "oapb_arnoldi_set_gram_operator": [vp, vp, C.c_uint32, C.c_uint32],
             "oapb_arnoldi_save": [vp, C.c_char_p],
             "oapb_arnoldi_load": [vp, C.c_char_p],
             "oapb_arnoldi_resume": [vp, P(C.c_double), P(C.c_double), P(C.c_double), P(Mat)],
@@ -268,6 +269,13 @@ class Arnoldi:
     def resume(self, vectors=None, allow_not_converged=False):
         """Continue from the loaded (or last) factorization (oapb_arnoldi_resume)."""
         return self.solve(vectors, allow_not_converged, _entry="oapb_arnoldi_resume")
+
+    def set_gram_operator(self, X):
+        """Implicit Gram operator A = X X^T of a (n, pixels) FP32 device tensor."""
+        assert X.dtype.is_floating_point and X.element_size() == 4 and X.is_contiguous() and X.is_cuda
+        self._ops = (X,)
+        check(lib().oapb_arnoldi_set_gram_operator(self.h, C.c_void_p(X.data_ptr()), X.shape[0], X.shape[1]),
+              "oapb_arnoldi_set_gram_operator")
 
     def save(self, path):
         check(lib().oapb_arnoldi_save(self.h, str(path).encode()), "oapb_arnoldi_save")

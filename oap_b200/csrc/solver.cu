@@ -35,6 +35,7 @@
 #include "blockdmma.cuh"
 #include "blocktc.cuh"
 #include "common.cuh"
+#include "gramop.cuh"
 #include "hess.cuh"
 #include "matio.cuh"
 #include "matvec.cuh"
@@ -424,6 +425,10 @@ struct oapb_arnoldi {
   float* a32im = nullptr;
   oapb_matvec_fn cb = nullptr;
   void* cb_user = nullptr;
+  // implicit Gram operator A = X X^T (FP32 images, rows = n)
+  const float* gX = nullptr;
+  int gcols = 0;
+  double* gws = nullptr;
   // vectors
   double *Vre = nullptr, *Vim = nullptr;
   double *Xre = nullptr, *Xim = nullptr;   // Ritz vectors / restart scratch (m vectors)
@@ -537,6 +542,10 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
     oapb_mat v = {1u, (uint32_t)n, (void*)xre, a->is_c ? (void*)xim : nullptr, OAPB_F64};
     int rc = a->cb(&w, &v, a->cb_user, type, (void*)s);
     return rc == 0 ? OAPB_OK : OAPB_ERR_CALLBACK;
+  }
+  if (a->gX) {
+    a->stats.kernel_launches += 3;
+    return launch_gram_apply(a->gX, n, a->gcols, xre, yre, a->gws, s);
   }
   Timed tm{nullptr, nullptr, 0, fp32 ? 1 : 0, 1};
   const bool prof = prof_begin(a, tm);
@@ -704,7 +713,7 @@ int alloc_blocks(oapb_arnoldi* a) {
     a->nsplit = (int)((a->n + ks - 1) / ks);
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
   }
-  if (!a->cb) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
+  if (!a->cb && !a->gX) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
     size_t need = btc_workspace(a->n, (a->n + 63) / 64 * 64);
     if (dmma_plan(a->n, &a->dplan)) {
       need = std::max(need, dmma_workspace(a->dplan));
@@ -747,7 +756,7 @@ void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, con
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
                 bool fp32 = false) {
-  if (a->cb) {
+  if (a->cb || a->gX) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
                         C ? wi + (long)q * a->n : nullptr, false, OAPB_TYPE_EIGENVECTOR);
@@ -1302,7 +1311,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   // and pays off only when the operator pass is HBM-bound: below n = 8192
   // (at most 1 GiB of complex FP64 operator) a pass is a few tens of
   // microseconds and the single-vector FP64 restart loop is faster.
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && k <= kBmMaxB && a->a32re &&
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && k <= kBmMaxB && a->a32re &&
                      a->n >= kMixedMinN;
   if (!resume) a->stats.restarts = 0;  // a resumed solve continues the saved count
   a->stats.matvecs = 0;
@@ -1334,7 +1343,7 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->bdone, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst};
   for (void* p : bs)
     if (p) cudaFree(p);
@@ -1486,6 +1495,7 @@ int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
   a->a64re = (const double*)A->re;
   a->a64im = (const double*)A->im;
   a->cb = nullptr;
+  a->gX = nullptr;
   if (a->cfg.precision == OAPB_PREC_MIXED) return make_fp32_copy(a);
   return OAPB_OK;
 }
@@ -1494,6 +1504,21 @@ int oapb_arnoldi_set_callback(oapb_arnoldi* a, oapb_matvec_fn fn, void* user) {
   if (!a || !fn) return OAPB_ERR_ARG;
   a->cb = fn;
   a->cb_user = user;
+  a->gX = nullptr;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_set_gram_operator(oapb_arnoldi* a, const float* X, uint32_t rows, uint32_t cols) {
+  if (!a || !X || a->is_c || rows != (uint32_t)a->n || cols < 1) return OAPB_ERR_ARG;
+  if (cols % 4 == 0 && ((uintptr_t)X & 15)) return OAPB_ERR_ARG;
+  if (a->gws && a->gcols != (int)cols) {
+    cudaFree(a->gws);
+    a->gws = nullptr;
+  }
+  if (!a->gws && dalloc(&a->gws, sizeof(double) * gram_op_workspace(a->n, (int)cols))) return OAPB_ERR_NOMEM;
+  a->gX = X;
+  a->gcols = (int)cols;
+  a->cb = nullptr;
   return OAPB_OK;
 }
 
@@ -1633,7 +1658,7 @@ int oapb_arnoldi_load(oapb_arnoldi* a, const char* path) {
 static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals, const oapb_mat* evecs,
                        bool resume) {
   if (!a) return OAPB_ERR_ARG;
-  if (!a->cb && !a->a64re) return OAPB_ERR_ARG;
+  if (!a->cb && !a->gX && !a->a64re) return OAPB_ERR_ARG;
   if (evecs && (evecs->columns != (uint32_t)a->k || evecs->rows != (uint32_t)a->n || evecs->dtype != OAPB_F64 ||
                 !evecs->re))
     return OAPB_ERR_ARG;

@@ -35,3 +35,28 @@ def check_gram(rows, cols, seed, fp64=True):
 @pytest.mark.parametrize("rows,cols", [(256, 256), (128, 64), (300, 1000), (512, 4096)])
 def test_gram_tensor_cores(rows, cols):
     check_gram(rows, cols, seed=rows + cols)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,cols", [(600, 3000), (513, 1027)])
+def test_implicit_gram_operator_matches_explicit(rows, cols):
+    # w = X (X^T v) never forming A; eigenpairs vs the solve on the FP64 Gram
+    # of the same FP32 images (the implicit operator is that Gram exactly)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(rows)
+    # images = 8 separated components + noise: well-separated top spectrum
+    U = torch.randn(rows, 8, generator=g, device="cuda", dtype=torch.float64)
+    V = torch.randn(8, cols, generator=g, device="cuda", dtype=torch.float64)
+    S = torch.tensor([10.0, 8.0, 6.5, 5.0, 4.0, 3.0, 2.4, 2.0], device="cuda", dtype=torch.float64)
+    X = ((U * S) @ V / cols ** 0.5 + 0.05 * torch.randn(rows, cols, generator=g, device="cuda",
+                                                         dtype=torch.float64)).float().contiguous()
+    A64 = X.double() @ X.double().T
+    ref = B.Arnoldi(rows, 24, 6, seed=3)
+    ref.set_operator(A64.contiguous())
+    ev_ref, res_ref, st = ref.solve()
+    assert st == B.OK
+    imp = B.Arnoldi(rows, 24, 6, seed=3)
+    imp.set_gram_operator(X)
+    ev, res, st = imp.solve()
+    assert st == B.OK and max(res) <= 1e-10
+    assert np.allclose(np.array(ev).real, np.array(ev_ref).real, rtol=1e-11, atol=0)
