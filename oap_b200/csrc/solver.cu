@@ -913,11 +913,25 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   // contraction predicts for the goal (each check costs a small dense
   // eigensolve and a host synchronisation).
   unsigned next_check = 5;
+  // FP32 phase: CholeskyQR only where the block's columns could drift
+  // apart by more than 1e3 since the last one (growth per iteration = the
+  // spread |theta|max / |theta|min of the last Rayleigh-Ritz values, known
+  // from the first check on) and always right before a check; otherwise the
+  // next pass takes W itself (the span is what the iteration carries).
+  double growth = 0, drift = 1;
   for (unsigned it = 0; it < max_it; ++it) {
     if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
     const bool check = fp32 ? (it >= next_check || it + 1 == max_it)
                             : ((int)it >= skip || it + 1 == max_it);
     if (!check) {
+      const bool before_check = it + 1 >= next_check || it + 2 == max_it;
+      if (fp32 && growth > 0 && !before_check && drift * growth <= 1e3) {
+        drift *= growth;
+        std::swap(X, W);
+        if (C) std::swap(Xi, Wi);
+        continue;
+      }
+      drift = 1;
       if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
       continue;
     }
@@ -938,6 +952,15 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     double scale = 0;
     for (int q = 0; q < kk; ++q) scale = fmax(scale, cabs_(th[q]));
     if (scale == 0) scale = 1;
+    {
+      double tmin = 1e300, tmax = 0;
+      for (int q = 0; q < b; ++q) {
+        tmin = fmin(tmin, cabs_(th[q]));
+        tmax = fmax(tmax, cabs_(th[q]));
+      }
+      growth = tmin > 0 ? tmax / tmin : 0;
+      drift = 1;
+    }
     double mx = 0;
     for (int q = 0; q < kk; ++q) {
       res_out[q] = norms[q] / scale;
@@ -951,6 +974,16 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     if (fp32) {
       unsigned step = 2;
       const size_t h = hist.size();
+      if (h == 1 && !done && a->cfg.sort == OAPB_SORT_LARGEST_VALUES && b > kk) {
+        // first check: the block iteration contracts the wanted residuals
+        // by about |lambda_{b+1}| / |lambda_k| <= |theta_b| / |theta_k|
+        const double r1 = cabs_(th[b - 1]) / fmax(cabs_(th[kk - 1]), 1e-300);
+        if (r1 > 0 && r1 < 0.9) {
+          const double need = log(tol / mx) / log(r1);
+          step = need < 1 ? 1u : (unsigned)ceil(0.9 * need);
+          if (step > 6) step = 6;
+        }
+      }
       if (h >= 2 && !done) {
         const double r2 = pow(mx / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2]));
         if (r2 > 0 && r2 < 0.9) {
