@@ -974,16 +974,6 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     if (fp32) {
       unsigned step = 2;
       const size_t h = hist.size();
-      if (h == 1 && !done && a->cfg.sort == OAPB_SORT_LARGEST_VALUES && b > kk) {
-        // first check: the block iteration contracts the wanted residuals
-        // by about |lambda_{b+1}| / |lambda_k| <= |theta_b| / |theta_k|
-        const double r1 = cabs_(th[b - 1]) / fmax(cabs_(th[kk - 1]), 1e-300);
-        if (r1 > 0 && r1 < 0.9) {
-          const double need = log(tol / mx) / log(r1);
-          step = need < 1 ? 1u : (unsigned)ceil(0.9 * need);
-          if (step > 6) step = 6;
-        }
-      }
       if (h >= 2 && !done) {
         const double r2 = pow(mx / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2]));
         if (r2 > 0 && r2 < 0.9) {
