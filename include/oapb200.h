@@ -442,6 +442,15 @@ OAPB_EXPORT int oapb_mlp_adam_step(oapb_mlp* handle, float lr, void* stream);
 /* which 0: parameters, 1: gradients -> dst (host or device FP32) */
 OAPB_EXPORT int oapb_mlp_copy(oapb_mlp* handle, int which, float* dst, void* stream);
 OAPB_EXPORT int oapb_mlp_set_params(oapb_mlp* handle, const float* src, void* stream);
+/* Layer count; sizes (may be NULL) receives the nlayers + 1 sizes. */
+OAPB_EXPORT uint32_t oapb_mlp_num_layers(const oapb_mlp* handle, uint32_t* sizes);
+/* Network::save / Network::load (oapNeuralDevice/oapNetwork.h:109-111) in
+ * the reference's matrix file format: the sizes (1 x nlayers+1), then per
+ * layer its weights (in columns x out rows) and biases (1 x out).  load
+ * creates a new handle (Adam state fresh; `seed` only fills it before the
+ * weights are set). */
+OAPB_EXPORT int oapb_mlp_save(oapb_mlp* handle, const char* path);
+OAPB_EXPORT int oapb_mlp_load(oapb_mlp** handle, const char* path, uint64_t seed);
 
 #ifdef __cplusplus
 }

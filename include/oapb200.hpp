@@ -257,6 +257,114 @@ class CuHArnoldiCallback {
   bool converged_ = false;
 };
 
+/* Network (oapNeuralDevice/oapNetwork.h:27-124) over the library's BF16
+ * network: createLayer per layer (the first is the input layer), tanh hidden
+ * layers and a linear output (the activations the library computes; any
+ * other is an argument error), inputs / expected outputs as device FP32
+ * samples x features, forwardPropagation / backPropagation / updateWeights
+ * (Adam with the learning rate), train = the three in one call, the MSE of
+ * the last backPropagation, save / load in the reference's matrix file
+ * format. */
+enum class Activation { TANH, LINEAR, SIGMOID, RELU, SIN };
+
+class Network {
+ public:
+  explicit Network(uint64_t seed = 1) : seed_(seed) {}
+  ~Network() {
+    if (h_) oapb_mlp_destroy(h_);
+  }
+  Network(const Network&) = delete;
+  Network& operator=(const Network&) = delete;
+
+  /* Layer* createLayer(neurons, activation): the input layer's activation
+   * is not used; hidden layers are tanh, the last layer linear. */
+  void createLayer(uint neurons, const Activation& activation = Activation::TANH) {
+    if (h_) throw Error(OAPB_ERR_ARG, "Network::createLayer: network already built");
+    if (neurons == 0 || (activation != Activation::TANH && activation != Activation::LINEAR))
+      throw Error(OAPB_ERR_ARG, "Network::createLayer: tanh hidden layers and a linear output only");
+    sizes_.push_back(neurons);
+    acts_.push_back(activation);
+  }
+  uint getLayersCount() const { return h_ ? oapb_mlp_num_layers(h_, nullptr) + 1 : (uint)sizes_.size(); }
+  void setLearningRate(floatt lr) { lr_ = lr; }
+  floatt getLearningRate() const { return lr_; }
+
+  /* device FP32 arrays of `samples` rows */
+  void setInputs(const float* inputs, uint samples) {
+    inputs_ = inputs;
+    samples_ = samples;
+  }
+  void setExpected(const float* expected, uint samples) {
+    expected_ = expected;
+    samples_ = samples;
+  }
+  /* outputs into the device array y (samples x outputs) */
+  void forwardPropagation(float* y) {
+    build();
+    check(oapb_mlp_forward(h_, inputs_, samples_, y, nullptr), "Network::forwardPropagation");
+  }
+  void backPropagation() {
+    build();
+    check(oapb_mlp_backward(h_, inputs_, expected_, samples_, &mse_, nullptr), "Network::backPropagation");
+  }
+  void updateWeights() {
+    build();
+    check(oapb_mlp_adam_step(h_, (float)lr_, nullptr), "Network::updateWeights");
+  }
+  /* one step on (inputs, expected); true while it ran */
+  bool train(const float* inputs, const float* expected, uint samples) {
+    setInputs(inputs, samples);
+    setExpected(expected, samples);
+    backPropagation();
+    updateWeights();
+    return true;
+  }
+  /* 1 / (2 samples) sum (y - expected)^2 of the last backPropagation */
+  floatt calculateMSE() const { return mse_; }
+
+  void getHostWeights(std::vector<float>& weights) {
+    build();
+    weights.resize(oapb_mlp_num_params(h_));
+    check(oapb_mlp_copy(h_, 0, weights.data(), nullptr), "Network::getHostWeights");
+  }
+  void setHostWeights(const std::vector<float>& weights) {
+    build();
+    if (weights.size() != oapb_mlp_num_params(h_)) throw Error(OAPB_ERR_ARG, "Network::setHostWeights: size");
+    check(oapb_mlp_set_params(h_, weights.data(), nullptr), "Network::setHostWeights");
+  }
+
+  void save(const std::string& path) {
+    build();
+    check(oapb_mlp_save(h_, path.c_str()), "Network::save");
+  }
+  static Network* load(const std::string& path, uint64_t seed = 1) {
+    Network* net = new Network(seed);
+    const int st = oapb_mlp_load(&net->h_, path.c_str(), seed);
+    if (st != OAPB_OK) {
+      delete net;
+      throw Error(st, "Network::load");
+    }
+    return net;
+  }
+
+ private:
+  void build() {
+    if (h_) return;
+    if (sizes_.size() < 2) throw Error(OAPB_ERR_ARG, "Network: fewer than two layers");
+    check(oapb_mlp_create(&h_, sizes_.data(), (uint32_t)sizes_.size() - 1, seed_), "Network (create)");
+  }
+
+  uint64_t seed_;
+  oapb_mlp* h_ = nullptr;
+  std::vector<uint32_t> sizes_;
+  std::vector<Activation> acts_;
+  floatt lr_ = 1e-3;
+  const float* inputs_ = nullptr;
+  const float* expected_ = nullptr;
+  uint samples_ = 0;
+  double mse_ = 0;
+};
+
 }  // namespace oapb
 
 #endif  // OAPB200_HPP

@@ -119,6 +119,8 @@ def lib():
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
             "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
             "oapb_arnoldi_set_gram_operator": [vp, vp, C.c_uint32, C.c_uint32],
+            "oapb_mlp_save": [vp, C.c_char_p],
+            "oapb_mlp_load": [P(vp), C.c_char_p, C.c_uint64],
             "oapb_arnoldi_save": [vp, C.c_char_p],
             "oapb_arnoldi_load": [vp, C.c_char_p],
             "oapb_arnoldi_resume": [vp, P(C.c_double), P(C.c_double), P(C.c_double), P(Mat)],
@@ -142,6 +144,8 @@ def lib():
             fn.restype = C.c_int
         L.oapb_mlp_num_params.argtypes = [vp]
         L.oapb_mlp_num_params.restype = C.c_uint64
+        L.oapb_mlp_num_layers.restype = C.c_uint32
+        L.oapb_mlp_num_layers.argtypes = [vp, vp]
         L.oapb_arnoldi_config_default.argtypes = [P(Config)]
         L.oapb_arnoldi_config_default.restype = None
         _LIB = L

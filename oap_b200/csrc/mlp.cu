@@ -22,6 +22,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "matio.cuh"
 
 namespace oapb {
 
@@ -401,6 +402,76 @@ int oapb_mlp_set_params(oapb_mlp* h, const float* src, void* stream) {
     return OAPB_ERR_CUDA;
   k_to_bf16<<<grid_for(h->nparam, 256), 256, 0, s>>>(h->w, h->nparam, h->wb);
   if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) return OAPB_ERR_CUDA;
+  return OAPB_OK;
+}
+
+uint32_t oapb_mlp_num_layers(const oapb_mlp* h, uint32_t* sizes) {
+  if (!h) return 0;
+  if (sizes)
+    for (int i = 0; i <= h->nl; ++i) sizes[i] = (uint32_t)h->sz[i];
+  return (uint32_t)h->nl;
+}
+
+// File (the reference's matrix format, matio.cuh): sizes (1 column x
+// nlayers + 1 rows), then per layer its weights (in columns x out rows) and
+// biases (1 column x out rows), FP64 values of the FP32 master weights.
+int oapb_mlp_save(oapb_mlp* h, const char* path) {
+  if (!h || !path) return OAPB_ERR_ARG;
+  std::vector<float> p((size_t)h->nparam);
+  int rc = oapb_mlp_copy(h, 0, p.data(), nullptr);
+  if (rc) return rc;
+  std::vector<char> payload;
+  HostMat sz;
+  sz.columns = 1;
+  sz.rows = (uint32_t)(h->nl + 1);
+  for (int v : h->sz) sz.re.push_back((double)v);
+  matio_append(payload, sz);
+  for (int l = 0; l < h->nl; ++l) {
+    HostMat W, bv;
+    W.columns = (uint32_t)h->sz[l];
+    W.rows = (uint32_t)h->sz[l + 1];
+    W.re.assign(p.begin() + h->woff[l], p.begin() + h->woff[l] + (long)W.columns * W.rows);
+    bv.columns = 1;
+    bv.rows = W.rows;
+    bv.re.assign(p.begin() + h->boff[l], p.begin() + h->boff[l] + W.rows);
+    matio_append(payload, W);
+    matio_append(payload, bv);
+  }
+  return matio_write_file(path, payload);
+}
+
+int oapb_mlp_load(oapb_mlp** out, const char* path, uint64_t seed) {
+  if (!out || !path) return OAPB_ERR_ARG;
+  std::vector<char> payload;
+  int rc = matio_read_file(path, &payload);
+  if (rc) return rc;
+  size_t off = 0;
+  HostMat sz;
+  if (!matio_parse(payload, off, &sz) || sz.columns != 1 || sz.rows < 2 || sz.rows > 9) return OAPB_ERR_ARG;
+  std::vector<uint32_t> sizes;
+  for (double v : sz.re) {
+    if (!(v >= 1 && v < 1e9)) return OAPB_ERR_ARG;
+    sizes.push_back((uint32_t)v);
+  }
+  const int nl = (int)sizes.size() - 1;
+  std::vector<HostMat> Ws(nl), bs(nl);
+  for (int l = 0; l < nl; ++l) {
+    if (!matio_parse(payload, off, &Ws[l]) || !matio_parse(payload, off, &bs[l])) return OAPB_ERR_ARG;
+    if (Ws[l].columns != sizes[l] || Ws[l].rows != sizes[l + 1] || bs[l].columns != 1 || bs[l].rows != sizes[l + 1])
+      return OAPB_ERR_ARG;
+  }
+  oapb_mlp* h = nullptr;
+  if ((rc = oapb_mlp_create(&h, sizes.data(), (uint32_t)nl, seed))) return rc;
+  std::vector<float> p((size_t)h->nparam);
+  for (int l = 0; l < nl; ++l) {
+    for (size_t e = 0; e < Ws[l].re.size(); ++e) p[h->woff[l] + e] = (float)Ws[l].re[e];
+    for (size_t e = 0; e < bs[l].re.size(); ++e) p[h->boff[l] + e] = (float)bs[l].re[e];
+  }
+  if ((rc = oapb_mlp_set_params(h, p.data(), nullptr))) {
+    oapb_mlp_destroy(h);
+    return rc;
+  }
+  *out = h;
   return OAPB_OK;
 }
 

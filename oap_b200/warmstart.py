@@ -140,6 +140,23 @@ class Net:
         check(lib().oapb_mlp_copy(self.h, 1, C.c_void_p(out.ctypes.data), None), "oapb_mlp_copy")
         return out
 
+    def save(self, path):
+        """Network::save in the reference's matrix file format (oapb_mlp_save)."""
+        check(lib().oapb_mlp_save(self.h, str(path).encode()), "oapb_mlp_save")
+
+    @classmethod
+    def load(cls, path, seed=1):
+        """Network::load (oapb_mlp_load)."""
+        net = cls.__new__(cls)
+        net.h = C.c_void_p()
+        check(lib().oapb_mlp_load(C.byref(net.h), str(path).encode(), seed), "oapb_mlp_load")
+        n = lib().oapb_mlp_num_layers(net.h, None)
+        sizes = (C.c_uint32 * (n + 1))()
+        lib().oapb_mlp_num_layers(net.h, sizes)
+        net.sizes = list(sizes)
+        net.nparam = int(lib().oapb_mlp_num_params(net.h))
+        return net
+
     def set_params(self, p):
         p = np.ascontiguousarray(p, dtype=np.float32)
         check(lib().oapb_mlp_set_params(self.h, C.c_void_p(p.ctypes.data), None), "oapb_mlp_set_params")

@@ -46,6 +46,16 @@ static int cpu_tests() {
     threw = e.status() == OAPB_ERR_ARG;
   }
   EXPECT(threw);
+  // Network: only tanh hidden layers and a linear output exist
+  oapb::Network net;
+  net.createLayer(4);
+  threw = false;
+  try {
+    net.createLayer(8, oapb::Activation::SIGMOID);
+  } catch (const oapb::Error& e) {
+    threw = e.status() == OAPB_ERR_ARG;
+  }
+  EXPECT(threw);
   return failures;
 }
 
@@ -165,6 +175,54 @@ static int gpu_tests() {
       EXPECT(arnoldi.testOutcome(i) <= 1e-10);
     }
     std::printf("mode %d: lambda_1 = %.12f%+.12fi, residual %.2e\n", mode, re[0], im[0], arnoldi.residuals()[0]);
+  }
+  // Network (oapNetwork.h names): learn y = M x on 256 samples, save, load
+  {
+    const int ni = 6, no = 3, S = 256;
+    std::vector<float> X(S * ni), Y(S * no), M(no * ni);
+    for (auto& v : M) v = (float)(0.3 * nd(rng));
+    for (int s = 0; s < S; ++s) {
+      for (int i = 0; i < ni; ++i) X[s * ni + i] = (float)nd(rng);
+      for (int o = 0; o < no; ++o) {
+        float acc = 0;
+        for (int i = 0; i < ni; ++i) acc += M[o * ni + i] * X[s * ni + i];
+        Y[s * no + o] = acc;
+      }
+    }
+    float *dX, *dY, *dOut1, *dOut2;
+    cudaMalloc(&dX, sizeof(float) * X.size());
+    cudaMalloc(&dY, sizeof(float) * Y.size());
+    cudaMalloc(&dOut1, sizeof(float) * Y.size());
+    cudaMalloc(&dOut2, sizeof(float) * Y.size());
+    cudaMemcpy(dX, X.data(), sizeof(float) * X.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(dY, Y.data(), sizeof(float) * Y.size(), cudaMemcpyHostToDevice);
+    oapb::Network net(7);
+    net.createLayer(ni);
+    net.createLayer(32, oapb::Activation::TANH);
+    net.createLayer(no, oapb::Activation::LINEAR);
+    net.setLearningRate(3e-3);
+    net.train(dX, dY, S);
+    const double first = net.calculateMSE();
+    for (int step = 0; step < 400; ++step) net.train(dX, dY, S);
+    const double last = net.calculateMSE();
+    std::printf("network mse %.4g -> %.4g\n", first, last);
+    EXPECT(last < 0.1 * first);
+    EXPECT(net.getLayersCount() == 3);
+    net.setInputs(dX, S);
+    net.forwardPropagation(dOut1);
+    net.save("/tmp/oapb_shim_network.bin");
+    oapb::Network* back = oapb::Network::load("/tmp/oapb_shim_network.bin");
+    back->setInputs(dX, S);
+    back->forwardPropagation(dOut2);
+    std::vector<float> o1(Y.size()), o2(Y.size());
+    cudaMemcpy(o1.data(), dOut1, sizeof(float) * o1.size(), cudaMemcpyDeviceToHost);
+    cudaMemcpy(o2.data(), dOut2, sizeof(float) * o2.size(), cudaMemcpyDeviceToHost);
+    EXPECT(o1 == o2);
+    delete back;
+    cudaFree(dX);
+    cudaFree(dY);
+    cudaFree(dOut1);
+    cudaFree(dOut2);
   }
   return failures;
 }

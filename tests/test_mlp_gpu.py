@@ -95,3 +95,18 @@ def test_learned_warm_start_on_parametric_family():
           "mean overlap pred", np.mean(overlap_pred), "random", np.mean(overlap_rand))
     # the network has learned the wanted subspace far beyond chance
     assert np.mean(overlap_pred) > 3 * np.mean(overlap_rand)
+
+
+@pytest.mark.gpu
+def test_network_save_load_round_trip(tmp_path):
+    # Network::save / load in the reference's matrix format: same outputs
+    from oap_b200 import warmstart as W
+    net = W.Net([5, 16, 3], seed=4)
+    x = torch.randn(64, 5, device="cuda")
+    y1 = net.forward(x)
+    p = tmp_path / "net.bin"
+    net.save(p)
+    back = W.Net.load(p)
+    assert back.sizes == [5, 16, 3]
+    assert torch.equal(back.forward(x), y1)
+    assert B.mat_read_info(p) == (1, 3, True, False)   # first record: the layer sizes
