@@ -368,6 +368,18 @@ OAPB_EXPORT int oapb_mat_read(const char* path, const oapb_mat* dst, void* strea
 OAPB_EXPORT int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols,
                                 float* A, double* A64, void* stream);
 
+/* Image ingestion: `count` decoded RGB8 images of `pixels` pixels each
+ * (rgb: count x pixels x 3 bytes, on the host when rgb_on_host, else on the
+ * device) -> X (device FP32, count x pixels, row-major), each pixel
+ * (r << 16 | g << 8 | b) / 0xFFFFFF as the reference's
+ * Image::convertRgbToFloatt (oapAppUtils/Image.cpp:155-180); X is the
+ * reference's DataLoader matrix (image i = column i,
+ * oapAppUtils/DataLoader.cpp:47-66) transposed, the layout of
+ * oapb_gram_build and oapb_arnoldi_set_gram_operator.  Synchronises
+ * `stream`. */
+OAPB_EXPORT int oapb_images_to_matrix(const uint8_t* rgb, int32_t rgb_on_host, uint32_t count,
+                                      uint32_t pixels, float* X, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Batched solver: many independent small problems in one persistent launch */
 /* ------------------------------------------------------------------------ */

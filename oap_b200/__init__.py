@@ -119,6 +119,7 @@ def lib():
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
             "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
             "oapb_arnoldi_set_gram_operator": [vp, vp, C.c_uint32, C.c_uint32],
+            "oapb_images_to_matrix": [vp, C.c_int32, C.c_uint32, C.c_uint32, vp, vp],
             "oapb_mlp_save": [vp, C.c_char_p],
             "oapb_mlp_load": [P(vp), C.c_char_p, C.c_uint64],
             "oapb_arnoldi_save": [vp, C.c_char_p],
@@ -422,3 +423,22 @@ def mat_read(path, device="cuda", stream=None):
     m = mat(re, im)
     check(lib().oapb_mat_read(str(path).encode(), C.byref(m), _stream(stream)), "oapb_mat_read")
     return re, im
+
+
+def images_to_matrix(rgb, stream=None):
+    """(count, pixels, 3) uint8 RGB images (numpy on the host or a torch
+    device tensor) -> X (count, pixels) FP32 device tensor, each pixel
+    (r << 16 | g << 8 | b) / 0xFFFFFF (oapb_images_to_matrix)."""
+    import numpy as np
+    import torch
+    count, pixels = int(rgb.shape[0]), int(rgb.shape[1])
+    X = torch.empty(count, pixels, dtype=torch.float32, device="cuda")
+    if isinstance(rgb, np.ndarray):
+        a = np.ascontiguousarray(rgb, dtype=np.uint8)
+        ptr, host = C.c_void_p(a.ctypes.data), 1
+    else:
+        a = rgb.contiguous()
+        ptr, host = C.c_void_p(a.data_ptr()), 0
+    check(lib().oapb_images_to_matrix(ptr, host, count, pixels, C.c_void_p(X.data_ptr()), _stream(stream)),
+          "oapb_images_to_matrix")
+    return X

@@ -80,6 +80,65 @@ __device__ __forceinline__ void givens(cplx x, cplx y, cplx& p, cplx& q) {
   q = {y.re * ir, -y.im * ir};
 }
 
+// FP32 complex (the working type of the FP32 small dense eigensolver)
+struct cplxf {
+  float re, im;
+};
+__host__ __device__ __forceinline__ cplxf operator+(cplxf a, cplxf b) { return {a.re + b.re, a.im + b.im}; }
+__host__ __device__ __forceinline__ cplxf operator-(cplxf a, cplxf b) { return {a.re - b.re, a.im - b.im}; }
+__host__ __device__ __forceinline__ cplxf operator-(cplxf a) { return {-a.re, -a.im}; }
+__host__ __device__ __forceinline__ cplxf operator*(cplxf a, cplxf b) {
+  return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re};
+}
+__host__ __device__ __forceinline__ cplxf operator*(float s, cplxf a) { return {s * a.re, s * a.im}; }
+__host__ __device__ __forceinline__ cplxf conj(cplxf a) { return {a.re, -a.im}; }
+__host__ __device__ __forceinline__ float abs2(cplxf a) { return a.re * a.re + a.im * a.im; }
+__host__ __device__ __forceinline__ float cabs_(cplxf a) { return hypotf(a.re, a.im); }
+__host__ __device__ __forceinline__ cplxf cdiv(cplxf a, cplxf b) {
+  if (fabsf(b.re) >= fabsf(b.im)) {
+    float r = b.im / b.re, d = b.re + b.im * r;
+    return {(a.re + a.im * r) / d, (a.im - a.re * r) / d};
+  } else {
+    float r = b.re / b.im, d = b.re * r + b.im;
+    return {(a.re * r + a.im) / d, (a.im * r - a.re) / d};
+  }
+}
+__host__ __device__ __forceinline__ cplxf csqrt_(cplxf z) {
+  float r = hypotf(z.re, z.im);
+  if (r == 0) return {0, 0};
+  float t = sqrtf(0.5f * (r + fabsf(z.re)));
+  if (z.re >= 0) return {t, z.im / (2 * t)};
+  return {fabsf(z.im) / (2 * t), z.im >= 0 ? t : -t};
+}
+__device__ __forceinline__ void givens(cplxf x, cplxf y, cplxf& p, cplxf& q) {
+  float r2 = x.re * x.re + x.im * x.im + y.re * y.re + y.im * y.im;
+  if (r2 == 0) {
+    p = {1, 0};
+    q = {0, 0};
+    return;
+  }
+  if (!(r2 < 1e36f) || r2 < 1e-36f) {
+    const float s = fmaxf(fmaxf(fabsf(x.re), fabsf(x.im)), fmaxf(fabsf(y.re), fabsf(y.im)));
+    const float is = 1.0f / s;
+    x = is * x;
+    y = is * y;
+    r2 = x.re * x.re + x.im * x.im + y.re * y.re + y.im * y.im;
+  }
+  const float ir = rsqrtf(r2);
+  p = {x.re * ir, -x.im * ir};
+  q = {y.re * ir, -y.im * ir};
+}
+
+// conversions between the FP64 storage type and a working type
+template <typename Cx>
+__host__ __device__ __forceinline__ Cx cx_from(cplx v);
+template <>
+__host__ __device__ __forceinline__ cplx cx_from<cplx>(cplx v) { return v; }
+template <>
+__host__ __device__ __forceinline__ cplxf cx_from<cplxf>(cplx v) { return {(float)v.re, (float)v.im}; }
+__host__ __device__ __forceinline__ cplx cx_to(cplx v) { return v; }
+__host__ __device__ __forceinline__ cplx cx_to(cplxf v) { return {(double)v.re, (double)v.im}; }
+
 // ------------------------------------------------------------ warp reduce --
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

@@ -77,6 +77,21 @@ __host__ __device__ __forceinline__ size_t hess_ws_cplx(int m) {
   return 2 * (size_t)hess_ld(m) * m + hess_scratch_cplx(m);
 }
 
+// precision constants of the working type
+template <typename R>
+struct HessK;
+template <>
+struct HessK<double> {
+  static constexpr double eps = 2.220446049250313e-16, tiny = 1e-300, big = 1e150, unbig = 1e-150;
+};
+template <>
+struct HessK<float> {
+  static constexpr float eps = 1.1920929e-7f, tiny = 1e-37f, big = 1e30f, unbig = 1e-30f;
+};
+
+__device__ __forceinline__ double warp_sum_t(double v) { return warp_sum(v); }
+__device__ __forceinline__ float warp_sum_t(float v) { return warp_sumf(v); }
+
 #define TT_(i, j) T[(i) + (j) * ld]
 #define ZZ_(i, j) Z[(i) + (j) * ld]
 
@@ -93,20 +108,26 @@ __device__ __forceinline__ double sort_key(cplx v, int which) {
 
 // |re| + |im| (LAPACK's CABS1): the deflation test only needs a norm-equivalent
 __device__ __forceinline__ double cabs1(cplx a) { return fabs(a.re) + fabs(a.im); }
+__device__ __forceinline__ float cabs1(cplxf a) { return fabsf(a.re) + fabsf(a.im); }
 
-__device__ __forceinline__ bool negligible(const cplx* T, int ld, int l) {
-  const double eps = 2.220446049250313e-16;
-  double s = cabs1(TT_(l - 1, l - 1)) + cabs1(TT_(l, l));
-  if (s == 0) s = 1e-300;
-  return cabs1(TT_(l, l - 1)) <= eps * s;
+template <typename Cx>
+__device__ __forceinline__ bool negligible(const Cx* T, int ld, int l) {
+  using R = decltype(Cx::re);
+  R s = cabs1(TT_(l - 1, l - 1)) + cabs1(TT_(l, l));
+  if (s == 0) s = HessK<R>::tiny;
+  return cabs1(TT_(l, l - 1)) <= HessK<R>::eps * s;
 }
 
 __device__ __forceinline__ cplx shfl_c(cplx v, int src) {
   return cplx{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
 }
+__device__ __forceinline__ cplxf shfl_c(cplxf v, int src) {
+  return cplxf{__shfl_sync(0xffffffffu, v.re, src), __shfl_sync(0xffffffffu, v.im, src)};
+}
 
 // The largest l in [1, h] with T[l][l-1] negligible, else 0 (all lanes).
-static __device__ int find_split(const cplx* T, int ld, int h, int lane) {
+template <typename Cx>
+static __device__ int find_split(const Cx* T, int ld, int h, int lane) {
   for (int base = h; base >= 1; base -= 32) {
     const int l = base - lane;
     const bool f = l >= 1 && negligible(T, ld, l);
@@ -119,10 +140,11 @@ static __device__ int find_split(const cplx* T, int ld, int h, int lane) {
 // One single-shift QR sweep on the active window [l, h] of Hessenberg T,
 // applied to whole rows / columns of T; Z <- Z G_l^H ... G_{h-1}^H at the end
 // of the sweep.  rot: 2 m cplx of scratch.
-static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int ld, int l, int h, cplx mu, cplx* rot, int lane) {
-  cplx x = TT_(l, l) - mu, y = TT_(l + 1, l);
+template <typename Cx>
+static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot, int lane) {
+  Cx x = TT_(l, l) - mu, y = TT_(l + 1, l);
   for (int k = l; k < h; ++k) {
-    cplx p, q;
+    Cx p, q;
     givens(x, y, p, q);
     if (lane == 0) {
       rot[2 * k] = p;
@@ -131,18 +153,18 @@ static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int ld, int l, int h,
     // rows k, k+1 (one lane per column)
     const int j0 = k > l ? k - 1 : k;
     for (int j = j0 + lane; j < m; j += 32) {
-      const cplx a = TT_(k, j), b = TT_(k + 1, j);
+      const Cx a = TT_(k, j), b = TT_(k + 1, j);
       TT_(k, j) = p * a + q * b;
-      TT_(k + 1, j) = (k > l && j == k - 1) ? cplx{0, 0} : (-conj(q)) * a + conj(p) * b;
+      TT_(k + 1, j) = (k > l && j == k - 1) ? Cx{0, 0} : (-conj(q)) * a + conj(p) * b;
     }
     __syncwarp();
     // columns k, k+1 (one lane per row); rows k+1 and k+2 of column k are
     // the next bulge pair
     const int ihi = (k + 2 < h) ? k + 2 : h;
-    cplx xn = {0, 0}, yn = {0, 0};
+    Cx xn = {0, 0}, yn = {0, 0};
     for (int i = lane; i <= ihi; i += 32) {
-      const cplx a = TT_(i, k), b = TT_(i, k + 1);
-      const cplx na = a * conj(p) + b * conj(q);
+      const Cx a = TT_(i, k), b = TT_(i, k + 1);
+      const Cx na = a * conj(p) + b * conj(q);
       TT_(i, k) = na;
       TT_(i, k + 1) = (-a) * q + b * p;
       if (i == k + 1) xn = na;
@@ -156,10 +178,10 @@ static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int ld, int l, int h,
   }
   if (Z) {
     for (int i = lane; i < m; i += 32) {
-      cplx c = ZZ_(i, l);
+      Cx c = ZZ_(i, l);
       for (int k = l; k < h; ++k) {
-        const cplx p = rot[2 * k], q = rot[2 * k + 1];
-        const cplx z1 = ZZ_(i, k + 1);
+        const Cx p = rot[2 * k], q = rot[2 * k + 1];
+        const Cx z1 = ZZ_(i, k + 1);
         ZZ_(i, k) = c * conj(p) + z1 * conj(q);
         c = (-c) * q + z1 * p;
       }
@@ -170,40 +192,42 @@ static __device__ void warp_sweep(cplx* T, cplx* Z, int m, int ld, int l, int h,
 }
 
 // Householder reduction of dense T to Hessenberg form, Z accumulating.
-static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int ld, int lane) {
+template <typename Cx>
+static __device__ void warp_hessenberg(Cx* T, Cx* Z, Cx* v, int m, int ld, int lane) {
+  using R = decltype(Cx::re);
   for (int k = 0; k + 2 < m; ++k) {
-    double s = 0;
+    R s = 0;
     for (int i = k + 1 + lane; i < m; i += 32) s += abs2(TT_(i, k));
-    s = warp_sum(s);
-    double a = sqrt(s);
+    s = warp_sum_t(s);
+    R a = sqrt(s);
     if (a == 0) continue;
-    cplx x0 = TT_(k + 1, k);
-    double ax0 = cabs_(x0);
-    cplx ph = ax0 > 0 ? cplx{x0.re / ax0, x0.im / ax0} : cplx{1, 0};
-    for (int i = lane; i < m; i += 32) v[i] = (i > k) ? TT_(i, k) : cplx{0, 0};
+    Cx x0 = TT_(k + 1, k);
+    R ax0 = cabs_(x0);
+    Cx ph = ax0 > 0 ? Cx{x0.re / ax0, x0.im / ax0} : Cx{1, 0};
+    for (int i = lane; i < m; i += 32) v[i] = (i > k) ? TT_(i, k) : Cx{0, 0};
     __syncwarp();
     if (lane == 0) v[k + 1] = v[k + 1] + a * ph;
     __syncwarp();
-    double vv = 0;
+    R vv = 0;
     for (int i = k + 1 + lane; i < m; i += 32) vv += abs2(v[i]);
-    vv = warp_sum(vv);
-    const double f = 2.0 / vv;
+    vv = warp_sum_t(vv);
+    const R f = R(2) / vv;
     // T <- P T : column j (two partial sums break the dependency chain)
     for (int j = lane; j < m; j += 32) {
-      cplx d0 = {0, 0}, d1 = {0, 0};
+      Cx d0 = {0, 0}, d1 = {0, 0};
       int i = k + 1;
       for (; i + 1 < m; i += 2) {
         d0 = d0 + conj(v[i]) * TT_(i, j);
         d1 = d1 + conj(v[i + 1]) * TT_(i + 1, j);
       }
       if (i < m) d0 = d0 + conj(v[i]) * TT_(i, j);
-      const cplx d = f * (d0 + d1);
+      const Cx d = f * (d0 + d1);
       for (i = k + 1; i < m; ++i) TT_(i, j) = TT_(i, j) - d * v[i];
     }
     __syncwarp();
     // T <- T P, Z <- Z P : row i
     for (int i = lane; i < m; i += 32) {
-      cplx d0 = {0, 0}, d1 = {0, 0}, e0 = {0, 0}, e1 = {0, 0};
+      Cx d0 = {0, 0}, d1 = {0, 0}, e0 = {0, 0}, e1 = {0, 0};
       int j = k + 1;
       for (; j + 1 < m; j += 2) {
         d0 = d0 + TT_(i, j) * v[j];
@@ -215,24 +239,26 @@ static __device__ void warp_hessenberg(cplx* T, cplx* Z, cplx* v, int m, int ld,
         d0 = d0 + TT_(i, j) * v[j];
         e0 = e0 + ZZ_(i, j) * v[j];
       }
-      const cplx d = f * (d0 + d1), e = f * (e0 + e1);
+      const Cx d = f * (d0 + d1), e = f * (e0 + e1);
       for (j = k + 1; j < m; ++j) {
         TT_(i, j) = TT_(i, j) - d * conj(v[j]);
         ZZ_(i, j) = ZZ_(i, j) - e * conj(v[j]);
       }
     }
     __syncwarp();
-    for (int i = k + 2 + lane; i < m; i += 32) TT_(i, k) = cplx{0, 0};
+    for (int i = k + 2 + lane; i < m; i += 32) TT_(i, k) = Cx{0, 0};
     __syncwarp();
   }
 }
 
 // Complex Schur form in place; returns false when the sweep budget ran out.
-static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int ld, cplx* rot, int lane) {
+template <typename Cx>
+static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane) {
+  using R = decltype(Cx::re);
   int h = m - 1, its = 0, total = 0;
   while (h > 0) {
     const int l = find_split(T, ld, h, lane);
-    if (l > 0 && lane == 0) TT_(l, l - 1) = cplx{0, 0};
+    if (l > 0 && lane == 0) TT_(l, l - 1) = Cx{0, 0};
     __syncwarp();
     if (l == h) {
       --h;
@@ -240,15 +266,15 @@ static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int ld, cplx* rot, in
       continue;
     }
     if (++total > 30 * m) return false;
-    cplx a = TT_(h - 1, h - 1), b = TT_(h - 1, h), c = TT_(h, h - 1), d = TT_(h, h);
-    cplx mu;
+    Cx a = TT_(h - 1, h - 1), b = TT_(h - 1, h), c = TT_(h, h - 1), d = TT_(h, h);
+    Cx mu;
     if (its > 0 && its % 10 == 0) {
-      mu = d + cplx{cabs_(c), 0};
+      mu = d + Cx{cabs_(c), 0};
     } else {
-      cplx tr2 = 0.5 * (a + d);
-      cplx amd = 0.5 * (a - d);
-      cplx disc = csqrt_(amd * amd + b * c);
-      cplx m1 = tr2 + disc, m2 = tr2 - disc;
+      Cx tr2 = R(0.5) * (a + d);
+      Cx amd = R(0.5) * (a - d);
+      Cx disc = csqrt_(amd * amd + b * c);
+      Cx m1 = tr2 + disc, m2 = tr2 - disc;
       mu = cabs_(m1 - d) < cabs_(m2 - d) ? m1 : m2;
     }
     warp_sweep(T, Z, m, ld, l, h, mu, rot, lane);
@@ -263,20 +289,23 @@ static __device__ bool warp_schur(cplx* T, cplx* Z, int m, int ld, cplx* rot, in
 // (columns of U in the scratch, stride min(32, nvec)); Y = Z U one lane per
 // row.  Returns max over q < k of the relative estimates beta |y_q[m-1]| /
 // (scale ||y_q||).
-static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int ld, const int* ord, int nvec, int k,
-                                      double small, double beta, double scale, cplx* U, cplx* Y, double* est,
+template <typename Cx>
+static __device__ double warp_eigvecs(const Cx* T, const Cx* Z, int m, int ld, const int* ord, int nvec, int k,
+                                      double small_d, double beta, double scale, Cx* U, cplx* Y, double* est,
                                       int lane) {
+  using R = decltype(Cx::re);
+  const R small = (R)small_d;
   double maxest = 0;
   const int W = nvec < 32 ? nvec : 32;
   for (int q0 = 0; q0 < nvec; q0 += 32) {
     const int q = q0 + lane;
     const bool act = lane < W && q < nvec;
     const int idx = act ? ord[q] : 0;
-    const cplx lam = TT_(idx, idx);
+    const Cx lam = TT_(idx, idx);
     if (lane < W)
-      for (int i = 0; i < m; ++i) U[i * W + lane] = (act && i == idx) ? cplx{1, 0} : cplx{0, 0};
+      for (int i = 0; i < m; ++i) U[i * W + lane] = (act && i == idx) ? Cx{1, 0} : Cx{0, 0};
     for (int i = m - 2; i >= 0; --i) {
-      cplx a0 = {0, 0}, a1 = {0, 0};
+      Cx a0 = {0, 0}, a1 = {0, 0};
       if (lane < W) {
         int j = i + 1;
         for (; j + 1 < m; j += 2) {
@@ -286,12 +315,12 @@ static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int l
         if (j < m) a0 = a0 + TT_(i, j) * U[j * W + lane];
       }
       if (act && i < idx) {
-        cplx den = TT_(i, i) - lam;
-        if (cabs_(den) < small) den = cplx{small, 0};
-        const cplx ui = -cdiv(a0 + a1, den);
+        Cx den = TT_(i, i) - lam;
+        if (cabs_(den) < small) den = Cx{small, 0};
+        const Cx ui = -cdiv(a0 + a1, den);
         U[i * W + lane] = ui;
-        if (cabs_(ui) > 1e150)  // rescale this column to avoid overflow
-          for (int j = i; j <= idx; ++j) U[j * W + lane] = 1e-150 * U[j * W + lane];
+        if (cabs_(ui) > HessK<R>::big)  // rescale this column to avoid overflow
+          for (int j = i; j <= idx; ++j) U[j * W + lane] = HessK<R>::unbig * U[j * W + lane];
       }
     }
     __syncwarp();
@@ -299,15 +328,15 @@ static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int l
     const int nq = (nvec - q0) < W ? (nvec - q0) : W;
     for (int c = 0; c < nq; ++c) {
       const int qq = q0 + c;
-      cplx yv[kMaxM / 32];
-      double nrm = 0;
-      cplx ylast = {0, 0};
+      Cx yv[kMaxM / 32];
+      R nrm = 0;
+      Cx ylast = {0, 0};
 #pragma unroll
       for (int t = 0; t < kMaxM / 32; ++t) {
         const int r = lane + 32 * t;
-        yv[t] = cplx{0, 0};
+        yv[t] = Cx{0, 0};
         if (r < m) {
-          cplx s0 = {0, 0}, s1 = {0, 0};
+          Cx s0 = {0, 0}, s1 = {0, 0};
           int j = 0;
           for (; j + 1 < m; j += 2) {
             s0 = s0 + ZZ_(r, j) * U[j * W + c];
@@ -319,16 +348,16 @@ static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int l
           if (r == m - 1) ylast = yv[t];
         }
       }
-      nrm = sqrt(warp_sum(nrm));
-      ylast.re = warp_sum(ylast.re);
-      ylast.im = warp_sum(ylast.im);
-      const double inv = nrm > 0 ? 1.0 / nrm : 0.0;
+      nrm = sqrt(warp_sum_t(nrm));
+      ylast.re = warp_sum_t(ylast.re);
+      ylast.im = warp_sum_t(ylast.im);
+      const R inv = nrm > 0 ? R(1) / nrm : R(0);
 #pragma unroll
       for (int t = 0; t < kMaxM / 32; ++t) {
         const int r = lane + 32 * t;
-        if (r < m) Y[(long)qq * m + r] = inv * yv[t];
+        if (r < m) Y[(long)qq * m + r] = cx_to(inv * yv[t]);
       }
-      const double e = beta * cabs_(ylast) * inv / scale;
+      const double e = beta * (double)cabs_(ylast) * (double)inv / scale;
       if (lane == 0) est[qq] = e;
       if (qq < k) maxest = fmax(maxest, e);
     }
@@ -342,18 +371,20 @@ static __device__ double warp_eigvecs(const cplx* T, const cplx* Z, int m, int l
 // each), u (m), key (m), ord (m), scratch (hess_scratch_cplx(m)).  Callable
 // from any kernel by one full warp; the outputs in `a` may point to shared
 // or global memory.
-static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, double* key, int* ord, cplx* scratch,
+template <typename Cx>
+static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double* key, int* ord, Cx* scratch,
                                  int lane) {
+  using R = decltype(Cx::re);
   const int m = a.m, k = a.k, ld = hess_ld(m);
   const long mm = (long)m * m;
   DevState* st = a.st;
-  cplx* rot = scratch;           // 2 m
-  cplx* U = scratch + 2 * m + 2; // m x 32
+  Cx* rot = scratch;           // 2 m
+  Cx* U = scratch + 2 * m + 2; // m x 32
 
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    TT_(r, c) = a.Hin[i];
-    ZZ_(r, c) = (r == c) ? cplx{1, 0} : cplx{0, 0};
+    TT_(r, c) = cx_from<Cx>(a.Hin[i]);
+    ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
   __syncwarp();
   if (a.dense) warp_hessenberg(T, Z, u, m, ld, lane);
@@ -363,7 +394,7 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   }
   // sort order of diag(T)
   for (int i = lane; i < m; i += 32) {
-    double kv = sort_key(TT_(i, i), a.which);
+    double kv = sort_key(cx_to(TT_(i, i)), a.which);
     key[i] = (kv != kv) ? INFINITY : kv;  // NaN sorts last; ranks stay a permutation
   }
   __syncwarp();
@@ -375,16 +406,16 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   __syncwarp();
   for (int q = lane; q < m; q += 32) {
     a.order[q] = ord[q];
-    a.ritz[q] = TT_(ord[q], ord[q]);
+    a.ritz[q] = cx_to(TT_(ord[q], ord[q]));
   }
   double scale = 0;
-  for (int q = 0; q < k; ++q) scale = fmax(scale, cabs_(TT_(ord[q], ord[q])));
+  for (int q = 0; q < k; ++q) scale = fmax(scale, (double)cabs_(TT_(ord[q], ord[q])));
   if (scale == 0) scale = 1;
   double tnorm = 0;
-  for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, cabs_(TT_(i, i)));
+  for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, (double)cabs_(TT_(i, i)));
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
-  const double small = 2.220446049250313e-16 * (tnorm > 0 ? tnorm : 1.0);
+  const double small = (double)HessK<R>::eps * (tnorm > 0 ? tnorm : 1.0);
   const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
 
   // eigenvectors of the first nvec Ritz values (the wanted k and optional
@@ -406,17 +437,17 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   __syncwarp();
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    TT_(r, c) = a.Hin[i];
-    ZZ_(r, c) = (r == c) ? cplx{1, 0} : cplx{0, 0};
+    TT_(r, c) = cx_from<Cx>(a.Hin[i]);
+    ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
   __syncwarp();
   for (int q = k; q < m; ++q) {
-    cplx mu = u[q];
+    Cx mu = u[q];
     if (a.real_shifts) mu.im = 0;
     int hb = m - 1;
     while (hb > 0) {
       const int l = find_split(T, ld, hb, lane);
-      if (l > 0 && lane == 0) TT_(l, l - 1) = cplx{0, 0};
+      if (l > 0 && lane == 0) TT_(l, l - 1) = Cx{0, 0};
       __syncwarp();
       if (l < hb) warp_sweep(T, Z, m, ld, l, hb, mu, rot, lane);
       hb = l - 1;
@@ -424,25 +455,39 @@ static __device__ void hess_core(const HessArgs& a, cplx* T, cplx* Z, cplx* u, d
   }
   __syncwarp();
   if (lane == 0) {
-    st->beta_hat = TT_(k, k - 1);
-    st->sigma = ZZ_(m - 1, k - 1);
+    st->beta_hat = cx_to(TT_(k, k - 1));
+    st->sigma = cx_to(ZZ_(m - 1, k - 1));
   }
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    a.Hout[i] = (r < k && c < k) ? TT_(r, c) : cplx{0, 0};
-    a.Qout[i] = ZZ_(r, c);
+    a.Hout[i] = (r < k && c < k) ? cx_to(TT_(r, c)) : cplx{0, 0};
+    a.Qout[i] = cx_to(ZZ_(r, c));
   }
 }
 
-// dynamic shared memory (or a.gws): T, Z, scratch
-static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
-  extern __shared__ cplx sws[];
-  __shared__ cplx u[kMaxM];
+// dynamic shared memory (or a.gws): T, Z, scratch of the working type Cx
+template <typename Cx>
+static __device__ void hess_kernel_body(const HessArgs& a, unsigned char* dyn) {
+  __shared__ Cx u[kMaxM];
   __shared__ double key[kMaxM];
   __shared__ int ord[kMaxM];
-  cplx* T = a.gws ? a.gws : sws;
+  Cx* T = a.gws ? reinterpret_cast<Cx*>(a.gws) : reinterpret_cast<Cx*>(dyn);
   const size_t tz = (size_t)hess_ld(a.m) * a.m;
-  hess_core(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x);
+  hess_core<Cx>(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x);
+}
+
+// FP64 working arithmetic (the restart loop and the refinement)
+static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
+  extern __shared__ __align__(16) unsigned char hess_dyn[];
+  hess_kernel_body<cplx>(a, hess_dyn);
+}
+
+// FP32 working arithmetic, FP64 inputs and outputs: the Rayleigh-Ritz checks
+// of the FP32-class phase (whose Ritz vectors are FP32-accurate at best);
+// dynamic shared memory hess_ws_cplx(m) * sizeof(cplxf)
+static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
+  extern __shared__ __align__(16) unsigned char hess_dyn[];
+  hess_kernel_body<cplxf>(a, hess_dyn);
 }
 
 #undef TT_

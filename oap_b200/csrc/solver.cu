@@ -847,8 +847,9 @@ int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* 
 }
 
 // small dense eigenproblem of the b x b matrix G on one warp (Hessenberg
-// reduction + Schur + eigenvectors of the first nv values in sort order)
-int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
+// reduction + Schur + eigenvectors of the first nv values in sort order);
+// fp32: FP32 working arithmetic (the FP32-class phase's checks)
+int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 = false) {
   HessArgs h;
   h.Hin = G;
   h.Hout = a->bH;
@@ -870,7 +871,10 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv) {
   h.tol = 0;
   h.beta = 0;
   ++a->stats.kernel_launches;
-  k_hess<<<1, 32, sizeof(cplx) * hess_ws_cplx(b), a->stream>>>(h);
+  if (fp32)
+    k_hess_f32<<<1, 32, sizeof(cplxf) * hess_ws_cplx(b), a->stream>>>(h);
+  else
+    k_hess<<<1, 32, sizeof(cplx) * hess_ws_cplx(b), a->stream>>>(h);
   return launch_check();
 }
 
@@ -938,7 +942,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
     a->stats.kernel_launches += 5;
     k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
-    if ((rc = small_eig(a, a->G, b, kk, nv))) return rc;
+    if ((rc = small_eig(a, a->G, b, kk, nv, fp32))) return rc;
     k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
     if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
     if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)

@@ -60,3 +60,16 @@ def test_implicit_gram_operator_matches_explicit(rows, cols):
     ev, res, st = imp.solve()
     assert st == B.OK and max(res) <= 1e-10
     assert np.allclose(np.array(ev).real, np.array(ev_ref).real, rtol=1e-11, atol=0)
+
+
+@pytest.mark.gpu
+def test_images_to_matrix_matches_reference_conversion():
+    # (r << 16 | g << 8 | b) / 0xFFFFFF per pixel (Image::convertRgbToFloatt),
+    # from host and from device buffers, one image per row of X
+    rng = np.random.default_rng(8)
+    rgb = rng.integers(0, 256, size=(7, 1000, 3), dtype=np.uint8)
+    expect = ((rgb[..., 0].astype(np.int64) << 16) | (rgb[..., 1].astype(np.int64) << 8) | rgb[..., 2]) / 16777215.0
+    X = B.images_to_matrix(rgb)
+    assert np.array_equal(X.cpu().numpy(), expect.astype(np.float32))
+    Xd = B.images_to_matrix(torch.from_numpy(rgb).cuda())
+    assert torch.equal(Xd, X)
