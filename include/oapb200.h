@@ -213,6 +213,11 @@ typedef struct oapb_arnoldi_config {
                               refines the FP32-phase subspace by FP64
                               residual + FP32-class Sylvester corrections;
                               0 runs FP64 subspace iteration instead */
+  int32_t autotune;        /* 1 (default): when a dense operator is set, time
+                              the launch variants of the single-vector
+                              operator pass and keep the fastest (cached per
+                              device, n, type); 0: the default variant;
+                              2 + v: variant v (0..5, diagnostics) */
 } oapb_arnoldi_config;
 
 /* Fill defaults: rho = 1/3.14, tolerance = 1e-10, LM, FP64, random start,
@@ -238,6 +243,7 @@ typedef struct oapb_arnoldi_stats {
   double block_fp32_seconds;
   uint32_t block_fp32_width; /* right-hand sides of the FP32 block matvec */
   uint32_t fallbacks;        /* solves restarted from the random start */
+  uint32_t matvec_variant;   /* launch variant of the FP64 operator pass */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

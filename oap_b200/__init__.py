@@ -41,7 +41,7 @@ class Config(C.Structure):
                 ("max_restarts", C.c_uint32), ("tolerance", C.c_double),
                 ("rho", C.c_double), ("seed", C.c_uint64), ("profile", C.c_int32),
                 ("fallback_random", C.c_int32), ("tensor_cores", C.c_int32),
-                ("refine", C.c_int32)]
+                ("refine", C.c_int32), ("autotune", C.c_int32)]
 
 
 class Stats(C.Structure):
@@ -53,7 +53,8 @@ class Stats(C.Structure):
                 ("matvec_fp32", C.c_uint32), ("kernel_launches", C.c_uint64),
                 ("block_seconds", C.c_double), ("block_timed", C.c_uint32),
                 ("block_fp32_timed", C.c_uint32), ("block_fp32_seconds", C.c_double),
-                ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32)]
+                ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32),
+                ("matvec_variant", C.c_uint32)]
 
 
 class BatchProblem(C.Structure):
@@ -198,7 +199,7 @@ class Arnoldi:
     def __init__(self, n, hdim, wanted, is_complex=False, sort="LM",
                  precision=PREC_FP64, tolerance=1e-10, max_restarts=300,
                  rho=1.0 / 3.14, seed=1, init=INIT_RANDOM, stream=None,
-                 profile=False, fallback_random=False, tensor_cores=True, refine=True):
+                 profile=False, fallback_random=False, tensor_cores=True, refine=True, autotune=True):
         L = lib()
         cfg = Config()
         L.oapb_arnoldi_config_default(C.byref(cfg))
@@ -211,6 +212,7 @@ class Arnoldi:
         cfg.fallback_random = int(bool(fallback_random))
         cfg.tensor_cores = int(bool(tensor_cores))
         cfg.refine = int(bool(refine))
+        cfg.autotune = int(autotune) if not isinstance(autotune, bool) else int(autotune)
         self.cfg = cfg
         self.h = C.c_void_p()
         check(L.oapb_arnoldi_create(C.byref(self.h), C.byref(cfg), _stream(stream)),

@@ -162,35 +162,51 @@ __global__ void k_matvec_scalar(const T* __restrict__ Are, const T* __restrict__
   }
 }
 
+// Launch variants of k_matvec: rows per CTA (R) and grid (persistent,
+// 148 x resident CTAs, or one CTA per row tile).  Variant 0 is the default
+// policy; an autotuner may pick another by timing them on the operator.
+constexpr int kMvVariants = 6;
+__host__ __device__ inline int mv_rows(int variant) { return variant % 3 == 0 ? 4 : variant % 3 == 1 ? 2 : 8; }
+__host__ __device__ inline bool mv_persistent(int variant) { return variant < 3; }
+
+template <typename T, bool CPLX, int R>
+cudaError_t launch_matvec_r(const T* Are, const T* Aim, int ncols, const T* xre, const T* xim, double* yre,
+                            double* yim, int ntiles, bool persistent, cudaStream_t s) {
+  static int occ = 0;  // per instantiation
+  if (occ == 0) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_matvec<T, CPLX, R>, kMvThreads, 0);
+    if (occ < 1) occ = 1;
+  }
+  int grid = persistent ? kNumSMs * occ : ntiles;
+  if (grid > ntiles) grid = ntiles;
+  k_matvec<T, CPLX, R><<<grid, kMvThreads, 0, s>>>(Are, Aim, ncols, xre, xim, yre, yim, ntiles);
+  return cudaGetLastError();
+}
+
 // Host launcher: y (FP64) = A (T) x (T).  Returns a CUDA error code.
 template <typename T>
 cudaError_t launch_matvec(const T* Are, const T* Aim, int nrows, int ncols,
                           const T* xre, const T* xim, double* yre, double* yim,
-                          cudaStream_t s) {
+                          cudaStream_t s, int variant = 0) {
   constexpr int VW = Vec16<T>::N;
   const bool cplx = Aim != nullptr;
   const bool aligned =
       nrows == ncols && ncols % (kMvWarps * VW) == 0 &&
       ((uintptr_t)Are % 16 == 0) && ((uintptr_t)xre % 16 == 0) &&
       (!cplx || (((uintptr_t)Aim % 16 == 0) && ((uintptr_t)xim % 16 == 0)));
-  constexpr int R = 4;
+  if (variant < 0 || variant >= kMvVariants) variant = 0;
+  const int R = mv_rows(variant);
   if (aligned && nrows % R == 0 && ncols >= 256) {
     const int ntiles = nrows / R;
-    static int occ[2] = {0, 0};
-    int& o = occ[cplx ? 1 : 0];
-    if (o == 0) {
-      if (cplx)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_matvec<T, true, R>, kMvThreads, 0);
-      else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_matvec<T, false, R>, kMvThreads, 0);
-      if (o < 1) o = 1;
+    const bool pers = mv_persistent(variant);
+    switch (R * (cplx ? -1 : 1)) {
+      case 2: return launch_matvec_r<T, false, 2>(Are, nullptr, ncols, xre, nullptr, yre, nullptr, ntiles, pers, s);
+      case 4: return launch_matvec_r<T, false, 4>(Are, nullptr, ncols, xre, nullptr, yre, nullptr, ntiles, pers, s);
+      case 8: return launch_matvec_r<T, false, 8>(Are, nullptr, ncols, xre, nullptr, yre, nullptr, ntiles, pers, s);
+      case -2: return launch_matvec_r<T, true, 2>(Are, Aim, ncols, xre, xim, yre, yim, ntiles, pers, s);
+      case -4: return launch_matvec_r<T, true, 4>(Are, Aim, ncols, xre, xim, yre, yim, ntiles, pers, s);
+      default: return launch_matvec_r<T, true, 8>(Are, Aim, ncols, xre, xim, yre, yim, ntiles, pers, s);
     }
-    int grid = kNumSMs * o;
-    if (grid > ntiles) grid = ntiles;
-    if (cplx)
-      k_matvec<T, true, R><<<grid, kMvThreads, 0, s>>>(Are, Aim, ncols, xre, xim, yre, yim, ntiles);
-    else
-      k_matvec<T, false, R><<<grid, kMvThreads, 0, s>>>(Are, nullptr, ncols, xre, nullptr, yre, nullptr, ntiles);
   } else {
     int grid = grid_for((long)nrows * 32, 256, kNumSMs * 8);
     if (cplx)

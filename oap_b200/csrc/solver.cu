@@ -26,6 +26,9 @@
 // restart.
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <new>
 #include <stdio.h>
 #include <string.h>
@@ -425,6 +428,8 @@ struct oapb_arnoldi {
   float* a32im = nullptr;
   oapb_matvec_fn cb = nullptr;
   void* cb_user = nullptr;
+  // single-vector matvec launch variants (autotuned per operator shape)
+  int mv64 = 0, mv32 = 0;
   // implicit Gram operator A = X X^T (FP32 images, rows = n)
   const float* gX = nullptr;
   int gcols = 0;
@@ -553,10 +558,10 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
   ++a->stats.kernel_launches;
   if (fp32)
     e = launch_matvec<float>(a->a32re, a->is_c ? a->a32im : nullptr, n, n, a->x32re, a->is_c ? a->x32im : nullptr,
-                             yre, a->is_c ? yim : nullptr, s);
+                             yre, a->is_c ? yim : nullptr, s, a->mv32);
   else
     e = launch_matvec<double>(a->a64re, a->is_c ? a->a64im : nullptr, n, n, xre, a->is_c ? xim : nullptr, yre,
-                              a->is_c ? yim : nullptr, s);
+                              a->is_c ? yim : nullptr, s, a->mv64);
   if (prof) prof_end(a, tm);
   if (fp32) a->stats.matvec_fp32++;
   return e == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
@@ -1382,6 +1387,58 @@ void free_all(oapb_arnoldi* a) {
 
 }  // namespace
 
+// Launch autotuner of the single-vector operator pass (replaces the
+// reference's fixed launch mapping, utils::mapper::SetThreadsBlocks,
+// oapUtils/ThreadsMapper.cpp:36-74): every k_matvec variant (rows per CTA,
+// persistent or one CTA per row tile) runs once to warm up and three times
+// timed with CUDA events on the handle's stream; the fastest is kept per
+// (device, n, element type, complex) for the life of the process.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int, int>, int> g_tune;
+
+template <typename T>
+int tune_matvec(oapb_arnoldi* a, const T* Are, const T* Aim, const T* xre, const T* xim) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const auto key = std::make_tuple(dev, a->n, (int)sizeof(T), a->is_c ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) return it->second;
+  }
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return 0;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return 0;
+  }
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int v = 0; v < kMvVariants; ++v) {
+    if (launch_matvec<T>(Are, Aim, a->n, a->n, xre, xim, a->wre, a->is_c ? a->wim : nullptr, a->stream, v) !=
+        cudaSuccess)
+      continue;
+    cudaEventRecord(e0, a->stream);
+    for (int r = 0; r < 3; ++r)
+      launch_matvec<T>(Are, Aim, a->n, a->n, xre, xim, a->wre, a->is_c ? a->wim : nullptr, a->stream, v);
+    cudaEventRecord(e1, a->stream);
+    float ms = 0;
+    if (cudaEventSynchronize(e1) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) continue;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaGetLastError();
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+  return best;
+}
+}  // namespace
+
 extern "C" {
 
 void oapb_arnoldi_config_default(oapb_arnoldi_config* c) {
@@ -1396,6 +1453,7 @@ void oapb_arnoldi_config_default(oapb_arnoldi_config* c) {
   c->seed = 1;
   c->tensor_cores = 1;
   c->refine = 1;
+  c->autotune = 1;
 }
 
 int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void* stream) {
@@ -1523,7 +1581,25 @@ int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
   a->a64im = (const double*)A->im;
   a->cb = nullptr;
   a->gX = nullptr;
-  if (a->cfg.precision == OAPB_PREC_MIXED) return make_fp32_copy(a);
+  if (a->cfg.precision == OAPB_PREC_MIXED) {
+    const int rc = make_fp32_copy(a);
+    if (rc) return rc;
+  }
+  if (a->cfg.autotune >= 2 && a->cfg.autotune < 2 + kMvVariants) {  // a forced variant
+    a->mv64 = a->mv32 = a->cfg.autotune - 2;
+  } else if (a->cfg.autotune == 1) {
+    // x: the residual buffers (zeroed), y: the work vector
+    if (cudaMemsetAsync(a->fre, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    if (a->is_c && cudaMemsetAsync(a->fim, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    a->mv64 = tune_matvec<double>(a, a->a64re, a->a64im, a->fre, a->is_c ? a->fim : nullptr);
+    if (a->a32re && a->x32re) {
+      if (cudaMemsetAsync(a->x32re, 0, sizeof(float) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+      if (a->is_c && cudaMemsetAsync(a->x32im, 0, sizeof(float) * a->n, a->stream) != cudaSuccess)
+        return OAPB_ERR_CUDA;
+      a->mv32 = tune_matvec<float>(a, a->a32re, a->a32im, a->x32re, a->is_c ? a->x32im : nullptr);
+    }
+  }
+  a->stats.matvec_variant = (uint32_t)a->mv64;
   return OAPB_OK;
 }
 

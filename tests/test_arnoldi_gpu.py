@@ -202,3 +202,20 @@ def test_block_pass_precisions(cplx, n, b):
         err = ((W - ref).abs() / scale).max().item()
         assert err <= tol, (prec, tc, err)
         s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cplx", [True, False])
+def test_matvec_autotune_variants(cplx):
+    # every launch variant of the single-vector pass (forced: autotune = 2 + v)
+    # and the autotuned one solve to the pairs of the default variant
+    n = 2048
+    A = planted_complex(n, seed=21, nplant=5) if cplx else planted_symmetric(n, seed=21)[0]
+    r0 = solve(A, 5, 24, autotune=False)
+    assert r0["stats"]["matvec_variant"] == 0 and r0["res"].max() <= TOL
+    for autotune in [True] + [2 + v for v in range(6)]:
+        r = solve(A, 5, 24, autotune=autotune)
+        v = r["stats"]["matvec_variant"]
+        assert 0 <= v < 6 and (autotune is True or v == autotune - 2)
+        assert r["res"].max() <= TOL
+        assert np.allclose(np.sort_complex(r0["ev"]), np.sort_complex(r["ev"]), rtol=1e-11, atol=0)
