@@ -293,7 +293,8 @@ def run_ours(args, world, rank, local):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         launches0 = s.stats()["kernel_launches"]
         prof = {"matvec_seconds": 0.0, "matvec_timed": 0, "block_seconds": 0.0, "block_timed": 0,
-                "block_fp32_seconds": 0.0, "block_fp32_timed": 0, "block_fp32_width": 0}
+                "block_fp32_seconds": 0.0, "block_fp32_timed": 0, "block_fp32_width": 0,
+                "block_bf16_seconds": 0.0, "block_bf16_timed": 0}
         conv = 0
         e0.record()
         for _ in range(steps):
@@ -360,8 +361,9 @@ def run_ours(args, world, rank, local):
     hbm, peak_kind = peaks()
     bw = prof["block_fp32_width"] or K_WANTED
     # algorithmic bytes per pass: the operator once (FP32-class pass: BF16
-    # hi + lo of both planes, 8 n^2; FP64 pass: 16 n^2) plus X in and W out
-    # (FP64 planes, 32 b n); flops 8 b n^2 (complex)
+    # hi + lo of both planes, 8 n^2; BF16 pass: the hi planes, 4 n^2; FP64
+    # pass: 16 n^2) plus X in and W out (FP64 planes, 32 b n); flops 8 b n^2
+    # (complex)
     fp32_name = ("k_block_matvec_tc<complex> (split-BF16 tcgen05 block pass, %d vectors)" % bw if not args.no_tc
                  else "k_block_matvec<float,complex> (FP32 CUDA-core block pass, %d vectors)" % bw)
     fp64_name = ("k_block_matvec_dmma<complex> (FP64 DMMA block pass)" if not args.no_tc
@@ -374,6 +376,9 @@ def run_ours(args, world, rank, local):
         fp64_name:
             (prof["block_seconds"], prof["block_timed"], 16.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
     }
+    if not args.no_tc:
+        kernels["k_block_matvec_tc<complex, BF16> (BF16 hi-plane tcgen05 block pass)"] = (
+            prof["block_bf16_seconds"], prof["block_bf16_timed"], 4.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n)
     name, (tot, cnt, alg_bytes, flops) = max(kernels.items(), key=lambda kv: kv[1][0])
     per_launch = tot / max(1, cnt)
     achieved = alg_bytes / per_launch / 1e9 if per_launch > 0 else 0.0
@@ -400,8 +405,9 @@ def run_ours(args, world, rank, local):
            "data": "synthetic (seeded)",
            "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
                       "tolerance": TOL,
-                      "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, then FP64-anchored "
-                                      "refinement: FP64 DMMA residual + FP32-class Sylvester corrections"),
+                      "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, its leading powers "
+                                      "on the BF16 hi planes, then FP64-anchored refinement: FP64 DMMA residual + "
+                                      "Sylvester corrections (leading sweeps BF16, the rest FP32-class)"),
                       "parallelism": "replicas" if world > 1 else "single GPU",
                       "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo operator) exceed L2; no flush"},
            "converged_steps": conv_all,
@@ -409,7 +415,8 @@ def run_ours(args, world, rank, local):
                           "steps": psteps, "restarts": pstt["restarts"], "matvecs": pstt["matvecs"]},
            "speedup_vs_plain_fp64": value / pvalue if pvalue else None,
            "solve": {"restarts": stt["restarts"], "matvecs": stt["matvecs"],
-                     "block_matvecs": stt["block_matvecs"], "refine_iterations": stt["refine_iterations"],
+                     "block_matvecs": stt["block_matvecs"], "bf16_passes": stt["block_bf16"],
+                     "refine_iterations": stt["refine_iterations"],
                      "max_residual": stt["max_residual"]},
            "e2e": {"value": e2e_value, "unit": "eigensolves/s",
                    "h2d_bytes_per_step": 2 * 8 * n * n,

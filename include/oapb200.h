@@ -239,11 +239,14 @@ typedef struct oapb_arnoldi_stats {
   uint64_t kernel_launches;  /* library kernel launches over the handle's life */
   double block_seconds;      /* device time of the timed FP64 block matvecs (profile) */
   uint32_t block_timed;
-  uint32_t block_fp32_timed; /* FP32 block matvecs timed (profile) */
+  uint32_t block_fp32_timed; /* FP32-class block matvecs timed (profile; BF16 passes apart) */
   double block_fp32_seconds;
   uint32_t block_fp32_width; /* right-hand sides of the FP32 block matvec */
   uint32_t fallbacks;        /* solves restarted from the random start */
   uint32_t matvec_variant;   /* launch variant of the FP64 operator pass */
+  uint32_t block_bf16;       /* block passes on the BF16 hi planes alone */
+  uint32_t block_bf16_timed; /* of which timed (profile) */
+  double block_bf16_seconds; /* their device time (profile) */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */
@@ -308,11 +311,33 @@ OAPB_EXPORT int oapb_arnoldi_solve_host(oapb_arnoldi* handle, const double* a_re
 
 OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_stats* out);
 
+/* One convergence check of the mixed form's block phases. */
+typedef struct oapb_trace_rec {
+  int32_t phase;        /* 1: FP32-class subspace iteration, 2: FP64 subspace
+                           iteration, 3: FP64-anchored refinement */
+  int32_t iteration;    /* iteration (outer step) of that phase */
+  uint32_t passes;      /* block operator passes of the solve so far */
+  uint32_t bf16_passes; /* of which on the BF16 hi planes alone */
+  double residual;      /* largest relative residual of the wanted pairs */
+} oapb_trace_rec;
+
+/* Convergence trace of the last solve: copies up to cap records, *count =
+ * the number recorded (the plain IRAM path records none). */
+OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_rec* out, uint32_t cap,
+                                       uint32_t* count);
+
+/* Pass precision of oapb_arnoldi_apply_block only (not a solve precision):
+ * the BF16 hi planes of the mixed form's operator copy on the tensor cores
+ * (products within about 2^-8 |A| |X|; FP32 CUDA-core pass when
+ * cfg.tensor_cores = 0). */
+#define OAPB_PASS_BF16 2
+
 /* W = A X for b <= 32 vectors (device FP64 planes, vector q at offset q n)
  * with the handle's dense operator: precision OAPB_PREC_FP64 reads the FP64
  * operator; OAPB_PREC_MIXED the FP32-class copy of the mixed form (tensor
- * cores when cfg.tensor_cores, else CUDA-core FP32).  The block pass of the
- * solver, exposed for multiple right-hand sides and for verification. */
+ * cores when cfg.tensor_cores, else CUDA-core FP32); OAPB_PASS_BF16 its
+ * BF16 hi planes.  The block pass of the solver, exposed for multiple
+ * right-hand sides and for verification. */
 OAPB_EXPORT int oapb_arnoldi_apply_block(oapb_arnoldi* handle, const double* x_re,
                                          const double* x_im, uint32_t b,
                                          double* w_re, double* w_im,

@@ -18,6 +18,7 @@ OK, ERR_ARG, ERR_CUDA, NOT_CONVERGED, ERR_TIMEOUT, ERR_BOUNDS, ERR_CALLBACK, ERR
 F64, F32 = 0, 1
 SORT = {"LM": 0, "LR": 1, "LI": 2, "SM": 3, "SR": 4, "SI": 5}
 PREC_FP64, PREC_MIXED = 0, 1
+PASS_BF16 = 2  # apply_block only: the BF16 hi planes of the operator copy
 INIT_RANDOM, INIT_FIRST_VALUE_IS_ONE, INIT_USER = 0, 1, 2
 TYPE_EIGENVECTOR, TYPE_WV = 0, 1
 
@@ -44,6 +45,11 @@ class Config(C.Structure):
                 ("refine", C.c_int32), ("autotune", C.c_int32)]
 
 
+class TraceRec(C.Structure):
+    _fields_ = [("phase", C.c_int32), ("iteration", C.c_int32), ("passes", C.c_uint32),
+                ("bf16_passes", C.c_uint32), ("residual", C.c_double)]
+
+
 class Stats(C.Structure):
     _fields_ = [("restarts", C.c_uint32), ("matvecs", C.c_uint32),
                 ("block_matvecs", C.c_uint32), ("dgks_passes", C.c_uint32),
@@ -54,7 +60,8 @@ class Stats(C.Structure):
                 ("block_seconds", C.c_double), ("block_timed", C.c_uint32),
                 ("block_fp32_timed", C.c_uint32), ("block_fp32_seconds", C.c_double),
                 ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32),
-                ("matvec_variant", C.c_uint32)]
+                ("matvec_variant", C.c_uint32), ("block_bf16", C.c_uint32),
+                ("block_bf16_timed", C.c_uint32), ("block_bf16_seconds", C.c_double)]
 
 
 class BatchProblem(C.Structure):
@@ -115,6 +122,7 @@ def lib():
             "oapb_arnoldi_solve_host": [vp, vp, vp, P(C.c_double), P(C.c_double),
                                         P(C.c_double), vp, vp],
             "oapb_arnoldi_get_stats": [vp, P(Stats)],
+            "oapb_arnoldi_get_trace": [vp, P(TraceRec), C.c_uint32, P(C.c_uint32)],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
@@ -316,6 +324,16 @@ class Arnoldi:
         check(lib().oapb_arnoldi_apply_block(self.h, p(xre), p(xim), b, p(wre), p(wim), precision),
               "oapb_arnoldi_apply_block")
         return wre, wim
+
+    def trace(self):
+        """Convergence checks of the last solve: (phase, iteration, passes,
+        bf16_passes, residual) tuples (phase 1: FP32-class subspace
+        iteration, 2: FP64 subspace iteration, 3: FP64-anchored refinement)."""
+        cnt = C.c_uint32()
+        check(lib().oapb_arnoldi_get_trace(self.h, None, 0, C.byref(cnt)), "oapb_arnoldi_get_trace")
+        recs = (TraceRec * max(cnt.value, 1))()
+        check(lib().oapb_arnoldi_get_trace(self.h, recs, cnt.value, C.byref(cnt)), "oapb_arnoldi_get_trace")
+        return [(r.phase, r.iteration, r.passes, r.bf16_passes, r.residual) for r in recs[:cnt.value]]
 
     def stats(self):
         s = Stats()

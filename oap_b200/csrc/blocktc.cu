@@ -12,6 +12,12 @@
 // swizzle), and the epilogue forms W_re = D1[:, :QB] - D2[:, QB:],
 // W_im = D1[:, QB:] + D2[:, :QB] in FP64.
 //
+// The BF16 variant (LO = false) reads the hi planes only and drops the
+// A_lo terms: 4 n^2 bytes per pass (complex), products within 2^-8 of
+// |A| |X| instead of about 2^-16, for the passes whose rounding a later
+// FP32-class pass removes (the first powers of a subspace iteration, the
+// first sweeps of a contracting fixed point).
+//
 // The kernel is persistent and stream-K scheduled (streamk.cuh): one CTA
 // per SM walks an equal share of the (tile, K chunk) iterations.  Warps are
 // specialised:
@@ -25,8 +31,8 @@
 //               release the accumulator (`acce`).
 // Two accumulator buffers in TMEM let the epilogue of one segment overlap
 // the MMAs of the next.  A segment is at most kBtcSub K chunks of one tile;
-// the epilogue writes the first segment of a tile and adds the others in
-// FP64.  The pass is HBM-bound: 8 n^2 bytes of operator per
+// the epilogue adds the segments of a tile in FP64 registers and stores
+// the tile's partial once.  The pass is HBM-bound: 8 n^2 bytes of operator per
 // pass (complex), read once.  Every wait is bounded; a timeout sets *err.
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -122,6 +128,21 @@ struct BtcArgs {
   uint32_t stage_bytes;
 };
 
+// the FP64 sums of one row of a tile (slot = tile - first tile of the CTA)
+template <bool CPLX, int QB>
+__device__ __forceinline__ void btc_store_partial(const BtcArgs& g, long slot, int row, const double (&s1)[QB],
+                                                  const double (&s2)[CPLX ? QB : 1]) {
+  constexpr int NP = CPLX ? 2 : 1;
+  double* out = g.ws + ((size_t)blockIdx.x * g.grid.slots + slot) * (size_t)NP * g.b * kSkRows + row;
+#pragma unroll
+  for (int q = 0; q < QB; ++q) {
+    if (q < g.b) {
+      out[(size_t)q * kSkRows] = s1[q];
+      if (CPLX) out[((size_t)g.b + q) * kSkRows] = s2[q];
+    }
+  }
+}
+
 // wait for `parity` of `bar`; gives up after the time limit or when another
 // role has already given up (*abort set)
 __device__ __forceinline__ bool btc_wait(uint64_t* bar, uint32_t parity, volatile int* abort) {
@@ -135,14 +156,83 @@ __device__ __forceinline__ bool btc_wait(uint64_t* bar, uint32_t parity, volatil
   return true;
 }
 
-template <bool CPLX>
+// Epilogue (warps 2-5).  Per tile segment the accumulator columns of this
+// thread's row leave TMEM 16 at a time and are added in FP64 to running
+// sums held in registers (QB is a compile-time constant, so every index is
+// static); a tile's sums are stored to its stream-K partial once, when the
+// CTA's share of the tile ends, so no global load waits in the loop.
+template <bool CPLX, int QB>
+__device__ __forceinline__ void btc_epilogue(const BtcArgs& g, uint32_t tmem, uint64_t* accf, uint64_t* acce,
+                                             volatile int* abort, long it0, long it1, long kch, long first_tile,
+                                             int warp, int lane) {
+  constexpr int NP = CPLX ? 2 : 1;
+  constexpr int NCH = (NP * QB + 15) / 16;  // 16-column TMEM loads per accumulator
+  const int wq = warp & 3;                  // TMEM lane quarter of this warp
+  const int row = wq * 32 + lane;
+  double s1[QB], s2[CPLX ? QB : 1];
+  long cur = -1, seg = 0;
+  bool ok = true;
+  for (long it = it0; it < it1; ++seg) {
+    const long tile = it / kch, kc = it % kch;
+    long kc_end = (kc / kBtcSub + 1) * kBtcSub;
+    if (kc_end > kch) kc_end = kch;
+    it = min(it1, tile * kch + kc_end);
+    const int buf = (int)(seg & 1);
+    if (!btc_wait(&accf[buf], (uint32_t)((seg / 2) & 1), abort)) {
+      ok = false;
+      break;
+    }
+    tc::tc_fence_after();
+    if (tile != cur) {
+      if (cur >= 0) btc_store_partial<CPLX, QB>(g, cur - first_tile, row, s1, s2);
+      cur = tile;
+#pragma unroll
+      for (int q = 0; q < QB; ++q) {
+        s1[q] = 0;
+        if (CPLX) s2[q] = 0;
+      }
+    }
+    const uint32_t tl = tmem + ((uint32_t)(wq * 32) << 16) + buf * 128;
+#pragma unroll
+    for (int c = 0; c < NCH; ++c) {
+      float v[16];
+      tmem_ld16(tl + c * 16, v);  // D1 = A_re B^T: W_re += [:, q], W_im += [:, QB + q]
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int col = c * 16 + j;
+        if (col < QB)
+          s1[col] += (double)v[j];
+        else if (CPLX && col < 2 * QB)
+          s2[col - QB] += (double)v[j];
+      }
+      if (CPLX) {
+        tmem_ld16(tl + 64 + c * 16, v);  // D2 = A_im B^T: W_im += [:, q], W_re -= [:, QB + q]
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = c * 16 + j;
+          if (col < QB)
+            s2[col] += (double)v[j];
+          else if (col < 2 * QB)
+            s1[col - QB] -= (double)v[j];
+        }
+      }
+    }
+    tc::tc_fence_before();
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&acce[buf]);
+  }
+  if (ok && cur >= 0) btc_store_partial<CPLX, QB>(g, cur - first_tile, row, s1, s2);
+}
+
+template <bool CPLX, bool LO>
 __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid_constant__ BtcArgs g) {
   extern __shared__ __align__(1024) uint8_t bsm_raw[];
   constexpr int kMaxStages = 4;
   __shared__ __align__(8) uint64_t full[kMaxStages], empty[kMaxStages], accf[2], acce[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
-  constexpr int NA = CPLX ? 4 : 2;  // operator tiles per stage
+  constexpr int NPL = CPLX ? 2 : 1;         // operator planes (re, im)
+  constexpr int NA = LO ? 2 * NPL : NPL;  // operator tiles per stage (hi [, lo] per plane)
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* sm = (uint8_t*)(((uintptr_t)bsm_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = tc::smem_u32(sm);
@@ -184,7 +274,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
         const int x = (int)((it % kch) * kBtcK), y = (int)((it / kch) * kBtcM);
         mbar_expect_tx(&full[s], tx);
 #pragma unroll
-        for (int p = 0; p < NA; ++p) tma_load_2d(st + p * a_tile, &g.tm[p], x, y, &full[s]);
+        for (int p = 0; p < NA; ++p) tma_load_2d(st + p * a_tile, &g.tm[LO ? p : 2 * p], x, y, &full[s]);
         tma_load_2d(st + NA * a_tile, &g.tm[4], x, 0, &full[s]);
         tma_load_2d(st + NA * a_tile + b_tile, &g.tm[5], x, 0, &full[s]);
       }
@@ -217,13 +307,15 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
           const uint64_t off = (uint64_t)(kk * 32) >> 4;
           const uint32_t acc0 = (seg_first && kk == 0) ? 0u : 1u;
 #pragma unroll
-          for (int p = 0; p < NA / 2; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
-            const uint64_t ah = tc::sdesc_k_sw128(st + (2 * p) * a_tile) + off;
-            const uint64_t al = tc::sdesc_k_sw128(st + (2 * p + 1) * a_tile) + off;
+          for (int p = 0; p < NPL; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
+            const uint64_t ah = tc::sdesc_k_sw128(st + (LO ? 2 * p : p) * a_tile) + off;
             const uint32_t d = tmem + buf * 128 + p * 64;
             tc::mma_bf16(d, ah, bh + off, idesc, acc0);
             tc::mma_bf16(d, ah, bl + off, idesc, 1u);
-            tc::mma_bf16(d, al, bh + off, idesc, 1u);
+            if (LO) {
+              const uint64_t al = tc::sdesc_k_sw128(st + (2 * p + 1) * a_tile) + off;
+              tc::mma_bf16(d, al, bh + off, idesc, 1u);
+            }
           }
         }
         tc::commit(&empty[s]);
@@ -238,50 +330,19 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
     }
   } else {
     // ---------------------------------------------------------- epilogue --
-    const int wq = warp & 3;  // TMEM lane quarter of this warp
-    const int row = wq * 32 + lane;
-    long seg = 0;
-    for (long it = it0; it < it1; ++seg) {
-      const long tile = it / kch, kc = it % kch;
-      long kc_end = (kc / kBtcSub + 1) * kBtcSub;
-      if (kc_end > kch) kc_end = kch;
-      const long end = min(it1, tile * kch + kc_end);
-      const bool add = !(it == it0 || kc == 0);  // not the first segment of this tile in this CTA
-      it = end;
-      const int buf = (int)(seg & 1);
-      if (!btc_wait(&accf[buf], (uint32_t)((seg / 2) & 1), &abort_flag)) break;
-      tc::tc_fence_after();
-      const uint32_t tl = tmem + ((uint32_t)(wq * 32) << 16) + buf * 128;
-      float d1[64], d2[64];
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        if (c * 16 < N) {
-          float v[16];
-          tmem_ld16(tl + c * 16, v);
-#pragma unroll
-          for (int j = 0; j < 16; ++j) d1[c * 16 + j] = v[j];
-          if (CPLX) {
-            tmem_ld16(tl + 64 + c * 16, v);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) d2[c * 16 + j] = v[j];
-          }
-        }
-      }
-      tc::tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive(&acce[buf]);
-      constexpr int NP = CPLX ? 2 : 1;
-      double* out = g.ws + ((size_t)blockIdx.x * g.grid.slots + (tile - first_tile)) * (size_t)NP * g.b * kSkRows;
-      for (int q = 0; q < g.b; ++q) {
-        double* o1 = out + (size_t)q * kSkRows + row;
-        const double v1 = CPLX ? (double)d1[q] - (double)d2[g.QB + q] : (double)d1[q];
-        *o1 = add ? *o1 + v1 : v1;
-        if (CPLX) {
-          double* o2 = out + ((size_t)g.b + q) * kSkRows + row;
-          const double v2 = (double)d1[g.QB + q] + (double)d2[q];
-          *o2 = add ? *o2 + v2 : v2;
-        }
-      }
+    switch (g.QB) {
+      case 8:
+        btc_epilogue<CPLX, 8>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        break;
+      case 16:
+        btc_epilogue<CPLX, 16>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        break;
+      case 24:
+        btc_epilogue<CPLX, 24>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        break;
+      default:
+        btc_epilogue<CPLX, 32>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        break;
     }
   }
   tc::tc_fence_before();
@@ -319,8 +380,8 @@ static bool make_tmap(CUtensorMap* m, const __nv_bfloat16* base, int kp, int row
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-static size_t btc_stage_bytes(int N, bool cplx) {
-  const int NA = cplx ? 4 : 2;
+static size_t btc_stage_bytes(int N, bool cplx, bool lo) {
+  const int NA = (cplx ? 2 : 1) * (lo ? 2 : 1);
   return ((size_t)(NA * kBtcM * 128 + 2 * N * 128) + 1023) & ~(size_t)1023;
 }
 
@@ -335,7 +396,7 @@ size_t btc_workspace(int n, int kp) { return sk_workspace(btc_grid(n, kp)); }
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s) {
+                           cudaStream_t s, bool bf16_only) {
   const bool cplx = op.aih != nullptr;
   if (b < 1 || b > 32 || op.kp % kBtcK != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
   const int QB = (b + 7) / 8 * 8;
@@ -354,13 +415,14 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   g.b = b;
   g.QB = QB;
   g.N = N;
-  const size_t stage = btc_stage_bytes(N, cplx);
+  const size_t stage = btc_stage_bytes(N, cplx, !bf16_only);
   g.stage_bytes = (uint32_t)stage;
   g.stages = (int)(kBtcSmemBudget / stage);
   if (g.stages > 4) g.stages = 4;
   if (g.stages < 2) return OAPB_ERR_ARG;
   const size_t smem = g.stages * stage + 1024;
-  auto kern = cplx ? k_block_matvec_tc<true> : k_block_matvec_tc<false>;
+  auto kern = bf16_only ? (cplx ? k_block_matvec_tc<true, false> : k_block_matvec_tc<false, false>)
+                        : (cplx ? k_block_matvec_tc<true, true> : k_block_matvec_tc<false, true>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return OAPB_ERR_CUDA;
   kern<<<g.grid.grid, kBtcThreads, smem, s>>>(g);

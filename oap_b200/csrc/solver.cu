@@ -456,6 +456,7 @@ struct oapb_arnoldi {
   static constexpr int kBlocks = 6;
   double *Bre[kBlocks] = {}, *Bim[kBlocks] = {};
   cplx* thinv = nullptr;  // 1 / Ritz values of the refinement (kBmMaxB)
+  std::vector<oapb_trace_rec> trace;  // convergence checks of the last solve
   cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
   cplx *britz = nullptr;
   double *best = nullptr, *bnorm = nullptr;
@@ -757,10 +758,11 @@ void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, con
                                                                        0, nullptr, nullptr);
 }
 
-// W = A X (b vectors); FP32 operator copy when fp32, else FP64
+// W = A X (b vectors); FP32-class operator copy when fp32, else FP64.
+// bf16 (with fp32): on the tensor cores, the BF16 hi planes alone.
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
-                bool fp32 = false) {
+                bool fp32 = false, bool bf16 = false) {
   if (a->cb || a->gX) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
@@ -772,13 +774,15 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   const int tiles = (a->n + kBmRows - 1) / kBmRows;
   dim3 grid(tiles, a->nsplit);
   a->stats.kernel_launches += 2;
-  Timed tm{nullptr, nullptr, 1, fp32 ? 1 : 0, b};
+  const bool tcp = fp32 && a->have_tc && a->cfg.tensor_cores;
+  Timed tm{nullptr, nullptr, 1, fp32 ? (tcp && bf16 ? 2 : 1) : 0, b};
   const bool prof = prof_begin(a, tm);
-  if (fp32 && a->have_tc && a->cfg.tensor_cores) {
+  if (tcp) {
     BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
                    C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
     int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
-                                    a->tcerr, a->stream);
+                                    a->tcerr, a->stream, bf16);
+    if (bf16) a->stats.block_bf16++;
     if (prof) prof_end(a, tm);
     if (rc) return rc;
     a->stats.block_matvecs++;
@@ -885,6 +889,22 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
 
 constexpr int kSlow = 100;   // subspace(): convergence too slow for the iteration budget
 constexpr int kMixedMinN = 8192;
+// BF16 operator passes (tensor cores only).  In the FP32-class subspace
+// iteration: the powers taken while the block is still far from the wanted
+// subspace (before the first check, then while the residual extrapolated
+// from the last check stays above kBf16Until), never the pass right before
+// a check, so that their rounding (about 2^-8 of the block, kBf16Err) is
+// damped by FP32-class powers before any residual is measured.  In the
+// refinement's fixed point: the leading sweeps, as many as leave the last
+// sweeps on the FP32-class operator to contract a 2^-8 error to the
+// correction's goal.
+constexpr double kBf16Until = 0.02;
+constexpr double kBf16Err = 4e-3;
+// Goal of the FP32-class phase, the hand-over to the refinement: one outer
+// refinement step leaves about 5e-6 (the FP32-class accuracy of the
+// correction) of the residual it starts from, so from 5e-6 a single step
+// reaches 1e-10 with margin; the FP32-class floor itself lies near 1e-6.
+constexpr double kFp32Goal = 5e-6;
 
 // Block subspace iteration with Rayleigh-Ritz on b vectors:
 //   W = A X; G = X^H W; R = W - X G; G = S diag(theta) S^-1;
@@ -929,7 +949,17 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   // next pass takes W itself (the span is what the iteration carries).
   double growth = 0, drift = 1;
   for (unsigned it = 0; it < max_it; ++it) {
-    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32))) return rc;
+    bool bf16 = false;
+    if (fp32 && !from_bx && it + 1 < next_check) {
+      const size_t h = hist.size();
+      double est = 1.0;  // before the first check: a random block
+      if (h) {
+        const double r = h >= 2 ? pow(hist[h - 1] / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2])) : 0.5;
+        est = hist[h - 1] * pow(r < 1.0 ? r : 1.0, (double)((int)it - hist_it[h - 1]));
+      }
+      bf16 = est >= kBf16Until;
+    }
+    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32, bf16))) return rc;
     const bool check = fp32 ? (it >= next_check || it + 1 == max_it)
                             : ((int)it >= skip || it + 1 == max_it);
     if (!check) {
@@ -978,6 +1008,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     hist.push_back(mx);
     hist_it.push_back((int)it);
     a->stats.refine_iterations++;
+    a->trace.push_back({fp32 ? 1 : 2, (int)it, a->stats.block_matvecs, a->stats.block_bf16, mx});
     const bool done = mx <= tol;
     bool stop = done;
     if (fp32) {
@@ -1104,6 +1135,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
       res_out[q] = norms[q] / scale;
       mx = fmax(mx, res_out[q]);
     }
+    a->trace.push_back({3, outer, a->stats.block_matvecs, a->stats.block_bf16, mx});
     if (mx <= tol) {  // Ritz vectors X S
       ++a->stats.kernel_launches;
       k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
@@ -1123,6 +1155,9 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff)) + 2;
     if (J < 2) J = 2;
     if (J > 30) J = 30;
+    // leading sweeps on the BF16 planes: the last Jf contract their error
+    const int Jf = (int)ceil(log(0.01 * tol / mx / kBf16Err) / log(rho_eff)) + 2;
+    const int Jb = J - Jf > 0 ? J - Jf : 0;
     const long len = (long)p * n;
     a->stats.kernel_launches++;
     // D = R S Theta^-1 (Y = 0)
@@ -1142,7 +1177,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     int every = spread > 1.0 + 1e-12 ? (int)floor(log(4.0) / log(spread)) : J;
     if (every < 1) every = 1;
     for (int j = 0; j < J; ++j) {
-      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true))) return rc;
+      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true, j < Jb))) return rc;
       if ((j + 1) % every == 0 || j + 1 == J) {
         block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
         a->stats.kernel_launches++;
@@ -1298,7 +1333,8 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   double rate = 0.0, floor1 = 1e-6;
   std::vector<double> r1(k);
   std::vector<cplx> th32;
-  int st = subspace<C>(a, b, true, tol > 1e-7 ? tol : 1e-7, 60, r1.data(), false, b64, &rate, 0, &floor1, &th32);
+  int st = subspace<C>(a, b, true, tol > kFp32Goal ? tol : kFp32Goal, 60, r1.data(), false, b64, &rate, 0, &floor1,
+                       &th32);
   if (st == OAPB_OK && C && a->cfg.sort == 0 && a->cfg.refine && (int)th32.size() > k && cabs_(th32[k - 1]) > 0) {
     // largest-magnitude wanted set: the correction contracts by |theta_{k+1}| / |theta_k|
     const double rho = cabs_(th32[k]) / cabs_(th32[k - 1]);
@@ -1348,7 +1384,9 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   if (!resume) a->stats.restarts = 0;  // a resumed solve continues the saved count
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
+  a->stats.block_bf16 = 0;
   a->stats.refine_iterations = 0;
+  a->trace.clear();
   a->stats.dgks_passes = 0;
   a->stats.fallbacks = 0;
   int rc = alloc_blocks(a);
@@ -1785,6 +1823,8 @@ static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
   a->stats.block_timed = 0;
   a->stats.block_fp32_seconds = 0;
   a->stats.block_fp32_timed = 0;
+  a->stats.block_bf16_seconds = 0;
+  a->stats.block_bf16_timed = 0;
   if (a->ev_used) {
     cudaStreamSynchronize(a->stream);
     for (size_t i = 0; i + 1 < a->ev_used; i += 2) {
@@ -1797,6 +1837,9 @@ static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
       } else if (kind == 1) {
         a->stats.block_seconds += ms * 1e-3;
         a->stats.block_timed++;
+      } else if (kind == 5) {
+        a->stats.block_bf16_seconds += ms * 1e-3;
+        a->stats.block_bf16_timed++;
       } else {
         a->stats.block_fp32_seconds += ms * 1e-3;
         a->stats.block_fp32_timed++;
@@ -1848,12 +1891,14 @@ int oapb_arnoldi_apply_block(oapb_arnoldi* a, const double* xre, const double* x
                              double* wim, int32_t precision) {
   if (!a || !xre || !wre || b == 0 || b > (uint32_t)kBmMaxB || a->cb || !a->a64re) return OAPB_ERR_ARG;
   if (a->is_c && (!xim || !wim)) return OAPB_ERR_ARG;
-  const bool fp32 = precision == OAPB_PREC_MIXED;
+  if (precision != OAPB_PREC_FP64 && precision != OAPB_PREC_MIXED && precision != OAPB_PASS_BF16)
+    return OAPB_ERR_ARG;
+  const bool fp32 = precision != OAPB_PREC_FP64, bf16 = precision == OAPB_PASS_BF16;
   if (fp32 && !a->a32re) return OAPB_ERR_ARG;
   int rc = alloc_blocks(a);
   if (rc) return rc;
-  rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32)
-               : block_apply<false>(a, xre, nullptr, (int)b, wre, nullptr, fp32);
+  rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32, bf16)
+               : block_apply<false>(a, xre, nullptr, (int)b, wre, nullptr, fp32, bf16);
   if (rc) return rc;
   int tcerr = 0;
   if (a->tcerr && cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
@@ -1865,6 +1910,13 @@ int oapb_arnoldi_apply_block(oapb_arnoldi* a, const double* xre, const double* x
 int oapb_arnoldi_get_stats(const oapb_arnoldi* a, oapb_arnoldi_stats* out) {
   if (!a || !out) return OAPB_ERR_ARG;
   *out = a->stats;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_get_trace(const oapb_arnoldi* a, oapb_trace_rec* out, uint32_t cap, uint32_t* count) {
+  if (!a || !count || (cap && !out)) return OAPB_ERR_ARG;
+  *count = (uint32_t)a->trace.size();
+  for (uint32_t i = 0; i < cap && i < *count; ++i) out[i] = a->trace[i];
   return OAPB_OK;
 }
 

@@ -34,7 +34,7 @@ def solve(A, k, m, sort="LM", precision=B.PREC_FP64, seed=1, vectors=False, **kw
 
 
 def test_planted_symmetric_n256():
-    # n=256 float64, lambda 1 .. 1e-3, top-5 LM, m=32
+    # the reference's CPU-sized case: n=256 float64, lambda 1 .. 1e-3, top-5 LM, m=32
     A, lam = planted_symmetric(256, seed=0)
     r = solve(A, 5, 32, vectors=True)
     assert np.allclose(np.sort(r["ev"].real)[::-1], lam[:5], rtol=1e-10, atol=0)
@@ -156,6 +156,27 @@ def test_mixed_precision_reaches_fp64_residual(n, refine):
         assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * np.abs(r["ev"]).max() * 1.01
 
 
+def test_mixed_trace_and_bf16_passes():
+    # the convergence trace of a mixed solve: FP32-class checks with falling
+    # residuals, then the refinement's outer steps down to the goal; the
+    # leading powers run on the BF16 planes, and the FP32-class passes before
+    # each check keep the measured residuals on the FP32-class operator
+    A = planted_complex(8192, seed=11, nplant=8)
+    r = solve(A, 8, 40, precision=B.PREC_MIXED)
+    tr = r["solver"].trace()
+    st = r["stats"]
+    assert st["converged"] == 1 and r["res"].max() <= TOL
+    assert [t[0] for t in tr if t[0] != 1] and all(t[0] in (1, 3) for t in tr)
+    p1 = [t for t in tr if t[0] == 1]
+    assert p1 and p1[0][3] >= 1 and st["block_bf16"] >= p1[0][3]
+    assert all(a[4] > b[4] for a, b in zip(p1, p1[1:3]))
+    assert tr[-1][0] == 3 and tr[-1][4] <= TOL
+    assert all(a[2] < b[2] for a, b in zip(tr, tr[1:]))
+    # CUDA-core passes (tensor_cores = 0) take no BF16 pass
+    r0 = solve(A, 8, 40, precision=B.PREC_MIXED, tensor_cores=False)
+    assert r0["stats"]["block_bf16"] == 0 and r0["res"].max() <= TOL
+
+
 @pytest.mark.parametrize("gap", ["separated", "clustered"])
 def test_mixed_precision_real_symmetric(gap):
     # separated: 4 eigenvalues well above the rest; clustered: the geometric
@@ -193,8 +214,9 @@ def test_block_pass_precisions(cplx, n, b):
     X = xr if not cplx else torch.complex(xr, xi)
     ref = (A @ X.T).T
     scale = (A.abs() @ X.abs().T).T
+    # (the BF16 pass: operator rounded to BF16, unit roundoff 2^-8 = 3.9e-3, X split)
     for prec, tc, tol in ((B.PREC_FP64, True, 1e-13), (B.PREC_FP64, False, 1e-13), (B.PREC_MIXED, False, 2e-6),
-                          (B.PREC_MIXED, True, 1e-4)):
+                          (B.PREC_MIXED, True, 1e-4), (B.PASS_BF16, True, 4e-3)):
         s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=tc)
         s.set_operator(are, aim)
         wr, wi = s.apply_block(xr, xi, precision=prec)
