@@ -161,7 +161,7 @@ __device__ __forceinline__ bool btc_wait(uint64_t* bar, uint32_t parity, volatil
 // sums held in registers (QB is a compile-time constant, so every index is
 // static); a tile's sums are stored to its stream-K partial once, when the
 // CTA's share of the tile ends, so no global load waits in the loop.
-template <bool CPLX, int QB>
+template <bool CPLX, int QB, int KSUB>
 __device__ __forceinline__ void btc_epilogue(const BtcArgs& g, uint32_t tmem, uint64_t* accf, uint64_t* acce,
                                              volatile int* abort, long it0, long it1, long kch, long first_tile,
                                              int warp, int lane) {
@@ -174,7 +174,7 @@ __device__ __forceinline__ void btc_epilogue(const BtcArgs& g, uint32_t tmem, ui
   bool ok = true;
   for (long it = it0; it < it1; ++seg) {
     const long tile = it / kch, kc = it % kch;
-    long kc_end = (kc / kBtcSub + 1) * kBtcSub;
+    long kc_end = (kc / KSUB + 1) * KSUB;
     if (kc_end > kch) kc_end = kch;
     it = min(it1, tile * kch + kc_end);
     const int buf = (int)(seg & 1);
@@ -232,7 +232,10 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   __shared__ uint32_t tmem_slot;
   __shared__ volatile int abort_flag;
   constexpr int NPL = CPLX ? 2 : 1;         // operator planes (re, im)
-  constexpr int NA = LO ? 2 * NPL : NPL;  // operator tiles per stage (hi [, lo] per plane)
+  constexpr int NR = LO ? 2 : 1;            // parts per plane (hi [, lo])
+  constexpr int KH = LO ? 1 : 2;            // 64-column K chunks per stage
+  constexpr int NA = NPL * NR * KH;         // operator tiles per stage, index (p * NR + r) * KH + h
+  constexpr int KSUB = kBtcSub / KH;        // stages per FP32 segment
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* sm = (uint8_t*)(((uintptr_t)bsm_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = tc::smem_u32(sm);
@@ -264,19 +267,27 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   if (warp == 0) {
     // ---------------------------------------------------------- producer --
     if (lane == 0) {
-      const uint32_t tx = NA * a_tile + 2 * b_tile;
+      const uint32_t tx = NA * a_tile + 2 * KH * b_tile;
       long it = it0;
       for (; it < it1; ++it) {
         const long i = it - it0;
         const int s = (int)(i % S);
         if (i >= S && !btc_wait(&empty[s], (uint32_t)((i / S - 1) & 1), &abort_flag)) break;
         const uint32_t st = sbase + s * g.stage_bytes;
-        const int x = (int)((it % kch) * kBtcK), y = (int)((it / kch) * kBtcM);
+        const int x = (int)((it % kch) * kBtcK * KH), y = (int)((it / kch) * kBtcM);
         mbar_expect_tx(&full[s], tx);
 #pragma unroll
-        for (int p = 0; p < NA; ++p) tma_load_2d(st + p * a_tile, &g.tm[LO ? p : 2 * p], x, y, &full[s]);
-        tma_load_2d(st + NA * a_tile, &g.tm[4], x, 0, &full[s]);
-        tma_load_2d(st + NA * a_tile + b_tile, &g.tm[5], x, 0, &full[s]);
+        for (int p = 0; p < NPL; ++p)
+#pragma unroll
+          for (int r = 0; r < NR; ++r)
+#pragma unroll
+            for (int h = 0; h < KH; ++h)
+              tma_load_2d(st + ((p * NR + r) * KH + h) * a_tile, &g.tm[2 * p + r], x + h * kBtcK, y, &full[s]);
+#pragma unroll
+        for (int h = 0; h < KH; ++h) {
+          tma_load_2d(st + NA * a_tile + h * b_tile, &g.tm[4], x + h * kBtcK, 0, &full[s]);
+          tma_load_2d(st + NA * a_tile + (KH + h) * b_tile, &g.tm[5], x + h * kBtcK, 0, &full[s]);
+        }
       }
       // no copy may still be landing in shared memory when the CTA exits:
       // wait for the last stage loads issued (already consumed normally)
@@ -295,31 +306,35 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
         const long i = it - it0;
         const int s = (int)(i % S);
         const long kc = it % kch;
-        const bool seg_first = it == it0 || kc % kBtcSub == 0;
+        const bool seg_first = it == it0 || kc % KSUB == 0;
         const int buf = (int)(seg & 1);
         if (seg_first && seg >= 2 && !btc_wait(&acce[buf], (uint32_t)((seg / 2 - 1) & 1), &abort_flag)) break;
         if (!btc_wait(&full[s], (uint32_t)((i / S) & 1), &abort_flag)) break;
         tc::tc_fence_after();
         const uint32_t st = sbase + s * g.stage_bytes;
-        const uint64_t bh = tc::sdesc_k_sw128(st + NA * a_tile), bl = tc::sdesc_k_sw128(st + NA * a_tile + b_tile);
 #pragma unroll
-        for (int kk = 0; kk < kBtcK / 16; ++kk) {
-          const uint64_t off = (uint64_t)(kk * 32) >> 4;
-          const uint32_t acc0 = (seg_first && kk == 0) ? 0u : 1u;
+        for (int h = 0; h < KH; ++h) {
+          const uint64_t bh = tc::sdesc_k_sw128(st + NA * a_tile + h * b_tile);
+          const uint64_t bl = tc::sdesc_k_sw128(st + NA * a_tile + (KH + h) * b_tile);
 #pragma unroll
-          for (int p = 0; p < NPL; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
-            const uint64_t ah = tc::sdesc_k_sw128(st + (LO ? 2 * p : p) * a_tile) + off;
-            const uint32_t d = tmem + buf * 128 + p * 64;
-            tc::mma_bf16(d, ah, bh + off, idesc, acc0);
-            tc::mma_bf16(d, ah, bl + off, idesc, 1u);
-            if (LO) {
-              const uint64_t al = tc::sdesc_k_sw128(st + (2 * p + 1) * a_tile) + off;
-              tc::mma_bf16(d, al, bh + off, idesc, 1u);
+          for (int kk = 0; kk < kBtcK / 16; ++kk) {
+            const uint64_t off = (uint64_t)(kk * 32) >> 4;
+            const uint32_t acc0 = (seg_first && h == 0 && kk == 0) ? 0u : 1u;
+#pragma unroll
+            for (int p = 0; p < NPL; ++p) {  // p = 0: real plane -> D1, p = 1: imaginary plane -> D2
+              const uint64_t ah = tc::sdesc_k_sw128(st + (p * NR * KH + h) * a_tile) + off;
+              const uint32_t d = tmem + buf * 128 + p * 64;
+              tc::mma_bf16(d, ah, bh + off, idesc, acc0);
+              tc::mma_bf16(d, ah, bl + off, idesc, 1u);
+              if (LO) {
+                const uint64_t al = tc::sdesc_k_sw128(st + ((p * NR + 1) * KH + h) * a_tile) + off;
+                tc::mma_bf16(d, al, bh + off, idesc, 1u);
+              }
             }
           }
         }
         tc::commit(&empty[s]);
-        if (it + 1 == it1 || (kc + 1) % kBtcSub == 0 || kc + 1 == kch) {
+        if (it + 1 == it1 || (kc + 1) % KSUB == 0 || kc + 1 == kch) {
           tc::commit(&accf[buf]);
           ++seg;
         }
@@ -332,16 +347,16 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
     // ---------------------------------------------------------- epilogue --
     switch (g.QB) {
       case 8:
-        btc_epilogue<CPLX, 8>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        btc_epilogue<CPLX, 8, KSUB>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
         break;
       case 16:
-        btc_epilogue<CPLX, 16>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        btc_epilogue<CPLX, 16, KSUB>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
         break;
       case 24:
-        btc_epilogue<CPLX, 24>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        btc_epilogue<CPLX, 24, KSUB>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
         break;
       default:
-        btc_epilogue<CPLX, 32>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
+        btc_epilogue<CPLX, 32, KSUB>(g, tmem, accf, acce, &abort_flag, it0, it1, kch, first_tile, warp, lane);
         break;
     }
   }
@@ -380,9 +395,11 @@ static bool make_tmap(CUtensorMap* m, const __nv_bfloat16* base, int kp, int row
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// one stage: lo -> 1 K chunk of hi + lo planes; else 2 K chunks of the hi planes
 static size_t btc_stage_bytes(int N, bool cplx, bool lo) {
-  const int NA = (cplx ? 2 : 1) * (lo ? 2 : 1);
-  return ((size_t)(NA * kBtcM * 128 + 2 * N * 128) + 1023) & ~(size_t)1023;
+  const int KH = lo ? 1 : 2;
+  const int NA = (cplx ? 2 : 1) * (lo ? 2 : 1) * KH;
+  return ((size_t)(NA * kBtcM * 128 + 2 * KH * N * 128) + 1023) & ~(size_t)1023;
 }
 
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s) {
@@ -390,15 +407,22 @@ int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 
-static SkGrid btc_grid(int n, int kp) { return sk_grid((n + kBtcM - 1) / kBtcM, kp / kBtcK, kNumSMs); }
+// stream-K grid over (tile, stage) iterations of kh K chunks each
+static SkGrid btc_grid(int n, int kp, int kh) {
+  return sk_grid((n + kBtcM - 1) / kBtcM, kp / (kBtcK * kh), kNumSMs);
+}
 
-size_t btc_workspace(int n, int kp) { return sk_workspace(btc_grid(n, kp)); }
+size_t btc_workspace(int n, int kp) {
+  const size_t a = sk_workspace(btc_grid(n, kp, 1)), b = sk_workspace(btc_grid(n, kp, 2));
+  return a > b ? a : b;
+}
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
                            cudaStream_t s, bool bf16_only) {
   const bool cplx = op.aih != nullptr;
-  if (b < 1 || b > 32 || op.kp % kBtcK != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
+  const int kh = bf16_only ? 2 : 1;
+  if (b < 1 || b > 32 || op.kp % (kBtcK * kh) != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
@@ -410,7 +434,7 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   if (!make_tmap(&g.tm[4], xbh, op.kp, N, N) || !make_tmap(&g.tm[5], xbl, op.kp, N, N)) return OAPB_ERR_CUDA;
   g.ws = ws;
   g.err = err;
-  g.grid = btc_grid(op.n, op.kp);
+  g.grid = btc_grid(op.n, op.kp, kh);
   g.n = op.n;
   g.b = b;
   g.QB = QB;

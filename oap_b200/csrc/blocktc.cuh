@@ -7,7 +7,7 @@
 
 namespace oapb {
 
-// Operator stored as BF16 hi / lo planes, n x kp (kp = n rounded up to 64,
+// Operator stored as BF16 hi / lo planes, n x kp (kp = n rounded up to 128,
 // zero-padded columns); aih / ail are NULL for a real operator.
 struct BtcOperator {
   const __nv_bfloat16 *arh, *arl, *aih, *ail;

@@ -464,6 +464,13 @@ struct oapb_arnoldi {
   DevState* bst = nullptr;
   int ndot = 0, nnorm = 0;
   unsigned* bdone = nullptr;  // arrival counter of k_block_reduce (self-resetting)
+  // the FP32-class phase's Rayleigh-Ritz checks run on a second stream while
+  // the main stream takes the next power: own Gram scratch, pinned outputs
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t ev_w = nullptr, ev_chk = nullptr;
+  cplx* bpart2 = nullptr;
+  unsigned* bdone2 = nullptr;
+  unsigned char* hpin = nullptr;  // pinned: norm partials, Ritz values, DevState, tcerr
   int nvec_hess = 0;
   double* Wp = nullptr;   // split-K partials of the block matvec
   double* wdm = nullptr;  // stream-K partials of the tensor-core passes
@@ -698,6 +705,14 @@ int ritz_vectors(oapb_arnoldi* a, int nv) {
 }
 
 // ---------------------------------------------------------------- blocks --
+// pinned check outputs: norm partials (kBmMaxB x nnorm), Ritz values
+// (kBmMaxB), DevState, the tensor-core error word
+size_t pin_norm_off(const oapb_arnoldi*) { return 0; }
+size_t pin_ritz_off(const oapb_arnoldi* a) { return (sizeof(double) * kBmMaxB * (size_t)a->nnorm + 63) & ~(size_t)63; }
+size_t pin_st_off(const oapb_arnoldi* a) { return pin_ritz_off(a) + ((sizeof(cplx) * kBmMaxB + 63) & ~(size_t)63); }
+size_t pin_err_off(const oapb_arnoldi* a) { return pin_st_off(a) + ((sizeof(DevState) + 63) & ~(size_t)63); }
+size_t pin_bytes(const oapb_arnoldi* a) { return pin_err_off(a) + 64; }
+
 int alloc_blocks(oapb_arnoldi* a) {
   if (a->Bre[0]) return OAPB_OK;
   const size_t vb = sizeof(double) * (size_t)a->n * kBmMaxB;
@@ -720,7 +735,7 @@ int alloc_blocks(oapb_arnoldi* a) {
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
   }
   if (!a->cb && !a->gX) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
-    size_t need = btc_workspace(a->n, (a->n + 63) / 64 * 64);
+    size_t need = btc_workspace(a->n, (a->n + 127) / 128 * 128);
     if (dmma_plan(a->n, &a->dplan)) {
       need = std::max(need, dmma_workspace(a->dplan));
       a->have_dmma = true;
@@ -745,6 +760,14 @@ int alloc_blocks(oapb_arnoldi* a) {
   rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
   rc |= dalloc(&a->bstatus, sizeof(int));
   rc |= dalloc(&a->bst, sizeof(DevState));
+  rc |= dalloc(&a->bpart2, bb * (size_t)a->ndot);
+  rc |= dalloc(&a->bdone2, sizeof(unsigned));
+  if (a->bdone2 && cudaMemset(a->bdone2, 0, sizeof(unsigned)) != cudaSuccess) rc |= OAPB_ERR_CUDA;
+  if (cudaMallocHost((void**)&a->hpin, pin_bytes(a)) != cudaSuccess) {
+    a->hpin = nullptr;
+    cudaGetLastError();
+    rc |= OAPB_ERR_NOMEM;
+  }
   return rc ? OAPB_ERR_NOMEM : OAPB_OK;
 }
 
@@ -887,6 +910,81 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
   return launch_check();
 }
 
+// Rayleigh-Ritz check of the block X (b vectors) with W = A X, enqueued on
+// stream cs: G = X^H W, R = W - X G, the eigenpairs (theta, S) of G, E = R S
+// (kk columns), the column-norm partials of E, the Ritz values, the small
+// eigensolver's state and the tensor-core error word copied to pinned host
+// memory; a->ev_chk is recorded on cs.  With cs != a->stream the check uses
+// the second Gram scratch, so that the main stream may run cholqr2 and the
+// next pass meanwhile (they read X and W and write neither).
+template <bool C>
+int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const double* Xi, const double* W,
+                  const double* Wi, double* R, double* Ri, double* E, double* Ei, int b, int kk, int nv, bool fp32) {
+  const int n = a->n;
+  const bool side = cs != a->stream;
+  cudaStream_t s0 = a->stream;
+  cplx* bp0 = a->bpart;
+  unsigned* bd0 = a->bdone;
+  a->stream = cs;
+  if (side) {
+    a->bpart = a->bpart2;
+    a->bdone = a->bdone2;
+  }
+  block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
+  a->stats.kernel_launches += 3;
+  k_block_update<C><<<grid_up(n), 256, 0, cs>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
+  int rc = small_eig(a, a->G, b, kk, nv, fp32);
+  if (!rc) {
+    k_block_update<C><<<grid_up(n), 256, 0, cs>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
+    k_colnorm2<C><<<a->nnorm, 256, 0, cs>>>(E, Ei, kk, n, a->bnorm);
+    rc = launch_check();
+  }
+  a->stream = s0;
+  a->bpart = bp0;
+  a->bdone = bd0;
+  if (rc) return rc;
+  unsigned char* hp = a->hpin;
+  if (cudaMemcpyAsync(hp + pin_norm_off(a), a->bnorm, sizeof(double) * kk * (size_t)a->nnorm, cudaMemcpyDeviceToHost,
+                      cs) != cudaSuccess ||
+      cudaMemcpyAsync(hp + pin_ritz_off(a), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
+      cudaMemcpyAsync(hp + pin_st_off(a), a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  *(int*)(hp + pin_err_off(a)) = 0;
+  if (a->tcerr &&
+      cudaMemcpyAsync(hp + pin_err_off(a), a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  return cudaEventRecord(a->ev_chk, cs) == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
+}
+
+// wait for the enqueued check: Ritz values (b) and residual norms ||E_q|| (kk)
+int check_collect(oapb_arnoldi* a, int b, int kk, cplx* th, double* norms) {
+  if (cudaEventSynchronize(a->ev_chk) != cudaSuccess) return OAPB_ERR_CUDA;
+  const unsigned char* hp = a->hpin;
+  const double* part = (const double*)(hp + pin_norm_off(a));
+  for (int q = 0; q < kk; ++q) {
+    double s = 0;
+    for (int blk = 0; blk < a->nnorm; ++blk) s += part[(size_t)blk * kk + q];
+    norms[q] = sqrt(s);
+  }
+  memcpy(th, hp + pin_ritz_off(a), sizeof(cplx) * b);
+  DevState bs;
+  memcpy(&bs, hp + pin_st_off(a), sizeof(DevState));
+  const int tcerr = *(const int*)(hp + pin_err_off(a));
+  return ((bs.status & 2) || tcerr) ? OAPB_ERR_TIMEOUT : OAPB_OK;
+}
+
+// second stream and events of the overlapped checks (created once)
+int ensure_side_stream(oapb_arnoldi* a) {
+  if (a->s2) return OAPB_OK;
+  if (cudaEventCreateWithFlags(&a->ev_w, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&a->ev_chk, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&a->s2, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    return OAPB_ERR_CUDA;
+  }
+  return OAPB_OK;
+}
+
 constexpr int kSlow = 100;   // subspace(): convergence too slow for the iteration budget
 constexpr int kMixedMinN = 8192;
 // BF16 operator passes (tensor cores only).  In the FP32-class subspace
@@ -927,9 +1025,11 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   const int n = a->n, kk = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3];
   double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3];
+  double *Xn = a->Bre[4], *Wn = a->Bre[5], *Xni = a->Bim[4], *Wni = a->Bim[5];  // the overlapped next power
   if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   int rc = OAPB_OK;
+  if (fp32 && (rc = ensure_side_stream(a))) return rc;
   if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei, 2))) return rc;
   const int nv = (fp32 && b_next > kk) ? b_next : kk;
   std::vector<double> norms(kk), hist;
@@ -948,6 +1048,10 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   // from the first check on) and always right before a check; otherwise the
   // next pass takes W itself (the span is what the iteration carries).
   double growth = 0, drift = 1;
+  // FP32 phase: a check that is not expected to meet the goal runs on the
+  // second stream while the main stream orthonormalises W and takes the
+  // next power into (Xn, Wn); `pre` marks an iteration whose W is there.
+  bool pre = false;
   for (unsigned it = 0; it < max_it; ++it) {
     bool bf16 = false;
     if (fp32 && !from_bx && it + 1 < next_check) {
@@ -959,7 +1063,8 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       }
       bf16 = est >= kBf16Until;
     }
-    if ((rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32, bf16))) return rc;
+    if (!pre && (rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32, bf16))) return rc;
+    pre = false;
     const bool check = fp32 ? (it >= next_check || it + 1 == max_it)
                             : ((int)it >= skip || it + 1 == max_it);
     if (!check) {
@@ -974,20 +1079,25 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
       continue;
     }
-    block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
-    a->stats.kernel_launches += 5;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
-    if ((rc = small_eig(a, a->G, b, kk, nv, fp32))) return rc;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
-    if ((rc = col_norms<C>(a, E, Ei, kk, norms.data()))) return rc;
-    if (cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * b, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
-      return OAPB_ERR_CUDA;
-    DevState bs;
-    int tcerr = 0;
-    cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
-    if (a->tcerr) cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
-    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-    if ((bs.status & 2) || tcerr) return OAPB_ERR_TIMEOUT;
+    // overlap unless this check is predicted to meet the goal
+    bool overlap = fp32 && it + 1 < max_it && hist.size() < 2;
+    if (fp32 && it + 1 < max_it && hist.size() >= 2) {
+      const size_t h = hist.size();
+      const double r = pow(hist[h - 1] / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2]));
+      overlap = !(r < 1.0 && hist[h - 1] * pow(r, (double)((int)it - hist_it[h - 1])) <= 1.5 * tol);
+    }
+    const uint32_t passes_now = a->stats.block_matvecs, bf16_now = a->stats.block_bf16;
+    if (overlap) {
+      if (cudaEventRecord(a->ev_w, a->stream) != cudaSuccess || cudaStreamWaitEvent(a->s2, a->ev_w, 0) != cudaSuccess)
+        return OAPB_ERR_CUDA;
+    }
+    if ((rc = check_enqueue<C>(a, overlap ? a->s2 : a->stream, X, Xi, W, Wi, R, Ri, E, Ei, b, kk, nv, fp32)))
+      return rc;
+    if (overlap) {  // X' = orth(W), W' = A X' meanwhile
+      if ((rc = cholqr2<C>(a, W, Wi, b, Xn, Xni, E, Ei, 1))) return rc;
+      if ((rc = block_apply<C>(a, Xn, Xni, b, Wn, Wni, true, false))) return rc;
+    }
+    if ((rc = check_collect(a, b, kk, th.data(), norms.data()))) return rc;
     double scale = 0;
     for (int q = 0; q < kk; ++q) scale = fmax(scale, cabs_(th[q]));
     if (scale == 0) scale = 1;
@@ -1008,7 +1118,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
     hist.push_back(mx);
     hist_it.push_back((int)it);
     a->stats.refine_iterations++;
-    a->trace.push_back({fp32 ? 1 : 2, (int)it, a->stats.block_matvecs, a->stats.block_bf16, mx});
+    a->trace.push_back({fp32 ? 1 : 2, (int)it, passes_now, bf16_now, mx});
     const bool done = mx <= tol;
     bool stop = done;
     if (fp32) {
@@ -1017,8 +1127,11 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       if (h >= 2 && !done) {
         const double r2 = pow(mx / hist[h - 2], 1.0 / (hist_it[h - 1] - hist_it[h - 2]));
         if (r2 > 0 && r2 < 0.9) {
+          // the iteration the observed contraction predicts for the goal: a
+          // check that comes one iteration early costs a Rayleigh-Ritz step
+          // and a host synchronisation, about as much as one pass more
           const double need = log(tol / mx) / log(r2);
-          step = need < 1 ? 1u : (unsigned)ceil(0.9 * need);
+          step = need < 1.1 ? 1u : (unsigned)ceil(need - 0.1);
           if (step > 6) step = 6;
         }
       }
@@ -1058,6 +1171,14 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       a->evals.assign(th.begin(), th.begin() + kk);
       if ((rc = launch_check())) return rc;
       return done ? OAPB_OK : OAPB_NOT_CONVERGED;
+    }
+    if (overlap) {  // the next power is there: X <- orth(W), W <- A X
+      std::swap(X, Xn);
+      std::swap(W, Wn);
+      std::swap(Xi, Xni);
+      std::swap(Wi, Wni);
+      pre = true;
+      continue;
     }
     if ((rc = cholqr2<C>(a, W, Wi, b, X, Xi, E, Ei, passes))) return rc;
   }
@@ -1414,13 +1535,17 @@ void free_all(oapb_arnoldi* a) {
   for (void* p : ps)
     if (p) cudaFree(p);
   void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
-                a->bstatus, a->bst};
+                a->bstatus, a->bst, a->bpart2, a->bdone2};
   for (void* p : bs)
     if (p) cudaFree(p);
   for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
     if (a->Bre[i]) cudaFree(a->Bre[i]);
     if (a->Bim[i]) cudaFree(a->Bim[i]);
   }
+  if (a->hpin) cudaFreeHost(a->hpin);
+  if (a->ev_w) cudaEventDestroy(a->ev_w);
+  if (a->ev_chk) cudaEventDestroy(a->ev_chk);
+  if (a->s2) cudaStreamDestroy(a->s2);
 }
 
 }  // namespace
@@ -1574,6 +1699,7 @@ int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void
 int oapb_arnoldi_destroy(oapb_arnoldi* a) {
   if (!a) return OAPB_ERR_ARG;
   cudaStreamSynchronize(a->stream);
+  if (a->s2) cudaStreamSynchronize(a->s2);
   for (cudaEvent_t e : a->ev_pool) cudaEventDestroy(e);
   free_all(a);
   if (a->own_stream) cudaStreamDestroy(a->stream);
@@ -1589,7 +1715,7 @@ static int make_fp32_copy(oapb_arnoldi* a) {
   if (a->is_c && !a->x32im && dalloc(&a->x32im, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   const int g = kNumSMs * 8;
   if (a->cfg.tensor_cores) {
-    a->kp = (a->n + 63) / 64 * 64;
+    a->kp = (a->n + 127) / 128 * 128;
     const size_t plane = (size_t)a->n * a->kp;
     const int np = a->is_c ? 4 : 2;
     if (!a->abf && dalloc(&a->abf, sizeof(__nv_bfloat16) * plane * np)) return OAPB_ERR_NOMEM;

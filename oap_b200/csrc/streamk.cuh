@@ -31,6 +31,10 @@ inline SkGrid sk_grid(long tiles, long kchunks, long ctas) {
   p.tiles = tiles;
   p.kchunks = kchunks;
   p.total = tiles * kchunks;
+  if (p.total <= 0) {  // nothing to do (no grid, no workspace)
+    p.grid = p.slots = 0;
+    return p;
+  }
   const long G = ctas < p.total ? ctas : p.total;
   p.grid = (int)G;
   // tiles one CTA can touch: its share spans at most ceil(share / kchunks) + 1
