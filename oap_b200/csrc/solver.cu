@@ -1271,13 +1271,15 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     if (cudaMemcpyAsync(a->thinv, thinv.data(), sizeof(cplx) * p, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
     // inner iterations for a correction about 100x below the goal; the
-    // observed contraction of non-normal problems is slower than rho
+    // observed contraction of non-normal problems is slower than rho, so
+    // the count assumes at least 0.3 per sweep (a shortfall costs one more
+    // outer step, not the result)
     const double rho_eff = rho > 0.3 ? rho : 0.3;
-    int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff)) + 2;
+    int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff));
     if (J < 2) J = 2;
     if (J > 30) J = 30;
     // leading sweeps on the BF16 planes: the last Jf contract their error
-    const int Jf = (int)ceil(log(0.01 * tol / mx / kBf16Err) / log(rho_eff)) + 2;
+    const int Jf = (int)ceil(log(0.01 * tol / mx / kBf16Err) / log(rho_eff));
     const int Jb = J - Jf > 0 ? J - Jf : 0;
     const long len = (long)p * n;
     a->stats.kernel_launches++;

@@ -47,31 +47,46 @@ inline SkGrid sk_grid(long tiles, long kchunks, long ctas) {
 inline size_t sk_workspace(const SkGrid& p) { return (size_t)p.grid * p.slots * 2 * 32 * kSkRows; }
 
 // W[plane][q][row] = sum of the partials of the row's tile; block (tile,
-// plane * b + q), one thread per row of the tile
+// group of kSkCols output columns pq = plane * b + q), one thread per row of
+// the tile: the owners of the tile are found once, then each owner's
+// partials of the group are independent loads
+constexpr int kSkCols = 8;
 template <bool CPLX>
 __global__ void __launch_bounds__(kSkRows) k_sk_reduce(const double* __restrict__ ws, SkGrid p, int n, int b,
                                                        double* wr, double* wi) {
   constexpr int NP = CPLX ? 2 : 1;
   const long tile = blockIdx.x;
-  const int pq = blockIdx.y;
+  const int pq0 = blockIdx.y * kSkCols, npq = NP * b;
   const long row = tile * kSkRows + threadIdx.x;
   if (row >= n) return;
   const long ilo = tile * p.kchunks;
   const long ihi = min(p.total, ilo + p.kchunks) - 1;
   const long c0 = sk_owner(ilo, p.total, p.grid), c1 = sk_owner(ihi, p.total, p.grid);
-  double s = 0.0;
+  double s[kSkCols];
+#pragma unroll
+  for (int j = 0; j < kSkCols; ++j) s[j] = 0.0;
   for (long c = c0; c <= c1; ++c) {
     const long slot = tile - sk_begin(c, p.total, p.grid) / p.kchunks;
-    s += ws[(((size_t)c * p.slots + slot) * NP * b + pq) * kSkRows + threadIdx.x];
+    const double* src = ws + (((size_t)c * p.slots + slot) * npq + pq0) * kSkRows + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < kSkCols; ++j)
+      if (pq0 + j < npq) s[j] += src[(size_t)j * kSkRows];
   }
-  const int q = pq % b, plane = pq / b;
-  (plane == 0 ? wr : wi)[(long)q * n + row] = s;
+#pragma unroll
+  for (int j = 0; j < kSkCols; ++j) {
+    const int pq = pq0 + j;
+    if (pq < npq) {
+      const int q = pq % b, plane = pq / b;
+      (plane == 0 ? wr : wi)[(long)q * n + row] = s[j];
+    }
+  }
 }
 
 template <bool CPLX>
 inline void launch_sk_reduce(const double* ws, const SkGrid& p, int n, int b, double* wr, double* wi,
                              cudaStream_t s) {
-  k_sk_reduce<CPLX><<<dim3((unsigned)p.tiles, (CPLX ? 2 : 1) * b), kSkRows, 0, s>>>(ws, p, n, b, wr, wi);
+  const int npq = (CPLX ? 2 : 1) * b;
+  k_sk_reduce<CPLX><<<dim3((unsigned)p.tiles, (npq + kSkCols - 1) / kSkCols), kSkRows, 0, s>>>(ws, p, n, b, wr, wi);
 }
 
 }  // namespace oapb
