@@ -9,7 +9,7 @@
 //   k_block_dot      part = X^H Y   per row chunk (b1 x b2)
 //   k_block_reduce   G = sum of chunk partials (optionally followed by the
 //                    Cholesky inverse in the last block to finish)
-//   k_block_update   Out = Base - X C   (C column-major b1 x b2)
+//   k_block_update   Out = Base - X C   (C column-major b1 x b2; X + Y with an addend Y)
 //   k_colnorm2       per-column ||Y_q||^2 partials
 //   k_chol_inv       one warp: G = R^H R (Cholesky), Rinv = R^-1
 #pragma once
@@ -330,6 +330,64 @@ __global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rin
   warp_chol_inv(G, b, Rinv, status, sm, threadIdx.x);
 }
 
+// Tinv = T^-1 of a general p x p complex T (column-major, p <= kBmMaxB) by
+// Gauss-Jordan elimination with partial pivoting on one warp: [T | I] is
+// reduced to [I | T^-1], lane l owning columns l and l + 32 of the
+// augmented matrix.  A zero pivot sets bit 8 of *status (Tinv undefined).
+__global__ void __launch_bounds__(32) k_small_inv(const cplx* __restrict__ T, int p, cplx* Tinv, int* status) {
+  constexpr int LD = kBmMaxB + 1;
+  __shared__ cplx M[2 * kBmMaxB * LD];  // column c at M + c LD
+  __shared__ cplx fk[kBmMaxB];
+  const int lane = threadIdx.x;
+  if (p < 1 || p > kBmMaxB) return;
+  for (int e = lane; e < p * p; e += 32) M[(e % p) + (e / p) * LD] = T[e];
+  for (int e = lane; e < p * p; e += 32) M[(e % p) + (p + e / p) * LD] = cplx{(e % p) == (e / p) ? 1.0 : 0.0, 0.0};
+  __syncwarp();
+  for (int k = 0; k < p; ++k) {
+    // pivot row: the largest |M[i][k]|, i >= k (lowest index on ties)
+    double best = -1;
+    int bi = k;
+    for (int i = k + lane; i < p; i += 32) {
+      const double v = fabs(M[i + k * LD].re) + fabs(M[i + k * LD].im);
+      if (v > best) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (!(best > 0)) {
+      if (lane == 0) atomicOr(status, 8);
+      return;
+    }
+    // swap rows k and bi, scale row k by 1 / pivot
+    const cplx inv = cdiv(cplx{1, 0}, M[bi + k * LD]);
+    for (int c = lane; c < 2 * p; c += 32) {
+      const cplx t = M[bi + c * LD];
+      M[bi + c * LD] = M[k + c * LD];
+      M[k + c * LD] = inv * t;
+    }
+    __syncwarp();
+    for (int i = lane; i < p; i += 32) fk[i] = M[i + k * LD];
+    __syncwarp();
+    // eliminate column k from every other row
+    for (int c = lane; c < 2 * p; c += 32) {
+      const cplx mk = M[k + c * LD];
+      for (int i = 0; i < p; ++i)
+        if (i != k) M[i + c * LD] = M[i + c * LD] - fk[i] * mk;
+    }
+    __syncwarp();
+  }
+  for (int e = lane; e < p * p; e += 32) Tinv[e] = M[(e % p) + (p + e / p) * LD];
+}
+
 // G[p] = sum_c part[c][p] (block order, deterministic): 32 entries per
 // block along x, the partials split over 32 rows of threads, four
 // independent sums per thread.  With Rinv set, the last block to finish
@@ -402,7 +460,8 @@ template <bool CPLX>
 __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__ Xre, const double* __restrict__ Xim,
                                                       int b1, const cplx* __restrict__ Cm, int ldc, int b2,
                                                       const double* Bre, const double* Bim, int negate, int n,
-                                                      double* Ore, double* Oim) {
+                                                      double* Ore, double* Oim, const double* __restrict__ Yre = nullptr,
+                                                      const double* __restrict__ Yim = nullptr) {
   __shared__ cplx cs[kBmMaxB * kBmMaxB];
   __shared__ double xs_r[kBmMaxB][kUpRows], xs_i[CPLX ? kBmMaxB : 1][kUpRows];
   for (int e = threadIdx.x; e < b1 * b2; e += blockDim.x) cs[e] = Cm[(e % b1) + (long)(e / b1) * ldc];
@@ -414,8 +473,8 @@ __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__
     for (int e = threadIdx.x; e < b1 * kUpRows; e += blockDim.x) {
       const int i = e / kUpRows, q = e % kUpRows;
       const long r = r0 + q;
-      xs_r[i][q] = r < n ? Xre[(long)i * n + r] : 0.0;
-      if (CPLX) xs_i[i][q] = r < n ? Xim[(long)i * n + r] : 0.0;
+      xs_r[i][q] = r < n ? Xre[(long)i * n + r] + (Yre ? Yre[(long)i * n + r] : 0.0) : 0.0;
+      if (CPLX) xs_i[i][q] = r < n ? Xim[(long)i * n + r] + (Yim ? Yim[(long)i * n + r] : 0.0) : 0.0;
     }
     __syncthreads();
     const long r = r0 + rr;

@@ -455,7 +455,7 @@ struct oapb_arnoldi {
   // block (multi-vector) buffers: X, W, R, E of up to kBmMaxB vectors each
   static constexpr int kBlocks = 6;
   double *Bre[kBlocks] = {}, *Bim[kBlocks] = {};
-  cplx* thinv = nullptr;  // 1 / Ritz values of the refinement (kBmMaxB)
+  cplx* Tinv = nullptr;   // T^-1 of the refinement's projected operator (kBmMaxB^2)
   std::vector<oapb_trace_rec> trace;  // convergence checks of the last solve
   cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
   cplx *britz = nullptr;
@@ -754,7 +754,7 @@ int alloc_blocks(oapb_arnoldi* a) {
   rc |= dalloc(&a->bQ, bb);
   rc |= dalloc(&a->bH, bb);
   rc |= dalloc(&a->britz, sizeof(cplx) * kBmMaxB);
-  rc |= dalloc(&a->thinv, sizeof(cplx) * kBmMaxB);
+  rc |= dalloc(&a->Tinv, bb);
   rc |= dalloc(&a->best, sizeof(double) * kBmMaxB);
   rc |= dalloc(&a->bnorm, sizeof(double) * kBmMaxB * (size_t)a->nnorm);
   rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
@@ -1185,19 +1185,6 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   return OAPB_NOT_CONVERGED;
 }
 
-// D_q = (Y_q + E_q) * s_q
-__global__ void k_scale_cols(const double* __restrict__ yr, const double* __restrict__ yi, const double* __restrict__ er,
-                             const double* __restrict__ ei, const cplx* __restrict__ s, int b, int n, double* dr,
-                             double* di) {
-  const long len = (long)b * n;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
-    const cplx v{yr[e] + er[e], yi[e] + ei[e]};
-    const cplx w = v * s[e / n];
-    dr[e] = w.re;
-    di[e] = w.im;
-  }
-}
-
 // Out = X + Y (b vectors)
 __global__ void k_block_add(const double* __restrict__ xr, const double* __restrict__ xi, const double* __restrict__ yr,
                             const double* __restrict__ yi, int b, int n, double* outr, double* outi) {
@@ -1210,70 +1197,69 @@ __global__ void k_block_add(const double* __restrict__ xr, const double* __restr
 
 // FP64-anchored refinement of the wanted invariant subspace (complex
 // operator, largest-magnitude wanted set, p = k vectors from a->Xre).
-// Outer step: W = A X on the FP64 operator, T = X^H W, R = W - X T,
-// Rayleigh-Ritz T S = S Theta; the pairs are accepted when every
-// ||R s_q|| / (max |theta| ||s_q||) <= tol.  Otherwise the correction D
-// (in the Ritz basis X S) of the projected Sylvester equation
-//     P A D - D Theta = -R S,   P = I - X X^H,
-// is computed by the fixed point D <- (P A D + R S) Theta^-1 on the
-// FP32-class operator (contraction about rho = |theta_{k+1}| / |theta_k|)
-// and X <- orth(X S + D).  The outer iteration converges quadratically, so
-// the FP64 operator is applied about twice per solve; the FP32-class
-// operator's rounding enters only through the small correction.
-// Returns OAPB_OK, kSlow (no quadratic progress) or an error.
+// Outer step: W = A X on the FP64 operator, T = X^H W, R = W - X T.  From
+// the second step on, Rayleigh-Ritz T S = S Theta checks the pairs, which
+// are accepted when every ||R s_q|| / (max |theta| ||s_q||) <= tol; the
+// first step starts from the FP32-class phase's residual res0 (Ritz values
+// th0) and takes no check.  The correction D (orthogonal to X) of the
+// projected Sylvester equation
+//     P A D - D T = -R,   P = I - X X^H,
+// is computed by the fixed point D <- (P A D + R) T^-1 on the FP32-class
+// operator (contraction about rho = |theta_{k+1}| / |theta_k|; T^-1 by
+// Gauss-Jordan on one warp) and X <- orth(X + D).  The outer iteration
+// converges quadratically, so the FP64 operator is applied about twice per
+// solve; the FP32-class operator's rounding enters only through the small
+// correction.  Returns OAPB_OK, kSlow (no quadratic progress) or an error.
 template <bool C>
-int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_outer = 3) {
+int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vector<cplx>& th0, double* res_out,
+           int max_outer = 3) {
   const int n = a->n, p = a->k;
   double *X = a->Bre[0], *W = a->Bre[1], *R = a->Bre[2], *E = a->Bre[3], *D = a->Bre[4], *Tm = a->Bre[5];
   double *Xi = a->Bim[0], *Wi = a->Bim[1], *Ri = a->Bim[2], *Ei = a->Bim[3], *Di = a->Bim[4], *Tmi = a->Bim[5];
+  if ((int)th0.size() < p || !(res0 > 0)) return kSlow;
   if (cudaMemsetAsync(a->bstatus, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   int rc = cholqr2<C>(a, a->Xre, a->Xim, p, X, Xi, Tm, Tmi, 2);
   if (rc) return rc;
   std::vector<double> norms(p);
-  std::vector<cplx> th(p), thinv(p);
-  double prev = 0;
+  std::vector<cplx> th(th0.begin(), th0.begin() + p);
+  double prev = res0;
+  const long len = (long)p * n;
   for (int outer = 0; outer < max_outer; ++outer) {
     if ((rc = block_apply<C>(a, X, Xi, p, W, Wi, false))) return rc;
-    block_gram<C>(a, X, Xi, p, W, Wi, p, a->G);
-    a->stats.kernel_launches += 2;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
-    if ((rc = small_eig(a, a->G, p, p, p))) return rc;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, p, a->bY, p, p, nullptr, nullptr, 0, n, E, Ei);
-    if ((rc = col_norms<C>(a, E, Ei, p, norms.data()))) return rc;
-    DevState bs;
-    int tcerr = 0;
-    cudaMemcpyAsync(th.data(), a->britz, sizeof(cplx) * p, cudaMemcpyDeviceToHost, a->stream);
-    cudaMemcpyAsync(&bs, a->bst, sizeof(DevState), cudaMemcpyDeviceToHost, a->stream);
-    if (a->tcerr) cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream);
-    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-    if ((bs.status & 2) || tcerr) return OAPB_ERR_TIMEOUT;
-    a->stats.refine_iterations++;
-    double scale = 0, mx = 0;
-    for (int q = 0; q < p; ++q) scale = fmax(scale, cabs_(th[q]));
-    if (scale == 0) return kSlow;
-    for (int q = 0; q < p; ++q) {
-      res_out[q] = norms[q] / scale;
-      mx = fmax(mx, res_out[q]);
-    }
-    a->trace.push_back({3, outer, a->stats.block_matvecs, a->stats.block_bf16, mx});
-    if (mx <= tol) {  // Ritz vectors X S
+    double mx = res0;
+    if (outer == 0) {  // T and R only
+      block_gram<C>(a, X, Xi, p, W, Wi, p, a->G);
       ++a->stats.kernel_launches;
-      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
-                                                          a->Xim);
-      a->evals.assign(th.begin(), th.end());
-      return launch_check();
+      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
+    } else {
+      const uint32_t passes_now = a->stats.block_matvecs, bf16_now = a->stats.block_bf16;
+      if ((rc = check_enqueue<C>(a, a->stream, X, Xi, W, Wi, R, Ri, E, Ei, p, p, p, false))) return rc;
+      if ((rc = check_collect(a, p, p, th.data(), norms.data()))) return rc;
+      a->stats.refine_iterations++;
+      double scale = 0;
+      for (int q = 0; q < p; ++q) scale = fmax(scale, cabs_(th[q]));
+      if (scale == 0) return kSlow;
+      mx = 0;
+      for (int q = 0; q < p; ++q) {
+        res_out[q] = norms[q] / scale;
+        mx = fmax(mx, res_out[q]);
+      }
+      a->trace.push_back({3, outer, passes_now, bf16_now, mx});
+      if (mx <= tol) {  // Ritz vectors X S
+        ++a->stats.kernel_launches;
+        k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
+                                                            a->Xim);
+        a->evals.assign(th.begin(), th.end());
+        return launch_check();
+      }
+      if (!(mx == mx) || mx > 1e-2 * prev) return kSlow;
+      prev = mx;
     }
-    if (!(mx == mx) || (outer > 0 && mx > 1e-2 * prev)) return kSlow;
-    prev = mx;
-    // inner fixed point on the FP32-class operator
-    for (int q = 0; q < p; ++q) thinv[q] = cdiv(cplx{1, 0}, th[q]);
-    if (cudaMemcpyAsync(a->thinv, thinv.data(), sizeof(cplx) * p, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
-      return OAPB_ERR_CUDA;
-    // inner iterations for a correction about 100x below the goal; the
-    // observed contraction of non-normal problems is slower than rho, so
-    // the count assumes at least 0.3 per sweep (a shortfall costs one more
-    // outer step, not the result)
+    // inner fixed point on the FP32-class operator, for a correction about
+    // 100x below the goal; the observed contraction of non-normal problems
+    // is slower than rho, so the count assumes at least 0.3 per sweep (a
+    // shortfall costs one more outer step, not the result)
     const double rho_eff = rho > 0.3 ? rho : 0.3;
     int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff));
     if (J < 2) J = 2;
@@ -1281,13 +1267,10 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
     // leading sweeps on the BF16 planes: the last Jf contract their error
     const int Jf = (int)ceil(log(0.01 * tol / mx / kBf16Err) / log(rho_eff));
     const int Jb = J - Jf > 0 ? J - Jf : 0;
-    const long len = (long)p * n;
-    a->stats.kernel_launches++;
-    // D = R S Theta^-1 (Y = 0)
-    if (cudaMemsetAsync(W, 0, sizeof(double) * len, a->stream) != cudaSuccess ||
-        cudaMemsetAsync(Wi, 0, sizeof(double) * len, a->stream) != cudaSuccess)
-      return OAPB_ERR_CUDA;
-    k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
+    a->stats.kernel_launches += 2;
+    k_small_inv<<<1, 32, 0, a->stream>>>(a->G, p, a->Tinv, a->bstatus);
+    // D = R T^-1 (the first sweep from D = 0)
+    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di);
     // Components of D inside span(X) do not move the subspace; between
     // projections they grow at most like |theta_1| / |theta_p| per
     // iteration, so project when that growth would pass 4x, and last.
@@ -1306,13 +1289,14 @@ int refine(oapb_arnoldi* a, double tol, double rho, double* res_out, int max_out
         a->stats.kernel_launches++;
         k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi);
       }
+      // D = (P A D + R) T^-1
       a->stats.kernel_launches++;
-      k_scale_cols<<<grid_n(len), 256, 0, a->stream>>>(W, Wi, E, Ei, a->thinv, p, n, D, Di);
+      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(W, Wi, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, R,
+                                                          Ri);
     }
-    // X <- orth(X S + D)
-    a->stats.kernel_launches += 2;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, R, Ri);
-    k_block_add<<<grid_n(len), 256, 0, a->stream>>>(R, Ri, D, Di, p, n, R, Ri);
+    // X <- orth(X + D)
+    a->stats.kernel_launches++;
+    k_block_add<<<grid_n(len), 256, 0, a->stream>>>(X, Xi, D, Di, p, n, R, Ri);
     if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 2))) return rc;
   }
   return kSlow;
@@ -1462,7 +1446,7 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
     // largest-magnitude wanted set: the correction contracts by |theta_{k+1}| / |theta_k|
     const double rho = cabs_(th32[k]) / cabs_(th32[k - 1]);
     if (rho < 0.6) {
-      const int rs = refine<C>(a, tol, rho, r);
+      const int rs = refine<C>(a, tol, rho, floor1, th32, r);
       if (rs == OAPB_OK) return OAPB_OK;
       if (rs != kSlow) return rs;
       a->stats.fallbacks++;
@@ -1536,8 +1520,8 @@ void free_all(oapb_arnoldi* a) {
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
     if (p) cudaFree(p);
-  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->thinv, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
-                a->bstatus, a->bst, a->bpart2, a->bdone2};
+  void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
+                a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv};
   for (void* p : bs)
     if (p) cudaFree(p);
   for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
