@@ -214,15 +214,17 @@ def test_block_pass_precisions(cplx, n, b):
     X = xr if not cplx else torch.complex(xr, xi)
     ref = (A @ X.T).T
     scale = (A.abs() @ X.abs().T).T
-    # (the BF16 pass: operator rounded to BF16, unit roundoff 2^-8 = 3.9e-3, X split)
-    for prec, tc, tol in ((B.PREC_FP64, True, 1e-13), (B.PREC_FP64, False, 1e-13), (B.PREC_MIXED, False, 2e-6),
-                          (B.PREC_MIXED, True, 1e-4), (B.PASS_BF16, True, 4e-3)):
-        s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=tc)
+    # (the BF16 pass: operator rounded to BF16, unit roundoff 2^-8 = 3.9e-3, X split;
+    # FP64 passes through a mixed-form handle and through an FP64 handle)
+    for prec, tc, tol, hp in ((B.PREC_FP64, True, 1e-13, B.PREC_MIXED), (B.PREC_FP64, True, 1e-13, B.PREC_FP64),
+                              (B.PREC_FP64, False, 1e-13, B.PREC_MIXED), (B.PREC_MIXED, False, 2e-6, B.PREC_MIXED),
+                              (B.PREC_MIXED, True, 1e-4, B.PREC_MIXED), (B.PASS_BF16, True, 4e-3, B.PREC_MIXED)):
+        s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=hp, tensor_cores=tc)
         s.set_operator(are, aim)
         wr, wi = s.apply_block(xr, xi, precision=prec)
         W = wr if not cplx else torch.complex(wr, wi)
         err = ((W - ref).abs() / scale).max().item()
-        assert err <= tol, (prec, tc, err)
+        assert err <= tol, (prec, tc, hp, err)
         s.close()
 
 
