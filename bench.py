@@ -386,12 +386,15 @@ def run_ours(args, world, rank, local):
     roof = {"bound": "hbm", "kernel": name,
             "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
             "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind),
-            "traffic": (traffic or {}).get(name.split(" ")[0], {}).get("bytes_per_launch") if traffic else None,
+            "traffic": (traffic or {}).get(name.split(" (")[0], {}).get("bytes_per_launch") if traffic else None,
             "launch_ms": per_launch * 1e3, "launches_timed": cnt, "algorithmic_bytes_per_launch": alg_bytes,
             "tflops": flops / per_launch / 1e12 if per_launch > 0 else 0.0,
             "share_of_step": tot / secs if secs > 0 else None,
             "all_kernels": {k: {"launches": v[1], "total_ms": v[0] * 1e3,
-                                "GBs": (v[2] / (v[0] / v[1]) / 1e9) if v[1] else None}
+                                "GBs": (v[2] / (v[0] / v[1]) / 1e9) if v[1] else None,
+                                "frac": (v[2] / (v[0] / v[1]) / 1e9 / hbm) if v[1] else None,
+                                "algorithmic_bytes_per_launch": v[2],
+                                "traffic": (traffic or {}).get(k.split(" (")[0], {}).get("bytes_per_launch")}
                             for k, v in kernels.items()},
             "plain_fp64_matvec_GBs": ((16.0 * n * n + 32.0 * n) / (pprof["matvec_seconds"] / pprof["matvec_timed"]) / 1e9
                                       if pprof["matvec_timed"] else None)}

@@ -322,7 +322,9 @@ typedef struct oapb_trace_rec {
 } oapb_trace_rec;
 
 /* Convergence trace of the last solve: copies up to cap records, *count =
- * the number recorded (the plain IRAM path records none). */
+ * the number recorded (the plain IRAM path records none).  The data behind
+ * the reference's per-step logInfo printouts
+ * (ArnoldiPackage/ArnoldiProcedures.cpp:391-395, 539). */
 OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_rec* out, uint32_t cap,
                                        uint32_t* count);
 
