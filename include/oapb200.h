@@ -247,6 +247,9 @@ typedef struct oapb_arnoldi_stats {
   uint32_t block_bf16;       /* block passes on the BF16 hi planes alone */
   uint32_t block_bf16_timed; /* of which timed (profile) */
   double block_bf16_seconds; /* their device time (profile) */
+  uint32_t eig_fast;         /* FP64 Rayleigh-Ritz eigensolves of the refinement
+                                delivered by inverse iteration on the nearly
+                                triangular projected matrix (the rest: Schur) */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

@@ -66,6 +66,7 @@ struct HessArgs {
   int m, k, nvec, which, do_shift, real_shifts, dense, use_beta;
   double tol;
   double beta;      // used when use_beta == 0 (dense mode: residual norms come separately)
+  const int* skip = nullptr;  // k_hess: when set and *skip != 0, return at once (another solver delivered)
 };
 
 // leading dimension of the T / Z work arrays (odd)
@@ -479,6 +480,7 @@ static __device__ void hess_kernel_body(const HessArgs& a, unsigned char* dyn) {
 // FP64 working arithmetic (the restart loop and the refinement)
 static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
   extern __shared__ __align__(16) unsigned char hess_dyn[];
+  if (a.skip && *(volatile const int*)a.skip) return;
   hess_kernel_body<cplx>(a, hess_dyn);
 }
 
@@ -492,5 +494,215 @@ static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
 
 #undef TT_
 #undef ZZ_
+
+// Eigenpairs of a nearly upper-triangular T (m x m complex, column-major,
+// m <= 32): the Rayleigh quotient of an orthonormalised basis of Ritz vectors
+// ordered like their values, whose strictly lower part is of the size of the
+// Ritz vectors' errors.  Warp w takes pairs q = w, w + kNtWarps, ...:
+// Rayleigh quotient iteration from v = e_q, sigma = T(q,q) (LU with partial
+// pivoting of T - sigma I, a zero pivot replaced by eps ||T||_F; v <- (T -
+// sigma I)^-1 v normalised; sigma <- v^H T v), at most kNtIters steps, until
+// ||T v - sigma v|| <= 16 eps ||T||_F.  Accepted when every such residual is
+// <= 64 eps ||T||_F and the values are pairwise apart by more than 1e-9
+// max |theta|:
+// then ritz / Y / order are written in the ArnUtils order of `which` (as
+// k_hess writes them, Y column q at Y + q m, unit 2-norm) and *delivered = 1;
+// otherwise *delivered = 0 and nothing else is written (k_hess follows with
+// skip = delivered).  Dynamic shared memory: nt_smem_bytes(m).
+constexpr int kNtWarps = 8;
+constexpr int kNtIters = 4;
+__host__ __device__ inline int nt_ld(int m) { return m + 1; }
+__host__ __device__ inline size_t nt_smem_bytes(int m) {
+  return sizeof(cplx) * ((size_t)(kNtWarps + 1) * m * nt_ld(m) + (size_t)2 * kNtWarps * m + (size_t)m * m + m) +
+         sizeof(double) * 2 * m + sizeof(int) * (kNtWarps * m + m + 1);
+}
+
+static __global__ void __launch_bounds__(kNtWarps * 32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, int which,
+                                                                cplx* ritz, cplx* Y, int* order, int* delivered) {
+  extern __shared__ __align__(16) unsigned char nt_dyn[];
+  const int LD = nt_ld(m);
+  cplx* T = reinterpret_cast<cplx*>(nt_dyn);                 // m x LD
+  cplx* Mw = T + (size_t)m * LD;                             // kNtWarps x (m x LD)
+  cplx* xw = Mw + (size_t)kNtWarps * m * LD;                 // kNtWarps x m
+  cplx* tw = xw + (size_t)kNtWarps * m;                      // kNtWarps x m
+  cplx* V = tw + (size_t)kNtWarps * m;                       // m x m eigenvectors (column q)
+  cplx* th = V + (size_t)m * m;                              // m
+  double* res = reinterpret_cast<double*>(th + m);           // m
+  double* key = res + m;                                     // m
+  int* piv = reinterpret_cast<int*>(key + m);                // kNtWarps x m
+  int* ord = piv + kNtWarps * m;                             // m
+  int* ok = ord + m;                                         // 1
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (m < 1 || m > 32) return;
+  for (int e = tid; e < m * m; e += blockDim.x) T[(e % m) + (e / m) * LD] = Tin[e];
+  if (tid == 0) *ok = 1;
+  __syncthreads();
+  double fro = 0;
+  for (int e = lane; e < m * m; e += 32) fro += abs2(T[(e % m) + (e / m) * LD]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) fro += __shfl_xor_sync(0xffffffffu, fro, o);
+  fro = sqrt(fro);
+  const double eps = 2.220446049250313e-16;
+  const double tiny = eps * (fro > 0 ? fro : 1.0);
+  cplx* M = Mw + (size_t)warp * m * LD;
+  cplx* x = xw + (size_t)warp * m;
+  cplx* t = tw + (size_t)warp * m;
+  int* pv = piv + warp * m;
+  for (int q = warp; q < m; q += kNtWarps) {
+    cplx sigma = T[q + q * LD], thq = {0, 0};
+    double rq = 1e300;
+    for (int i = lane; i < m; i += 32) x[i] = cplx{i == q ? 1.0 : 0.0, 0.0};
+    __syncwarp();
+    for (int itr = 0; itr < kNtIters && !(rq <= 16 * eps * fro); ++itr) {
+      for (int e = lane; e < m * m; e += 32) {
+        const int r = e % m, c = e / m;
+        M[r + c * LD] = T[r + c * LD] - (r == c ? sigma : cplx{0, 0});
+      }
+      __syncwarp();
+      // LU with partial pivoting, lane = column
+      for (int k = 0; k < m; ++k) {
+        double best = -1;
+        int bi = k;
+        for (int i = k + lane; i < m; i += 32) {
+          const double v = abs2(M[i + k * LD]);
+          if (v > best) {
+            best = v;
+            bi = i;
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+          if (ob > best || (ob == best && oi < bi)) {
+            best = ob;
+            bi = oi;
+          }
+        }
+        if (lane == 0) pv[k] = bi;
+        for (int c = lane; c < m; c += 32) {  // swap rows k and bi
+          const cplx tmp = M[k + c * LD];
+          M[k + c * LD] = M[bi + c * LD];
+          M[bi + c * LD] = tmp;
+        }
+        __syncwarp();
+        if (lane == 0 && cabs_(M[k + k * LD]) < tiny) M[k + k * LD] = cplx{tiny, 0};
+        __syncwarp();
+        const cplx inv = cdiv(cplx{1, 0}, M[k + k * LD]);
+        for (int i = k + 1 + lane; i < m; i += 32) M[i + k * LD] = M[i + k * LD] * inv;  // multipliers
+        __syncwarp();
+        for (int c = k + 1 + lane; c < m; c += 32) {
+          const cplx ukc = M[k + c * LD];
+          for (int i = k + 1; i < m; ++i) M[i + c * LD] = M[i + c * LD] - M[i + k * LD] * ukc;
+        }
+        __syncwarp();
+      }
+      // x <- (T - sigma I)^-1 x, normalised
+      if (lane == 0) {
+        for (int k = 0; k < m; ++k) {  // P b
+          const int r = pv[k];
+          const cplx tmp = x[k];
+          x[k] = x[r];
+          x[r] = tmp;
+        }
+      }
+      __syncwarp();
+      for (int i = 1; i < m; ++i) {  // L y = P b (unit lower)
+        cplx acc = {0, 0};
+        for (int j = lane; j < i; j += 32) acc = acc + M[i + j * LD] * x[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+          acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+        }
+        if (lane == 0) x[i] = x[i] - acc;
+        __syncwarp();
+      }
+      for (int i = m - 1; i >= 0; --i) {  // U x = y
+        cplx acc = {0, 0};
+        for (int j = i + 1 + lane; j < m; j += 32) acc = acc + M[i + j * LD] * x[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+          acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+        }
+        if (lane == 0) x[i] = cdiv(x[i] - acc, M[i + i * LD]);
+        __syncwarp();
+      }
+      double nrm = 0;
+      for (int i = lane; i < m; i += 32) nrm += abs2(x[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
+      nrm = sqrt(nrm);
+      const double sc = nrm > 0 ? 1.0 / nrm : 0.0;
+      for (int i = lane; i < m; i += 32) x[i] = sc * x[i];
+      __syncwarp();
+      // Rayleigh quotient (the next shift) and residual ||T x - theta x||
+      for (int i = lane; i < m; i += 32) {
+        cplx acc = {0, 0};
+        for (int j = 0; j < m; ++j) acc = acc + T[i + j * LD] * x[j];
+        t[i] = acc;
+      }
+      __syncwarp();
+      thq = cplx{0, 0};
+      for (int i = lane; i < m; i += 32) thq = thq + conj(x[i]) * t[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        thq.re += __shfl_xor_sync(0xffffffffu, thq.re, o);
+        thq.im += __shfl_xor_sync(0xffffffffu, thq.im, o);
+      }
+      double r2 = 0;
+      for (int i = lane; i < m; i += 32) r2 += abs2(t[i] - thq * x[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+      rq = sqrt(r2);
+      sigma = thq;
+    }
+    for (int i = lane; i < m; i += 32) V[i + (size_t)q * m] = x[i];
+    if (lane == 0) {
+      th[q] = thq;
+      res[q] = rq;
+      if (!(rq <= 64 * eps * fro)) *ok = 0;
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // distinct values, then the ArnUtils order
+  if (warp == 0) {
+    double tmax = 0;
+    for (int q = lane; q < m; q += 32) tmax = fmax(tmax, cabs_(th[q]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+    int bad = 0;
+    for (int e = lane; e < m * m; e += 32) {
+      const int q = e % m, r = e / m;
+      if (q < r && !(cabs_(th[q] - th[r]) > 1e-9 * tmax)) bad = 1;
+    }
+    bad = __any_sync(0xffffffffu, bad);
+    if (lane == 0 && bad) *ok = 0;
+    for (int i = lane; i < m; i += 32) {
+      const double kv = sort_key(th[i], which);
+      key[i] = (kv != kv) ? INFINITY : kv;
+    }
+    __syncwarp();
+    for (int i = lane; i < m; i += 32) {
+      int r = 0;
+      for (int j = 0; j < m; ++j) r += (key[j] < key[i]) || (key[j] == key[i] && j < i);
+      ord[r] = i;
+    }
+  }
+  __syncthreads();
+  const int good = *ok;
+  if (tid == 0) *delivered = good;
+  if (!good) return;
+  for (int q = tid; q < m; q += blockDim.x) {
+    ritz[q] = th[ord[q]];
+    order[q] = ord[q];
+  }
+  for (int e = tid; e < m * m; e += blockDim.x) {
+    const int i = e % m, q = e / m;
+    Y[i + (size_t)q * m] = V[i + (size_t)ord[q] * m];
+  }
+}
 
 }  // namespace oapb

@@ -456,6 +456,7 @@ struct oapb_arnoldi {
   static constexpr int kBlocks = 6;
   double *Bre[kBlocks] = {}, *Bim[kBlocks] = {};
   cplx* Tinv = nullptr;   // T^-1 of the refinement's projected operator (kBmMaxB^2)
+  int* ntflag = nullptr;  // the near-triangular eigensolver delivered (device word)
   std::vector<oapb_trace_rec> trace;  // convergence checks of the last solve
   cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
   cplx *britz = nullptr;
@@ -711,7 +712,8 @@ size_t pin_norm_off(const oapb_arnoldi*) { return 0; }
 size_t pin_ritz_off(const oapb_arnoldi* a) { return (sizeof(double) * kBmMaxB * (size_t)a->nnorm + 63) & ~(size_t)63; }
 size_t pin_st_off(const oapb_arnoldi* a) { return pin_ritz_off(a) + ((sizeof(cplx) * kBmMaxB + 63) & ~(size_t)63); }
 size_t pin_err_off(const oapb_arnoldi* a) { return pin_st_off(a) + ((sizeof(DevState) + 63) & ~(size_t)63); }
-size_t pin_bytes(const oapb_arnoldi* a) { return pin_err_off(a) + 64; }
+size_t pin_nt_off(const oapb_arnoldi* a) { return pin_err_off(a) + 64; }
+size_t pin_bytes(const oapb_arnoldi* a) { return pin_nt_off(a) + 64; }
 
 int alloc_blocks(oapb_arnoldi* a) {
   if (a->Bre[0]) return OAPB_OK;
@@ -755,6 +757,7 @@ int alloc_blocks(oapb_arnoldi* a) {
   rc |= dalloc(&a->bH, bb);
   rc |= dalloc(&a->britz, sizeof(cplx) * kBmMaxB);
   rc |= dalloc(&a->Tinv, bb);
+  rc |= dalloc(&a->ntflag, sizeof(int));
   rc |= dalloc(&a->best, sizeof(double) * kBmMaxB);
   rc |= dalloc(&a->bnorm, sizeof(double) * kBmMaxB * (size_t)a->nnorm);
   rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
@@ -881,7 +884,10 @@ int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* 
 // small dense eigenproblem of the b x b matrix G on one warp (Hessenberg
 // reduction + Schur + eigenvectors of the first nv values in sort order);
 // fp32: FP32 working arithmetic (the FP32-class phase's checks)
-int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 = false) {
+// near_tri (FP64, b <= 32): G is nearly upper triangular (the Rayleigh
+// quotient of orthonormalised Ritz vectors): inverse iteration per pair
+// first, the Schur path only when that does not deliver.
+int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 = false, bool near_tri = false) {
   HessArgs h;
   h.Hin = G;
   h.Hout = a->bH;
@@ -903,6 +909,16 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
   h.tol = 0;
   h.beta = 0;
   ++a->stats.kernel_launches;
+  if (near_tri && !fp32 && b <= 32 && a->ntflag) {
+    // the opt-in above 48 KB of dynamic shared memory (per device)
+    if (cudaFuncSetAttribute(k_eig_near_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nt_smem_bytes(32)) !=
+        cudaSuccess)
+      return OAPB_ERR_CUDA;
+    ++a->stats.kernel_launches;
+    k_eig_near_tri<<<1, kNtWarps * 32, nt_smem_bytes(b), a->stream>>>(G, b, a->cfg.sort, a->britz, a->bY, a->border,
+                                                                      a->ntflag);
+    h.skip = a->ntflag;
+  }
   if (fp32)
     k_hess_f32<<<1, 32, sizeof(cplxf) * hess_ws_cplx(b), a->stream>>>(h);
   else
@@ -919,7 +935,8 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
 // next pass meanwhile (they read X and W and write neither).
 template <bool C>
 int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const double* Xi, const double* W,
-                  const double* Wi, double* R, double* Ri, double* E, double* Ei, int b, int kk, int nv, bool fp32) {
+                  const double* Wi, double* R, double* Ri, double* E, double* Ei, int b, int kk, int nv, bool fp32,
+                  bool near_tri = false) {
   const int n = a->n;
   const bool side = cs != a->stream;
   cudaStream_t s0 = a->stream;
@@ -933,7 +950,7 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
   block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
   a->stats.kernel_launches += 3;
   k_block_update<C><<<grid_up(n), 256, 0, cs>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
-  int rc = small_eig(a, a->G, b, kk, nv, fp32);
+  int rc = small_eig(a, a->G, b, kk, nv, fp32, near_tri);
   if (!rc) {
     k_block_update<C><<<grid_up(n), 256, 0, cs>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
     k_colnorm2<C><<<a->nnorm, 256, 0, cs>>>(E, Ei, kk, n, a->bnorm);
@@ -953,6 +970,10 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
   if (a->tcerr &&
       cudaMemcpyAsync(hp + pin_err_off(a), a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
     return OAPB_ERR_CUDA;
+  *(int*)(hp + pin_nt_off(a)) = 0;
+  if (near_tri && b <= 32 &&
+      cudaMemcpyAsync(hp + pin_nt_off(a), a->ntflag, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+    return OAPB_ERR_CUDA;
   return cudaEventRecord(a->ev_chk, cs) == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 
@@ -970,6 +991,7 @@ int check_collect(oapb_arnoldi* a, int b, int kk, cplx* th, double* norms) {
   DevState bs;
   memcpy(&bs, hp + pin_st_off(a), sizeof(DevState));
   const int tcerr = *(const int*)(hp + pin_err_off(a));
+  if (*(const int*)(hp + pin_nt_off(a))) a->stats.eig_fast++;
   return ((bs.status & 2) || tcerr) ? OAPB_ERR_TIMEOUT : OAPB_OK;
 }
 
@@ -1234,7 +1256,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
     } else {
       const uint32_t passes_now = a->stats.block_matvecs, bf16_now = a->stats.block_bf16;
-      if ((rc = check_enqueue<C>(a, a->stream, X, Xi, W, Wi, R, Ri, E, Ei, p, p, p, false))) return rc;
+      if ((rc = check_enqueue<C>(a, a->stream, X, Xi, W, Wi, R, Ri, E, Ei, p, p, p, false, true))) return rc;
       if ((rc = check_collect(a, p, p, th.data(), norms.data()))) return rc;
       a->stats.refine_iterations++;
       double scale = 0;
@@ -1492,6 +1514,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
   a->stats.block_bf16 = 0;
+  a->stats.eig_fast = 0;
   a->stats.refine_iterations = 0;
   a->trace.clear();
   a->stats.dgks_passes = 0;
@@ -1521,7 +1544,7 @@ void free_all(oapb_arnoldi* a) {
   for (void* p : ps)
     if (p) cudaFree(p);
   void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
-                a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv};
+                a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv, a->ntflag};
   for (void* p : bs)
     if (p) cudaFree(p);
   for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {

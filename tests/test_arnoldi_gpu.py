@@ -171,6 +171,9 @@ def test_mixed_trace_and_bf16_passes():
     assert p1 and p1[0][3] >= 1 and st["block_bf16"] >= p1[0][3]
     assert all(a[4] > b[4] for a, b in zip(p1, p1[1:3]))
     assert tr[-1][0] == 3 and tr[-1][4] <= TOL
+    # the refinement's Rayleigh-Ritz matrix is nearly triangular: inverse
+    # iteration delivered its eigenpairs
+    assert st["eig_fast"] >= 1
     assert all(a[2] < b[2] for a, b in zip(tr, tr[1:]))
     # CUDA-core passes (tensor_cores = 0) take no BF16 pass
     r0 = solve(A, 8, 40, precision=B.PREC_MIXED, tensor_cores=False)
