@@ -263,6 +263,9 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tmem_slot;
+  // launched as a dependent of the B-operand split: set-up above overlaps
+  // its tail; nothing below may read B before it has completed
+  tc::griddep_wait();
 
   if (warp == 0) {
     // ---------------------------------------------------------- producer --
@@ -362,6 +365,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   }
   tc::tc_fence_before();
   __syncthreads();
+  tc::griddep_launch();  // the stream-K reduction may launch (it waits for this grid to complete)
   if (abort_flag && tid == 0) atomicOr(g.err, 1);
   if (warp == 1) {
     tc::tc_fence_after();
@@ -449,7 +453,7 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
                         : (cplx ? k_block_matvec_tc<true, true> : k_block_matvec_tc<false, true>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return OAPB_ERR_CUDA;
-  kern<<<g.grid.grid, kBtcThreads, smem, s>>>(g);
+  if (launch_dependent(kern, dim3(g.grid.grid), dim3(kBtcThreads), smem, s, g) != cudaSuccess) return OAPB_ERR_CUDA;
   if (cplx)
     launch_sk_reduce<true>(ws, g.grid, op.n, b, wr, wi, s);
   else

@@ -10,6 +10,8 @@
 // Partial layout: ws[((c * slots + slot) * planes * b + plane * b + q) * 128 + row].
 #pragma once
 
+#include <utility>
+
 #include "common.cuh"
 
 namespace oapb {
@@ -55,6 +57,8 @@ template <bool CPLX>
 __global__ void __launch_bounds__(kSkRows) k_sk_reduce(const double* __restrict__ ws, SkGrid p, int n, int b,
                                                        double* wr, double* wi) {
   constexpr int NP = CPLX ? 2 : 1;
+  // launched as a dependent of the pass that wrote the partials
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const long tile = blockIdx.x;
   const int pq0 = blockIdx.y * kSkCols, npq = NP * b;
   const long row = tile * kSkRows + threadIdx.x;
@@ -82,11 +86,31 @@ __global__ void __launch_bounds__(kSkRows) k_sk_reduce(const double* __restrict_
   }
 }
 
+// Launch with programmatic stream serialization: the kernel may start before
+// the preceding grid in the stream completes and must griddepcontrol.wait
+// before it reads that grid's output.
+template <typename... P, typename... A>
+inline cudaError_t launch_dependent(void (*kern)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                    A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, std::forward<A>(args)...);
+}
+
 template <bool CPLX>
 inline void launch_sk_reduce(const double* ws, const SkGrid& p, int n, int b, double* wr, double* wi,
                              cudaStream_t s) {
   const int npq = (CPLX ? 2 : 1) * b;
-  k_sk_reduce<CPLX><<<dim3((unsigned)p.tiles, (npq + kSkCols - 1) / kSkCols), kSkRows, 0, s>>>(ws, p, n, b, wr, wi);
+  launch_dependent(k_sk_reduce<CPLX>, dim3((unsigned)p.tiles, (npq + kSkCols - 1) / kSkCols), dim3(kSkRows), 0, s,
+                   ws, p, n, b, wr, wi);
 }
 
 }  // namespace oapb
