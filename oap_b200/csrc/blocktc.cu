@@ -77,10 +77,11 @@ __global__ void k_split_block_bf16(const double* __restrict__ xr, const double* 
 }
 
 // A (FP64 plane, n x n) -> hi / lo BF16 planes (n x kp, zero-padded columns)
-__global__ void k_split_operator_bf16(const double* __restrict__ a, int n, int kp, __nv_bfloat16* hi,
-                                      __nv_bfloat16* lo) {
-  const long total = (long)n * kp;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+__global__ void k_split_operator_bf16(const double* __restrict__ a, int n, int kp, long row0, long rows,
+                                      __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  const long total = rows * kp;
+  for (long e0 = (long)blockIdx.x * blockDim.x + threadIdx.x; e0 < total; e0 += (long)gridDim.x * blockDim.x) {
+    const long e = row0 * kp + e0;
     const long r = e / kp, c = e % kp;
     const float v = c < n ? (float)a[r * n + c] : 0.f;
     const __nv_bfloat16 h = __float2bfloat16_rn(v);
@@ -406,8 +407,12 @@ static size_t btc_stage_bytes(int N, bool cplx, bool lo) {
   return ((size_t)(NA * kBtcM * 128 + 2 * KH * N * 128) + 1023) & ~(size_t)1023;
 }
 
-int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s) {
-  k_split_operator_bf16<<<kNumSMs * 8, 256, 0, s>>>(a, n, kp, hi, lo);
+int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
+                        long row0, long rows) {
+  if (rows < 0) rows = n - row0;
+  if (row0 < 0 || row0 + rows > n) return OAPB_ERR_ARG;
+  if (rows == 0) return OAPB_OK;
+  k_split_operator_bf16<<<kNumSMs * 8, 256, 0, s>>>(a, n, kp, row0, rows, hi, lo);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 

@@ -426,6 +426,8 @@ struct oapb_arnoldi {
   double* own64im = nullptr;
   float* a32re = nullptr;
   float* a32im = nullptr;
+  bool fp32_ready = false;   // a32 holds the current operator (built on first use)
+  bool mixed_ready = false;  // the mixed form's operator data (BF16 planes or FP32 copy) is current
   oapb_matvec_fn cb = nullptr;
   void* cb_user = nullptr;
   // single-vector matvec launch variants (autotuned per operator shape)
@@ -493,6 +495,8 @@ struct oapb_arnoldi {
   // last solve outputs (host)
   std::vector<cplx> evals;
 };
+
+static int ensure_fp32_copy(oapb_arnoldi* a);
 
 namespace {
 
@@ -801,6 +805,10 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   dim3 grid(tiles, a->nsplit);
   a->stats.kernel_launches += 2;
   const bool tcp = fp32 && a->have_tc && a->cfg.tensor_cores;
+  if (fp32 && !tcp) {  // the CUDA-core FP32 pass reads the FP32 copy
+    const int rc = ensure_fp32_copy(a);
+    if (rc) return rc;
+  }
   Timed tm{nullptr, nullptr, 1, fp32 ? (tcp && bf16 ? 2 : 1) : 0, b};
   const bool prof = prof_begin(a, tm);
   if (tcp) {
@@ -1489,8 +1497,9 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   int bi = k + (m - k < 4 ? m - k : 4);
   if (bi > kBmMaxB) bi = kBmMaxB;
   a->nvec_hess = bi;
-  int rc = iram_start<C>(a);
+  int rc = ensure_fp32_copy(a);
   if (rc) return rc;
+  if ((rc = iram_start<C>(a))) return rc;
   st = iram<C>(a, true, tol > 1e-7 ? tol : 1e-7, a->cfg.max_restarts, 0);
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   if ((rc = ritz_vectors<C>(a, bi))) return rc;
@@ -1508,7 +1517,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   // and pays off only when the operator pass is HBM-bound: below n = 8192
   // (at most 1 GiB of complex FP64 operator) a pass is a few tens of
   // microseconds and the single-vector FP64 restart loop is faster.
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && k <= kBmMaxB && a->a32re &&
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && k <= kBmMaxB && a->mixed_ready &&
                      a->n >= kMixedMinN;
   if (!resume) a->stats.restarts = 0;  // a resumed solve continues the saved count
   a->stats.matvecs = 0;
@@ -1716,35 +1725,80 @@ int oapb_arnoldi_destroy(oapb_arnoldi* a) {
   return OAPB_OK;
 }
 
-static int make_fp32_copy(oapb_arnoldi* a) {
+}  // extern "C"
+
+// BF16 hi / lo planes of the tensor-core passes: buffers (first call), then
+// the split of rows row0 .. row0 + rows - 1 of both operator planes
+static int build_tc_planes(oapb_arnoldi* a, long row0, long rows) {
+  a->kp = (a->n + 127) / 128 * 128;
+  const size_t plane = (size_t)a->n * a->kp;
+  const int np = a->is_c ? 4 : 2;
+  if (!a->abf && dalloc(&a->abf, sizeof(__nv_bfloat16) * plane * np)) return OAPB_ERR_NOMEM;
+  if (!a->xbf && dalloc(&a->xbf, sizeof(__nv_bfloat16) * 2 * 64 * (size_t)a->kp)) return OAPB_ERR_NOMEM;
+  if (!a->tcerr) {
+    if (dalloc(&a->tcerr, sizeof(int))) return OAPB_ERR_NOMEM;
+    if (cudaMemsetAsync(a->tcerr, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+  }
+  a->stats.kernel_launches += np / 2;
+  if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream, row0, rows)) return OAPB_ERR_CUDA;
+  if (a->is_c &&
+      split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream, row0, rows))
+    return OAPB_ERR_CUDA;
+  a->have_tc = true;
+  return OAPB_OK;
+}
+
+// FP32 copy of the operator for the CUDA-core passes (tensor_cores = 0) and
+// the FP32 restart loop, built when first needed (it is not on the
+// tensor-core path), with the launch variant of its single-vector pass
+static int ensure_fp32_copy(oapb_arnoldi* a) {
+  if (a->fp32_ready) return OAPB_OK;
   const long nn = (long)a->n * a->n;
   if (!a->a32re && dalloc(&a->a32re, sizeof(float) * nn)) return OAPB_ERR_NOMEM;
   if (a->is_c && !a->a32im && dalloc(&a->a32im, sizeof(float) * nn)) return OAPB_ERR_NOMEM;
   if (!a->x32re && dalloc(&a->x32re, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   if (a->is_c && !a->x32im && dalloc(&a->x32im, sizeof(float) * a->n)) return OAPB_ERR_NOMEM;
   const int g = kNumSMs * 8;
-  if (a->cfg.tensor_cores) {
-    a->kp = (a->n + 127) / 128 * 128;
-    const size_t plane = (size_t)a->n * a->kp;
-    const int np = a->is_c ? 4 : 2;
-    if (!a->abf && dalloc(&a->abf, sizeof(__nv_bfloat16) * plane * np)) return OAPB_ERR_NOMEM;
-    if (!a->xbf && dalloc(&a->xbf, sizeof(__nv_bfloat16) * 2 * 64 * (size_t)a->kp)) return OAPB_ERR_NOMEM;
-    if (!a->tcerr && dalloc(&a->tcerr, sizeof(int))) return OAPB_ERR_NOMEM;
-    cudaMemsetAsync(a->tcerr, 0, sizeof(int), a->stream);
-    a->stats.kernel_launches += np / 2;
-    if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream)) return OAPB_ERR_CUDA;
-    if (a->is_c && split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream))
-      return OAPB_ERR_CUDA;
-    a->have_tc = true;
-  }
   ++a->stats.kernel_launches;
   k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64re, a->a32re, nn);
   if (a->is_c) {
     ++a->stats.kernel_launches;
     k_to_f32<float><<<g, 256, 0, a->stream>>>(a->a64im, a->a32im, nn);
   }
-  return launch_check();
+  if (launch_check()) return OAPB_ERR_CUDA;
+  if (a->cfg.autotune == 1) {
+    if (cudaMemsetAsync(a->x32re, 0, sizeof(float) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    if (a->is_c && cudaMemsetAsync(a->x32im, 0, sizeof(float) * a->n, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    a->mv32 = tune_matvec<float>(a, a->a32re, a->a32im, a->x32re, a->is_c ? a->x32im : nullptr);
+  }
+  a->fp32_ready = true;
+  return OAPB_OK;
 }
+
+// the mixed form's operator data for the operator now set
+static int make_mixed(oapb_arnoldi* a) {
+  const int rc = a->cfg.tensor_cores ? build_tc_planes(a, 0, a->n) : ensure_fp32_copy(a);
+  if (rc) return rc;
+  a->mixed_ready = true;
+  return OAPB_OK;
+}
+
+// launch variants of the FP64 single-vector pass (forced or autotuned)
+static int tune_operator(oapb_arnoldi* a) {
+  if (a->cfg.autotune >= 2 && a->cfg.autotune < 2 + kMvVariants) {  // a forced variant
+    a->mv64 = a->mv32 = a->cfg.autotune - 2;
+  } else if (a->cfg.autotune == 1) {
+    // x: the residual buffers (zeroed), y: the work vector
+    if (cudaMemsetAsync(a->fre, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    if (a->is_c && cudaMemsetAsync(a->fim, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    a->mv64 = tune_matvec<double>(a, a->a64re, a->a64im, a->fre, a->is_c ? a->fim : nullptr);
+  }
+  a->stats.matvec_variant = (uint32_t)a->mv64;
+  return OAPB_OK;
+}
+
+extern "C" {
 
 int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
   if (!a || !A || A->dtype != OAPB_F64 || !A->re) return OAPB_ERR_ARG;
@@ -1754,26 +1808,13 @@ int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
   a->a64im = (const double*)A->im;
   a->cb = nullptr;
   a->gX = nullptr;
+  a->fp32_ready = false;
+  a->mixed_ready = false;
   if (a->cfg.precision == OAPB_PREC_MIXED) {
-    const int rc = make_fp32_copy(a);
+    const int rc = make_mixed(a);
     if (rc) return rc;
   }
-  if (a->cfg.autotune >= 2 && a->cfg.autotune < 2 + kMvVariants) {  // a forced variant
-    a->mv64 = a->mv32 = a->cfg.autotune - 2;
-  } else if (a->cfg.autotune == 1) {
-    // x: the residual buffers (zeroed), y: the work vector
-    if (cudaMemsetAsync(a->fre, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-    if (a->is_c && cudaMemsetAsync(a->fim, 0, sizeof(double) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-    a->mv64 = tune_matvec<double>(a, a->a64re, a->a64im, a->fre, a->is_c ? a->fim : nullptr);
-    if (a->a32re && a->x32re) {
-      if (cudaMemsetAsync(a->x32re, 0, sizeof(float) * a->n, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-      if (a->is_c && cudaMemsetAsync(a->x32im, 0, sizeof(float) * a->n, a->stream) != cudaSuccess)
-        return OAPB_ERR_CUDA;
-      a->mv32 = tune_matvec<float>(a, a->a32re, a->a32im, a->x32re, a->is_c ? a->x32im : nullptr);
-    }
-  }
-  a->stats.matvec_variant = (uint32_t)a->mv64;
-  return OAPB_OK;
+  return tune_operator(a);
 }
 
 int oapb_arnoldi_set_callback(oapb_arnoldi* a, oapb_matvec_fn fn, void* user) {
@@ -1993,12 +2034,44 @@ int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* hi
   const size_t bytes = sizeof(double) * (size_t)a->n * a->n;
   if (!a->own64re && dalloc(&a->own64re, bytes)) return OAPB_ERR_NOMEM;
   if (a->is_c && !a->own64im && dalloc(&a->own64im, bytes)) return OAPB_ERR_NOMEM;
-  if (cudaMemcpyAsync(a->own64re, hre, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
-  if (a->is_c && cudaMemcpyAsync(a->own64im, him, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
-    return OAPB_ERR_CUDA;
-  oapb_mat A = {(uint32_t)a->n, (uint32_t)a->n, a->own64re, a->is_c ? a->own64im : nullptr, OAPB_F64};
-  int rc = oapb_arnoldi_set_dense_operator(a, &A);
-  if (rc) return rc;
+  int rc = OAPB_OK;
+  if (a->cfg.precision == OAPB_PREC_MIXED && a->cfg.tensor_cores) {
+    // The host -> device copy in row blocks on the second stream; the BF16
+    // split of each block runs on the solver stream while the next block
+    // crosses the bus.
+    if ((rc = ensure_side_stream(a))) return rc;
+    a->a64re = a->own64re;
+    a->a64im = a->is_c ? a->own64im : nullptr;
+    a->cb = nullptr;
+    a->gX = nullptr;
+    a->fp32_ready = false;
+    a->mixed_ready = false;
+    // the previous solve's work on the solver stream precedes the copies
+    if (cudaEventRecord(a->ev_w, a->stream) != cudaSuccess || cudaStreamWaitEvent(a->s2, a->ev_w, 0) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    constexpr int kChunks = 8;
+    const long rows = (a->n + kChunks - 1) / kChunks;
+    for (long r0 = 0; r0 < a->n; r0 += rows) {
+      const long nr = r0 + rows <= a->n ? rows : a->n - r0;
+      const size_t off = (size_t)r0 * a->n, cb = sizeof(double) * (size_t)nr * a->n;
+      if (cudaMemcpyAsync(a->own64re + off, hre + off, cb, cudaMemcpyHostToDevice, a->s2) != cudaSuccess)
+        return OAPB_ERR_CUDA;
+      if (a->is_c && cudaMemcpyAsync(a->own64im + off, him + off, cb, cudaMemcpyHostToDevice, a->s2) != cudaSuccess)
+        return OAPB_ERR_CUDA;
+      if (cudaEventRecord(a->ev_chk, a->s2) != cudaSuccess || cudaStreamWaitEvent(a->stream, a->ev_chk, 0) != cudaSuccess)
+        return OAPB_ERR_CUDA;
+      if ((rc = build_tc_planes(a, r0, nr))) return rc;
+    }
+    a->mixed_ready = true;
+    if ((rc = tune_operator(a))) return rc;
+  } else {
+    if (cudaMemcpyAsync(a->own64re, hre, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    if (a->is_c && cudaMemcpyAsync(a->own64im, him, bytes, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    oapb_mat A = {(uint32_t)a->n, (uint32_t)a->n, a->own64re, a->is_c ? a->own64im : nullptr, OAPB_F64};
+    if ((rc = oapb_arnoldi_set_dense_operator(a, &A))) return rc;
+  }
   int st = oapb_arnoldi_solve(a, eig_re, eig_im, residuals, nullptr);
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   if (vre || vim) {
@@ -2029,7 +2102,7 @@ int oapb_arnoldi_apply_block(oapb_arnoldi* a, const double* xre, const double* x
   if (precision != OAPB_PREC_FP64 && precision != OAPB_PREC_MIXED && precision != OAPB_PASS_BF16)
     return OAPB_ERR_ARG;
   const bool fp32 = precision != OAPB_PREC_FP64, bf16 = precision == OAPB_PASS_BF16;
-  if (fp32 && !a->a32re) return OAPB_ERR_ARG;
+  if (fp32 && !a->mixed_ready) return OAPB_ERR_ARG;
   int rc = alloc_blocks(a);
   if (rc) return rc;
   rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32, bf16)
