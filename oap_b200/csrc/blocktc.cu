@@ -61,6 +61,8 @@ constexpr int kBtcSub = 32;
 // QB + q for im; K = n padded to kp), zero rows / columns beyond b / n
 __global__ void k_split_block_bf16(const double* __restrict__ xr, const double* __restrict__ xi, int b, int QB,
                                    int nrows, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo) {
+  // launched as a dependent of whatever wrote X (or last read hi / lo)
+  tc::griddep_wait();
   const long total = (long)nrows * kp;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
     const int row = (int)(e / kp);
@@ -435,7 +437,9 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
-  k_split_block_bf16<<<kNumSMs * 4, 256, 0, s>>>(xr, cplx ? xi : nullptr, b, QB, N, op.n, op.kp, xbh, xbl);
+  if (launch_dependent(k_split_block_bf16, dim3(kNumSMs * 4), dim3(256), 0, s, xr, cplx ? xi : nullptr, b, QB, N, op.n,
+                       op.kp, xbh, xbl) != cudaSuccess)
+    return OAPB_ERR_CUDA;
   BtcArgs g;
   const __nv_bfloat16* planes[4] = {op.arh, op.arl, cplx ? op.aih : op.arh, cplx ? op.ail : op.arl};
   for (int p = 0; p < 4; ++p)

@@ -123,6 +123,30 @@ def test_solve_from_host_buffers():
         assert np.linalg.norm(A @ X[:, q] - ev[q] * X[:, q]) <= TOL * max(abs(e) for e in ev)
 
 
+@pytest.mark.parametrize("n", [8192, 1000])
+def test_mixed_solve_from_host_buffers(n):
+    # the mixed form's host-input solve copies the operator in row blocks and
+    # splits each block while the next one is copied: the same pairs as the
+    # solve on the device-resident operator (n = 1000: ragged last block,
+    # the plain path solving on the same handle)
+    A = planted_complex(n, seed=21, nplant=6)
+    s = B.Arnoldi(n, 32, 6, is_complex=True, precision=B.PREC_MIXED, seed=4)
+    ev, res, st, X = s.solve_host(np.ascontiguousarray(A.real), np.ascontiguousarray(A.imag), vectors=True)
+    assert st == B.OK and max(res) <= TOL
+    scale = max(abs(e) for e in ev)
+    for q in range(6):
+        assert np.linalg.norm(A @ X[:, q] - ev[q] * X[:, q]) <= TOL * scale * 1.01
+    d = solve(A, 6, 32, precision=B.PREC_MIXED, seed=4)
+    for lam in d["ev"]:
+        assert np.min(np.abs(np.array(ev) - lam)) < 1e-9 * abs(lam)
+    if n >= 8192:  # the BF16 planes built block by block equal the ones built at once
+        xr = torch.randn(4, n, dtype=torch.float64, device="cuda")
+        xi = torch.randn(4, n, dtype=torch.float64, device="cuda")
+        w1 = s.apply_block(xr, xi, precision=B.PREC_MIXED)
+        w2 = d["solver"].apply_block(xr, xi, precision=B.PREC_MIXED)
+        assert torch.equal(w1[0], w2[0]) and torch.equal(w1[1], w2[1])
+
+
 def test_first_value_is_one_start():
     A, lam = planted_symmetric(200, seed=5)
     r = solve(A, 3, 20, init=B.INIT_FIRST_VALUE_IS_ONE)
