@@ -1286,16 +1286,19 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       if (!(mx == mx) || mx > 1e-2 * prev) return kSlow;
       prev = mx;
     }
-    // inner fixed point on the FP32-class operator, for a correction about
-    // 100x below the goal; the observed contraction of non-normal problems
-    // is slower than rho, so the count assumes at least 0.3 per sweep (a
-    // shortfall costs one more outer step, not the result)
+    // inner fixed point on the FP32-class operator, for a truncation error
+    // of 3 % of the goal (the correction's FP32-class rounding, about 5e-6 of
+    // the starting residual, dominates the result); the observed contraction
+    // of non-normal problems is slower than rho, so the count assumes at
+    // least 0.3 per sweep: a contraction up to 0.37 still leaves the
+    // truncation below a third of the goal, and a shortfall costs one more
+    // outer step, not the result
     const double rho_eff = rho > 0.3 ? rho : 0.3;
-    int J = (int)ceil(log(0.01 * tol / mx) / log(rho_eff));
+    int J = (int)ceil(log(0.03 * tol / mx) / log(rho_eff));
     if (J < 2) J = 2;
     if (J > 30) J = 30;
     // leading sweeps on the BF16 planes: the last Jf contract their error
-    const int Jf = (int)ceil(log(0.01 * tol / mx / kBf16Err) / log(rho_eff));
+    const int Jf = (int)ceil(log(0.03 * tol / mx / kBf16Err) / log(rho_eff));
     const int Jb = J - Jf > 0 ? J - Jf : 0;
     a->stats.kernel_launches += 2;
     k_small_inv<<<1, 32, 0, a->stream>>>(a->G, p, a->Tinv, a->bstatus);
