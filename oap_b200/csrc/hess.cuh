@@ -498,7 +498,7 @@ static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
 // Eigenpairs of a nearly upper-triangular T (m x m complex, column-major,
 // m <= 32): the Rayleigh quotient of an orthonormalised basis of Ritz vectors
 // ordered like their values, whose strictly lower part is of the size of the
-// Ritz vectors' errors.  Warp w takes pairs q = w, w + kNtWarps, ...:
+// Ritz vectors' errors.  Warp w of nw takes pairs q = w, w + nw, ...:
 // Rayleigh quotient iteration from v = e_q, sigma = T(q,q) (LU with partial
 // pivoting of T - sigma I, a zero pivot replaced by eps ||T||_F; v <- (T -
 // sigma I)^-1 v normalised; sigma <- v^H T v), at most kNtIters steps, until
@@ -508,29 +508,37 @@ static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
 // then ritz / Y / order are written in the ArnUtils order of `which` (as
 // k_hess writes them, Y column q at Y + q m, unit 2-norm) and *delivered = 1;
 // otherwise *delivered = 0 and nothing else is written (k_hess follows with
-// skip = delivered).  Dynamic shared memory: nt_smem_bytes(m).
-constexpr int kNtWarps = 8;
+// skip = delivered).  Launch nt_warps(m) warps, dynamic shared memory
+// nt_smem_bytes(m, nt_warps(m)).
+constexpr int kNtWarpsMax = 16;
 constexpr int kNtIters = 4;
 __host__ __device__ inline int nt_ld(int m) { return m + 1; }
-__host__ __device__ inline size_t nt_smem_bytes(int m) {
-  return sizeof(cplx) * ((size_t)(kNtWarps + 1) * m * nt_ld(m) + (size_t)2 * kNtWarps * m + (size_t)m * m + m) +
-         sizeof(double) * 2 * m + sizeof(int) * (kNtWarps * m + m + 1);
+__host__ __device__ inline size_t nt_smem_bytes(int m, int nw) {
+  return sizeof(cplx) * ((size_t)(nw + 1) * m * nt_ld(m) + (size_t)2 * nw * m + (size_t)m * m + m) +
+         sizeof(double) * 2 * m + sizeof(int) * (nw * m + m + 1);
+}
+// warps for m: one per pair while the workspace stays within 200 KB
+inline int nt_warps(int m) {
+  int nw = m < kNtWarpsMax ? m : kNtWarpsMax;
+  while (nw > 1 && nt_smem_bytes(m, nw) > 200 * 1024) --nw;
+  return nw;
 }
 
-static __global__ void __launch_bounds__(kNtWarps * 32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, int which,
+static __global__ void __launch_bounds__(kNtWarpsMax * 32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, int which,
                                                                 cplx* ritz, cplx* Y, int* order, int* delivered) {
   extern __shared__ __align__(16) unsigned char nt_dyn[];
   const int LD = nt_ld(m);
   cplx* T = reinterpret_cast<cplx*>(nt_dyn);                 // m x LD
-  cplx* Mw = T + (size_t)m * LD;                             // kNtWarps x (m x LD)
-  cplx* xw = Mw + (size_t)kNtWarps * m * LD;                 // kNtWarps x m
-  cplx* tw = xw + (size_t)kNtWarps * m;                      // kNtWarps x m
-  cplx* V = tw + (size_t)kNtWarps * m;                       // m x m eigenvectors (column q)
+  const int nw = blockDim.x >> 5;
+  cplx* Mw = T + (size_t)m * LD;                             // nw x (m x LD)
+  cplx* xw = Mw + (size_t)nw * m * LD;                       // nw x m
+  cplx* tw = xw + (size_t)nw * m;                            // nw x m
+  cplx* V = tw + (size_t)nw * m;                             // m x m eigenvectors (column q)
   cplx* th = V + (size_t)m * m;                              // m
   double* res = reinterpret_cast<double*>(th + m);           // m
   double* key = res + m;                                     // m
-  int* piv = reinterpret_cast<int*>(key + m);                // kNtWarps x m
-  int* ord = piv + kNtWarps * m;                             // m
+  int* piv = reinterpret_cast<int*>(key + m);                // nw x m
+  int* ord = piv + nw * m;                                   // m
   int* ok = ord + m;                                         // 1
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (m < 1 || m > 32) return;
@@ -548,7 +556,7 @@ static __global__ void __launch_bounds__(kNtWarps * 32) k_eig_near_tri(const cpl
   cplx* x = xw + (size_t)warp * m;
   cplx* t = tw + (size_t)warp * m;
   int* pv = piv + warp * m;
-  for (int q = warp; q < m; q += kNtWarps) {
+  for (int q = warp; q < m; q += nw) {
     cplx sigma = T[q + q * LD], thq = {0, 0};
     double rq = 1e300;
     for (int i = lane; i < m; i += 32) x[i] = cplx{i == q ? 1.0 : 0.0, 0.0};

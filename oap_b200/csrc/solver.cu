@@ -919,12 +919,12 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
   ++a->stats.kernel_launches;
   if (near_tri && !fp32 && b <= 32 && a->ntflag) {
     // the opt-in above 48 KB of dynamic shared memory (per device)
-    if (cudaFuncSetAttribute(k_eig_near_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nt_smem_bytes(32)) !=
-        cudaSuccess)
+    const int nw = nt_warps(b);
+    const size_t nsm = nt_smem_bytes(b, nw);
+    if (cudaFuncSetAttribute(k_eig_near_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nsm) != cudaSuccess)
       return OAPB_ERR_CUDA;
     ++a->stats.kernel_launches;
-    k_eig_near_tri<<<1, kNtWarps * 32, nt_smem_bytes(b), a->stream>>>(G, b, a->cfg.sort, a->britz, a->bY, a->border,
-                                                                      a->ntflag);
+    k_eig_near_tri<<<1, nw * 32, nsm, a->stream>>>(G, b, a->cfg.sort, a->britz, a->bY, a->border, a->ntflag);
     h.skip = a->ntflag;
   }
   if (fp32)
