@@ -226,6 +226,16 @@ class CuHArnoldiCallback {
     if (h_) oapb_arnoldi_get_stats(h_, &s);
     return s;
   }
+  // convergence checks of the last execute (the data behind the reference's
+  // per-step logInfo printouts, ArnoldiPackage/ArnoldiProcedures.cpp:391-395, 539)
+  std::vector<oapb_trace_rec> trace() const {
+    std::vector<oapb_trace_rec> t;
+    uint32_t n = 0;
+    if (!h_ || oapb_arnoldi_get_trace(h_, nullptr, 0, &n) != OAPB_OK) return t;
+    t.resize(n);
+    if (n && oapb_arnoldi_get_trace(h_, t.data(), n, &n) != OAPB_OK) t.clear();
+    return t;
+  }
   CuProceduresApi& api() { return api_; }
 
  private:

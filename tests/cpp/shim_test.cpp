@@ -174,6 +174,7 @@ static int gpu_tests() {
       EXPECT(arnoldi.residuals()[i] <= 1e-10);
       EXPECT(arnoldi.testOutcome(i) <= 1e-10);
     }
+    EXPECT(arnoldi.trace().empty());  // the plain restart loop records no block-phase checks
     std::printf("mode %d: lambda_1 = %.12f%+.12fi, residual %.2e\n", mode, re[0], im[0], arnoldi.residuals()[0]);
   }
   // Network (oapNetwork.h names): learn y = M x on 256 samples, save, load

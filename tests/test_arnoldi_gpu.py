@@ -147,6 +147,26 @@ def test_mixed_solve_from_host_buffers(n):
         assert torch.equal(w1[0], w2[0]) and torch.equal(w1[1], w2[1])
 
 
+def test_mixed_solve_on_a_user_stream():
+    # the mixed form on a caller's non-default stream: its overlapped checks
+    # (second stream, events) order against that stream; same pairs as on the
+    # default stream, and the caller's stream sees the results in order
+    n = 8192
+    A = planted_complex(n, seed=31, nplant=6)
+    are, aim = planes(A, True)
+    d = solve(A, 6, 32, precision=B.PREC_MIXED, seed=5)
+    user = torch.cuda.Stream()
+    user.wait_stream(torch.cuda.current_stream())  # the operator planes were written on the default stream
+    with torch.cuda.stream(user):
+        s = B.Arnoldi(n, 32, 6, is_complex=True, precision=B.PREC_MIXED, seed=5, stream=user.cuda_stream)
+        s.set_operator(are, aim)
+        ev, res, st = s.solve()
+    user.synchronize()
+    assert st == B.OK and max(res) <= TOL
+    assert s.stats()["refine_iterations"] >= 2
+    assert np.allclose(np.array(ev), d["ev"], rtol=0, atol=1e-12 * np.abs(d["ev"]).max())
+
+
 def test_first_value_is_one_start():
     A, lam = planted_symmetric(200, seed=5)
     r = solve(A, 3, 20, init=B.INIT_FIRST_VALUE_IS_ONE)
