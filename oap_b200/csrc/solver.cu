@@ -1327,10 +1327,12 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(W, Wi, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, R,
                                                           Ri);
     }
-    // X <- orth(X + D)
+    // X <- orth(X + D): X is orthonormal and D orthogonal to it, so X + D is
+    // conditioned like 1 + ||D|| and one CholeskyQR pass is orthonormal to
+    // rounding (a diverging D is rejected by the next step's check)
     a->stats.kernel_launches++;
     k_block_add<<<grid_n(len), 256, 0, a->stream>>>(X, Xi, D, Di, p, n, R, Ri);
-    if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 2))) return rc;
+    if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 1))) return rc;
   }
   return kSlow;
 }
