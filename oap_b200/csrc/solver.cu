@@ -1067,11 +1067,11 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   std::vector<cplx> th(b);
   // In the FP32 phase the first Rayleigh-Ritz checks carry no decision:
   // from a random block the wanted directions need several powers before
-  // the residuals mean anything, so the first check is at iteration 5, the
-  // second two later, and from then on at the iteration the observed
-  // contraction predicts for the goal (each check costs a small dense
-  // eigensolve and a host synchronisation).
-  unsigned next_check = 5;
+  // the residuals mean anything, so the first check is at iteration 6 (after
+  // five BF16 powers and one FP32-class one), the second two later, and from
+  // then on at the iteration the observed contraction predicts for the goal
+  // (each check costs a small dense eigensolve and a host synchronisation).
+  unsigned next_check = 6;
   // FP32 phase: CholeskyQR only where the block's columns could drift
   // apart by more than 1e3 since the last one (growth per iteration = the
   // spread |theta|max / |theta|min of the last Rayleigh-Ritz values, known
