@@ -18,6 +18,13 @@
 #include "matvec.cuh"
 
 namespace oapb {
+// The kernels below may be launched as programmatic dependents of the
+// kernel before them in the stream: they wait for it to complete (and its
+// memory to be visible) before touching global memory; a no-op otherwise.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+}  // namespace oapb
+
+namespace oapb {
 
 constexpr int kBmRows = 128;  // rows per CTA tile
 constexpr int kBmTM = 4;      // rows per thread
@@ -221,6 +228,7 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
                                                    const double* __restrict__ Yim, int b2, int n, cplx* part) {
   __shared__ double xr[kBmMaxB][kDotChunk + 1], xi[kBmMaxB][kDotChunk + 1];
   __shared__ double yr[kBmMaxB][kDotChunk + 1], yi[kBmMaxB][kDotChunk + 1];
+  pdl_wait();
   const int cnt = b1 * b2;
   double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
   const long nchunks = (n + kDotChunk - 1) / kDotChunk;
@@ -406,6 +414,7 @@ __global__ void __launch_bounds__(1024) k_block_reduce(const cplx* __restrict__ 
   auto& sr = sm.r.sr;
   auto& si = sm.r.si;
   if (blockDim.x != 32 || blockDim.y != 32) return;  // the layout below assumes 32 x 32
+  pdl_wait();
   const int tx = threadIdx.x, ty = threadIdx.y;
   const int p = blockIdx.x * 32 + tx;
   double a[4] = {0, 0, 0, 0}, c4[4] = {0, 0, 0, 0};
@@ -464,6 +473,7 @@ __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__
                                                       const double* __restrict__ Yim = nullptr) {
   __shared__ cplx cs[kBmMaxB * kBmMaxB];
   __shared__ double xs_r[kBmMaxB][kUpRows], xs_i[CPLX ? kBmMaxB : 1][kUpRows];
+  pdl_wait();
   for (int e = threadIdx.x; e < b1 * b2; e += blockDim.x) cs[e] = Cm[(e % b1) + (long)(e / b1) * ldc];
   const int rr = threadIdx.x % kUpRows, g = threadIdx.x / kUpRows;
   const long nblk = (n + kUpRows - 1) / kUpRows;
@@ -498,6 +508,7 @@ __global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restr
                            double* part) {
   __shared__ double red[kBmMaxB][8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  pdl_wait();
   for (int q = 0; q < b; ++q) {
     double s = 0;
     for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {

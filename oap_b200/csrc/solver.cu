@@ -42,6 +42,7 @@
 #include "hess.cuh"
 #include "matio.cuh"
 #include "matvec.cuh"
+#include "streamk.cuh"
 
 namespace oapb {
 
@@ -783,9 +784,9 @@ template <bool C>
 void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, const double* yr, const double* yi,
                 int b2, cplx* G) {
   a->stats.kernel_launches += 2;
-  k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(xr, xi, b1, yr, yi, b2, a->n, a->bpart);
-  k_block_reduce<<<(b1 * b2 + 31) / 32, dim3(32, 32), 0, a->stream>>>(a->bpart, a->ndot, b1 * b2, G, a->bdone,
-                                                                       0, nullptr, nullptr);
+  launch_dependent(k_block_dot<C>, dim3(a->ndot), dim3(256), 0, a->stream, xr, xi, b1, yr, yi, b2, a->n, a->bpart);
+  launch_dependent(k_block_reduce, dim3((b1 * b2 + 31) / 32), dim3(32, 32), 0, a->stream, a->bpart, a->ndot, b1 * b2,
+                   G, a->bdone, 0, nullptr, nullptr);
 }
 
 // W = A X (b vectors); FP32-class operator copy when fp32, else FP64.
@@ -853,7 +854,7 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
 template <bool C>
 int col_norms(oapb_arnoldi* a, const double* yr, const double* yi, int b, double* out) {
   ++a->stats.kernel_launches;
-  k_colnorm2<C><<<a->nnorm, 256, 0, a->stream>>>(yr, yi, b, a->n, a->bnorm);
+  launch_dependent(k_colnorm2<C>, dim3(a->nnorm), dim3(256), 0, a->stream, yr, yi, b, a->n, a->bnorm);
   std::vector<double> h((size_t)b * a->nnorm);
   if (cudaMemcpyAsync(h.data(), a->bnorm, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, a->stream) !=
       cudaSuccess)
@@ -878,11 +879,10 @@ int cholqr2(oapb_arnoldi* a, const double* wr, const double* wi, int b, double* 
     double* di = pass + 1 < passes ? ti : xi;
     // Gram matrix, then (last reduce block) its Cholesky factor and R^-1
     a->stats.kernel_launches += 3;
-    k_block_dot<C><<<a->ndot, 256, 0, a->stream>>>(sr, si, b, sr, si, b, a->n, a->bpart);
-    k_block_reduce<<<(b * b + 31) / 32, dim3(32, 32), 0, a->stream>>>(a->bpart, a->ndot, b * b, a->G2, a->bdone, b,
-                                                                       a->Rinv, a->bstatus);
-    k_block_update<C><<<grid_up(a->n), 256, 0, a->stream>>>(sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr,
-                                                           di);
+    launch_dependent(k_block_dot<C>, dim3(a->ndot), dim3(256), 0, a->stream, sr, si, b, sr, si, b, a->n, a->bpart);
+    launch_dependent(k_block_reduce, dim3((b * b + 31) / 32), dim3(32, 32), 0, a->stream, a->bpart, a->ndot, b * b,
+                     a->G2, a->bdone, b, a->Rinv, a->bstatus);
+    launch_dependent(k_block_update<C>, dim3(grid_up(a->n)), dim3(256), 0, a->stream, sr, si, b, a->Rinv, b, b, nullptr, nullptr, 0, a->n, dr, di, nullptr, nullptr);
     sr = dr;
     si = di;
   }
@@ -957,11 +957,11 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
   }
   block_gram<C>(a, X, Xi, b, W, Wi, b, a->G);
   a->stats.kernel_launches += 3;
-  k_block_update<C><<<grid_up(n), 256, 0, cs>>>(X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri);
+  launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, cs, X, Xi, b, a->G, b, b, W, Wi, 1, n, R, Ri, nullptr, nullptr);
   int rc = small_eig(a, a->G, b, kk, nv, fp32, near_tri);
   if (!rc) {
-    k_block_update<C><<<grid_up(n), 256, 0, cs>>>(R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei);
-    k_colnorm2<C><<<a->nnorm, 256, 0, cs>>>(E, Ei, kk, n, a->bnorm);
+    launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, cs, R, Ri, b, a->bY, b, kk, nullptr, nullptr, 0, n, E, Ei, nullptr, nullptr);
+    launch_dependent(k_colnorm2<C>, dim3(a->nnorm), dim3(256), 0, cs, E, Ei, kk, n, a->bnorm);
     rc = launch_check();
   }
   a->stream = s0;
@@ -1188,16 +1188,14 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
         if (bn == b) {
           if ((rc = cholqr2<C>(a, W, Wi, b, a->Xre, a->Xim, E, Ei, 1))) return rc;
         } else {
-          k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n,
-                                                              a->Xre, a->Xim);
+          launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, b, a->bY, b, bn, nullptr, nullptr, 0, n, a->Xre, a->Xim, nullptr, nullptr);
         }
         if (floor_out) *floor_out = mx;
         if (ritz_out) *ritz_out = th;
         return launch_check();
       }
       a->stats.kernel_launches += 1;
-      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre,
-                                                          a->Xim);
+      launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, b, a->bY, b, kk, nullptr, nullptr, 0, n, a->Xre, a->Xim, nullptr, nullptr);
       a->evals.assign(th.begin(), th.begin() + kk);
       if ((rc = launch_check())) return rc;
       return done ? OAPB_OK : OAPB_NOT_CONVERGED;
@@ -1261,7 +1259,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     if (outer == 0) {  // T and R only
       block_gram<C>(a, X, Xi, p, W, Wi, p, a->G);
       ++a->stats.kernel_launches;
-      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri);
+      launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, p, a->G, p, p, W, Wi, 1, n, R, Ri, nullptr, nullptr);
     } else {
       const uint32_t passes_now = a->stats.block_matvecs, bf16_now = a->stats.block_bf16;
       if ((rc = check_enqueue<C>(a, a->stream, X, Xi, W, Wi, R, Ri, E, Ei, p, p, p, false, true))) return rc;
@@ -1278,8 +1276,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       a->trace.push_back({3, outer, passes_now, bf16_now, mx});
       if (mx <= tol) {  // Ritz vectors X S
         ++a->stats.kernel_launches;
-        k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre,
-                                                            a->Xim);
+        launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, p, a->bY, p, p, nullptr, nullptr, 0, n, a->Xre, a->Xim, nullptr, nullptr);
         a->evals.assign(th.begin(), th.end());
         return launch_check();
       }
@@ -1303,7 +1300,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     a->stats.kernel_launches += 2;
     k_small_inv<<<1, 32, 0, a->stream>>>(a->G, p, a->Tinv, a->bstatus);
     // D = R T^-1 (the first sweep from D = 0)
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(R, Ri, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di);
+    launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, R, Ri, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, nullptr, nullptr);
     // Components of D inside span(X) do not move the subspace; between
     // projections they grow at most like |theta_1| / |theta_p| per
     // iteration, so project when that growth would pass 4x, and last.
@@ -1320,12 +1317,11 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       if ((j + 1) % every == 0 || j + 1 == J) {
         block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
         a->stats.kernel_launches++;
-        k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi);
+        launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi, nullptr, nullptr);
       }
       // D = (P A D + R) T^-1
       a->stats.kernel_launches++;
-      k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(W, Wi, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, R,
-                                                          Ri);
+      launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, W, Wi, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, R, Ri);
     }
     // X <- orth(X + D): X is orthonormal and D orthogonal to it, so X + D is
     // conditioned like 1 + ||D|| and one CholeskyQR pass is orthonormal to
@@ -1354,8 +1350,7 @@ int verify(oapb_arnoldi* a, double scale, double* out) {
     if (cudaMemcpyAsync(a->G, diag.data(), sizeof(cplx) * b * b, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
       return OAPB_ERR_CUDA;
     ++a->stats.kernel_launches;
-    k_block_update<C><<<grid_up(n), 256, 0, a->stream>>>(xr, xi, b, a->G, b, b, a->Bre[1], a->Bim[1], 1, n,
-                                                        a->Bre[2], a->Bim[2]);
+    launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, xr, xi, b, a->G, b, b, a->Bre[1], a->Bim[1], 1, n, a->Bre[2], a->Bim[2], nullptr, nullptr);
     std::vector<double> rn(b), xn(b);
     if ((rc = col_norms<C>(a, a->Bre[2], a->Bim[2], b, rn.data()))) return rc;
     if ((rc = col_norms<C>(a, xr, xi, b, xn.data()))) return rc;
