@@ -124,6 +124,7 @@ def lib():
                                         P(C.c_double), vp, vp],
             "oapb_arnoldi_get_stats": [vp, P(Stats)],
             "oapb_arnoldi_get_trace": [vp, P(TraceRec), C.c_uint32, P(C.c_uint32)],
+            "oapb_arnoldi_set_profile": [vp, C.c_int32],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
@@ -325,6 +326,10 @@ class Arnoldi:
         check(lib().oapb_arnoldi_apply_block(self.h, p(xre), p(xim), b, p(wre), p(wim), precision),
               "oapb_arnoldi_apply_block")
         return wre, wim
+
+    def set_profile(self, on):
+        """Per-launch CUDA-event timing of the operator passes on / off."""
+        check(lib().oapb_arnoldi_set_profile(self.h, int(bool(on))), "oapb_arnoldi_set_profile")
 
     def trace(self):
         """Convergence checks of the last solve: (phase, iteration, passes,

@@ -2121,6 +2121,12 @@ int oapb_arnoldi_get_stats(const oapb_arnoldi* a, oapb_arnoldi_stats* out) {
   return OAPB_OK;
 }
 
+int oapb_arnoldi_set_profile(oapb_arnoldi* a, int32_t on) {
+  if (!a) return OAPB_ERR_ARG;
+  a->cfg.profile = on != 0;
+  return OAPB_OK;
+}
+
 int oapb_arnoldi_get_trace(const oapb_arnoldi* a, oapb_trace_rec* out, uint32_t cap, uint32_t* count) {
   if (!a || !count || (cap && !out)) return OAPB_ERR_ARG;
   *count = (uint32_t)a->trace.size();
