@@ -150,6 +150,40 @@ def ncu_traffic():
         return None
 
 
+class gpu_local_cpus:
+    """Within the block, run on the CPUs NVML reports as local to GPU
+    `index` (so host memory allocated there lands on its NUMA node); the
+    previous affinity is restored on exit.  No-op where NVML or affinity
+    control is unavailable."""
+
+    def __init__(self, index):
+        self.index = index
+        self.old = None
+
+    def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, 16)
+            cpus = {i * 64 + b for i, w in enumerate(words) for b in range(64) if (int(w) >> b) & 1}
+            cpus &= set(range(os.cpu_count() or 1))
+            if cpus:
+                self.old = os.sched_getaffinity(0)
+                os.sched_setaffinity(0, cpus)
+        except Exception:
+            self.old = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.old:
+            try:
+                os.sched_setaffinity(0, self.old)
+            except OSError:
+                pass
+        return False
+
+
 def dist_init(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -341,10 +375,13 @@ def run_ours(args, world, rank, local):
     pvalue = allsum(world, pconv) / allmax(world, psecs)
     plain.close()
     # end to end through the host-buffer entry point (pinned host planes)
-    are_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
-    aim_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
-    are_h.copy_(are)
-    aim_h.copy_(aim)
+    # the pinned host planes on the GPU's own NUMA node (as a serving process
+    # bound to its GPU's socket would have them)
+    with gpu_local_cpus(local):
+        are_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        aim_h = torch.empty((n, n), dtype=torch.float64, pin_memory=True)
+        are_h.copy_(are)
+        aim_h.copy_(aim)
     e2e_solver = B.Arnoldi(n, M_KRYLOV, K_WANTED, is_complex=True, precision=B.PREC_MIXED,
                            tolerance=TOL, seed=3 + rank)
     ar_np, ai_np = are_h.numpy(), aim_h.numpy()
