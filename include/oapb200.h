@@ -315,7 +315,8 @@ OAPB_EXPORT int oapb_arnoldi_solve_host(oapb_arnoldi* handle, const double* a_re
 OAPB_EXPORT int oapb_arnoldi_get_stats(const oapb_arnoldi* handle, oapb_arnoldi_stats* out);
 
 /* Switch the per-launch CUDA-event timing of the operator passes (config
- * field profile) on or off for the following solves. */
+ * field profile) on or off for the following solves; the device-side
+ * counterpart of the reference's host clock macros (oapUtils/oapClock.h:74-78). */
 OAPB_EXPORT int oapb_arnoldi_set_profile(oapb_arnoldi* handle, int32_t on);
 
 /* One convergence check of the mixed form's block phases. */
