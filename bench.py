@@ -163,8 +163,12 @@ class gpu_local_cpus:
     def __enter__(self):
         try:
             import pynvml
+            import torch
             pynvml.nvmlInit()
-            h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            # NVML numbers GPUs without CUDA_VISIBLE_DEVICES: find ours by PCI address
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus.encode())
             words = pynvml.nvmlDeviceGetCpuAffinity(h, 16)
             cpus = {i * 64 + b for i, w in enumerate(words) for b in range(64) if (int(w) >> b) & 1}
             cpus &= set(range(os.cpu_count() or 1))
