@@ -35,6 +35,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N, K_WANTED, M_KRYLOV, NPLANT, SHIFT, TOL = 16384, 16, 64, 16, 4.0, 1e-10
+DMMA_PEAK_TFLOPS = 37.1  # mma.sync.m16n8k4.f64 throughput measured on B200 (register operands)
+FMA64_PEAK_TFLOPS = 34.0  # FP64 FMA throughput measured on B200 (register operands)
 METRIC = "eigensolves/s at residual≤1e-10: chosen form vs plain FP64 GPU Arnoldi"
 WORKLOAD = "complex non-Hermitian dense A, n=16384, split re/im FP64, N(0,1/n) + 4 on 16 planted diagonal entries; top-16 LM, m=64"
 
@@ -444,8 +446,19 @@ def run_ours(args, world, rank, local):
                                 "GBs": (v[2] / (v[0] / v[1]) / 1e9) if v[1] else None,
                                 "frac": (v[2] / (v[0] / v[1]) / 1e9 / hbm) if v[1] else None,
                                 "algorithmic_bytes_per_launch": v[2],
+                                "tflops": (v[3] / (v[0] / v[1]) / 1e12) if v[1] else None,
                                 "traffic": (traffic or {}).get(k.split(" (")[0], {}).get("bytes_per_launch")}
                             for k, v in kernels.items()},
+            # the FP64 pass is bound by the FP64 tensor pipe, not by HBM: its
+            # fraction of the DMMA throughput measured on this pool with a
+            # register-only mma.sync.m16n8k4.f64 loop
+            "fp64_pass": ({"bound": "fp64 fma" if args.no_tc else "fp64 tensor",
+                           "tflops": kernels[fp64_name][3] / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e12,
+                           "peak_tflops": FMA64_PEAK_TFLOPS if args.no_tc else DMMA_PEAK_TFLOPS,
+                           "frac": kernels[fp64_name][3] / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e12 /
+                           (FMA64_PEAK_TFLOPS if args.no_tc else DMMA_PEAK_TFLOPS),
+                           "peak_source": "own throughput probe (register operands)"}
+                          if kernels[fp64_name][1] else None),
             "plain_fp64_matvec_GBs": ((16.0 * n * n + 32.0 * n) / (pprof["matvec_seconds"] / pprof["matvec_timed"]) / 1e9
                                       if pprof["matvec_timed"] else None)}
 
