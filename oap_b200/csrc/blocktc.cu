@@ -78,17 +78,35 @@ __global__ void k_split_block_bf16(const double* __restrict__ xr, const double* 
   }
 }
 
-// A (FP64 plane, n x n) -> hi / lo BF16 planes (n x kp, zero-padded columns)
-__global__ void k_split_operator_bf16(const double* __restrict__ a, int n, int kp, long row0, long rows,
-                                      __nv_bfloat16* hi, __nv_bfloat16* lo) {
+// A (FP64 plane, n x n) -> hi / lo BF16 planes (n x kp, zero-padded
+// columns); with err2 set, adds sum (a - hi)^2 (the squared Frobenius norm
+// of the BF16 planes' rounding) to *err2
+__global__ void __launch_bounds__(256) k_split_operator_bf16(const double* __restrict__ a, int n, int kp, long row0,
+                                                             long rows, __nv_bfloat16* hi, __nv_bfloat16* lo,
+                                                             double* err2) {
+  __shared__ double red[8];
   const long total = rows * kp;
+  double acc = 0;
   for (long e0 = (long)blockIdx.x * blockDim.x + threadIdx.x; e0 < total; e0 += (long)gridDim.x * blockDim.x) {
     const long e = row0 * kp + e0;
     const long r = e / kp, c = e % kp;
-    const float v = c < n ? (float)a[r * n + c] : 0.f;
+    const double ad = c < n ? a[r * n + c] : 0.0;
+    const float v = (float)ad;
     const __nv_bfloat16 h = __float2bfloat16_rn(v);
     hi[e] = h;
     lo[e] = __float2bfloat16_rn(v - __bfloat162float(h));
+    const double d = ad - (double)__bfloat162float(h);
+    acc += d * d;
+  }
+  if (!err2) return;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    atomicAdd(err2, t);
   }
 }
 
@@ -410,11 +428,11 @@ static size_t btc_stage_bytes(int N, bool cplx, bool lo) {
 }
 
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
-                        long row0, long rows) {
+                        long row0, long rows, double* err2) {
   if (rows < 0) rows = n - row0;
   if (row0 < 0 || row0 + rows > n) return OAPB_ERR_ARG;
   if (rows == 0) return OAPB_OK;
-  k_split_operator_bf16<<<kNumSMs * 8, 256, 0, s>>>(a, n, kp, row0, rows, hi, lo);
+  k_split_operator_bf16<<<kNumSMs * 8, 256, 0, s>>>(a, n, kp, row0, rows, hi, lo, err2);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 

@@ -15,9 +15,9 @@ struct BtcOperator {
 };
 
 // hi / lo BF16 planes of one FP64 operator plane (rows row0 .. row0 + rows - 1;
-// rows < 0: to the last row)
+// rows < 0: to the last row); err2 (optional) accumulates sum (a - hi)^2
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
-                        long row0 = 0, long rows = -1);
+                        long row0 = 0, long rows = -1, double* err2 = nullptr);
 
 // Doubles of stream-K partial workspace for an n x n operator (b <= 32).
 size_t btc_workspace(int n, int kp);

@@ -487,6 +487,10 @@ struct oapb_arnoldi {
   int kp = 0;
   int* tcerr = nullptr;
   bool have_tc = false;
+  // ||A - hi||_F^2 of the BF16 hi planes (device, summed by the split) and
+  // its host copy as ||A - hi||_F (read once per operator; < 0: not read)
+  double* bf16err2 = nullptr;
+  double bf16_err = -1;
   size_t hess_smem = 0;
   oapb_arnoldi_stats stats{};
   std::vector<cudaEvent_t> ev_pool;   // profiling events (pairs)
@@ -718,7 +722,8 @@ size_t pin_ritz_off(const oapb_arnoldi* a) { return (sizeof(double) * kBmMaxB * 
 size_t pin_st_off(const oapb_arnoldi* a) { return pin_ritz_off(a) + ((sizeof(cplx) * kBmMaxB + 63) & ~(size_t)63); }
 size_t pin_err_off(const oapb_arnoldi* a) { return pin_st_off(a) + ((sizeof(DevState) + 63) & ~(size_t)63); }
 size_t pin_nt_off(const oapb_arnoldi* a) { return pin_err_off(a) + 64; }
-size_t pin_bytes(const oapb_arnoldi* a) { return pin_nt_off(a) + 64; }
+size_t pin_e2_off(const oapb_arnoldi* a) { return pin_nt_off(a) + 64; }
+size_t pin_bytes(const oapb_arnoldi* a) { return pin_e2_off(a) + 64; }
 
 int alloc_blocks(oapb_arnoldi* a) {
   if (a->Bre[0]) return OAPB_OK;
@@ -982,6 +987,10 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
   if (near_tri && b <= 32 &&
       cudaMemcpyAsync(hp + pin_nt_off(a), a->ntflag, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
     return OAPB_ERR_CUDA;
+  *(double*)(hp + pin_e2_off(a)) = -1;  // the BF16 rounding energy rides along until known
+  if (a->bf16_err < 0 && a->bf16err2 &&
+      cudaMemcpyAsync(hp + pin_e2_off(a), a->bf16err2, sizeof(double), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
+    return OAPB_ERR_CUDA;
   return cudaEventRecord(a->ev_chk, cs) == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
 
@@ -1000,6 +1009,8 @@ int check_collect(oapb_arnoldi* a, int b, int kk, cplx* th, double* norms) {
   memcpy(&bs, hp + pin_st_off(a), sizeof(DevState));
   const int tcerr = *(const int*)(hp + pin_err_off(a));
   if (*(const int*)(hp + pin_nt_off(a))) a->stats.eig_fast++;
+  const double e2 = *(const double*)(hp + pin_e2_off(a));
+  if (a->bf16_err < 0 && e2 >= 0) a->bf16_err = sqrt(e2);
   return ((bs.status & 2) || tcerr) ? OAPB_ERR_TIMEOUT : OAPB_OK;
 }
 
@@ -1021,11 +1032,11 @@ constexpr int kMixedMinN = 8192;
 // iteration: the powers taken while the block is still far from the wanted
 // subspace (before the first check, then while the residual extrapolated
 // from the last check stays above kBf16Until), never the pass right before
-// a check, so that their rounding (about 2^-8 of the block, kBf16Err) is
-// damped by FP32-class powers before any residual is measured.  In the
-// refinement's fixed point: the leading sweeps, as many as leave the last
-// sweeps on the FP32-class operator to contract a 2^-8 error to the
-// correction's goal.
+// a check, so that their rounding (about 2^-8 of the block) is damped by
+// FP32-class powers before any residual is measured.  In the refinement's
+// fixed point: the leading sweeps, as many as leave the last sweeps on the
+// FP32-class operator to contract the BF16 error (bf16_sweep_error, at most
+// kBf16Err) to the correction's goal.
 constexpr double kBf16Until = 0.02;
 constexpr double kBf16Err = 4e-3;
 // Goal of the FP32-class phase, the hand-over to the refinement: one outer
@@ -1223,6 +1234,25 @@ __global__ void k_block_add(const double* __restrict__ xr, const double* __restr
   }
 }
 
+// Relative error a BF16 sweep of the refinement leaves in the correction:
+// ||A - hi||_2 / min |theta|, with ||A - hi||_2 estimated from the rounding
+// energy the split summed as 2 ||A - hi||_F / sqrt(n) (rounding errors act
+// like independent random entries, whose matrix has that norm), clamped to
+// [kBf16Err / 16, kBf16Err].
+static double bf16_sweep_error(oapb_arnoldi* a, const std::vector<cplx>& th) {
+  if (a->bf16_err < 0 && a->bf16err2) {
+    double e2 = -1;
+    if (cudaMemcpyAsync(&e2, a->bf16err2, sizeof(double), cudaMemcpyDeviceToHost, a->stream) == cudaSuccess &&
+        cudaStreamSynchronize(a->stream) == cudaSuccess && e2 >= 0)
+      a->bf16_err = sqrt(e2);
+  }
+  double tmin = 1e300;
+  for (const cplx& t : th) tmin = fmin(tmin, cabs_(t));
+  if (!(a->bf16_err >= 0) || !(tmin > 0) || tmin >= 1e300) return kBf16Err;
+  const double e = 2.0 * a->bf16_err / sqrt((double)a->n) / tmin;
+  return e < kBf16Err / 16 ? kBf16Err / 16 : (e > kBf16Err ? kBf16Err : e);
+}
+
 // FP64-anchored refinement of the wanted invariant subspace (complex
 // operator, largest-magnitude wanted set, p = k vectors from a->Xre).
 // Outer step: W = A X on the FP64 operator, T = X^H W, R = W - X T.  From
@@ -1295,7 +1325,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     if (J < 2) J = 2;
     if (J > 30) J = 30;
     // leading sweeps on the BF16 planes: the last Jf contract their error
-    const int Jf = (int)ceil(log(0.03 * tol / mx / kBf16Err) / log(rho_eff));
+    const int Jf = (int)ceil(log(0.03 * tol / mx / bf16_sweep_error(a, th)) / log(rho_eff));
     const int Jb = J - Jf > 0 ? J - Jf : 0;
     a->stats.kernel_launches += 2;
     k_small_inv<<<1, 32, 0, a->stream>>>(a->G, p, a->Tinv, a->bstatus);
@@ -1553,7 +1583,8 @@ void free_all(oapb_arnoldi* a) {
   for (void* p : ps)
     if (p) cudaFree(p);
   void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
-                a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv, a->ntflag};
+                a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv, a->ntflag,
+                a->bf16err2};
   for (void* p : bs)
     if (p) cudaFree(p);
   for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
@@ -1739,10 +1770,16 @@ static int build_tc_planes(oapb_arnoldi* a, long row0, long rows) {
     if (dalloc(&a->tcerr, sizeof(int))) return OAPB_ERR_NOMEM;
     if (cudaMemsetAsync(a->tcerr, 0, sizeof(int), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   }
+  if (!a->bf16err2 && dalloc(&a->bf16err2, sizeof(double))) return OAPB_ERR_NOMEM;
+  if (row0 == 0) {  // a new operator: its BF16 rounding energy from zero
+    if (cudaMemsetAsync(a->bf16err2, 0, sizeof(double), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
+    a->bf16_err = -1;
+  }
   a->stats.kernel_launches += np / 2;
-  if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream, row0, rows)) return OAPB_ERR_CUDA;
-  if (a->is_c &&
-      split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream, row0, rows))
+  if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream, row0, rows, a->bf16err2))
+    return OAPB_ERR_CUDA;
+  if (a->is_c && split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream, row0,
+                                     rows, a->bf16err2))
     return OAPB_ERR_CUDA;
   a->have_tc = true;
   return OAPB_OK;
