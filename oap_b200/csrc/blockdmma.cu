@@ -7,7 +7,7 @@
 //   complex: B1 = [X_re | X_im] (N = 2 b columns), B2 = [-X_im | X_re], so
 //            C = A_re B1 + A_im B2 = [W_re | W_im] in one accumulator;
 //   real:    C = A_re X (N = b).
-// Both products run as mma.sync.m16n8k4.f64 over n-tiles of 8 columns with
+// Both products run as mma.sync.m16n8k8.f64 over n-tiles of 8 columns with
 // FP64 accumulation (the same rounding class as the FP64 CUDA-core pass).
 // B2 is not stored: its fragment is read from the B1 row of the permuted
 // column, negated where the column is an X_im column.
@@ -44,10 +44,14 @@ __device__ __forceinline__ void dwait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-__device__ __forceinline__ void dmma(double (&c)[4], double a0, double a1, double b0) {
-  asm volatile("mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};"
-               : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
-               : "d"(a0), "d"(a1), "d"(b0));
+// C += A B over k = 8: the k = 4 fragments of two consecutive K chunks (a0,
+// a1 and b0 of chunk 0, a2, a3 and b1 of chunk 1), one instruction
+__device__ __forceinline__ void dmma8(double (&c)[4], double a0, double a1, double a2, double a3, double b0,
+                                      double b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a0), "d"(a1), "d"(a2), "d"(a3), "d"(b0), "d"(b1));
 }
 
 struct DmArgs {
@@ -168,27 +172,30 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
     const double* xs = base + (size_t)NP * kDmM * kDmK;
     const int ra = warp * 16 + gq;  // rows ra and ra + 8 share the swizzle
 #pragma unroll
-    for (int k4 = 0; k4 < kDmK / 4; ++k4) {
+    // the stage's 8 columns as one m16n8k8 per plane and n-tile
+    static_assert(kDmK == 8, "one k = 8 MMA per stage");
+    double ar[2][2], ai[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, b1[2][NT], b2[2][NT];
+#pragma unroll
+    for (int k4 = 0; k4 < 2; ++k4) {
       const int kk = k4 * 4 + tq;
       const int off = dm_aoff(ra, kk >> 1) + (kk & 1);
-      const double ar0 = base[off], ar1 = base[off + 8 * kDmK];
-      double ai0 = 0.0, ai1 = 0.0;
+      ar[k4][0] = base[off];
+      ar[k4][1] = base[off + 8 * kDmK];
       if (CPLX) {
-        ai0 = base[kDmM * kDmK + off];
-        ai1 = base[kDmM * kDmK + off + 8 * kDmK];
+        ai[k4][0] = base[kDmM * kDmK + off];
+        ai[k4][1] = base[kDmM * kDmK + off + 8 * kDmK];
       }
-      double b1[NT], b2[NT];
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        b1[j] = xs[(j * 8 + gq) * kDmXStride + kk];
-        if (CPLX) b2[j] = sg[j] * xs[r2[j] + kk];
+        b1[k4][j] = xs[(j * 8 + gq) * kDmXStride + kk];
+        if (CPLX) b2[k4][j] = sg[j] * xs[r2[j] + kk];
       }
+    }
 #pragma unroll
-      for (int j = 0; j < NT; ++j) dmma(acc[j], ar0, ar1, b1[j]);
-      if (CPLX) {
+    for (int j = 0; j < NT; ++j) dmma8(acc[j], ar[0][0], ar[0][1], ar[1][0], ar[1][1], b1[0][j], b1[1][j]);
+    if (CPLX) {
 #pragma unroll
-        for (int j = 0; j < NT; ++j) dmma(acc[j], ai0, ai1, b2[j]);
-      }
+      for (int j = 0; j < NT; ++j) dmma8(acc[j], ai[0][0], ai[0][1], ai[1][0], ai[1][1], b2[0][j], b2[1][j]);
     }
     if ((it + 1) % g.kchunks == 0 || it + 1 == it1) flush(it / g.kchunks);
   }
