@@ -1,24 +1,23 @@
 // FP64 block operator pass W = A X on the FP64 tensor cores.
 //
-// Each iteration stages a 128 x 8 tile of every operator plane and the
-// 8-wide slice of X in shared memory (cp.async, four stages; two CTAs per SM
-// up to 48 output columns).  Warp w owns
+// Each iteration stages a 128 x 16 tile of every operator plane and the
+// 16-wide slice of X in shared memory (cp.async, three stages; two CTAs per
+// SM up to 32 output columns).  Warp w owns
 // operator rows 16 w .. 16 w + 15 of the tile and all N output columns:
 //   complex: B1 = [X_re | X_im] (N = 2 b columns), B2 = [-X_im | X_re], so
 //            C = A_re B1 + A_im B2 = [W_re | W_im] in one accumulator;
 //   real:    C = A_re X (N = b).
-// Both products run as mma.sync.m16n8k8.f64 over n-tiles of 8 columns with
+// Both products run as mma.sync.m16n8k16.f64 over n-tiles of 8 columns with
 // FP64 accumulation (the same rounding class as the FP64 CUDA-core pass).
 // B2 is not stored: its fragment is read from the B1 row of the permuted
 // column, negated where the column is an X_im column.
 //
 // Shared layout per stage:
-//   A plane: 128 rows x 64 bytes, 16-byte chunk c of row r at chunk
-//            c ^ ((r >> 1) & 3) (a fragment read is two wavefronts, the
-//            minimum for 256 bytes);
-//   X:       NT x 8 rows (B1 columns) x 12 doubles (row stride 12: a B
-//            fragment read is two wavefronts); rows beyond N are zero and
-//            never written.
+//   A plane: 128 rows x 128 bytes, 16-byte chunk c of row r at chunk
+//            c ^ (r & 7) (a fragment read is two wavefronts, the minimum
+//            for 256 bytes);
+//   X:       NT x 8 rows (B1 columns) x 16 doubles, swizzled the same way;
+//            rows beyond N are zero and never written.
 #include "blockdmma.cuh"
 #include "common.cuh"
 #include "streamk.cuh"
@@ -26,10 +25,10 @@
 namespace oapb {
 
 constexpr int kDmM = 128;        // operator rows per tile
-constexpr int kDmK = 8;          // columns per iteration
-constexpr int kDmStages = 4;
+constexpr int kDmK = 16;         // columns per iteration (one 128-byte row segment)
+constexpr int kDmStages = 3;
 constexpr int kDmThreads = 256;  // 8 warps x 16 rows
-constexpr int kDmXStride = 12;   // doubles per staged X row
+constexpr int kDmXStride = kDmK; // doubles per staged X row (swizzled like the operator rows)
 
 __host__ __device__ inline size_t dmma_stage_doubles(int np, int nt) {
   return (size_t)np * kDmM * kDmK + (size_t)nt * 8 * kDmXStride;
@@ -42,6 +41,17 @@ __device__ __forceinline__ void dcommit() { asm volatile("cp.async.commit_group;
 template <int N>
 __device__ __forceinline__ void dwait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// C += A B over k = 16: the k = 4 fragments of four consecutive K chunks
+// (a[2c], a[2c + 1] and b[c] of chunk c), one instruction
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+      "{%12,%13,%14,%15}, {%0,%1,%2,%3};"
+      : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+        "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 // C += A B over k = 8: the k = 4 fragments of two consecutive K chunks (a0,
@@ -66,7 +76,7 @@ struct DmArgs {
 };
 
 // 16-byte chunk c (0..3) of operator row r inside a staged plane, in doubles
-__device__ __forceinline__ int dm_aoff(int r, int c) { return r * kDmK + ((c ^ ((r >> 1) & 3)) << 1); }
+__device__ __forceinline__ int dm_aoff(int r, int c) { return r * kDmK + ((c ^ (r & 7)) << 1); }
 
 template <bool CPLX, int NT>
 __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_dmma(DmArgs g) {
@@ -98,7 +108,7 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
 #pragma unroll
       for (int u = 0; u < kDmM * (kDmK / 2) / kDmThreads; ++u) {
         const int e = tid + u * kDmThreads;
-        const int r = e >> 2, ch = e & 3;
+        const int r = e / (kDmK / 2), ch = e % (kDmK / 2);
         const long row = tile * kDmM + r, col = k0 + 2 * ch;
         const bool ok = row < n && col < n;
         const double* src = ok ? pl + row * n + col : pl;
@@ -109,11 +119,11 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
     // X slice: N rows x 4 chunks
     const uint32_t xbase = sbase + (uint32_t)(NP * kDmM * kDmK * 8);
     for (int e = tid; e < N * (kDmK / 2); e += kDmThreads) {
-      const int r = e >> 2, ch = e & 3;
+      const int r = e / (kDmK / 2), ch = e % (kDmK / 2);
       const long col = k0 + 2 * ch;
       const double* pl = (CPLX && r >= b) ? g.xi + (long)(r - b) * n : g.xr + (long)r * n;
       const bool ok = col < n;
-      cp_async16_zfill(xbase + (uint32_t)((r * kDmXStride + 2 * ch) * 8), ok ? pl + col : pl, ok ? 16 : 0);
+      cp_async16_zfill(xbase + (uint32_t)(dm_aoff(r, ch) * 8), ok ? pl + col : pl, ok ? 16 : 0);
     }
   };
 
@@ -124,10 +134,10 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
   for (int j = 0; j < NT; ++j) {
     const int c = j * 8 + gq;
     if (CPLX && c < 2 * b) {
-      r2[j] = (c < b ? c + b : c - b) * kDmXStride;
+      r2[j] = c < b ? c + b : c - b;
       sg[j] = c < b ? -1.0 : 1.0;
     } else {
-      r2[j] = c * kDmXStride;
+      r2[j] = c;
       sg[j] = 1.0;
     }
   }
@@ -171,31 +181,30 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
     const double* base = dsm + (size_t)((it - it0) % kDmStages) * stage_d;
     const double* xs = base + (size_t)NP * kDmM * kDmK;
     const int ra = warp * 16 + gq;  // rows ra and ra + 8 share the swizzle
+    // the stage's 16 columns as one m16n8k16 per plane and n-tile: the
+    // k = 4 fragments of the four K chunks (A rows ra, ra + 8; B row kk)
+    static_assert(kDmK == 16, "one k = 16 MMA per stage");
 #pragma unroll
-    // the stage's 8 columns as one m16n8k8 per plane and n-tile
-    static_assert(kDmK == 8, "one k = 8 MMA per stage");
-    double ar[2][2], ai[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, b1[2][NT], b2[2][NT];
+    for (int p = 0; p < NP; ++p) {
+      double a[8];
 #pragma unroll
-    for (int k4 = 0; k4 < 2; ++k4) {
-      const int kk = k4 * 4 + tq;
-      const int off = dm_aoff(ra, kk >> 1) + (kk & 1);
-      ar[k4][0] = base[off];
-      ar[k4][1] = base[off + 8 * kDmK];
-      if (CPLX) {
-        ai[k4][0] = base[kDmM * kDmK + off];
-        ai[k4][1] = base[kDmM * kDmK + off + 8 * kDmK];
+      for (int c4 = 0; c4 < 4; ++c4) {
+        const int kk = c4 * 4 + tq;
+        const int off = p * kDmM * kDmK + dm_aoff(ra, kk >> 1) + (kk & 1);
+        a[2 * c4] = base[off];
+        a[2 * c4 + 1] = base[off + 8 * kDmK];
       }
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        b1[k4][j] = xs[(j * 8 + gq) * kDmXStride + kk];
-        if (CPLX) b2[k4][j] = sg[j] * xs[r2[j] + kk];
+        double bv[4];
+#pragma unroll
+        for (int c4 = 0; c4 < 4; ++c4) {
+          const int kk = c4 * 4 + tq;
+          bv[c4] = p == 0 ? xs[dm_aoff(j * 8 + gq, kk >> 1) + (kk & 1)]
+                          : sg[j] * xs[dm_aoff(r2[j], kk >> 1) + (kk & 1)];
+        }
+        dmma16(acc[j], a, bv);
       }
-    }
-#pragma unroll
-    for (int j = 0; j < NT; ++j) dmma8(acc[j], ar[0][0], ar[0][1], ar[1][0], ar[1][1], b1[0][j], b1[1][j]);
-    if (CPLX) {
-#pragma unroll
-      for (int j = 0; j < NT; ++j) dmma8(acc[j], ai[0][0], ai[0][1], ai[1][0], ai[1][1], b2[0][j], b2[1][j]);
     }
     if ((it + 1) % g.kchunks == 0 || it + 1 == it1) flush(it / g.kchunks);
   }
