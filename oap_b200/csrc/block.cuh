@@ -333,6 +333,59 @@ __device__ void warp_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Cho
   }
 }
 
+// The same with a whole block (nthr threads, tid = 0 .. nthr - 1, all
+// calling): per step k one thread takes the pivot, then every trailing entry
+// R[i][j] (k < i <= j) has a thread of its own; the inverse X = R^-1 goes up
+// the rows, X[i][j] for all j > i in parallel.  A barrier per phase.
+__device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, CholSmem& sm, int tid, int nthr) {
+  constexpr int LD = kCholLD;
+  cplx* R = sm.R;
+  cplx* X = sm.X;
+  double* rd = sm.rd;
+  for (int e = tid; e < b * b; e += nthr) {  // L2 loads: G may come from other blocks of the caller
+    const double* gp = reinterpret_cast<const double*>(G + e);
+    R[e % b + (e / b) * LD] = cplx{__ldcg(gp), __ldcg(gp + 1)};
+  }
+  __syncthreads();
+  for (int k = 0; k < b; ++k) {
+    if (tid == 0) {
+      const double piv = R[k + k * LD].re;
+      const double rkk = piv > 0 ? sqrt(piv) : 1e-300;
+      if (!(piv > 0)) atomicOr(status, 4);
+      rd[k] = 1.0 / rkk;
+      R[k + k * LD] = cplx{rkk, 0};
+    }
+    __syncthreads();
+    for (int j = k + 1 + tid; j < b; j += nthr) R[k + j * LD] = rd[k] * R[k + j * LD];
+    __syncthreads();
+    const int t = b - k - 1;
+    for (int e = tid; e < t * t; e += nthr) {
+      const int i = k + 1 + e / t, j = k + 1 + e % t;
+      if (i <= j) R[i + j * LD] = R[i + j * LD] - conj(R[k + i * LD]) * R[k + j * LD];
+    }
+    __syncthreads();
+  }
+  for (int j = tid; j < b; j += nthr) X[j + j * LD] = cplx{rd[j], 0};
+  __syncthreads();
+  for (int i = b - 2; i >= 0; --i) {
+    for (int j = i + 1 + tid; j < b; j += nthr) {
+      cplx a0 = {0, 0}, a1 = {0, 0};
+      int p = i + 1;
+      for (; p + 1 <= j; p += 2) {
+        a0 = a0 + R[i + p * LD] * X[p + j * LD];
+        a1 = a1 + R[i + (p + 1) * LD] * X[p + 1 + j * LD];
+      }
+      if (p <= j) a0 = a0 + R[i + p * LD] * X[p + j * LD];
+      X[i + j * LD] = (-rd[i]) * (a0 + a1);
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < b * b; e += nthr) {
+    const int r = e % b, c = e / b;
+    Rinv[e] = r <= c ? X[r + c * LD] : cplx{0, 0};
+  }
+}
+
 __global__ void __launch_bounds__(32) k_chol_inv(const cplx* G, int b, cplx* Rinv, int* status) {
   __shared__ CholSmem sm;
   warp_chol_inv(G, b, Rinv, status, sm, threadIdx.x);
@@ -452,10 +505,8 @@ __global__ void __launch_bounds__(1024) k_block_reduce(const cplx* __restrict__ 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  if (ty == 0) {
-    warp_chol_inv(G, b, Rinv, status, sm.chol, tx);
-    if (tx == 0) *done = 0;
-  }
+  block_chol_inv(G, b, Rinv, status, sm.chol, ty * 32 + tx, 1024);
+  if (tx == 0 && ty == 0) *done = 0;
 }
 
 // Out_j = Base_j - sum_i X_i C[i + j ldc]  (Base may be null: Out = -X C, or
