@@ -399,6 +399,7 @@ __global__ void __launch_bounds__(32) k_small_inv(const cplx* __restrict__ T, in
   constexpr int LD = kBmMaxB + 1;
   __shared__ cplx M[2 * kBmMaxB * LD];  // column c at M + c LD
   __shared__ cplx fk[kBmMaxB];
+  pdl_wait();
   const int lane = threadIdx.x;
   if (p < 1 || p > kBmMaxB) return;
   for (int e = lane; e < p * p; e += 32) M[(e % p) + (e / p) * LD] = T[e];

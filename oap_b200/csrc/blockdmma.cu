@@ -95,6 +95,8 @@ __global__ void __launch_bounds__(kDmThreads, (NT <= 6 ? 2 : 1)) k_block_matvec_
     double* xs = dsm + s * stage_d + (size_t)NP * kDmM * kDmK;
     for (int e = tid; e < (NT * 8 - N) * kDmXStride; e += kDmThreads) xs[N * kDmXStride + e] = 0.0;
   }
+  // dependent launch: the operand blocks are the previous kernel's output
+  asm volatile("griddepcontrol.wait;" ::: "memory");
 
   auto load = [&](long it, int stage) {
     const long tile = it / g.kchunks;
@@ -257,7 +259,7 @@ static int dmma_launch(const DmArgs& g0, int n, double* wr, double* wi, cudaStre
   g.kchunks = p.kchunks;
   g.total = p.total;
   g.slots = p.slots;
-  kern<<<p.grid, kDmThreads, smem, s>>>(g);
+  launch_dependent(kern, dim3(p.grid), dim3(kDmThreads), smem, s, g);
   const SkGrid sg{p.tiles, p.kchunks, p.total, p.grid, p.slots};
   launch_sk_reduce<CPLX>(g.ws, sg, n, g.b, wr, wi, s);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;

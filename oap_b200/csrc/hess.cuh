@@ -480,6 +480,7 @@ static __device__ void hess_kernel_body(const HessArgs& a, unsigned char* dyn) {
 // FP64 working arithmetic (the restart loop and the refinement)
 static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
   extern __shared__ __align__(16) unsigned char hess_dyn[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   if (a.skip && *(volatile const int*)a.skip) return;
   hess_kernel_body<cplx>(a, hess_dyn);
 }
@@ -489,6 +490,7 @@ static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
 // dynamic shared memory hess_ws_cplx(m) * sizeof(cplxf)
 static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
   extern __shared__ __align__(16) unsigned char hess_dyn[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   hess_kernel_body<cplxf>(a, hess_dyn);
 }
 
@@ -527,6 +529,7 @@ inline int nt_warps(int m) {
 static __global__ void __launch_bounds__(kNtWarpsMax * 32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, int which,
                                                                 cplx* ritz, cplx* Y, int* order, int* delivered) {
   extern __shared__ __align__(16) unsigned char nt_dyn[];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   const int LD = nt_ld(m);
   cplx* T = reinterpret_cast<cplx*>(nt_dyn);                 // m x LD
   const int nw = blockDim.x >> 5;

@@ -649,7 +649,7 @@ int hess(oapb_arnoldi* a, int do_shift, double tol) {
   h.tol = tol;
   h.beta = 0;
   ++a->stats.kernel_launches;
-  k_hess<<<1, 32, a->hess_smem, a->stream>>>(h);
+  launch_dependent(k_hess, dim3(1), dim3(32), a->hess_smem, a->stream, h);
   return launch_check();
 }
 
@@ -929,13 +929,14 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
     if (cudaFuncSetAttribute(k_eig_near_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nsm) != cudaSuccess)
       return OAPB_ERR_CUDA;
     ++a->stats.kernel_launches;
-    k_eig_near_tri<<<1, nw * 32, nsm, a->stream>>>(G, b, a->cfg.sort, a->britz, a->bY, a->border, a->ntflag);
+    launch_dependent(k_eig_near_tri, dim3(1), dim3(nw * 32), nsm, a->stream, (const cplx*)G, b, (int)a->cfg.sort, a->britz,
+                     a->bY, a->border, a->ntflag);
     h.skip = a->ntflag;
   }
   if (fp32)
-    k_hess_f32<<<1, 32, sizeof(cplxf) * hess_ws_cplx(b), a->stream>>>(h);
+    launch_dependent(k_hess_f32, dim3(1), dim3(32), sizeof(cplxf) * hess_ws_cplx(b), a->stream, h);
   else
-    k_hess<<<1, 32, sizeof(cplx) * hess_ws_cplx(b), a->stream>>>(h);
+    launch_dependent(k_hess, dim3(1), dim3(32), sizeof(cplx) * hess_ws_cplx(b), a->stream, h);
   return launch_check();
 }
 
@@ -1071,7 +1072,9 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
   if (cudaMemsetAsync(a->bst, 0, sizeof(DevState), a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   int rc = OAPB_OK;
   if (fp32 && (rc = ensure_side_stream(a))) return rc;
-  if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei, 2))) return rc;
+  // the FP32 phase starts from a zero-mean uniform random block (condition
+  // number near 1): one CholeskyQR pass is orthonormal to rounding
+  if (!from_bx && (rc = cholqr2<C>(a, a->Xre, a->Xim, b, X, Xi, E, Ei, passes))) return rc;
   const int nv = (fp32 && b_next > kk) ? b_next : kk;
   std::vector<double> norms(kk), hist;
   std::vector<int> hist_it;
@@ -1227,6 +1230,7 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
 // Out = X + Y (b vectors)
 __global__ void k_block_add(const double* __restrict__ xr, const double* __restrict__ xi, const double* __restrict__ yr,
                             const double* __restrict__ yi, int b, int n, double* outr, double* outi) {
+  pdl_wait();
   const long len = (long)b * n;
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
     outr[e] = xr[e] + yr[e];
@@ -1328,7 +1332,7 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     const int Jf = (int)ceil(log(0.03 * tol / mx / bf16_sweep_error(a, th)) / log(rho_eff));
     const int Jb = J - Jf > 0 ? J - Jf : 0;
     a->stats.kernel_launches += 2;
-    k_small_inv<<<1, 32, 0, a->stream>>>(a->G, p, a->Tinv, a->bstatus);
+    launch_dependent(k_small_inv, dim3(1), dim3(32), 0, a->stream, (const cplx*)a->G, p, a->Tinv, a->bstatus);
     // D = R T^-1 (the first sweep from D = 0)
     launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, R, Ri, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, nullptr, nullptr);
     // Components of D inside span(X) do not move the subspace; between
@@ -1357,7 +1361,8 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     // conditioned like 1 + ||D|| and one CholeskyQR pass is orthonormal to
     // rounding (a diverging D is rejected by the next step's check)
     a->stats.kernel_launches++;
-    k_block_add<<<grid_n(len), 256, 0, a->stream>>>(X, Xi, D, Di, p, n, R, Ri);
+    launch_dependent(k_block_add, dim3(grid_n(len)), dim3(256), 0, a->stream, (const double*)X, (const double*)Xi,
+                     (const double*)D, (const double*)Di, p, n, R, Ri);
     if ((rc = cholqr2<C>(a, R, Ri, p, X, Xi, Tm, Tmi, 1))) return rc;
   }
   return kSlow;
