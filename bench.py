@@ -11,8 +11,9 @@ larger than L2, so no L2 flush is needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
 One JSON line on rank 0.  `value` is the chosen form (split-BF16 tcgen05
-block subspace iteration, then FP64-anchored refinement: FP64 DMMA residual
-passes and FP32-class Sylvester corrections) with A resident in HBM;
+block subspace iteration, then FP64-anchored refinement: FP64-class residual
+passes on int8 operator slices (integer tcgen05) and FP32-class Sylvester
+corrections) with A resident in HBM;
 `plain_fp64` is the plain FP64 GPU
 Arnoldi on the same problem; `e2e` runs the C-ABI entry that takes HOST
 buffers (pinned), with the 4 GiB host-to-device copy of A inside every step.
@@ -417,15 +418,24 @@ def run_ours(args, world, rank, local):
     # (complex)
     fp32_name = ("k_block_matvec_tc<complex> (split-BF16 tcgen05 block pass, %d vectors)" % bw if not args.no_tc
                  else "k_block_matvec<float,complex> (FP32 CUDA-core block pass, %d vectors)" % bw)
-    fp64_name = ("k_block_matvec_dmma<complex> (FP64 DMMA block pass)" if not args.no_tc
+    # the FP64-class pass of the chosen form: int8 operator slices on the
+    # integer tensor cores (6 slices of both planes, 12 n kp bytes a pass;
+    # 27 slice products of M 128, N 2 QB, K kp) or, where it does not apply,
+    # the FP64 DMMA pass (16 n^2 bytes)
+    i8 = (not args.no_tc) and stt.get("block_i8", 0) > 0
+    kp = (n + 127) // 128 * 128
+    qb = (bw + 7) // 8 * 8
+    fp64_name = ("k_block_matvec_i8<complex> (FP64-class int8-slice tcgen05 block pass)" if i8
+                 else "k_block_matvec_dmma<complex> (FP64 DMMA block pass)" if not args.no_tc
                  else "k_block_matvec<double,complex> (FP64 CUDA-core block pass)")
+    fp64_bytes = (12.0 * n * kp if i8 else 16.0 * n * n) + 32.0 * bw * n
     kernels = {
         "k_matvec<float,complex> (FP32 complex matvec)":
             (prof["matvec_seconds"], prof["matvec_timed"], 8.0 * n * n + 16.0 * n, 8.0 * n * n),
         fp32_name:
             (prof["block_fp32_seconds"], prof["block_fp32_timed"], 8.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
         fp64_name:
-            (prof["block_seconds"], prof["block_timed"], 16.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
+            (prof["block_seconds"], prof["block_timed"], fp64_bytes, 8.0 * bw * n * n),
     }
     if not args.no_tc:
         kernels["k_block_matvec_tc<complex, BF16> (BF16 hi-plane tcgen05 block pass)"] = (
@@ -449,10 +459,20 @@ def run_ours(args, world, rank, local):
                                 "tflops": (v[3] / (v[0] / v[1]) / 1e12) if v[1] else None,
                                 "traffic": (traffic or {}).get(k.split(" (")[0], {}).get("bytes_per_launch")}
                             for k, v in kernels.items()},
-            # the FP64 pass is bound by the FP64 tensor pipe, not by HBM: its
-            # fraction of the DMMA throughput measured on this pool with a
-            # register-only mma.sync.m16n8k4.f64 loop
-            "fp64_pass": ({"bound": "fp64 fma" if args.no_tc else "fp64 tensor",
+            # the int8-slice pass is HBM-bound (its fraction of the measured
+            # copy bandwidth, and its integer tensor throughput: 2 x 2 planes x
+            # 27 products x 2 QB x n x kp ops); the FP64 DMMA pass is bound by
+            # the FP64 tensor pipe (its fraction of the DMMA throughput measured
+            # on this pool with a register-only mma.sync f64 loop)
+            "fp64_pass": ({"bound": "hbm", "kernel": fp64_name,
+                           "GBs": fp64_bytes / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e9,
+                           "peak": hbm, "frac": fp64_bytes / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e9 / hbm,
+                           "int8_tops": 2.0 * 2 * 27 * 2 * qb * n * kp /
+                           (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e12,
+                           "launch_ms": kernels[fp64_name][0] / kernels[fp64_name][1] * 1e3,
+                           "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"}
+                          if i8 and kernels[fp64_name][1] else
+                          {"bound": "fp64 fma" if args.no_tc else "fp64 tensor",
                            "tflops": kernels[fp64_name][3] / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e12,
                            "peak_tflops": FMA64_PEAK_TFLOPS if args.no_tc else DMMA_PEAK_TFLOPS,
                            "frac": kernels[fp64_name][3] / (kernels[fp64_name][0] / kernels[fp64_name][1]) / 1e12 /
@@ -467,15 +487,16 @@ def run_ours(args, world, rank, local):
         cpu = cpu_sample(ar_np, ai_np, args.cpu_seconds, n)
     out = {"metric": METRIC, "value": value, "unit": "eigensolves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs_max * 1e3 / args.steps,
-           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3(fp32-class)+f64",
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3(fp32-class)+int8-slice(fp64-class)+f64",
            "data": "synthetic (seeded)",
            "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
                       "tolerance": TOL,
                       "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, its leading powers "
-                                      "on the BF16 hi planes, then FP64-anchored refinement: FP64 DMMA residual + "
+                                      "on the BF16 hi planes, then FP64-anchored refinement: FP64-class residual on "
+                                      "int8 operator slices (integer tcgen05) + "
                                       "Sylvester corrections (leading sweeps BF16, the rest FP32-class)"),
                       "parallelism": "replicas" if world > 1 else "single GPU",
-                      "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo operator) exceed L2; no flush"},
+                      "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo + 3 GiB int8-slice operator) exceed L2; no flush"},
            "converged_steps": conv_all,
            "plain_fp64": {"value": pvalue, "ms_per_step": allmax(world, psecs) * 1e3 / psteps,
                           "steps": psteps, "restarts": pstt["restarts"], "matvecs": pstt["matvecs"]},

@@ -250,6 +250,8 @@ typedef struct oapb_arnoldi_stats {
   uint32_t eig_fast;         /* FP64 Rayleigh-Ritz eigensolves of the refinement
                                 delivered by inverse iteration on the nearly
                                 triangular projected matrix (the rest: Schur) */
+  uint32_t block_i8;         /* FP64-class block passes on the integer tensor
+                                cores (int8 slices of the mixed form's operator) */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */
@@ -344,10 +346,13 @@ OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_re
 
 /* W = A X for b <= 32 vectors (device FP64 planes, vector q at offset q n)
  * with the handle's dense operator: precision OAPB_PREC_FP64 reads the FP64
- * operator; OAPB_PREC_MIXED the FP32-class copy of the mixed form (tensor
- * cores when cfg.tensor_cores, else CUDA-core FP32); OAPB_PASS_BF16 its
- * BF16 hi planes.  The block pass of the solver, exposed for multiple
- * right-hand sides and for verification. */
+ * operator (on a mixed-form handle with cfg.tensor_cores and b <= 16
+ * complex / 32 real vectors: its int8 slices on the integer tensor cores,
+ * within 2^-42 of each row's maximum times |x|_1); OAPB_PREC_MIXED the
+ * FP32-class copy of the mixed form (tensor cores when cfg.tensor_cores,
+ * else CUDA-core FP32); OAPB_PASS_BF16 its BF16 hi planes.  The block pass
+ * of the solver, exposed for multiple right-hand sides and for
+ * verification. */
 OAPB_EXPORT int oapb_arnoldi_apply_block(oapb_arnoldi* handle, const double* x_re,
                                          const double* x_im, uint32_t b,
                                          double* w_re, double* w_im,

@@ -36,6 +36,7 @@
 
 #include "block.cuh"
 #include "blockdmma.cuh"
+#include "blocki8.cuh"
 #include "blocktc.cuh"
 #include "common.cuh"
 #include "gramop.cuh"
@@ -487,6 +488,13 @@ struct oapb_arnoldi {
   int kp = 0;
   int* tcerr = nullptr;
   bool have_tc = false;
+  // FP64-class block pass on the integer tensor cores: int8 operator slices
+  // (row scales), vector-slice scratch and its scales
+  int8_t* ai8 = nullptr;
+  double* ai8s = nullptr;
+  int8_t* xi8 = nullptr;
+  double* xi8s = nullptr;
+  bool have_i8 = false;
   // ||A - hi||_F^2 of the BF16 hi planes (device, summed by the split) and
   // its host copy as ||A - hi||_F (read once per operator; < 0: not read)
   double* bf16err2 = nullptr;
@@ -748,6 +756,7 @@ int alloc_blocks(oapb_arnoldi* a) {
   }
   if (!a->cb && !a->gX) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
     size_t need = btc_workspace(a->n, (a->n + 127) / 128 * 128);
+    need = std::max(need, i8_workspace(a->n, (a->n + 127) / 128 * 128));
     if (dmma_plan(a->n, &a->dplan)) {
       need = std::max(need, dmma_workspace(a->dplan));
       a->have_dmma = true;
@@ -826,6 +835,15 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     if (prof) prof_end(a, tm);
     if (rc) return rc;
     a->stats.block_matvecs++;
+    return launch_check();
+  }
+  if (!fp32 && a->have_i8 && a->mixed_ready && a->cfg.tensor_cores && b <= i8_max_vectors(C)) {
+    const I8Operator op{a->ai8, a->ai8s, a->n, a->kp, C};
+    int rc = launch_block_matvec_i8(op, xr, xi, b, wr, wi, a->xi8, a->xi8s, a->wdm, a->tcerr, a->stream);
+    if (prof) prof_end(a, tm);
+    if (rc) return rc;
+    a->stats.block_matvecs++;
+    a->stats.block_i8++;
     return launch_check();
   }
   if (!fp32 && a->have_dmma && a->cfg.tensor_cores) {
@@ -1558,6 +1576,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   a->stats.matvecs = 0;
   a->stats.block_matvecs = 0;
   a->stats.block_bf16 = 0;
+  a->stats.block_i8 = 0;
   a->stats.eig_fast = 0;
   a->stats.refine_iterations = 0;
   a->trace.clear();
@@ -1589,7 +1608,7 @@ void free_all(oapb_arnoldi* a) {
     if (p) cudaFree(p);
   void* bs[] = {a->abf, a->xbf, a->tcerr, a->Wp, a->wdm, a->bpart, a->bdone, a->gws, a->G, a->G2, a->Rinv, a->bY, a->bQ, a->bH, a->britz, a->best, a->bnorm, a->border,
                 a->bstatus, a->bst, a->bpart2, a->bdone2, a->Tinv, a->ntflag,
-                a->bf16err2};
+                a->bf16err2, a->ai8, a->ai8s, a->xi8, a->xi8s};
   for (void* p : bs)
     if (p) cudaFree(p);
   for (int i = 0; i < oapb_arnoldi::kBlocks; ++i) {
@@ -1781,6 +1800,28 @@ static int build_tc_planes(oapb_arnoldi* a, long row0, long rows) {
     a->bf16_err = -1;
   }
   a->stats.kernel_launches += np / 2;
+  // int8 slices of the FP64-class pass (optional: without the memory the
+  // FP64 pass stays on the FP64 tensor cores)
+  if (row0 == 0) {
+    a->have_i8 = false;
+    if (!a->ai8 && (dalloc(&a->ai8, i8_operator_bytes(a->n, a->kp, a->is_c)) ||
+                    dalloc(&a->ai8s, sizeof(double) * a->n) || dalloc(&a->xi8, i8_block_bytes(a->kp)) ||
+                    dalloc(&a->xi8s, sizeof(double) * kI8BlockScales))) {
+      for (void** p : {(void**)&a->ai8, (void**)&a->ai8s, (void**)&a->xi8, (void**)&a->xi8s})
+        if (*p) {
+          cudaFree(*p);
+          *p = nullptr;
+        }
+      cudaGetLastError();
+    }
+  }
+  if (a->ai8) {
+    ++a->stats.kernel_launches;
+    if (split_operator_i8(a->a64re, a->is_c ? a->a64im : nullptr, a->n, a->kp, a->ai8, a->ai8s, a->stream, row0,
+                          rows))
+      return OAPB_ERR_CUDA;
+    a->have_i8 = true;
+  }
   if (split_operator_bf16(a->a64re, a->n, a->kp, a->abf, a->abf + plane, a->stream, row0, rows, a->bf16err2))
     return OAPB_ERR_CUDA;
   if (a->is_c && split_operator_bf16(a->a64im, a->n, a->kp, a->abf + 2 * plane, a->abf + 3 * plane, a->stream, row0,

@@ -263,7 +263,9 @@ def test_block_pass_precisions(cplx, n, b):
     scale = (A.abs() @ X.abs().T).T
     # (the BF16 pass: operator rounded to BF16, unit roundoff 2^-8 = 3.9e-3, X split;
     # FP64 passes through a mixed-form handle and through an FP64 handle)
-    for prec, tc, tol, hp in ((B.PREC_FP64, True, 1e-13, B.PREC_MIXED), (B.PREC_FP64, True, 1e-13, B.PREC_FP64),
+    # (the FP64 pass of a mixed-form handle takes the int8-slice pass for b <= 16
+    # complex / 32 real vectors: 2^-43 of the row scale per element)
+    for prec, tc, tol, hp in ((B.PREC_FP64, True, 1e-12, B.PREC_MIXED), (B.PREC_FP64, True, 1e-13, B.PREC_FP64),
                               (B.PREC_FP64, False, 1e-13, B.PREC_MIXED), (B.PREC_MIXED, False, 2e-6, B.PREC_MIXED),
                               (B.PREC_MIXED, True, 1e-4, B.PREC_MIXED), (B.PASS_BF16, True, 4e-3, B.PREC_MIXED)):
         s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=hp, tensor_cores=tc)
@@ -273,6 +275,49 @@ def test_block_pass_precisions(cplx, n, b):
         err = ((W - ref).abs() / scale).max().item()
         assert err <= tol, (prec, tc, hp, err)
         s.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cplx", [True, False])
+@pytest.mark.parametrize("n,b", [(1000, 7), (4096, 16), (130, 3), (2, 1), (8192, 16), (999, 32), (4096, 24)])
+def test_i8_block_pass(cplx, n, b):
+    # the FP64-class pass on the integer tensor cores (6 int8 slices of each
+    # operator row below its power-of-two scale, 7 of each vector, slice
+    # products of order <= 8) against the FP64 torch product, on rows and
+    # columns of widely different magnitude and a planted diagonal: the
+    # error stays below 2^-40 of the row maximum times |x|_1 plus the
+    # truncated slice products, 2^-45 n of row maximum times vector maximum
+    if cplx and b > 16:
+        pytest.skip("complex operators take the int8 pass for b <= 16")
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7 * n + b)
+    rs = torch.logspace(-6, 6, n, dtype=torch.float64, device="cuda")[torch.randperm(n, generator=g, device="cuda")]
+    are = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    are += torch.diag(4.0 * (torch.arange(n, device="cuda") % 17 == 0).double())
+    are *= rs[:, None]
+    aim = (torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5 * rs[:, None]
+           if cplx else None)
+    cs = torch.logspace(-3, 3, b, dtype=torch.float64, device="cuda")
+    xr = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g) * cs[:, None]
+    xr[:, ::5] *= 1e-9  # entries far below their vector's maximum
+    xi = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g) * cs[:, None] if cplx else None
+    A = are if not cplx else torch.complex(are, aim)
+    X = xr if not cplx else torch.complex(xr, xi)
+    ref = (A @ X.T).T
+    rowmax = are.abs().amax(1) if not cplx else torch.maximum(are.abs().amax(1), aim.abs().amax(1))
+    xmax = xr.abs().amax(1) if not cplx else torch.maximum(xr.abs().amax(1), xi.abs().amax(1))
+    x1 = xr.abs().sum(1) + (xi.abs().sum(1) if cplx else 0)
+    bound = 2.0 ** -40 * rowmax[None, :] * x1[:, None] + 2.0 ** -45 * n * rowmax[None, :] * xmax[:, None]
+    s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=B.PREC_MIXED, tensor_cores=True)
+    s.set_operator(are, aim)
+    before = s.stats()["block_i8"]
+    for _ in range(2):  # the vector-slice scratch is reused
+        wr, wi = s.apply_block(xr, xi, precision=B.PREC_FP64)
+        W = wr if not cplx else torch.complex(wr, wi)
+        err = (W - ref).abs()
+        assert bool((err <= bound).all()), (err / bound).max().item()
+    assert s.stats()["block_i8"] == before + 2
+    s.close()
 
 
 @pytest.mark.gpu
