@@ -129,30 +129,55 @@ __global__ void __launch_bounds__(256) k_split_operator_i8(const double* __restr
   }
 }
 
-// One block per vector q (< QB): the vector scale of its re / im parts,
-// then the 7 slices into B rows j N + q (re) and j N + QB + q (im); blocks
-// q >= b write zero rows (the padding of B up to N rows).
-__global__ void __launch_bounds__(256) k_split_block_i8(const double* __restrict__ xr, const double* __restrict__ xi,
-                                                        int b, int QB, int N, int n, int kp, int8_t* __restrict__ xs,
-                                                        double* __restrict__ xscale) {
+constexpr int kI8MaxBlocks = 148;  // blocks of the vector maximum pass (partials per vector)
+constexpr int kI8SplitCols = 1024;  // columns of one block of the vector split
+
+// Partial maxima of |x| over both planes of the b vectors: block k covers a
+// contiguous column range and writes part[k * 32 + q].
+__global__ void __launch_bounds__(256) k_block_absmax_i8(const double* __restrict__ xr,
+                                                         const double* __restrict__ xi, int b, int n,
+                                                         double* __restrict__ part) {
   __shared__ double red[8];
-  tc::griddep_wait();  // launched as a dependent of whatever wrote X (or last read xs)
-  const int q = blockIdx.x;
-  const bool live = q < b;
-  const double* pr = live ? xr + (long)q * n : nullptr;
-  const double* pi = (live && xi) ? xi + (long)q * n : nullptr;
-  double m = 0.0;
-  if (live)
-    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+  tc::griddep_wait();  // launched as a dependent of whatever wrote X
+  const long per = ((long)n + gridDim.x - 1) / gridDim.x;
+  const long c0 = (long)blockIdx.x * per, c1 = min((long)n, c0 + per);
+  for (int q = 0; q < b; ++q) {
+    const double* pr = xr + (long)q * n;
+    const double* pi = xi ? xi + (long)q * n : nullptr;
+    double m = 0.0;
+    for (long c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
       m = fmax(m, fabs(pr[c]));
       if (pi) m = fmax(m, fabs(pi[c]));
     }
+    m = block_max(m, red);
+    if (threadIdx.x == 0) part[blockIdx.x * 32 + q] = m;
+  }
+}
+
+// Block (q, k): vector q's scale from the partial maxima (written by the
+// blocks k = 0), then the 7 slices of columns k 1024 .. k 1024 + 1023 into
+// B rows j N + q (re) and j N + QB + q (im); vectors q >= b give zero rows
+// (the padding of B up to N rows).
+__global__ void __launch_bounds__(256) k_split_block_i8(const double* __restrict__ xr, const double* __restrict__ xi,
+                                                        int b, int QB, int N, int n, int kp,
+                                                        const double* __restrict__ part, int nparts,
+                                                        int8_t* __restrict__ xs, double* __restrict__ xscale) {
+  __shared__ double red[8];
+  tc::griddep_wait();  // launched as a dependent of the maximum pass
+  const int q = blockIdx.x;
+  const bool live = q < b;
+  double m = 0.0;
+  if (live)
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) m = fmax(m, part[k * 32 + q]);
   m = block_max(m, red);
   const int e = scale_exponent(m);
-  if (threadIdx.x == 0 && live) xscale[q] = ldexp(1.0, e);
+  if (threadIdx.x == 0 && live && blockIdx.y == 0) xscale[q] = ldexp(1.0, e);
   const double inv = ldexp(1.0, -e);
+  const double* pr = live ? xr + (long)q * n : nullptr;
+  const double* pi = (live && xi) ? xi + (long)q * n : nullptr;
   const int nrow = xi ? 2 : 1;
-  for (int c4 = threadIdx.x; c4 < kp / 4; c4 += blockDim.x) {
+  const int c4end = min(kp / 4, (int)(blockIdx.y + 1) * (kI8SplitCols / 4));
+  for (int c4 = blockIdx.y * (kI8SplitCols / 4) + threadIdx.x; c4 < c4end; c4 += blockDim.x) {
     for (int h = 0; h < nrow; ++h) {
       const double* src = h == 0 ? pr : pi;
       const int row = h == 0 ? q : QB + q;
@@ -532,9 +557,16 @@ int launch_block_matvec_i8(const I8Operator& op, const double* xr, const double*
   if (b < 1 || b > i8_max_vectors(cplx) || op.kp % 128 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
   const int QB = (b + 7) / 8 * 8;
   const int N = cplx ? 2 * QB : (QB + 15) / 16 * 16;  // i8_rows<cplx, QB>()
-  // vector slices (rows beyond the vectors zeroed: the real case's N > QB)
-  if (launch_dependent(k_split_block_i8, dim3(QB), dim3(256), 0, s, xr, cplx ? xi : nullptr, b, QB, N, op.n, op.kp,
-                       xs, xscale) != cudaSuccess)
+  // vector maxima (partials), then the vector slices (rows beyond the
+  // vectors zeroed: the real case's N > QB)
+  const int nparts = op.n < kI8MaxBlocks ? op.n : kI8MaxBlocks;
+  double* part = xscale + kI8BlockScales;
+  if (launch_dependent(k_block_absmax_i8, dim3(nparts), dim3(256), 0, s, xr, cplx ? xi : nullptr, b, op.n, part) !=
+      cudaSuccess)
+    return OAPB_ERR_CUDA;
+  if (launch_dependent(k_split_block_i8, dim3(QB, (op.kp + kI8SplitCols - 1) / kI8SplitCols), dim3(256), 0, s, xr,
+                       cplx ? xi : nullptr, b, QB, N, op.n, op.kp, (const double*)part, nparts, xs,
+                       xscale) != cudaSuccess)
     return OAPB_ERR_CUDA;
   const int used = cplx ? 2 * QB : QB;
   if (used < N && launch_dependent(k_zero_rows_i8, dim3(kNumSMs), dim3(256), 0, s, used, N, N, op.kp, xs) !=

@@ -26,9 +26,11 @@ struct I8Operator {
 inline size_t i8_operator_bytes(int n, int kp, bool cplx) {
   return (size_t)(cplx ? 2 : 1) * kI8SlicesA * (size_t)n * kp;
 }
-// Bytes of the vector-slice scratch (b <= 32 vectors) and doubles of its scales.
+// Bytes of the vector-slice scratch (b <= 32 vectors) and doubles of its
+// scales (kI8BlockScales) followed by the partial maxima of the scale pass.
 inline size_t i8_block_bytes(int kp) { return (size_t)kI8SlicesX * 64 * kp; }
 constexpr int kI8BlockScales = 64;
+constexpr int kI8ScaleDoubles = kI8BlockScales + 148 * 32;
 
 // Slices of rows row0 .. row0 + rows - 1 (rows < 0: to the last row) of the
 // FP64 operator (aim NULL for a real operator).
@@ -43,7 +45,7 @@ size_t i8_workspace(int n, int kp);
 
 // W (planes wr / wi, vector q at offset q n) = A X for b <= i8_max_vectors
 // vectors (X vector-contiguous FP64).  xs: i8_block_bytes(kp) bytes, xscale:
-// kI8BlockScales doubles, ws: i8_workspace() doubles; *err receives
+// kI8ScaleDoubles doubles, ws: i8_workspace() doubles; *err receives
 // timeout bits.
 int launch_block_matvec_i8(const I8Operator& op, const double* xr, const double* xi, int b, double* wr, double* wi,
                            int8_t* xs, double* xscale, double* ws, int* err, cudaStream_t s);

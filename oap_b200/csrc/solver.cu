@@ -1806,7 +1806,7 @@ static int build_tc_planes(oapb_arnoldi* a, long row0, long rows) {
     a->have_i8 = false;
     if (!a->ai8 && (dalloc(&a->ai8, i8_operator_bytes(a->n, a->kp, a->is_c)) ||
                     dalloc(&a->ai8s, sizeof(double) * a->n) || dalloc(&a->xi8, i8_block_bytes(a->kp)) ||
-                    dalloc(&a->xi8s, sizeof(double) * kI8BlockScales))) {
+                    dalloc(&a->xi8s, sizeof(double) * kI8ScaleDoubles))) {
       for (void** p : {(void**)&a->ai8, (void**)&a->ai8s, (void**)&a->xi8, (void**)&a->xi8s})
         if (*p) {
           cudaFree(*p);
