@@ -346,9 +346,9 @@ OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_re
 
 /* W = A X for b <= 32 vectors (device FP64 planes, vector q at offset q n)
  * with the handle's dense operator: precision OAPB_PREC_FP64 reads the FP64
- * operator (on a mixed-form handle with cfg.tensor_cores and b <= 16
- * complex / 32 real vectors: its int8 slices on the integer tensor cores,
- * within 2^-42 of each row's maximum times |x|_1); OAPB_PREC_MIXED the
+ * operator (on a mixed-form handle with cfg.tensor_cores, cfg.tolerance
+ * >= 1e-12 and b <= 16 complex / 32 real vectors: its int8 slices on the
+ * integer tensor cores, within 2^-42 of each row's maximum times |x|_1); OAPB_PREC_MIXED the
  * FP32-class copy of the mixed form (tensor cores when cfg.tensor_cores,
  * else CUDA-core FP32); OAPB_PASS_BF16 its BF16 hi planes.  The block pass
  * of the solver, exposed for multiple right-hand sides and for

@@ -805,6 +805,9 @@ void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, con
 
 // W = A X (b vectors); FP32-class operator copy when fp32, else FP64.
 // bf16 (with fp32): on the tensor cores, the BF16 hi planes alone.
+// smallest residual goal the FP64-class int8-slice pass serves
+constexpr double kI8MinTolerance = 1e-12;
+
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
                 bool fp32 = false, bool bf16 = false) {
@@ -837,7 +840,10 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     a->stats.block_matvecs++;
     return launch_check();
   }
-  if (!fp32 && a->have_i8 && a->mixed_ready && a->cfg.tensor_cores && b <= i8_max_vectors(C)) {
+  // the int8-slice pass certifies residuals to about 2^-42 of the row scale:
+  // tighter goals keep the FP64 DMMA pass
+  if (!fp32 && a->have_i8 && a->mixed_ready && a->cfg.tensor_cores && b <= i8_max_vectors(C) &&
+      a->cfg.tolerance >= kI8MinTolerance) {
     const I8Operator op{a->ai8, a->ai8s, a->n, a->kp, C};
     int rc = launch_block_matvec_i8(op, xr, xi, b, wr, wi, a->xi8, a->xi8s, a->wdm, a->tcerr, a->stream);
     if (prof) prof_end(a, tm);

@@ -321,6 +321,29 @@ def test_i8_block_pass(cplx, n, b):
 
 
 @pytest.mark.gpu
+def test_i8_pass_gated_by_tolerance():
+    # residual goals below 1e-12 keep the exact FP64 (DMMA) pass on a
+    # mixed-form handle; 1e-12 and above take the int8-slice pass
+    n, b = 1024, 8
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    are = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    aim = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g) / n ** 0.5
+    xr = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g)
+    xi = torch.randn(b, n, dtype=torch.float64, device="cuda", generator=g)
+    ref = (torch.complex(are, aim) @ torch.complex(xr, xi).T).T
+    scale = (torch.complex(are, aim).abs() @ torch.complex(xr, xi).abs().T).T
+    for tol, i8 in ((1e-13, False), (1e-12, True), (1e-10, True)):
+        s = B.Arnoldi(n, 16, 4, is_complex=True, precision=B.PREC_MIXED, tensor_cores=True, tolerance=tol)
+        s.set_operator(are, aim)
+        wr, wi = s.apply_block(xr, xi, precision=B.PREC_FP64)
+        assert s.stats()["block_i8"] == (1 if i8 else 0), tol
+        err = ((torch.complex(wr, wi) - ref).abs() / scale).max().item()
+        assert err <= (1e-12 if i8 else 1e-13), (tol, err)
+        s.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("cplx", [True, False])
 def test_matvec_autotune_variants(cplx):
     # every launch variant of the single-vector pass (forced: autotune = 2 + v)
