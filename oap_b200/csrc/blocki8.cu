@@ -133,24 +133,26 @@ constexpr int kI8MaxBlocks = 148;  // blocks of the vector maximum pass (partial
 constexpr int kI8SplitCols = 1024;  // columns of one block of the vector split
 
 // Partial maxima of |x| over both planes of the b vectors: block k covers a
-// contiguous column range and writes part[k * 32 + q].
+// contiguous column range and writes part[k * 32 + q]; warp w takes the
+// vectors w, w + 8, ... (shuffle reductions, no block barrier).
 __global__ void __launch_bounds__(256) k_block_absmax_i8(const double* __restrict__ xr,
                                                          const double* __restrict__ xi, int b, int n,
                                                          double* __restrict__ part) {
-  __shared__ double red[8];
   tc::griddep_wait();  // launched as a dependent of whatever wrote X
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   const long per = ((long)n + gridDim.x - 1) / gridDim.x;
   const long c0 = (long)blockIdx.x * per, c1 = min((long)n, c0 + per);
-  for (int q = 0; q < b; ++q) {
+  for (int q = warp; q < b; q += nw) {
     const double* pr = xr + (long)q * n;
     const double* pi = xi ? xi + (long)q * n : nullptr;
     double m = 0.0;
-    for (long c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+    for (long c = c0 + lane; c < c1; c += 32) {
       m = fmax(m, fabs(pr[c]));
       if (pi) m = fmax(m, fabs(pi[c]));
     }
-    m = block_max(m, red);
-    if (threadIdx.x == 0) part[blockIdx.x * 32 + q] = m;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (lane == 0) part[blockIdx.x * 32 + q] = m;
   }
 }
 
