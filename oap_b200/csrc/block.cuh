@@ -561,19 +561,29 @@ __global__ void k_colnorm2(const double* __restrict__ Yre, const double* __restr
   __shared__ double red[kBmMaxB][8];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   pdl_wait();
-  for (int q = 0; q < b; ++q) {
-    double s = 0;
-    for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
-      double a = Yre[(long)q * n + r];
-      s += a * a;
-      if (CPLX) {
-        double c = Yim[(long)q * n + r];
-        s += c * c;
+  // every vector's loads of a row issued together (static register index),
+  // each vector summed over the rows in the same order as one at a time
+  double s[kBmMaxB];
+#pragma unroll
+  for (int q = 0; q < kBmMaxB; ++q) s[q] = 0;
+  for (long r = (long)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += (long)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int q = 0; q < kBmMaxB; ++q)
+      if (q < b) {
+        const double a = Yre[(long)q * n + r];
+        s[q] += a * a;
+        if (CPLX) {
+          const double c = Yim[(long)q * n + r];
+          s[q] += c * c;
+        }
       }
-    }
-    s = warp_sum(s);
-    if (lane == 0) red[q][warp] = s;
   }
+#pragma unroll
+  for (int q = 0; q < kBmMaxB; ++q)
+    if (q < b) {
+      const double t = warp_sum(s[q]);
+      if (lane == 0) red[q][warp] = t;
+    }
   __syncthreads();
   for (int q = threadIdx.x; q < b; q += blockDim.x) {
     double s = 0;
