@@ -228,21 +228,37 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
                                                    const double* __restrict__ Yim, int b2, int n, cplx* part) {
   __shared__ double xr[kBmMaxB][kDotChunk + 1], xi[kBmMaxB][kDotChunk + 1];
   __shared__ double yr[kBmMaxB][kDotChunk + 1], yi[kBmMaxB][kDotChunk + 1];
+  if (blockDim.x != 256) return;  // the staging below assumes 256 threads
   pdl_wait();
   const int cnt = b1 * b2;
   double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
   const long nchunks = (n + kDotChunk - 1) / kDotChunk;
+  // 256 threads: each stages kDotPer elements of every plane, loaded into
+  // registers before the barrier (they overlap the previous chunk's products)
+  constexpr int kDotPer = kBmMaxB * kDotChunk / 256;
   for (long ch = blockIdx.x; ch < nchunks; ch += gridDim.x) {
     const long r0 = ch * kDotChunk;
-    __syncthreads();
-    for (int e = threadIdx.x; e < kBmMaxB * kDotChunk; e += blockDim.x) {
+    double vxr[kDotPer], vxi[kDotPer], vyr[kDotPer], vyi[kDotPer];
+#pragma unroll
+    for (int u = 0; u < kDotPer; ++u) {
+      const int e = threadIdx.x + u * 256;
       const int q = e / kDotChunk, rr = e % kDotChunk;
       const long r = r0 + rr;
       const bool in = r < n;
-      xr[q][rr] = (in && q < b1) ? Xre[(long)q * n + r] : 0.0;
-      xi[q][rr] = (in && q < b1 && CPLX) ? Xim[(long)q * n + r] : 0.0;
-      yr[q][rr] = (in && q < b2) ? Yre[(long)q * n + r] : 0.0;
-      yi[q][rr] = (in && q < b2 && CPLX) ? Yim[(long)q * n + r] : 0.0;
+      vxr[u] = (in && q < b1) ? Xre[(long)q * n + r] : 0.0;
+      vxi[u] = (in && q < b1 && CPLX) ? Xim[(long)q * n + r] : 0.0;
+      vyr[u] = (in && q < b2) ? Yre[(long)q * n + r] : 0.0;
+      vyi[u] = (in && q < b2 && CPLX) ? Yim[(long)q * n + r] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kDotPer; ++u) {
+      const int e = threadIdx.x + u * 256;
+      const int q = e / kDotChunk, rr = e % kDotChunk;
+      xr[q][rr] = vxr[u];
+      xi[q][rr] = vxi[u];
+      yr[q][rr] = vyr[u];
+      yi[q][rr] = vyi[u];
     }
     __syncthreads();
 #pragma unroll
@@ -333,10 +349,15 @@ __device__ void warp_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Cho
   }
 }
 
-// The same with a whole block (nthr threads, tid = 0 .. nthr - 1, all
-// calling): per step k one thread takes the pivot, then every trailing entry
-// R[i][j] (k < i <= j) has a thread of its own; the inverse X = R^-1 goes up
-// the rows, X[i][j] for all j > i in parallel.  A barrier per phase.
+// barrier of the nthr threads (whole warps, from thread 0) that run
+// block_chol_inv: named barrier 1, so the rest of the block may have left
+__device__ __forceinline__ void chol_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
+
+// The same with nthr threads of a block (whole warps, tid = 0 .. nthr - 1,
+// all calling): per step k one thread takes the pivot, then every trailing
+// entry R[i][j] (k < i <= j) has a thread of its own; the inverse X = R^-1
+// goes up the rows, X[i][j] for all j > i in parallel.  A barrier (chol_bar)
+// per phase.
 __device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, CholSmem& sm, int tid, int nthr) {
   constexpr int LD = kCholLD;
   cplx* R = sm.R;
@@ -346,7 +367,7 @@ __device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Ch
     const double* gp = reinterpret_cast<const double*>(G + e);
     R[e % b + (e / b) * LD] = cplx{__ldcg(gp), __ldcg(gp + 1)};
   }
-  __syncthreads();
+  chol_bar(nthr);
   for (int k = 0; k < b; ++k) {
     if (tid == 0) {
       const double piv = R[k + k * LD].re;
@@ -355,18 +376,18 @@ __device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Ch
       rd[k] = 1.0 / rkk;
       R[k + k * LD] = cplx{rkk, 0};
     }
-    __syncthreads();
+    chol_bar(nthr);
     for (int j = k + 1 + tid; j < b; j += nthr) R[k + j * LD] = rd[k] * R[k + j * LD];
-    __syncthreads();
+    chol_bar(nthr);
     const int t = b - k - 1;
     for (int e = tid; e < t * t; e += nthr) {
       const int i = k + 1 + e / t, j = k + 1 + e % t;
       if (i <= j) R[i + j * LD] = R[i + j * LD] - conj(R[k + i * LD]) * R[k + j * LD];
     }
-    __syncthreads();
+    chol_bar(nthr);
   }
   for (int j = tid; j < b; j += nthr) X[j + j * LD] = cplx{rd[j], 0};
-  __syncthreads();
+  chol_bar(nthr);
   for (int i = b - 2; i >= 0; --i) {
     for (int j = i + 1 + tid; j < b; j += nthr) {
       cplx a0 = {0, 0}, a1 = {0, 0};
@@ -378,7 +399,7 @@ __device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Ch
       if (p <= j) a0 = a0 + R[i + p * LD] * X[p + j * LD];
       X[i + j * LD] = (-rd[i]) * (a0 + a1);
     }
-    __syncthreads();
+    chol_bar(nthr);
   }
   for (int e = tid; e < b * b; e += nthr) {
     const int r = e % b, c = e / b;
@@ -506,7 +527,11 @@ __global__ void __launch_bounds__(1024) k_block_reduce(const cplx* __restrict__ 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  block_chol_inv(G, b, Rinv, status, sm.chol, ty * 32 + tx, 1024);
+  // the factor and its inverse on 8 warps (a barrier per phase costs less
+  // with fewer warps; the trailing updates have at most 31 x 31 entries)
+  constexpr int kCholThreads = 256;
+  if (ty * 32 + tx >= kCholThreads) return;
+  block_chol_inv(G, b, Rinv, status, sm.chol, ty * 32 + tx, kCholThreads);
   if (tx == 0 && ty == 0) *done = 0;
 }
 
@@ -525,18 +550,35 @@ __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__
                                                       const double* __restrict__ Yim = nullptr) {
   __shared__ cplx cs[kBmMaxB * kBmMaxB];
   __shared__ double xs_r[kBmMaxB][kUpRows], xs_i[CPLX ? kBmMaxB : 1][kUpRows];
+  if (blockDim.x != 256) return;  // the staging below assumes 256 threads
   pdl_wait();
   for (int e = threadIdx.x; e < b1 * b2; e += blockDim.x) cs[e] = Cm[(e % b1) + (long)(e / b1) * ldc];
   const int rr = threadIdx.x % kUpRows, g = threadIdx.x / kUpRows;
   const long nblk = (n + kUpRows - 1) / kUpRows;
+  // 256 threads: each stages kUpPer rows x vectors, loaded into registers
+  // before the barrier
+  constexpr int kUpPer = kBmMaxB * kUpRows / 256;
   for (long blk = blockIdx.x; blk < nblk; blk += gridDim.x) {
     const long r0 = blk * kUpRows;
-    __syncthreads();
-    for (int e = threadIdx.x; e < b1 * kUpRows; e += blockDim.x) {
+    double vr[kUpPer], vi[kUpPer];
+#pragma unroll
+    for (int u = 0; u < kUpPer; ++u) {
+      const int e = threadIdx.x + u * 256;
       const int i = e / kUpRows, q = e % kUpRows;
       const long r = r0 + q;
-      xs_r[i][q] = r < n ? Xre[(long)i * n + r] + (Yre ? Yre[(long)i * n + r] : 0.0) : 0.0;
-      if (CPLX) xs_i[i][q] = r < n ? Xim[(long)i * n + r] + (Yim ? Yim[(long)i * n + r] : 0.0) : 0.0;
+      const bool in = i < b1 && r < n;
+      vr[u] = in ? Xre[(long)i * n + r] + (Yre ? Yre[(long)i * n + r] : 0.0) : 0.0;
+      vi[u] = (CPLX && in) ? Xim[(long)i * n + r] + (Yim ? Yim[(long)i * n + r] : 0.0) : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < kUpPer; ++u) {
+      const int e = threadIdx.x + u * 256;
+      const int i = e / kUpRows, q = e % kUpRows;
+      if (i < b1) {
+        xs_r[i][q] = vr[u];
+        if (CPLX) xs_i[i][q] = vi[u];
+      }
     }
     __syncthreads();
     const long r = r0 + rr;
