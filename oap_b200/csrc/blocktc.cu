@@ -16,7 +16,10 @@
 // A_lo terms: 4 n^2 bytes per pass (complex), products within 2^-8 of
 // |A| |X| instead of about 2^-16, for the passes whose rounding a later
 // FP32-class pass removes (the first powers of a subspace iteration, the
-// first sweeps of a contracting fixed point).
+// first sweeps of a contracting fixed point).  Its coarse form (XLO =
+// false) also drops X's lo part, for the first powers (a block still far
+// from the wanted subspace): one B tile per K chunk instead of two, half the
+// MMAs, and fewer bytes through the shared-memory fill.
 //
 // The kernel is persistent and stream-K scheduled (streamk.cuh): one CTA
 // per SM walks an equal share of the (tile, K chunk) iterations.  Warps are
@@ -245,7 +248,7 @@ __device__ __forceinline__ void btc_epilogue(const BtcArgs& g, uint32_t tmem, ui
   if (ok && cur >= 0) btc_store_partial<CPLX, QB>(g, cur - first_tile, row, s1, s2);
 }
 
-template <bool CPLX, bool LO>
+template <bool CPLX, bool LO, bool XLO>
 __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid_constant__ BtcArgs g) {
   extern __shared__ __align__(1024) uint8_t bsm_raw[];
   constexpr int kMaxStages = 4;
@@ -256,6 +259,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   constexpr int NR = LO ? 2 : 1;            // parts per plane (hi [, lo])
   constexpr int KH = LO ? 1 : 2;            // 64-column K chunks per stage
   constexpr int NA = NPL * NR * KH;         // operator tiles per stage, index (p * NR + r) * KH + h
+  constexpr int NB = XLO ? 2 : 1;           // B parts per K chunk (hi [, lo])
   constexpr int KSUB = kBtcSub / KH;        // stages per FP32 segment
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* sm = (uint8_t*)(((uintptr_t)bsm_raw + 1023) & ~(uintptr_t)1023);
@@ -291,7 +295,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
   if (warp == 0) {
     // ---------------------------------------------------------- producer --
     if (lane == 0) {
-      const uint32_t tx = NA * a_tile + 2 * KH * b_tile;
+      const uint32_t tx = NA * a_tile + NB * KH * b_tile;
       long it = it0;
       for (; it < it1; ++it) {
         const long i = it - it0;
@@ -310,7 +314,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
 #pragma unroll
         for (int h = 0; h < KH; ++h) {
           tma_load_2d(st + NA * a_tile + h * b_tile, &g.tm[4], x + h * kBtcK, 0, &full[s]);
-          tma_load_2d(st + NA * a_tile + (KH + h) * b_tile, &g.tm[5], x + h * kBtcK, 0, &full[s]);
+          if (XLO) tma_load_2d(st + NA * a_tile + (KH + h) * b_tile, &g.tm[5], x + h * kBtcK, 0, &full[s]);
         }
       }
       // no copy may still be landing in shared memory when the CTA exits:
@@ -339,7 +343,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
 #pragma unroll
         for (int h = 0; h < KH; ++h) {
           const uint64_t bh = tc::sdesc_k_sw128(st + NA * a_tile + h * b_tile);
-          const uint64_t bl = tc::sdesc_k_sw128(st + NA * a_tile + (KH + h) * b_tile);
+          const uint64_t bl = XLO ? tc::sdesc_k_sw128(st + NA * a_tile + (KH + h) * b_tile) : 0;
 #pragma unroll
           for (int kk = 0; kk < kBtcK / 16; ++kk) {
             const uint64_t off = (uint64_t)(kk * 32) >> 4;
@@ -349,7 +353,7 @@ __global__ void __launch_bounds__(kBtcThreads, 1) k_block_matvec_tc(const __grid
               const uint64_t ah = tc::sdesc_k_sw128(st + (p * NR * KH + h) * a_tile) + off;
               const uint32_t d = tmem + buf * 128 + p * 64;
               tc::mma_bf16(d, ah, bh + off, idesc, acc0);
-              tc::mma_bf16(d, ah, bl + off, idesc, 1u);
+              if (XLO) tc::mma_bf16(d, ah, bl + off, idesc, 1u);
               if (LO) {
                 const uint64_t al = tc::sdesc_k_sw128(st + ((p * NR + 1) * KH + h) * a_tile) + off;
                 tc::mma_bf16(d, al, bh + off, idesc, 1u);
@@ -420,11 +424,12 @@ static bool make_tmap(CUtensorMap* m, const __nv_bfloat16* base, int kp, int row
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-// one stage: lo -> 1 K chunk of hi + lo planes; else 2 K chunks of the hi planes
-static size_t btc_stage_bytes(int N, bool cplx, bool lo) {
+// one stage: lo -> 1 K chunk of hi + lo planes; else 2 K chunks of the hi
+// planes; the B operand's hi (and with xlo its lo) tile per K chunk
+static size_t btc_stage_bytes(int N, bool cplx, bool lo, bool xlo) {
   const int KH = lo ? 1 : 2;
   const int NA = (cplx ? 2 : 1) * (lo ? 2 : 1) * KH;
-  return ((size_t)(NA * kBtcM * 128 + 2 * KH * N * 128) + 1023) & ~(size_t)1023;
+  return ((size_t)(NA * kBtcM * 128 + (xlo ? 2 : 1) * KH * N * 128) + 1023) & ~(size_t)1023;
 }
 
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
@@ -448,7 +453,7 @@ size_t btc_workspace(int n, int kp) {
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only) {
+                           cudaStream_t s, bool bf16_only, bool x_hi_only) {
   const bool cplx = op.aih != nullptr;
   const int kh = bf16_only ? 2 : 1;
   if (b < 1 || b > 32 || op.kp % (kBtcK * kh) != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
@@ -470,14 +475,16 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   g.b = b;
   g.QB = QB;
   g.N = N;
-  const size_t stage = btc_stage_bytes(N, cplx, !bf16_only);
+  const bool xlo = !(bf16_only && x_hi_only);
+  const size_t stage = btc_stage_bytes(N, cplx, !bf16_only, xlo);
   g.stage_bytes = (uint32_t)stage;
   g.stages = (int)(kBtcSmemBudget / stage);
   if (g.stages > 4) g.stages = 4;
   if (g.stages < 2) return OAPB_ERR_ARG;
   const size_t smem = g.stages * stage + 1024;
-  auto kern = bf16_only ? (cplx ? k_block_matvec_tc<true, false> : k_block_matvec_tc<false, false>)
-                        : (cplx ? k_block_matvec_tc<true, true> : k_block_matvec_tc<false, true>);
+  auto kern = bf16_only ? (xlo ? (cplx ? k_block_matvec_tc<true, false, true> : k_block_matvec_tc<false, false, true>)
+                              : (cplx ? k_block_matvec_tc<true, false, false> : k_block_matvec_tc<false, false, false>))
+                        : (cplx ? k_block_matvec_tc<true, true, true> : k_block_matvec_tc<false, true, true>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return OAPB_ERR_CUDA;
   if (launch_dependent(kern, dim3(g.grid.grid), dim3(kBtcThreads), smem, s, g) != cudaSuccess) return OAPB_ERR_CUDA;

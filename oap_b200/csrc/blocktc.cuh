@@ -25,9 +25,10 @@ size_t btc_workspace(int n, int kp);
 // W (planes wr / wi, vector q at offset q n) = A X for b <= 32 vectors (X
 // vector-contiguous FP64).  xbh / xbl hold 64 x kp BF16 each (the split
 // block); ws: btc_workspace() doubles; *err receives timeout bits.
-// bf16_only: the operator's hi planes only (half the bytes, BF16 accuracy).
+// bf16_only: the operator's hi planes only (half the bytes, BF16 accuracy);
+// x_hi_only (with bf16_only): X rounded to BF16 as well (its lo part unused).
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only = false);
+                           cudaStream_t s, bool bf16_only = false, bool x_hi_only = false);
 
 }  // namespace oapb

@@ -810,7 +810,7 @@ constexpr double kI8MinTolerance = 1e-12;
 
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
-                bool fp32 = false, bool bf16 = false) {
+                bool fp32 = false, bool bf16 = false, bool coarse = false) {
   if (a->cb || a->gX) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
@@ -833,7 +833,7 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
                    C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
     int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
-                                    a->tcerr, a->stream, bf16);
+                                    a->tcerr, a->stream, bf16, bf16 && coarse);
     if (bf16) a->stats.block_bf16++;
     if (prof) prof_end(a, tm);
     if (rc) return rc;
@@ -1131,7 +1131,9 @@ int subspace(oapb_arnoldi* a, int b, bool fp32, double tol, unsigned max_it, dou
       }
       bf16 = est >= kBf16Until;
     }
-    if (!pre && (rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32, bf16))) return rc;
+    // (the BF16 powers of a block still far from the subspace round X to
+    // BF16 too: its 2^-8 is as far below that distance as the operator's)
+    if (!pre && (rc = block_apply<C>(a, X, Xi, b, W, Wi, fp32, bf16, bf16))) return rc;
     pre = false;
     const bool check = fp32 ? (it >= next_check || it + 1 == max_it)
                             : ((int)it >= skip || it + 1 == max_it);
