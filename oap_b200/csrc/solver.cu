@@ -1373,7 +1373,10 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     int every = spread > 1.0 + 1e-12 ? (int)floor(log(4.0) / log(spread)) : J;
     if (every < 1) every = 1;
     for (int j = 0; j < J; ++j) {
-      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true, j < Jb))) return rc;
+      // BF16 sweeps before the last one also round D to BF16 (coarse): an
+      // error a sweep leaves is damped by every later sweep, so only the last
+      // BF16 sweep's, contracted by the Jf that follow, reaches the result
+      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true, j < Jb, j + 1 < Jb))) return rc;
       if ((j + 1) % every == 0 || j + 1 == J) {
         block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
         a->stats.kernel_launches++;
