@@ -18,8 +18,10 @@
 // FP32-class pass removes (the first powers of a subspace iteration, the
 // first sweeps of a contracting fixed point).  Its coarse form (XLO =
 // false) also drops X's lo part, for the first powers (a block still far
-// from the wanted subspace): one B tile per K chunk instead of two, half the
-// MMAs, and fewer bytes through the shared-memory fill.
+// from the wanted subspace) and the fixed point's sweeps before its last
+// BF16 one (their errors are damped by the sweeps that follow): one B tile
+// per K chunk instead of two, half the MMAs, and fewer bytes through the
+// shared-memory fill.
 //
 // The kernel is persistent and stream-K scheduled (streamk.cuh): one CTA
 // per SM walks an equal share of the (tile, K chunk) iterations.  Warps are
