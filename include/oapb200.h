@@ -343,6 +343,10 @@ OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_re
  * (products within about 2^-8 |A| |X|; FP32 CUDA-core pass when
  * cfg.tensor_cores = 0). */
 #define OAPB_PASS_BF16 2
+/* Pass precision of oapb_arnoldi_apply_block only: the BF16 hi planes with X
+ * rounded to BF16 as well (the coarse pass of the mixed form's leading
+ * powers and early sweeps; products within about 2^-7 |A| |X|). */
+#define OAPB_PASS_BF16_COARSE 3
 
 /* W = A X for b <= 32 vectors (device FP64 planes, vector q at offset q n)
  * with the handle's dense operator: precision OAPB_PREC_FP64 reads the FP64
@@ -350,7 +354,8 @@ OAPB_EXPORT int oapb_arnoldi_get_trace(const oapb_arnoldi* handle, oapb_trace_re
  * >= 1e-12 and b <= 16 complex / 32 real vectors: its int8 slices on the
  * integer tensor cores, within 2^-42 of each row's maximum times |x|_1); OAPB_PREC_MIXED the
  * FP32-class copy of the mixed form (tensor cores when cfg.tensor_cores,
- * else CUDA-core FP32); OAPB_PASS_BF16 its BF16 hi planes.  The block pass
+ * else CUDA-core FP32); OAPB_PASS_BF16 its BF16 hi planes;
+ * OAPB_PASS_BF16_COARSE those with X rounded to BF16 too.  The block pass
  * of the solver, exposed for multiple right-hand sides and for
  * verification. */
 OAPB_EXPORT int oapb_arnoldi_apply_block(oapb_arnoldi* handle, const double* x_re,

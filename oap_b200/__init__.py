@@ -19,6 +19,7 @@ F64, F32 = 0, 1
 SORT = {"LM": 0, "LR": 1, "LI": 2, "SM": 3, "SR": 4, "SI": 5}
 PREC_FP64, PREC_MIXED = 0, 1
 PASS_BF16 = 2  # apply_block only: the BF16 hi planes of the operator copy
+PASS_BF16_COARSE = 3  # apply_block only: the BF16 hi planes, X rounded to BF16 too
 INIT_RANDOM, INIT_FIRST_VALUE_IS_ONE, INIT_USER = 0, 1, 2
 TYPE_EIGENVECTOR, TYPE_WV = 0, 1
 

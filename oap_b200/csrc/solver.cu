@@ -2193,14 +2193,17 @@ int oapb_arnoldi_apply_block(oapb_arnoldi* a, const double* xre, const double* x
                              double* wim, int32_t precision) {
   if (!a || !xre || !wre || b == 0 || b > (uint32_t)kBmMaxB || a->cb || !a->a64re) return OAPB_ERR_ARG;
   if (a->is_c && (!xim || !wim)) return OAPB_ERR_ARG;
-  if (precision != OAPB_PREC_FP64 && precision != OAPB_PREC_MIXED && precision != OAPB_PASS_BF16)
+  if (precision != OAPB_PREC_FP64 && precision != OAPB_PREC_MIXED && precision != OAPB_PASS_BF16 &&
+      precision != OAPB_PASS_BF16_COARSE)
     return OAPB_ERR_ARG;
-  const bool fp32 = precision != OAPB_PREC_FP64, bf16 = precision == OAPB_PASS_BF16;
+  const bool fp32 = precision != OAPB_PREC_FP64;
+  const bool coarse = precision == OAPB_PASS_BF16_COARSE;
+  const bool bf16 = precision == OAPB_PASS_BF16 || coarse;
   if (fp32 && !a->mixed_ready) return OAPB_ERR_ARG;
   int rc = alloc_blocks(a);
   if (rc) return rc;
-  rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32, bf16)
-               : block_apply<false>(a, xre, nullptr, (int)b, wre, nullptr, fp32, bf16);
+  rc = a->is_c ? block_apply<true>(a, xre, xim, (int)b, wre, wim, fp32, bf16, coarse)
+               : block_apply<false>(a, xre, nullptr, (int)b, wre, nullptr, fp32, bf16, coarse);
   if (rc) return rc;
   int tcerr = 0;
   if (a->tcerr && cudaMemcpyAsync(&tcerr, a->tcerr, sizeof(int), cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)

@@ -262,12 +262,14 @@ def test_block_pass_precisions(cplx, n, b):
     ref = (A @ X.T).T
     scale = (A.abs() @ X.abs().T).T
     # (the BF16 pass: operator rounded to BF16, unit roundoff 2^-8 = 3.9e-3, X split;
+    # its coarse form rounds X to BF16 too: each product within 2^-7 = 7.8e-3;
     # FP64 passes through a mixed-form handle and through an FP64 handle)
     # (the FP64 pass of a mixed-form handle takes the int8-slice pass for b <= 16
     # complex / 32 real vectors: 2^-43 of the row scale per element)
     for prec, tc, tol, hp in ((B.PREC_FP64, True, 1e-12, B.PREC_MIXED), (B.PREC_FP64, True, 1e-13, B.PREC_FP64),
                               (B.PREC_FP64, False, 1e-13, B.PREC_MIXED), (B.PREC_MIXED, False, 2e-6, B.PREC_MIXED),
-                              (B.PREC_MIXED, True, 1e-4, B.PREC_MIXED), (B.PASS_BF16, True, 4e-3, B.PREC_MIXED)):
+                              (B.PREC_MIXED, True, 1e-4, B.PREC_MIXED), (B.PASS_BF16, True, 4e-3, B.PREC_MIXED),
+                              (B.PASS_BF16_COARSE, True, 8e-3, B.PREC_MIXED)):
         s = B.Arnoldi(n, min(16, n), min(4, n - 1), is_complex=cplx, precision=hp, tensor_cores=tc)
         s.set_operator(are, aim)
         wr, wi = s.apply_block(xr, xi, precision=prec)
