@@ -64,6 +64,8 @@ def parse():
                    help="single: the n=16384 complex solve (default line); batched: 2048 uneven "
                         "complex problems n in [32, 512], top-4, hdim=min(n, 24)")
     p.add_argument("--batch", type=int, default=2048)
+    p.add_argument("--no-others", action="store_true",
+                   help="default line without the bounded n=256, Gram-build and batched sub-results")
     return p.parse_args()
 
 
@@ -78,6 +80,28 @@ def make_operator(n, seed, device):
     pos = torch.randperm(n, generator=g, device=device)[:NPLANT]
     are[pos, pos] += SHIFT
     return are, aim
+
+
+def fp64_residuals(are, aim, ev, xre, xim):
+    """||A x_q - l_q x_q|| / (|l_1| ||x_q||) for every pair, recomputed from
+    the FP64 operator planes with torch (cuBLAS DGEMM, outside the library):
+    are / aim (n, n) device FP64, xre / xim (n, k) device FP64 (column q =
+    eigenvector q), ev the k eigenvalues (l_1 = the largest |l|)."""
+    import torch
+    lr = torch.tensor([e.real for e in ev], dtype=torch.float64, device=are.device)
+    li = torch.tensor([e.imag for e in ev], dtype=torch.float64, device=are.device)
+    if aim is None:
+        wr, wi = are @ xre, are @ xim if xim is not None else None
+    else:
+        wr = are @ xre - aim @ xim
+        wi = are @ xim + aim @ xre
+    xi = xim if xim is not None else torch.zeros_like(xre)
+    wi = wi if wi is not None else torch.zeros_like(xre)
+    rr = wr - (xre * lr - xi * li)
+    ri = wi - (xre * li + xi * lr)
+    num = torch.sqrt((rr * rr + ri * ri).sum(0))
+    den = torch.sqrt((xre * xre + xi * xi).sum(0)) * max(abs(e) for e in ev)
+    return (num / den).tolist()
 
 
 class Clocks:
@@ -231,58 +255,50 @@ def allsum(world, x):
 
 
 # --------------------------------------------------------------- CPU arm --
-def cpu_sample(are_h, aim_h, budget_s, n):
-    """Oracle FP64 IRAM cost on the host: the operator-application count of
-    one solve (oracle IRAM on the same ensemble at n = 2048) times the
-    measured time of the oracle's FP64 complex matvec on the full operator."""
-    import numpy as np
+def config_dict(world, n):
+    """The workload description both arms print (the same dict)."""
+    return {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV, "tolerance": TOL,
+            "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, its leading powers "
+                            "on the BF16 hi planes, then FP64-anchored refinement: FP64-class residual on "
+                            "int8 operator slices (integer tcgen05) + "
+                            "Sylvester corrections (leading sweeps BF16, the rest FP32-class)"),
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo + 3 GiB int8-slice operator) exceed L2; no flush"}
+
+
+def oracle_solve(are_h, aim_h):
+    """One whole FP64 eigensolve of the workload by the CPU oracle (textbook
+    IRAM, OpenMP matvec on all host cores): (seconds, converged, result)."""
     import oracle as O
-    rng = np.random.default_rng(5)
-    ns = 2048
-    s = (1.0 / (2.0 * ns)) ** 0.5
-    A_s = rng.normal(scale=s, size=(ns, ns)) + 1j * rng.normal(scale=s, size=(ns, ns))
-    pos = rng.choice(ns, NPLANT, replace=False)
-    A_s[pos, pos] += SHIFT
     t0 = time.perf_counter()
-    r = O.iram(A_s, K_WANTED, M_KRYLOV, which="LM", tol=TOL, seed=1)
-    t_small = time.perf_counter() - t0
-    applications = r["matvecs"] + K_WANTED  # + the residual check of the k pairs
-    x = np.random.default_rng(1).normal(size=n) + 0j
-    times = []
+    r = O.iram_planes(are_h, aim_h, K_WANTED, M_KRYLOV, which="LM", tol=TOL, seed=1)
+    dt = time.perf_counter() - t0
+    ok = r["rc"] == 0 and r["converged"] and float(r["residuals"].max()) <= TOL
+    return dt, ok, r
+
+
+def cpu_sample(are_h, aim_h, budget_s, n):
+    """The CPU implementation of the path timed on this host: whole oracle
+    FP64 IRAM solves of the full workload until `budget_s` is spent (at
+    least one); eigensolves/s = converged solves / their time."""
+    import oracle as O
+    times, conv, r = [], 0, None
     t_start = time.perf_counter()
-    while time.perf_counter() - t_start < budget_s or not times:
-        t0 = time.perf_counter()
-        _oracle_matvec(O, are_h, aim_h, x)
-        times.append(time.perf_counter() - t0)
-        if len(times) >= 200:
-            break
-    t_mv = statistics.median(times)
-    solve_s = applications * t_mv
-    return {"value": 1.0 / solve_s, "unit": "eigensolves/s", "cores": O.num_threads(), "kind": "port",
-            "sample": ("%d oracle FP64 complex matvecs (%.3f s each) on the n=%d operator, scaled by the %d "
-                       "operator applications of one oracle FP64 IRAM solve (counted on the same ensemble "
-                       "at n=2048, %d restarts, %.1f s)") % (len(times), t_mv, n, applications,
-                                                             r["restarts"], t_small),
-            "matvec_seconds": t_mv, "applications": applications}
-
-
-def _oracle_matvec(O, are_h, aim_h, x):
-    """y = A x with the oracle's OpenMP FP64 matvec on split host planes."""
-    import numpy as np
-    lib = O.lib()
-    n = are_h.shape[0]
-    xr = np.ascontiguousarray(x.real)
-    xi = np.ascontiguousarray(x.imag)
-    yr, yi = np.zeros(n), np.zeros(n)
-    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
-    lib.orc_matvec(n, P(are_h), P(aim_h), P(xr), P(xi), P(yr), P(yi))
-    return yr + 1j * yi
+    while not times or time.perf_counter() - t_start < budget_s:
+        dt, ok, r = oracle_solve(are_h, aim_h)
+        times.append(dt)
+        conv += int(ok)
+    total = sum(times)
+    return {"value": conv / total, "unit": "eigensolves/s", "cores": O.num_threads(), "kind": "port",
+            "sample": ("%d whole oracle FP64 IRAM solves of the n=%d workload (%d converged, %.2f s each, "
+                       "%d restarts, %d operator applications + %d residual checks each)")
+            % (len(times), n, conv, total / len(times), r["restarts"], r["matvecs"], K_WANTED),
+            "solve_seconds": total / len(times), "eigenvalues": r["eigenvalues"]}
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    import numpy as np
     import torch
     n = args.n
     dev = "cuda" if torch.cuda.is_available() else "cpu"
@@ -290,22 +306,31 @@ def run_reference(args, world, rank):
     are_h = are.cpu().numpy()
     aim_h = aim.cpu().numpy()
     del are, aim
-    vals = []
-    base = None
-    for _ in range(args.warmup + args.steps):
-        base = cpu_sample(are_h, aim_h, max(1.0, args.cpu_seconds / max(1, args.steps)), n)
-        vals.append(base["value"])
-    timed = vals[args.warmup:]
-    v = statistics.median(timed)
+    import oracle as O
+    # every step is one whole solve of the workload by the oracle's FP64 IRAM
+    # on all host cores; the timed region is the K timed steps
+    for _ in range(args.warmup):
+        oracle_solve(are_h, aim_h)
+    t0 = time.perf_counter()
+    conv, per = 0, []
+    r = None
+    for _ in range(args.steps):
+        dt, ok, r = oracle_solve(are_h, aim_h)
+        per.append(dt)
+        conv += int(ok)
+    secs = time.perf_counter() - t0
+    v = conv / secs
+    sample = ("one whole oracle FP64 IRAM solve of the n=%d workload per step (%.2f s median, %d restarts, "
+              "%d operator applications + %d residual checks), %d of %d converged to 1e-10") % (
+        n, statistics.median(per), r["restarts"], r["matvecs"], K_WANTED, conv, args.steps)
     out = {"metric": METRIC, "value": v, "unit": "eigensolves/s", "impl": "reference",
-           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v,
+           "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3 / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
            "data": "synthetic (seeded)",
-           "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
-                      "tolerance": TOL, "parallelism": "replicas"},
-           "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+           "config": config_dict(world, n),
+           "cpu_baseline": {"value": v, "unit": "eigensolves/s", "cores": O.num_threads(), "kind": "port",
+                            "sample": sample},
            "e2e": {"value": v, "unit": "eigensolves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    out["cpu_baseline"]["value"] = v
     print(json.dumps(out), flush=True)
 
 
@@ -356,11 +381,11 @@ def run_ours(args, world, rank, local):
         barrier(world)
         ms = e0.elapsed_time(e1)
         prof["profiled_solves"] = nprof
-        return ms / 1e3, conv, prof, s.stats()["kernel_launches"] - launches0, stt
+        return ms / 1e3, conv, prof, s.stats()["kernel_launches"] - launches0, stt, ev
 
     if args.quick:
         s_q = solver(B.PREC_MIXED if args.form == "mixed" else B.PREC_FP64)
-        secs, conv, prof, launches, stt = timed(s_q, args.steps, args.warmup)
+        secs, conv, prof, launches, stt, _ = timed(s_q, args.steps, args.warmup)
         if rank == 0:
             print(json.dumps({"quick": True, "form": args.form, "n": n, "steps": args.steps,
                               "seconds": secs, "converged": conv, "launches": launches, "profile": prof,
@@ -370,7 +395,7 @@ def run_ours(args, world, rank, local):
     # chosen form
     mixed = solver(B.PREC_MIXED)
     with Clocks(local) as clk:
-        secs, conv, prof, launches, stt = timed(mixed, args.steps, args.warmup)
+        secs, conv, prof, launches, stt, ev_mixed = timed(mixed, args.steps, args.warmup)
     clocks = clk.summary()
     secs_max = allmax(world, secs)
     conv_all = allsum(world, conv)
@@ -378,9 +403,35 @@ def run_ours(args, world, rank, local):
     # plain FP64 GPU Arnoldi
     plain = solver(B.PREC_FP64)
     psteps = args.plain_steps or max(2, args.steps // 2)
-    psecs, pconv, pprof, _, pstt = timed(plain, psteps, 1)
+    psecs, pconv, pprof, _, pstt, ev_plain = timed(plain, psteps, 1)
     pvalue = allsum(world, pconv) / allmax(world, psecs)
     plain.close()
+    # parity of the timed solves: one chosen-form solve's eigenpairs rechecked
+    # outside the library (FP64 planes x eigenvectors by torch's FP64 GEMM),
+    # and its eigenvalues against the plain FP64 GPU Arnoldi's, matched in the
+    # SortLargestValues order
+    import oracle as O
+    xr = torch.zeros(n, K_WANTED, dtype=torch.float64, device="cuda")
+    xi = torch.zeros(n, K_WANTED, dtype=torch.float64, device="cuda")
+    ev_chk, res_chk, st_chk = mixed.solve(vectors=(xr, xi), allow_not_converged=True)
+    fp64_res = fp64_residuals(are, aim, ev_chk, xr, xi)
+    del xr, xi
+    lm = lambda ev: sorted(ev, key=lambda e: -abs(e))
+    fp64_check = {"max_residual": max(fp64_res), "library_max_residual": max(res_chk), "status": st_chk,
+                  "method": "torch FP64 GEMM of the FP64 operator planes with the returned eigenvectors",
+                  "eig_err_vs_fp64": O.match_eigenvalues(lm(ev_mixed), lm(ev_plain)),
+                  "eig_err_note": "max |l_chosen - l_plain| / max|l| over the 16 wanted values, "
+                                  "plain FP64 GPU Arnoldi of the same run, SortLargestValues order"}
+    # per-operator preparation of the chosen form (BF16 hi / lo planes and
+    # int8 slices), outside `value`'s timed loop: a fresh handle's set_operator
+    prep = B.Arnoldi(n, M_KRYLOV, K_WANTED, is_complex=True, precision=B.PREC_MIXED, tolerance=TOL,
+                     seed=3 + rank)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    prep.set_operator(are, aim)
+    torch.cuda.synchronize()
+    prep_ms = (time.perf_counter() - t0) * 1e3
+    prep.close()
     # end to end through the host-buffer entry point (pinned host planes)
     # the pinned host planes on the GPU's own NUMA node (as a serving process
     # bound to its GPU's socket would have them)
@@ -485,18 +536,18 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and world == 1:
         cpu = cpu_sample(ar_np, ai_np, args.cpu_seconds, n)
+        fp64_check["eig_err_vs_oracle"] = O.match_eigenvalues(lm(ev_chk), lm(cpu["eigenvalues"]))
+    # the other configurations, bounded, at one GPU (their own workloads)
+    others = None
+    if world == 1 and not args.no_others:
+        del ar_np, ai_np, are_h, aim_h
+        others = {"c1_n256_real_symmetric": c1_result(), "c3_gram_build": c3_result(),
+                  "c4_batched": c4_result()}
     out = {"metric": METRIC, "value": value, "unit": "eigensolves/s", "n_gpus": world,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs_max * 1e3 / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16x3(fp32-class)+int8-slice(fp64-class)+f64",
            "data": "synthetic (seeded)",
-           "config": {"workload": WORKLOAD, "n": n, "wanted": K_WANTED, "hdim": M_KRYLOV,
-                      "tolerance": TOL,
-                      "chosen_form": ("split-BF16 tcgen05 (FP32-class) block subspace iteration, its leading powers "
-                                      "on the BF16 hi planes, then FP64-anchored refinement: FP64-class residual on "
-                                      "int8 operator slices (integer tcgen05) + "
-                                      "Sylvester corrections (leading sweeps BF16, the rest FP32-class)"),
-                      "parallelism": "replicas" if world > 1 else "single GPU",
-                      "l2": "inputs (4 GiB FP64 + 2 GiB BF16 hi/lo + 3 GiB int8-slice operator) exceed L2; no flush"},
+           "config": config_dict(world, n),
            "converged_steps": conv_all,
            "plain_fp64": {"value": pvalue, "ms_per_step": allmax(world, psecs) * 1e3 / psteps,
                           "steps": psteps, "restarts": pstt["restarts"], "matvecs": pstt["matvecs"]},
@@ -509,12 +560,160 @@ def run_ours(args, world, rank, local):
                    "h2d_bytes_per_step": 2 * 8 * n * n,
                    "d2h_bytes_per_step": 3 * 8 * K_WANTED + 2 * 8 * n * K_WANTED,
                    "steps": esteps},
+           "fp64_check": fp64_check,
+           "prep_ms": prep_ms,
+           "value_incl_prep": conv_all / (secs_max + prep_ms / 1e3 * args.steps),
+           "other_configs": others,
            "roofline": roof, "clocks": clocks,
            "gpu_launches": int(launches),
            "cpu_baseline": None if cpu is None else {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}}
     mixed.close()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def make_batch(count, seed):
+    """`count` complex problems, n ~ U{32..512} (numpy seed), entries N(0, 1/n)
+    split re / im FP64 plus 4 on 4 seeded diagonal positions, on the device."""
+    import numpy as np
+    import torch
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(32, 513, size=count)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(seed)
+    mats = []
+    for n in sizes:
+        n = int(n)
+        s = (1.0 / (2.0 * n)) ** 0.5
+        re = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g).mul_(s)
+        im = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g).mul_(s)
+        pos = torch.randperm(n, generator=g, device="cuda")[:4]
+        re[pos, pos] += SHIFT
+        mats.append((re, im))
+    return rng, sizes, mats
+
+
+def c1_result():
+    """The reference's CPU-sized case (n = 256 real symmetric, Q diag(l) Q^T
+    with Q from the QR of a seeded N(0,1) matrix, l geometric 1 .. 1e-3,
+    top-5 LM, m = 32, residual goal 1e-10): GPU solves/s (the chosen form's
+    handle; below n = 8192 it runs the plain FP64 restart loop) beside the
+    CPU oracle's whole solves, and the eigenvalue errors against the exact
+    values and the oracle."""
+    import numpy as np
+    import torch
+    import oap_b200 as B
+    import oracle as O
+    n, k, m = 256, 5, 32
+    rng = np.random.default_rng(0)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)))
+    lam = 10.0 ** (-3.0 * np.arange(n) / (n - 1))
+    A = (Q * lam) @ Q.T
+    s = B.Arnoldi(n, m, k, precision=B.PREC_MIXED, tolerance=TOL, seed=1)
+    s.set_operator(torch.from_numpy(A).cuda())
+    for _ in range(3):
+        s.solve()
+    steps, conv = 50, 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        ev, res, st = s.solve(allow_not_converged=True)
+        conv += int(st == B.OK and max(res) <= TOL)
+    e1.record()
+    torch.cuda.synchronize()
+    secs = e0.elapsed_time(e1) / 1e3
+    stt = s.stats()
+    s.close()
+    ev = np.array(sorted(ev, key=lambda e: -abs(e)))
+    t0, cnt, o = time.perf_counter(), 0, None
+    while cnt < 3 or time.perf_counter() - t0 < 1.0:
+        o = O.iram(A, k, m, which="LM", tol=TOL, seed=1)
+        cnt += 1
+    cpu_s = (time.perf_counter() - t0) / cnt
+    oev = np.array(sorted(o["eigenvalues"], key=lambda e: -abs(e)))
+    return {"workload": "n=256 real symmetric, l geometric 1..1e-3, top-5 LM, m=32, residual<=1e-10",
+            "gpu_solves_per_s": conv / secs, "gpu_ms_per_solve": secs * 1e3 / steps, "converged": conv,
+            "steps": steps, "restarts": stt["restarts"], "matvecs": stt["matvecs"],
+            "cpu_oracle_solves_per_s": 1.0 / cpu_s, "cpu_oracle_cores": O.num_threads(),
+            "eig_err_vs_exact": float(np.abs(ev.real - lam[:k]).max() / lam[0]),
+            "eig_err_vs_oracle": O.match_eigenvalues(ev, oev),
+            "max_residual": float(max(res))}
+
+
+def c3_result():
+    """Gram build of 4096 synthetic 256 x 256 images (A = X X^T, split-BF16
+    tcgen05, FP32 accumulation): milliseconds and algorithmic TFLOP/s
+    (2 N^2 P counted once) against the measured bf16 peak."""
+    import torch
+    import oap_b200 as B
+    count, side = 4096, 256
+    X = synthetic_images(count, side, 21, "cuda")
+    A, _ = B.gram_build(X)
+    torch.cuda.synchronize()
+    reps = 5
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        B.gram_build(X)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    flops = 2.0 * count * count * side * side
+    peak, kind = bf16_peak()
+    idx = torch.arange(0, count, 128, device="cuda")
+    Xd = X.double()
+    ref = Xd[idx] @ Xd.T
+    rel = ((A[idx].double() - ref).abs() / ref.abs().clamp_min(1e-300)).max().item()
+    del X, Xd, A
+    return {"workload": "A = X X^T, X 4096 x 65536 FP32 synthetic images (8 Gaussian blobs + U[0,16) noise)",
+            "build_ms": ms, "tflops_algorithmic": flops / ms / 1e9, "peak_bf16_tflops": peak,
+            "peak_source": kind, "frac": flops / ms / 1e9 / peak, "rel_error_vs_fp64_max": rel,
+            "note": "2 N^2 P flops counted once (the split runs three BF16 products)"}
+
+
+def c4_result():
+    """2048 uneven complex problems (n ~ U{32..512}, top-4 LM, hdim =
+    min(n, 24)) in one persistent launch: solves/s, converged count, and the
+    eigenvalue error against the plain FP64 Arnoldi on a sample of them."""
+    import numpy as np
+    import torch
+    import oap_b200 as B
+    import oracle as O
+    rng, sizes, mats = make_batch(2048, 11)
+    B.solve_batched(mats, 4, hdim=24, tolerance=TOL)
+    torch.cuda.synchronize()
+    reps, conv = 3, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        ev, res, st, stats, rc = B.solve_batched(mats, 4, hdim=24, tolerance=TOL)
+        conv += int((st == B.OK).sum())
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    err = 0.0
+    for i in rng.choice(len(mats), 8, replace=False):
+        re, im = mats[i]
+        n = re.shape[0]
+        p = B.Arnoldi(n, min(n, 24), 4, is_complex=True, tolerance=TOL, seed=3)
+        p.set_operator(re, im)
+        pev, _, _ = p.solve(allow_not_converged=True)
+        p.close()
+        err = max(err, O.match_eigenvalues(ev[i], pev))
+    del mats
+    return {"workload": "2048 complex problems n~U[32,512], top-4 LM, hdim=min(n,24), one persistent launch",
+            "solves_per_s": conv / reps / (ms / 1e3), "launch_ms": ms, "converged_per_launch": conv / reps,
+            "problems": len(sizes), "max_residual": float(res.max()),
+            "eig_err_vs_plain_fp64_sample8": err}
+
+
+def bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (MEASURED_PEAKS.json bf16_tflops)"
+    except (OSError, KeyError, ValueError):
+        return 1590.0, "fallback"
 
 
 def run_batched(args, world, rank, local):
@@ -526,19 +725,7 @@ def run_batched(args, world, rank, local):
     import torch
     import oap_b200 as B
     torch.cuda.set_device(local)
-    rng = np.random.default_rng(11 + rank)
-    sizes = rng.integers(32, 513, size=args.batch)
-    g = torch.Generator(device="cuda")
-    g.manual_seed(11 + rank)
-    mats = []
-    for n in sizes:
-        n = int(n)
-        s = (1.0 / (2.0 * n)) ** 0.5
-        re = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g).mul_(s)
-        im = torch.randn(n, n, dtype=torch.float64, device="cuda", generator=g).mul_(s)
-        pos = torch.randperm(n, generator=g, device="cuda")[:4]
-        re[pos, pos] += SHIFT
-        mats.append((re, im))
+    rng, sizes, mats = make_batch(args.batch, 11 + rank)
     torch.cuda.synchronize()
     for _ in range(args.warmup):
         B.solve_batched(mats, 4, hdim=24, tolerance=TOL)

@@ -46,7 +46,9 @@ typedef enum oapb_status {
   OAPB_ERR_BOUNDS = 5,       /* a device-side bounds check fired */
   OAPB_ERR_CALLBACK = 6,     /* the user matvec callback returned non-zero */
   OAPB_ERR_NOMEM = 7,        /* device allocation failed */
-  OAPB_ERR_BREAKDOWN = 8     /* the Krylov space became invariant before hdim */
+  OAPB_ERR_BREAKDOWN = 8,    /* the Krylov space became invariant before hdim */
+  OAPB_ERR_NONFINITE = 9     /* a NaN or infinity reached the Krylov vectors
+                                (operator or callback output) or a residual */
 } oapb_status;
 
 /* Element type of a plane. */
@@ -128,7 +130,9 @@ OAPB_EXPORT int oapb_qr_givens(const oapb_mat* Q, const oapb_mat* R, const oapb_
  * results as oapb_qr_givens; the workspace is a static 512 KiB device array
  * of the library, so n <= 128 (OAPB_ERR_ARG beyond).  The first call on a
  * device resolves the array's address and should precede any stream
- * capture; calls that overlap on the GPU share the array and race. */
+ * capture; the address stays cached, so the entry point must not be used
+ * on a device after cudaDeviceReset; calls that overlap on the GPU share
+ * the array and race. */
 OAPB_EXPORT int oapb_qr_givens_noalloc(const oapb_mat* Q, const oapb_mat* R,
                                        const oapb_mat* A, void* stream);
 
@@ -150,6 +154,17 @@ OAPB_EXPORT int oapb_is_upper_triangular(int* output, const oapb_mat* matrix,
 OAPB_EXPORT int oapb_calc_triangular_h(const oapb_mat* H, const oapb_mat* Q,
                            uint32_t max_iterations, uint32_t* iterations,
                            void* stream);
+
+/* Self-test of the bounded device-side wait used by every tensor-core kernel
+ * (no counterpart in the reference, whose host aborts on CUDA errors,
+ * oapCuda/KernelExecutor.h:34-41).  One CTA waits on a shared-memory
+ * mbarrier for at most limit_us microseconds (1 .. 1000000); with arrive = 0
+ * nothing arrives, the wait runs out, the kernel returns and the call
+ * returns OAPB_ERR_TIMEOUT with *timed_out = 1; with arrive = 1 the wait
+ * completes (OAPB_OK, *timed_out = 0).  The context stays usable either
+ * way.  Synchronises `stream`; allocates nothing. */
+OAPB_EXPORT int oapb_selftest_bounded_wait(uint32_t limit_us, int32_t arrive, int32_t* timed_out,
+                                           void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Solver: CuHArnoldi / CuHArnoldiCallback (ArnoldiPackage)                  */

@@ -14,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liboapb200.so")
 _LIB = None
 
-OK, ERR_ARG, ERR_CUDA, NOT_CONVERGED, ERR_TIMEOUT, ERR_BOUNDS, ERR_CALLBACK, ERR_NOMEM, ERR_BREAKDOWN = range(9)
+(OK, ERR_ARG, ERR_CUDA, NOT_CONVERGED, ERR_TIMEOUT, ERR_BOUNDS, ERR_CALLBACK, ERR_NOMEM, ERR_BREAKDOWN,
+ ERR_NONFINITE) = range(10)
 F64, F32 = 0, 1
 SORT = {"LM": 0, "LR": 1, "LI": 2, "SM": 3, "SR": 4, "SI": 5}
 PREC_FP64, PREC_MIXED = 0, 1
@@ -113,6 +114,7 @@ def lib():
             "oapb_qr_givens": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_qr_householder": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_qr_givens_noalloc": [P(Mat), P(Mat), P(Mat), vp],
+            "oapb_selftest_bounded_wait": [C.c_uint32, C.c_int32, P(C.c_int32), vp],
             "oapb_is_upper_triangular": [P(C.c_int), P(Mat), C.c_double, vp],
             "oapb_calc_triangular_h": [P(Mat), P(Mat), C.c_uint32, P(C.c_uint32), vp],
             "oapb_arnoldi_create": [P(vp), P(Config), vp],
@@ -352,6 +354,14 @@ class Arnoldi:
         check(lib().oapb_arnoldi_test_outcome(self.h, index, C.byref(out)),
               "oapb_arnoldi_test_outcome")
         return out.value
+
+
+def selftest_bounded_wait(limit_us, arrive=False, stream=None):
+    """Run the bounded device-side wait self-test (oapb_selftest_bounded_wait):
+    returns (status, timed_out).  arrive=False lets the wait run out."""
+    out = C.c_int32(-1)
+    st = lib().oapb_selftest_bounded_wait(int(limit_us), int(bool(arrive)), C.byref(out), _stream(stream))
+    return st, out.value
 
 
 def start_vector(n, seed, is_complex=False):

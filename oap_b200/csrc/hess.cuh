@@ -43,7 +43,7 @@ struct DevState {
   double hnorm2;
   int dgks;         // second Gram-Schmidt pass needed for the current column
   int converged;
-  int status;       // bit 0: breakdown (||f|| = 0), bit 1: Schur sweep limit
+  int status;       // bit 0: breakdown (||f|| = 0), bit 1: Schur sweep limit, bit 2: ||f|| not finite
   int dgks_count;
   int brk;          // the current basis vector replaces a zero residual (H[j][j-1] = 0)
   int brk_count;

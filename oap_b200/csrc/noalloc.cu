@@ -11,7 +11,11 @@
 //
 // The first call on a device looks up the array's device address with
 // cudaGetSymbolAddress (once per device, with that device current); make
-// that first call before any stream capture.  All calls share the array:
+// that first call before any stream capture.  The looked-up address stays
+// cached for the life of the process: after cudaDeviceReset (or any reset of
+// the device's primary context) the library's module is loaded again and
+// the cached address no longer names the array, so do not call this entry
+// point on a device after resetting it.  All calls share the array:
 // calls whose kernels overlap on the GPU (different streams, or different
 // host threads on one device) race on it and must be serialised by the
 // caller.  The kernel overwrites the whole workspace it uses before reading

@@ -392,6 +392,7 @@ const char* oapb_status_string(int st) {
     case OAPB_ERR_CALLBACK: return "user callback failed";
     case OAPB_ERR_NOMEM: return "out of device memory";
     case OAPB_ERR_BREAKDOWN: return "Krylov breakdown";
+    case OAPB_ERR_NONFINITE: return "non-finite value (NaN or infinity) in the solve";
   }
   return "unknown status";
 }

@@ -26,6 +26,7 @@
 // restart.
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -129,7 +130,7 @@ __global__ void k_normalize(const double* __restrict__ fre, const double* __rest
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     if (j > 0) H[j + (long)(j - 1) * m] = cplx{st->brk ? 0.0 : beta, 0};
-    if (!(beta > 0)) wst->status |= 1;
+    if (!(beta > 0) || isinf(beta)) wst->status |= isfinite(beta) ? 1 : 4;
   }
 }
 
@@ -702,6 +703,7 @@ int iram(oapb_arnoldi* a, bool fp32, double tol, unsigned max_restarts, int star
     int rc = hess(a, do_shift, tol);
     if (rc) return rc;
     if ((rc = read_state(a, &hs))) return rc;
+    if (hs.status & 4) return OAPB_ERR_NONFINITE;
     if (hs.status & 1) return OAPB_ERR_BREAKDOWN;
     if (hs.status & 2) return OAPB_ERR_TIMEOUT;
     a->stats.dgks_passes = hs.dgks_count;
@@ -1600,14 +1602,18 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   int st = resume ? resume_plain<C>(a, r.data()) : mixed ? solve_mixed<C>(a, r.data()) : solve_plain<C>(a, r.data());
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   double mx = 0;
+  bool finite = true;
   for (int q = 0; q < k; ++q) {
     if (eig_re) eig_re[q] = a->evals[q].re;
     if (eig_im) eig_im[q] = a->evals[q].im;
     if (res) res[q] = r[q];
+    // a NaN residual (or eigenvalue) never counts as converged
+    if (!std::isfinite(r[q]) || !std::isfinite(a->evals[q].re) || !std::isfinite(a->evals[q].im)) finite = false;
     mx = r[q] > mx ? r[q] : mx;
   }
-  a->stats.max_residual = mx;
-  a->stats.converged = mx <= a->cfg.tolerance;
+  a->stats.max_residual = finite ? mx : NAN;
+  a->stats.converged = finite && mx <= a->cfg.tolerance;
+  if (!finite) return OAPB_ERR_NONFINITE;
   return a->stats.converged ? OAPB_OK : OAPB_NOT_CONVERGED;
 }
 

@@ -189,9 +189,17 @@ def iram(a, k, m, which="LM", tol=1e-10, maxit=300, rho=1.0 / 3.14,
 
     Returns dict(eigenvalues, vectors (k x n), residuals, restarts, matvecs,
     converged, dgks, rc)."""
-    a = np.asarray(a)
-    n = a.shape[0]
-    ar, ai = _split(a)
+    ar, ai = _split(np.asarray(a))
+    return iram_planes(ar, ai, k, m, which, tol, maxit, rho, v0, seed)
+
+
+def iram_planes(are, aim, k, m, which="LM", tol=1e-10, maxit=300, rho=1.0 / 3.14, v0=None, seed=0):
+    """iram() on an operator given as its split FP64 planes (C-contiguous
+    numpy arrays, aim None for a real operator), without forming the complex
+    matrix: the form for large n (one n = 16384 complex operator is 4 GiB)."""
+    n = are.shape[0]
+    assert are.dtype == np.float64 and are.flags.c_contiguous
+    assert aim is None or (aim.dtype == np.float64 and aim.flags.c_contiguous)
     if v0 is None:
         v0 = np.random.default_rng(seed).uniform(-1.0, 1.0, n)
     v0r, v0i = _split(np.asarray(v0))
@@ -199,13 +207,29 @@ def iram(a, k, m, which="LM", tol=1e-10, maxit=300, rho=1.0 / 3.14,
     xr, xi = np.zeros(k * n), np.zeros(k * n)
     res = np.zeros(k)
     stats = (C.c_int * 4)()
-    rc = lib().orc_iram(n, _p(ar), _p(ai), m, k, WHICH[which], C.c_double(tol),
+    rc = lib().orc_iram(n, _p(are), _p(aim), m, k, WHICH[which], C.c_double(tol),
                         maxit, C.c_double(rho), _p(v0r), _p(v0i), _p(evr),
                         _p(evi), _p(xr), _p(xi), _p(res), stats)
     return {"eigenvalues": evr + 1j * evi,
             "vectors": (xr + 1j * xi).reshape(k, n),
             "residuals": res, "restarts": stats[0], "matvecs": stats[1],
             "converged": bool(stats[2]), "dgks": stats[3], "rc": rc}
+
+
+def match_eigenvalues(ev, ref):
+    """Largest |ev_i - ref_j| / max|ref| over a one-to-one matching of two
+    eigenvalue lists (each value of `ev` to the nearest unused one of `ref`,
+    taken in `ref`'s order: the wanted-set order of SortLargestValues,
+    ArnoldiPackage/ArnoldiUtils.cpp:24-28, when both lists are sorted so)."""
+    ev = list(np.asarray(ev, dtype=np.complex128))
+    ref = np.asarray(ref, dtype=np.complex128)
+    scale = np.abs(ref).max() if ref.size else 1.0
+    worst = 0.0
+    for r in ref:
+        j = int(np.argmin([abs(e - r) for e in ev]))
+        worst = max(worst, abs(ev[j] - r) / scale)
+        ev.pop(j)
+    return worst
 
 
 def num_threads():

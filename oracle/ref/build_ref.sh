@@ -4,7 +4,14 @@
 # sources where they lie, unchanged) plus ref_driver.cpp's C entry points.
 # Test infrastructure only; outputs go to oracle/_ref/ (git-ignored).
 set -euo pipefail
-REF=${OAP_REFERENCE:-/root/reference}
+# The oap checkout: $OAP_REFERENCE, else the first argument, else the
+# location this build's container mounts it at.  Without a checkout there is
+# nothing to build (the GPU box uses the prebuilt library).
+REF=${OAP_REFERENCE:-${1:-/root/reference}}
+if [ ! -d "$REF/oapMatrixCpu" ]; then
+  echo "no oap checkout at $REF; oracle/_ref not built"
+  exit 0
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/../_ref"
 OBJ="$OUT/obj"

@@ -27,6 +27,9 @@ def test_reference_arm_json_line():
     assert d["value"] > 0 and abs(d["ms_per_step"] - 1e3 / d["value"]) < 1e-6 * d["ms_per_step"]
     assert d["n_gpus"] == 1 and d["steps"] == 1 and d["warmup"] == 0
     assert "workload" in d["config"] and d["config"]["n"] == 1024
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.config_dict(1, 1024)  # the GPU arm's config dict
     cb = d["cpu_baseline"]
     assert set(cb) >= {"value", "unit", "cores", "kind", "sample"}
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"]
