@@ -498,11 +498,23 @@ OAPB_EXPORT int oapb_param_operators(const double* A0, const double* const* B,
                                      uint32_t count, uint32_t n, double* out,
                                      void* stream);
 
-/* Dense network sizes[0] -> ... -> sizes[nlayers], tanh hidden layers, linear
- * output; BF16 weights / activations, FP32 accumulation, FP32 master weights
- * with Adam.  Nearest reference analogue: oapNeuralDevice/oapNetwork.h:27-124
+/* Dense network sizes[0] -> ... -> sizes[nlayers]; by default tanh hidden
+ * layers and a linear output (oapb_mlp_set_activations chooses per layer);
+ * BF16 weights / activations, FP32 accumulation, FP32 master weights with
+ * Adam.  Nearest reference analogue: oapNeuralDevice/oapNetwork.h:27-124
  * and the generic propagation of oapNeuralHost/oapGenericNeuralApi.h:195-360. */
 typedef struct oapb_mlp oapb_mlp;
+
+/* Activation of a layer's outputs: the reference's Activation
+ * (oapNeuralHost/oapLayerStructure.h:32-38, same order), applied with its
+ * derivative as activateFunc / derivativeFunc do
+ * (oapNeuralHost/oapGenericNeuralApi.h:43-120). */
+typedef enum oapb_activation {
+  OAPB_ACT_LINEAR = 0,
+  OAPB_ACT_SIGMOID = 1,   /* 1 / (1 + exp(-z)) */
+  OAPB_ACT_TANH = 2,
+  OAPB_ACT_SIN = 3
+} oapb_activation;
 OAPB_EXPORT int oapb_mlp_create(oapb_mlp** handle, const uint32_t* sizes,
                                 uint32_t nlayers, uint64_t seed);
 OAPB_EXPORT int oapb_mlp_destroy(oapb_mlp* handle);
@@ -520,11 +532,18 @@ OAPB_EXPORT int oapb_mlp_adam_step(oapb_mlp* handle, float lr, void* stream);
 /* which 0: parameters, 1: gradients -> dst (host or device FP32) */
 OAPB_EXPORT int oapb_mlp_copy(oapb_mlp* handle, int which, float* dst, void* stream);
 OAPB_EXPORT int oapb_mlp_set_params(oapb_mlp* handle, const float* src, void* stream);
+/* Activations of the nlayers layers' outputs (acts[l] for layer l, count ==
+ * nlayers; the Layer activation of Network::createLayer,
+ * oapNeuralDevice/oapNetwork.h:53-54); OAPB_ERR_ARG for another count or an
+ * unknown value. */
+OAPB_EXPORT int oapb_mlp_set_activations(oapb_mlp* handle, const int32_t* acts, uint32_t count);
+OAPB_EXPORT int oapb_mlp_get_activations(const oapb_mlp* handle, int32_t* acts, uint32_t count);
 /* Layer count; sizes (may be NULL) receives the nlayers + 1 sizes. */
 OAPB_EXPORT uint32_t oapb_mlp_num_layers(const oapb_mlp* handle, uint32_t* sizes);
 /* Network::save / Network::load (oapNeuralDevice/oapNetwork.h:109-111) in
  * the reference's matrix file format: the sizes (1 x nlayers+1), then per
- * layer its weights (in columns x out rows) and biases (1 x out).  load
+ * layer its weights (in columns x out rows) and biases (1 x out), then the
+ * activations (1 x nlayers; absent: the defaults).  load
  * creates a new handle (Adam state fresh; `seed` only fills it before the
  * weights are set). */
 OAPB_EXPORT int oapb_mlp_save(oapb_mlp* handle, const char* path);

@@ -268,14 +268,14 @@ class CuHArnoldiCallback {
 };
 
 /* Network (oapNeuralDevice/oapNetwork.h:27-124) over the library's BF16
- * network: createLayer per layer (the first is the input layer), tanh hidden
- * layers and a linear output (the activations the library computes; any
- * other is an argument error), inputs / expected outputs as device FP32
- * samples x features, forwardPropagation / backPropagation / updateWeights
- * (Adam with the learning rate), train = the three in one call, the MSE of
- * the last backPropagation, save / load in the reference's matrix file
- * format. */
-enum class Activation { TANH, LINEAR, SIGMOID, RELU, SIN };
+ * network: createLayer per layer (the first is the input layer, whose
+ * activation is not used) with the reference's activations, inputs /
+ * expected outputs as device FP32 samples x features, forwardPropagation /
+ * backPropagation / updateWeights (Adam with the learning rate), train =
+ * the three in one call, the MSE of the last backPropagation, save / load
+ * in the reference's matrix file format. */
+/* oapNeuralHost/oapLayerStructure.h:32-38, the same order (= oapb_activation). */
+enum class Activation { LINEAR = OAPB_ACT_LINEAR, SIGMOID = OAPB_ACT_SIGMOID, TANH = OAPB_ACT_TANH, SIN = OAPB_ACT_SIN };
 
 class Network {
  public:
@@ -286,12 +286,13 @@ class Network {
   Network(const Network&) = delete;
   Network& operator=(const Network&) = delete;
 
-  /* Layer* createLayer(neurons, activation): the input layer's activation
-   * is not used; hidden layers are tanh, the last layer linear. */
-  void createLayer(uint neurons, const Activation& activation = Activation::TANH) {
+  /* Layer* createLayer(neurons, activation = SIGMOID) (oapNetwork.h:53):
+   * the input layer's activation is not used. */
+  void createLayer(uint neurons, const Activation& activation = Activation::SIGMOID) {
     if (h_) throw Error(OAPB_ERR_ARG, "Network::createLayer: network already built");
-    if (neurons == 0 || (activation != Activation::TANH && activation != Activation::LINEAR))
-      throw Error(OAPB_ERR_ARG, "Network::createLayer: tanh hidden layers and a linear output only");
+    const int a = static_cast<int>(activation);
+    if (neurons == 0 || a < OAPB_ACT_LINEAR || a > OAPB_ACT_SIN)
+      throw Error(OAPB_ERR_ARG, "Network::createLayer: no neurons or unknown activation");
     sizes_.push_back(neurons);
     acts_.push_back(activation);
   }
@@ -362,6 +363,9 @@ class Network {
     if (h_) return;
     if (sizes_.size() < 2) throw Error(OAPB_ERR_ARG, "Network: fewer than two layers");
     check(oapb_mlp_create(&h_, sizes_.data(), (uint32_t)sizes_.size() - 1, seed_), "Network (create)");
+    std::vector<int32_t> acts;
+    for (size_t l = 1; l < acts_.size(); ++l) acts.push_back(static_cast<int32_t>(acts_[l]));
+    check(oapb_mlp_set_activations(h_, acts.data(), (uint32_t)acts.size()), "Network (activations)");
   }
 
   uint64_t seed_;

@@ -22,6 +22,7 @@ PREC_FP64, PREC_MIXED = 0, 1
 PASS_BF16 = 2  # apply_block only: the BF16 hi planes of the operator copy
 PASS_BF16_COARSE = 3  # apply_block only: the BF16 hi planes, X rounded to BF16 too
 INIT_RANDOM, INIT_FIRST_VALUE_IS_ONE, INIT_USER = 0, 1, 2
+ACT_LINEAR, ACT_SIGMOID, ACT_TANH, ACT_SIN = 0, 1, 2, 3  # oapb_activation
 TYPE_EIGENVECTOR, TYPE_WV = 0, 1
 
 
@@ -150,6 +151,8 @@ def lib():
             "oapb_mlp_adam_step": [vp, C.c_float, vp],
             "oapb_mlp_copy": [vp, C.c_int, vp, vp],
             "oapb_mlp_set_params": [vp, vp, vp],
+            "oapb_mlp_set_activations": [vp, P(C.c_int32), C.c_uint32],
+            "oapb_mlp_get_activations": [vp, P(C.c_int32), C.c_uint32],
             "oapb_arnoldi_solve_batched": [P(Config), P(BatchProblem), C.c_uint32,
                                            P(C.c_double), P(C.c_double), P(C.c_double),
                                            P(C.c_int32), P(BatchStats), vp],

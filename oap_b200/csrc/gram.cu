@@ -7,10 +7,28 @@
 // pixels) is split into BF16 hi + lo parts (hi = bf16(x), lo = bf16(x - hi)),
 // and every 128 x 256 output tile accumulates
 //     hi hi^T + hi lo^T + lo hi^T
-// in FP32 in tensor memory with tcgen05.mma (kind::f16, both operands
-// K-major in 128-byte-swizzled shared memory, filled by cp.async, two
-// stages).  Only tiles touching the upper triangle are computed; the
-// epilogue writes each (i <= j) element and its mirror.
+// in FP32 in tensor memory with tcgen05.mma (kind::f16, M = 128, N = 256,
+// both operands K-major).  Only tiles touching the upper triangle are
+// computed; a second kernel writes each (i <= j) element and its mirror.
+//
+// k_gram_tc is persistent and stream-K scheduled: one CTA per SM walks an
+// equal share of the (tile, 32-column K chunk) iterations, so the 272 tiles
+// of a 4096-row Gram do not leave the second wave of SMs a quarter idle.
+// Each CTA's share is at least one tile long, so a tile is split between at
+// most two CTAs: the part that starts at the tile's first chunk goes to
+// slot 0 of the tile's FP32 partials, the rest to slot 1, and k_gram_finish
+// adds the slots in that order (deterministic).  Warps are specialised:
+//   warp 0      TMA producer: per stage 4 tiled loads (A hi / lo: 128 rows,
+//               B hi / lo: 256 rows, 32 columns = 64 bytes, 64-byte swizzle)
+//               completing on the stage's `full` mbarrier; 4 stages of 48 KB;
+//   warp 1      MMA issuer (one lane) and TMEM owner: 3 products per K=16
+//               step into one of two 256-column FP32 accumulators;
+//               tcgen05.commit frees the stage (`empty`) and hands a finished
+//               segment to the epilogue (`accf`);
+//   warps 2-5   epilogue: TMEM -> registers -> the segment's FP32 partial
+//               (column-major, coalesced), then release the accumulator
+//               (`acce`), so the next segment's MMAs overlap the drain.
+// Every wait is bounded (2 s); a timeout sets the error word (OAPB_ERR_TIMEOUT).
 //
 // Algorithmic work: 2 rows^2 cols flops (one product, counted once).
 #include <stdio.h>
@@ -19,16 +37,21 @@
 
 #include "common.cuh"
 #include "tc.cuh"
+#include "tma.cuh"
 
 namespace oapb {
 
 constexpr int kGmM = 128;   // tile rows (A operand)
 constexpr int kGmN = 256;   // tile columns (B operand)
-constexpr int kGmK = 64;    // BF16 per 128-byte row segment
-constexpr int kGmThreads = 128;
-constexpr uint32_t kGmStageBytes = (2 * kGmM + 2 * kGmN) * 128;  // Ahi, Alo, Bhi, Blo
-constexpr uint32_t kGmSmem = 2 * kGmStageBytes + 1024;           // + alignment slack
-constexpr uint64_t kGmWaitNs = 2000000000ull;                    // 2 s per wait
+constexpr int kGmK = 32;    // BF16 per 64-byte row segment (one stage)
+constexpr int kGmStages = 4;
+constexpr int kGmThreads = 192;
+constexpr uint32_t kGmATile = kGmM * kGmK * 2;                 // 8 KB
+constexpr uint32_t kGmBTile = kGmN * kGmK * 2;                 // 16 KB
+constexpr uint32_t kGmStageBytes = 2 * kGmATile + 2 * kGmBTile;  // Ahi, Alo, Bhi, Blo: 48 KB
+constexpr uint32_t kGmSmem = kGmStages * kGmStageBytes + 1024;  // + alignment slack
+constexpr uint64_t kGmWaitNs = 2000000000ull;                   // 2 s per wait
+constexpr int kGmTileElems = kGmM * kGmN;
 
 // hi / lo split into zero-padded (rows_p x cols_p) BF16 arrays
 __global__ void k_split_bf16(const float* __restrict__ X, int rows, int cols, int rows_p, int cols_p,
@@ -44,31 +67,44 @@ __global__ void k_split_bf16(const float* __restrict__ X, int rows, int cols, in
 }
 
 struct GramArgs {
-  const __nv_bfloat16* hi;
-  const __nv_bfloat16* lo;
-  int rows, cols_p;        // cols_p % 64 == 0; rows of hi / lo padded to a multiple of 256
-  const int2* tiles;       // (row tile, column tile)
-  float* C;                // rows x rows
-  double* C64;             // optional FP64 copy
+  CUtensorMap ahi, alo, bhi, blo;  // the hi / lo planes with A (128-row) and B (256-row) boxes
+  const int4* tiles;               // (row tile, column tile, split, 0)
+  float* ws;                       // FP32 partials: tile x 2 slots x (256 columns x 128 rows)
   int* err;
+  long total;                      // tiles x K chunks
+  int kch;                         // K chunks per tile
+  int ctas;
 };
 
-__global__ void __launch_bounds__(kGmThreads, 1) k_gram_tc(GramArgs g) {
+// Shared-memory descriptor of a K-major tile with 64-byte rows (32 BF16),
+// 64-byte swizzle (layout type 4), 8-row groups 512 bytes apart.
+__device__ __forceinline__ uint64_t gm_sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+__global__ void __launch_bounds__(kGmThreads, 1) k_gram_tc(const __grid_constant__ GramArgs g) {
   extern __shared__ __align__(1024) uint8_t gsm_raw[];
-  __shared__ __align__(8) uint64_t bar[2];
+  __shared__ __align__(8) uint64_t full[kGmStages], empty[kGmStages], accf[2], acce[2], done;
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   uint8_t* gsm = (uint8_t*)(((uintptr_t)gsm_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t sbase = tc::smem_u32(gsm);
-  const int2 tile = g.tiles[blockIdx.x];
-  const long i0 = (long)tile.x * kGmM, j0 = (long)tile.y * kGmN;
-  const int niter = g.cols_p / kGmK;
+  const long it0 = (long)blockIdx.x * g.total / g.ctas, it1 = (long)(blockIdx.x + 1) * g.total / g.ctas;
+  const int kch = g.kch;
 
-  if (warp == 0) tc::tmem_alloc(&tmem_slot, kGmN);
+  if (warp == 1) tc::tmem_alloc(&tmem_slot, 512);
   if (tid == 0) {
-    tc::mbar_init(&bar[0], 1);
-    tc::mbar_init(&bar[1], 1);
+    for (int i = 0; i < kGmStages; ++i) {
+      tc::mbar_init(&full[i], 1);
+      tc::mbar_init(&empty[i], 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&accf[i], 1);
+      tc::mbar_init(&acce[i], 4);
+    }
+    tc::mbar_init(&done, 1);
     tc::fence_mbar_init();
     abort_flag = 0;
   }
@@ -76,103 +112,140 @@ __global__ void __launch_bounds__(kGmThreads, 1) k_gram_tc(GramArgs g) {
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = tmem_slot;
-  constexpr uint32_t idesc = tc::idesc_bf16_f32(kGmM, kGmN);
 
-  // stage s: Ahi at s*stage, Alo +16K, Bhi +32K, Blo +64K
-  auto load_stage = [&](int it, int s) {
-    const uint32_t st = sbase + s * kGmStageBytes;
-    const long k0 = (long)it * kGmK;
-    // A: 2 x 1024 chunks, B: 2 x 2048 chunks of 16 bytes
-    for (int c = tid; c < 2 * kGmM * 8; c += kGmThreads) {
-      const int part = c / (kGmM * 8), q = c % (kGmM * 8);
-      const int r = q >> 3, ch = q & 7;
-      const __nv_bfloat16* src = (part ? g.lo : g.hi) + (i0 + r) * (long)g.cols_p + k0 + ch * 8;
-      tc::cp_async16(st + part * (kGmM * 128) + tc::sw128(r, ch), src);
+  if (warp == 0) {
+    // ---------------------------------------------------------- producer --
+    if (lane == 0) {
+      long it = it0;
+      for (; it < it1; ++it) {
+        const long i = it - it0;
+        const int s = (int)(i % kGmStages);
+        if (i >= kGmStages && !tma::wait(&empty[s], (uint32_t)((i / kGmStages - 1) & 1), &abort_flag, kGmWaitNs))
+          break;
+        const int4 t = g.tiles[it / kch];
+        const int x = (int)(it % kch) * kGmK;
+        const uint32_t st = sbase + s * kGmStageBytes;
+        tma::expect_tx(&full[s], kGmStageBytes);
+        tma::load_2d(st, &g.ahi, x, t.x * kGmM, &full[s]);
+        tma::load_2d(st + kGmATile, &g.alo, x, t.x * kGmM, &full[s]);
+        tma::load_2d(st + 2 * kGmATile, &g.bhi, x, t.y * kGmN, &full[s]);
+        tma::load_2d(st + 2 * kGmATile + kGmBTile, &g.blo, x, t.y * kGmN, &full[s]);
+      }
+      // no copy may still be landing in shared memory when the CTA exits
+      for (long j = (it - kGmStages > it0 ? it - kGmStages : it0); j < it; ++j) {
+        const long i = j - it0;
+        tc::mbar_wait(&full[i % kGmStages], (uint32_t)((i / kGmStages) & 1), kGmWaitNs);
+      }
     }
-    for (int c = tid; c < 2 * kGmN * 8; c += kGmThreads) {
-      const int part = c / (kGmN * 8), q = c % (kGmN * 8);
-      const int r = q >> 3, ch = q & 7;
-      const __nv_bfloat16* src = (part ? g.lo : g.hi) + (j0 + r) * (long)g.cols_p + k0 + ch * 8;
-      tc::cp_async16(st + 2 * kGmM * 128 + part * (kGmN * 128) + tc::sw128(r, ch), src);
-    }
-    tc::cp_async_commit();
-  };
-
-  bool ok = true;
-  load_stage(0, 0);
-  for (int it = 0; it < niter; ++it) {
-    const int s = it & 1;
-    if (it + 1 < niter) {
-      const int s1 = (it + 1) & 1;
-      if (it >= 1) {
-        // the MMAs of iteration it - 1 read stage s1: wait for their commit
-        if (!tc::mbar_wait(&bar[s1], ((it - 1) >> 1) & 1, kGmWaitNs)) {
-          atomicOr(&abort_flag, 1);
+  } else if (warp == 1) {
+    // --------------------------------------------------------------- MMA --
+    if (lane == 0) {
+      constexpr uint32_t idesc = tc::idesc_bf16_f32(kGmM, kGmN);
+      long seg = 0;
+      for (long it = it0; it < it1; ++it) {
+        const long i = it - it0;
+        const int s = (int)(i % kGmStages);
+        const long kc = it % kch;
+        const bool seg_first = it == it0 || kc == 0;
+        const int buf = (int)(seg & 1);
+        if (seg_first && seg >= 2 && !tma::wait(&acce[buf], (uint32_t)((seg / 2 - 1) & 1), &abort_flag, kGmWaitNs))
+          break;
+        if (!tma::wait(&full[s], (uint32_t)((i / kGmStages) & 1), &abort_flag, kGmWaitNs)) break;
+        tc::tc_fence_after();
+        const uint32_t st = sbase + s * kGmStageBytes;
+        const uint64_t ahi = gm_sdesc(st), alo = gm_sdesc(st + kGmATile);
+        const uint64_t bhi = gm_sdesc(st + 2 * kGmATile), blo = gm_sdesc(st + 2 * kGmATile + kGmBTile);
+        const uint32_t d = tmem + buf * kGmN;
+#pragma unroll
+        for (int kk = 0; kk < kGmK / 16; ++kk) {
+          const uint64_t off = (uint64_t)(kk * 32) >> 4;  // 32 bytes per K = 16 step
+          tc::mma_bf16(d, ahi + off, bhi + off, idesc, (seg_first && kk == 0) ? 0u : 1u);
+          tc::mma_bf16(d, ahi + off, blo + off, idesc, 1u);
+          tc::mma_bf16(d, alo + off, bhi + off, idesc, 1u);
+        }
+        tc::commit(&empty[s]);
+        if (it + 1 == it1 || kc + 1 == kch) {
+          tc::commit(&accf[buf]);
+          ++seg;
         }
       }
-      __syncthreads();
-      if (abort_flag) {
-        ok = false;
-        break;
-      }
-      load_stage(it + 1, s1);
-      tc::cp_async_wait<1>();
-    } else {
-      tc::cp_async_wait<0>();
+      // every MMA issued so far has completed once `done` flips
+      tc::commit(&done);
+      if (!tc::mbar_wait(&done, 0, kGmWaitNs)) abort_flag = 1;
     }
-    tc::fence_proxy_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+  } else {
+    // ---------------------------------------------------------- epilogue --
+    const int wq = warp & 3;  // TMEM lane quarter of this warp
+    const int row = wq * 32 + lane;
+    long seg = 0;
+    for (long it = it0; it < it1; ++seg) {
+      const long tile = it / kch;
+      const long seg_end = (tile + 1) * kch < it1 ? (tile + 1) * kch : it1;
+      const int slot = it == tile * kch ? 0 : 1;
+      const int buf = (int)(seg & 1);
+      if (!tma::wait(&accf[buf], (uint32_t)((seg / 2) & 1), &abort_flag, kGmWaitNs)) break;
       tc::tc_fence_after();
-      const uint32_t st = sbase + s * kGmStageBytes;
-      const uint64_t ahi = tc::sdesc_k_sw128(st), alo = tc::sdesc_k_sw128(st + kGmM * 128);
-      const uint64_t bhi = tc::sdesc_k_sw128(st + 2 * kGmM * 128);
-      const uint64_t blo = tc::sdesc_k_sw128(st + 2 * kGmM * 128 + kGmN * 128);
-#pragma unroll
-      for (int kk = 0; kk < kGmK / 16; ++kk) {
-        const uint64_t off = (uint64_t)(kk * 32) >> 4;  // 32 bytes per K=16 step
-        tc::mma_bf16(tmem, ahi + off, bhi + off, idesc, (it > 0 || kk > 0) ? 1u : 0u);
-        tc::mma_bf16(tmem, ahi + off, blo + off, idesc, 1u);
-        tc::mma_bf16(tmem, alo + off, bhi + off, idesc, 1u);
-      }
-      tc::commit(&bar[s]);
-    }
-  }
-  // all MMAs done before reading the accumulator
-  if (ok && niter > 0) {
-    const int last = niter - 1;
-    if (!tc::mbar_wait(&bar[last & 1], (last >> 1) & 1, kGmWaitNs)) atomicOr(&abort_flag, 2);
-  }
-  tc::cp_async_wait<0>();
-  __syncthreads();
-  tc::tc_fence_after();
-  if (!abort_flag) {
-    const long i = i0 + warp * 32 + lane;
+      float* out = g.ws + ((size_t)tile * 2 + slot) * kGmTileElems + row;
 #pragma unroll 1
-    for (int cc = 0; cc < kGmN / 32; ++cc) {
-      float v[32];
-      tc::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + cc * 32, v);
-      if (i < g.rows) {
+      for (int cc = 0; cc < kGmN / 32; ++cc) {
+        float v[32];
+        tc::tmem_ld32(tmem + ((uint32_t)(wq * 32) << 16) + buf * kGmN + cc * 32, v);
 #pragma unroll
-        for (int q = 0; q < 32; ++q) {
-          const long j = j0 + cc * 32 + q;
-          if (j < g.rows && i <= j) {
-            g.C[i * g.rows + j] = v[q];
-            if (i != j) g.C[j * g.rows + i] = v[q];
-            if (g.C64) {
-              g.C64[i * g.rows + j] = (double)v[q];
-              if (i != j) g.C64[j * g.rows + i] = (double)v[q];
-            }
-          }
-        }
+        for (int q = 0; q < 32; ++q) out[(size_t)(cc * 32 + q) * kGmM] = v[q];
       }
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tma::arrive(&acce[buf]);
+      it = seg_end;
     }
-  } else if (tid == 0) {
-    atomicOr(g.err, abort_flag);
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, kGmN);
+  if (abort_flag && tid == 0) atomicOr(g.err, 1);
+  if (warp == 1) {
+    tc::tc_fence_after();
+    tc::tmem_dealloc(tmem, 512);
+  }
+}
+
+// A (and its FP64 copy) from the tile partials: one block per 32 x 32 piece
+// of a tile; element (i, j), i <= j, and its mirror (j, i).  The piece goes
+// through shared memory so both the direct and the mirrored rows are
+// written with consecutive lanes on consecutive columns.
+__global__ void k_gram_finish(const float* __restrict__ ws, const int4* __restrict__ tiles, int rows, float* C,
+                              double* C64) {
+  __shared__ float t[32][33];
+  const int tile = blockIdx.x / 32, piece = blockIdx.x % 32;
+  const int a = piece / 8, b = piece % 8;  // 32-row strip a of 4, 32-column strip b of 8
+  const int4 T = tiles[tile];
+  const long i0 = (long)T.x * kGmM + a * 32, j0 = (long)T.y * kGmN + b * 32;
+  if (i0 > j0 + 31) return;  // every element below the diagonal
+  const float* s0 = ws + (size_t)tile * 2 * kGmTileElems;
+  const float* s1 = s0 + kGmTileElems;
+  const int r = threadIdx.x, cy = threadIdx.y;
+  for (int c = cy; c < 32; c += 8) {
+    const size_t idx = (size_t)(b * 32 + c) * kGmM + a * 32 + r;
+    float v = s0[idx];
+    if (T.z) v += s1[idx];
+    t[c][r] = v;
+  }
+  __syncthreads();
+  for (int rr = cy; rr < 32; rr += 8) {  // direct: row i0 + rr, lanes over columns
+    const long i = i0 + rr, j = j0 + r;
+    if (i < rows && j < rows && i <= j) {
+      const float v = t[r][rr];
+      C[i * rows + j] = v;
+      if (C64) C64[i * rows + j] = (double)v;
+    }
+  }
+  for (int cc = cy; cc < 32; cc += 8) {  // mirror: row j0 + cc, lanes over columns i
+    const long j = j0 + cc, i = i0 + r;
+    if (i < rows && j < rows && i < j) {
+      const float v = t[cc][r];
+      C[j * rows + i] = v;
+      if (C64) C64[j * rows + i] = (double)v;
+    }
+  }
 }
 
 }  // namespace oapb
@@ -186,13 +259,28 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
   cudaStream_t s = (cudaStream_t)stream;
   const int rows_p = (int)((rows + kGmN - 1) / kGmN) * kGmN;
   const int cols_p = (int)((cols + kGmK - 1) / kGmK) * kGmK;
-  // tiles touching the upper triangle
-  std::vector<int2> tiles;
+  const int kch = cols_p / kGmK;
+  // tiles touching the upper triangle, and the stream-K split of
+  // (tile, K chunk) iterations over at most one CTA per SM
+  std::vector<int4> tiles;
   for (int r = 0; r * kGmM < (int)rows; ++r)
     for (int c = 0; c * kGmN < (int)rows; ++c)
-      if (r * kGmM <= c * kGmN + kGmN - 1) tiles.push_back(make_int2(r, c));
+      if (r * kGmM <= c * kGmN + kGmN - 1) tiles.push_back(make_int4(r, c, 0, 0));
+  const long ntiles = (long)tiles.size();
+  const int ctas = (int)(ntiles < kNumSMs ? ntiles : kNumSMs);
+  const long total = ntiles * kch;
+  // with at least one tile per CTA a tile meets at most two CTAs: it is
+  // split when the CTA holding its first chunk ends inside it
+  for (long t = 0; t < ntiles; ++t) {
+    const long first = t * kch;
+    long b = (first * ctas) / total;  // the CTA whose [b total / ctas, (b + 1) total / ctas) holds `first`
+    while (b > 0 && b * total / ctas > first) --b;
+    while ((b + 1) * total / ctas <= first) ++b;
+    tiles[t].z = (b + 1) * total / ctas < first + kch ? 1 : 0;
+  }
   const size_t half = (size_t)rows_p * cols_p;
-  const size_t bytes = 2 * half * sizeof(__nv_bfloat16) + tiles.size() * sizeof(int2) + 256;
+  const size_t ws_elems = (size_t)ntiles * 2 * kGmTileElems;
+  const size_t bytes = 2 * half * sizeof(__nv_bfloat16) + ws_elems * sizeof(float) + tiles.size() * sizeof(int4) + 256;
   char* buf = nullptr;
   if (cudaMallocAsync((void**)&buf, bytes, s) != cudaSuccess) {
     cudaGetLastError();
@@ -200,11 +288,20 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
   }
   __nv_bfloat16* hi = (__nv_bfloat16*)buf;
   __nv_bfloat16* lo = hi + half;
-  int2* dtiles = (int2*)(lo + half);
+  float* ws = (float*)(lo + half);
+  int4* dtiles = (int4*)(ws + ws_elems);
   int* err = (int*)(dtiles + tiles.size());
   int rc = OAPB_OK;
   do {
-    if (cudaMemcpyAsync(dtiles, tiles.data(), tiles.size() * sizeof(int2), cudaMemcpyHostToDevice, s) !=
+    GramArgs g;
+    if (!tma::map_bf16(&g.ahi, hi, cols_p, rows_p, kGmK, kGmM, CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !tma::map_bf16(&g.alo, lo, cols_p, rows_p, kGmK, kGmM, CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !tma::map_bf16(&g.bhi, hi, cols_p, rows_p, kGmK, kGmN, CU_TENSOR_MAP_SWIZZLE_64B) ||
+        !tma::map_bf16(&g.blo, lo, cols_p, rows_p, kGmK, kGmN, CU_TENSOR_MAP_SWIZZLE_64B)) {
+      rc = OAPB_ERR_CUDA;
+      break;
+    }
+    if (cudaMemcpyAsync(dtiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
             cudaSuccess ||
         cudaMemsetAsync(err, 0, sizeof(int), s) != cudaSuccess) {
       rc = OAPB_ERR_CUDA;
@@ -216,8 +313,14 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
       rc = OAPB_ERR_CUDA;
       break;
     }
-    GramArgs g{hi, lo, (int)rows, cols_p, dtiles, A, A64, err};
-    k_gram_tc<<<(unsigned)tiles.size(), kGmThreads, kGmSmem, s>>>(g);
+    g.tiles = dtiles;
+    g.ws = ws;
+    g.err = err;
+    g.total = total;
+    g.kch = kch;
+    g.ctas = ctas;
+    k_gram_tc<<<(unsigned)ctas, kGmThreads, kGmSmem, s>>>(g);
+    k_gram_finish<<<(unsigned)(ntiles * 32), dim3(32, 8), 0, s>>>(ws, dtiles, (int)rows, A, A64);
     if (cudaGetLastError() != cudaSuccess) {
       rc = OAPB_ERR_CUDA;
       break;

@@ -2,9 +2,13 @@
 //
 // 1. oapb_param_operators: A(theta_p) = A0 + sum_i theta_p[i] B_i for a batch
 //    of parameter vectors (each basis element read once, written P times).
-// 2. A dense MLP (tanh hidden layers, linear output) with BF16 weights and
-//    activations and FP32 accumulation: forward, backward (data and weight
-//    gradients) and an Adam step on FP32 master weights, all on the device.
+// 2. A dense MLP with BF16 weights and activations and FP32 accumulation:
+//    forward, backward (data and weight gradients) and an Adam step on FP32
+//    master weights, all on the device.  Each layer's outputs pass through
+//    one of the reference's activations (oapNeuralHost/oapLayerStructure.h:
+//    32-38, applied by activateFunc / derivativeFunc,
+//    oapGenericNeuralApi.h:43-120): LINEAR, SIGMOID, TANH or SIN; by
+//    default tanh hidden layers and a linear output.
 //    The network maps an operator's parameters theta to a warm-start vector
 //    and a shift set for the Arnoldi method.  Nearest reference analogue:
 //    the generic forward / back-propagation of the neural library
@@ -14,7 +18,8 @@
 // Every layer product is one kernel: C[M x N] = sum_k A(m, k) B(n, k) with
 // strided BF16 operands (the forward product, the data gradient and the
 // weight gradient differ only in strides), 32 x 32 output tiles, FP32
-// accumulation, optional bias + tanh epilogue and a BF16 copy of the output.
+// accumulation, optional bias + activation epilogue (the pre-activation
+// kept for SIN, whose derivative needs it) and a BF16 copy of the output.
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -45,12 +50,32 @@ __global__ void k_param_operators(const double* __restrict__ A0, const double* c
 constexpr int kLT = 32;  // output tile
 constexpr int kLK = 16;  // k chunk
 
-// C[m][n] (ldc) = sum_k A[m*sam + k*sak] * B[n*sbn + k*sbk]   (+ bias[n], tanh)
-template <bool BIAS_TANH>
+// activation of a layer's outputs (oapb_activation) and its derivative from
+// the pre-activation z and the output h
+__device__ __forceinline__ float act_f(float z, int act) {
+  switch (act) {
+    case OAPB_ACT_SIGMOID: return 1.f / (1.f + expf(-z));
+    case OAPB_ACT_TANH: return tanhf(z);
+    case OAPB_ACT_SIN: return sinf(z);
+    default: return z;
+  }
+}
+__device__ __forceinline__ float act_df(float z, float h, int act) {
+  switch (act) {
+    case OAPB_ACT_SIGMOID: return h * (1.f - h);
+    case OAPB_ACT_TANH: return 1.f - h * h;
+    case OAPB_ACT_SIN: return cosf(z);
+    default: return 1.f;
+  }
+}
+
+// C[m][n] (ldc) = sum_k A[m*sam + k*sak] * B[n*sbn + k*sbk]; with EPI:
+// z = C + bias[n] (kept in Z when given), C = act(z)
+template <bool EPI>
 __global__ void __launch_bounds__(256) k_layer_gemm(const __nv_bfloat16* __restrict__ A, long sam, long sak,
                                                     const __nv_bfloat16* __restrict__ Bm, long sbn, long sbk, int M,
-                                                    int N, int K, const float* __restrict__ bias, float* C,
-                                                    __nv_bfloat16* Cb, int ldc) {
+                                                    int N, int K, const float* __restrict__ bias, int act, float* C,
+                                                    float* Z, __nv_bfloat16* Cb, int ldc) {
   __shared__ float As[kLK][kLT + 1];
   __shared__ float Bsm[kLK][kLT + 1];
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;  // 16 x 16 threads, 2 x 2 outputs each
@@ -82,23 +107,19 @@ __global__ void __launch_bounds__(256) k_layer_gemm(const __nv_bfloat16* __restr
       const int m = m0 + ty * 2 + i, n = n0 + tx * 2 + j;
       if (m < M && n < N) {
         float v = acc[i][j];
-        if (BIAS_TANH) v = tanhf(v + bias[n]);
+        if (EPI) {
+          v += bias[n];
+          if (Z) Z[(long)m * ldc + n] = v;
+          v = act_f(v, act);
+        }
         if (C) C[(long)m * ldc + n] = v;
         if (Cb) Cb[(long)m * ldc + n] = __float2bfloat16_rn(v);
       }
     }
 }
 
-// y = out + bias (output layer without activation), in place, + BF16 copy
-__global__ void k_add_bias(float* Y, const float* bias, int B, int N, __nv_bfloat16* Yb) {
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < (long)B * N; e += (long)gridDim.x * blockDim.x) {
-    const float v = Y[e] + bias[e % N];
-    Y[e] = v;
-    if (Yb) Yb[e] = __float2bfloat16_rn(v);
-  }
-}
-
-// dY = (Y - T) / B (BF16 for the backward products); loss partial sums
+// dY = (Y - T) / B (FP32, and BF16 for the backward products when given);
+// loss partial sums
 __global__ void k_mse_grad(const float* Y, const float* T, int B, long len, __nv_bfloat16* dYb, float* dYf,
                            double* loss) {
   double s = 0;
@@ -106,18 +127,19 @@ __global__ void k_mse_grad(const float* Y, const float* T, int B, long len, __nv
     const float d = Y[e] - T[e];
     s += (double)d * d;
     const float g = d / (float)B;
-    dYb[e] = __float2bfloat16_rn(g);
+    if (dYb) dYb[e] = __float2bfloat16_rn(g);
     if (dYf) dYf[e] = g;
   }
   s = warp_sum(s);
   if ((threadIdx.x & 31) == 0) atomicAdd(loss, 0.5 * s / B);
 }
 
-// dZ = dH * (1 - h^2)  (tanh), BF16 out
-__global__ void k_tanh_grad(const float* dH, const float* H, long len, __nv_bfloat16* dZb, float* dZf) {
+// dZ = dH * act'(z) (from the output h, or the pre-activation z for SIN),
+// FP32 and BF16 out
+__global__ void k_act_grad(const float* dH, const float* H, const float* Z, int act, long len,
+                           __nv_bfloat16* dZb, float* dZf) {
   for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < len; e += (long)gridDim.x * blockDim.x) {
-    const float h = H[e];
-    const float g = dH[e] * (1.f - h * h);
+    const float g = dH[e] * act_df(Z ? Z[e] : 0.f, H[e], act);
     dZb[e] = __float2bfloat16_rn(g);
     if (dZf) dZf[e] = g;
   }
@@ -169,9 +191,11 @@ struct oapb_mlp {
   float *w = nullptr, *g = nullptr, *m1 = nullptr, *m2 = nullptr;  // FP32 [all weights | all biases]
   __nv_bfloat16* wb = nullptr;                                     // BF16 copy of the weights
   int step = 0;
+  std::vector<int> act;                // activation of each layer's outputs (oapb_activation)
   // activations for the last forward (capacity batch)
   int cap = 0;
   std::vector<float*> hf;              // FP32 activations per layer output (nl)
+  std::vector<float*> zf;              // FP32 pre-activations per layer output (nl)
   std::vector<__nv_bfloat16*> hb;      // BF16 activations: input + per layer
   float *dA = nullptr, *dB2 = nullptr; // FP32 gradient scratch (cap x max size)
   __nv_bfloat16 *dAb = nullptr;
@@ -183,8 +207,10 @@ namespace {
 int g_mlp_free_acts(oapb_mlp* h) {
   for (auto p : h->hf) cudaFree(p);
   for (auto p : h->hb) cudaFree(p);
+  for (auto p : h->zf) cudaFree(p);
   h->hf.clear();
   h->hb.clear();
+  h->zf.clear();
   if (h->dA) cudaFree(h->dA);
   if (h->dB2) cudaFree(h->dB2);
   if (h->dAb) cudaFree(h->dAb);
@@ -201,10 +227,13 @@ int ensure_acts(oapb_mlp* h, int batch) {
   for (int s : h->sz) mx = s > mx ? s : mx;
   h->hb.resize(h->nl + 1, nullptr);
   h->hf.resize(h->nl, nullptr);
+  h->zf.resize(h->nl, nullptr);
   for (int l = 0; l <= h->nl; ++l)
     if (cudaMalloc(&h->hb[l], sizeof(__nv_bfloat16) * (size_t)batch * h->sz[l]) != cudaSuccess) return OAPB_ERR_NOMEM;
   for (int l = 0; l < h->nl; ++l)
-    if (cudaMalloc(&h->hf[l], sizeof(float) * (size_t)batch * h->sz[l + 1]) != cudaSuccess) return OAPB_ERR_NOMEM;
+    if (cudaMalloc(&h->hf[l], sizeof(float) * (size_t)batch * h->sz[l + 1]) != cudaSuccess ||
+        cudaMalloc(&h->zf[l], sizeof(float) * (size_t)batch * h->sz[l + 1]) != cudaSuccess)
+      return OAPB_ERR_NOMEM;
   if (cudaMalloc(&h->dA, sizeof(float) * (size_t)batch * mx) != cudaSuccess ||
       cudaMalloc(&h->dB2, sizeof(float) * (size_t)batch * mx) != cudaSuccess ||
       cudaMalloc(&h->dAb, sizeof(__nv_bfloat16) * (size_t)batch * mx) != cudaSuccess)
@@ -213,13 +242,14 @@ int ensure_acts(oapb_mlp* h, int batch) {
   return OAPB_OK;
 }
 
-void layer_gemm(bool bias_tanh, const __nv_bfloat16* A, long sam, long sak, const __nv_bfloat16* Bm, long sbn, long sbk,
-                int M, int N, int K, const float* bias, float* C, __nv_bfloat16* Cb, int ldc, cudaStream_t s) {
+void layer_gemm(bool epi, int act, const __nv_bfloat16* A, long sam, long sak, const __nv_bfloat16* Bm, long sbn,
+                long sbk, int M, int N, int K, const float* bias, float* C, float* Z, __nv_bfloat16* Cb, int ldc,
+                cudaStream_t s) {
   dim3 grid((N + kLT - 1) / kLT, (M + kLT - 1) / kLT);
-  if (bias_tanh)
-    k_layer_gemm<true><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, C, Cb, ldc);
+  if (epi)
+    k_layer_gemm<true><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, act, C, Z, Cb, ldc);
   else
-    k_layer_gemm<false><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, C, Cb, ldc);
+    k_layer_gemm<false><<<grid, 256, 0, s>>>(A, sam, sak, Bm, sbn, sbk, M, N, K, bias, act, C, Z, Cb, ldc);
 }
 
 int forward_impl(oapb_mlp* h, const float* x, int B, cudaStream_t s) {
@@ -229,11 +259,10 @@ int forward_impl(oapb_mlp* h, const float* x, int B, cudaStream_t s) {
   k_to_bf16<<<grid_for(n0, 256), 256, 0, s>>>(x, n0, h->hb[0]);
   for (int l = 0; l < h->nl; ++l) {
     const int in = h->sz[l], out = h->sz[l + 1];
-    const bool last = l + 1 == h->nl;
     const __nv_bfloat16* W = h->wb + h->woff[l];
     const float* bias = h->w + h->boff[l];
-    layer_gemm(!last, h->hb[l], in, 1, W, in, 1, B, out, in, bias, h->hf[l], last ? nullptr : h->hb[l + 1], out, s);
-    if (last) k_add_bias<<<grid_for((long)B * out, 256), 256, 0, s>>>(h->hf[l], bias, B, out, h->hb[l + 1]);
+    layer_gemm(true, h->act[l], h->hb[l], in, 1, W, in, 1, B, out, in, bias, h->hf[l],
+               h->act[l] == OAPB_ACT_SIN ? h->zf[l] : nullptr, h->hb[l + 1], out, s);
   }
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
 }
@@ -283,6 +312,8 @@ int oapb_mlp_create(oapb_mlp** out, const uint32_t* sizes, uint32_t nlayers, uin
     off += h->sz[l + 1];
   }
   h->nparam = off;
+  h->act.assign(h->nl, OAPB_ACT_TANH);
+  h->act[h->nl - 1] = OAPB_ACT_LINEAR;
   const size_t fb = sizeof(float) * (size_t)off;
   if (cudaMalloc(&h->w, fb) != cudaSuccess || cudaMalloc(&h->g, fb) != cudaSuccess ||
       cudaMalloc(&h->m1, fb) != cudaSuccess || cudaMalloc(&h->m2, fb) != cudaSuccess ||
@@ -351,18 +382,28 @@ int oapb_mlp_backward(oapb_mlp* h, const float* x, const float* target, uint32_t
   if (cudaMemsetAsync(h->loss, 0, sizeof(double), s) != cudaSuccess) return OAPB_ERR_CUDA;
   const int L = h->nl;
   const long lenY = (long)B * h->sz[L];
-  // dY of the output layer into dAb (BF16) / dA (FP32)
-  k_mse_grad<<<grid_for(lenY, 256), 256, 0, s>>>(h->hf[L - 1], target, B, lenY, h->dAb, h->dA, h->loss);
+  // dZ of the output layer into dAb (BF16) / dA (FP32): dY itself for a
+  // linear output, else dY through the activation's derivative
+  if (h->act[L - 1] == OAPB_ACT_LINEAR) {
+    k_mse_grad<<<grid_for(lenY, 256), 256, 0, s>>>(h->hf[L - 1], target, B, lenY, h->dAb, h->dA, h->loss);
+  } else {
+    k_mse_grad<<<grid_for(lenY, 256), 256, 0, s>>>(h->hf[L - 1], target, B, lenY, nullptr, h->dB2, h->loss);
+    k_act_grad<<<grid_for(lenY, 256), 256, 0, s>>>(h->dB2, h->hf[L - 1], h->zf[L - 1], h->act[L - 1], lenY, h->dAb,
+                                                    h->dA);
+  }
   for (int l = L - 1; l >= 0; --l) {
     const int in = h->sz[l], out = h->sz[l + 1];
     // dZ (B x out) in dAb / dA; weight gradient dW[o][i] = sum_b dZ[b][o] X[b][i]
-    layer_gemm(false, h->dAb, 1, out, h->hb[l], 1, in, out, in, B, nullptr, h->g + h->woff[l], nullptr, in, s);
+    layer_gemm(false, 0, h->dAb, 1, out, h->hb[l], 1, in, out, in, B, nullptr, h->g + h->woff[l], nullptr, nullptr,
+               in, s);
     k_bias_grad<<<grid_for(out, 256), 256, 0, s>>>(h->dA, B, out, h->g + h->boff[l]);
     if (l == 0) break;
-    // data gradient dX[b][i] = sum_o dZ[b][o] W[o][i], then through tanh
+    // data gradient dX[b][i] = sum_o dZ[b][o] W[o][i], then through layer
+    // l - 1's activation
     const __nv_bfloat16* W = h->wb + h->woff[l];
-    layer_gemm(false, h->dAb, out, 1, W, 1, in, B, in, out, nullptr, h->dB2, nullptr, in, s);
-    k_tanh_grad<<<grid_for((long)B * in, 256), 256, 0, s>>>(h->dB2, h->hf[l - 1], (long)B * in, h->dAb, h->dA);
+    layer_gemm(false, 0, h->dAb, out, 1, W, 1, in, B, in, out, nullptr, h->dB2, nullptr, nullptr, in, s);
+    k_act_grad<<<grid_for((long)B * in, 256), 256, 0, s>>>(h->dB2, h->hf[l - 1], h->zf[l - 1], h->act[l - 1],
+                                                            (long)B * in, h->dAb, h->dA);
   }
   if (cudaGetLastError() != cudaSuccess) return OAPB_ERR_CUDA;
   if (loss_out) {
@@ -405,6 +446,20 @@ int oapb_mlp_set_params(oapb_mlp* h, const float* src, void* stream) {
   return OAPB_OK;
 }
 
+int oapb_mlp_set_activations(oapb_mlp* h, const int32_t* acts, uint32_t count) {
+  if (!h || !acts || count != (uint32_t)h->nl) return OAPB_ERR_ARG;
+  for (uint32_t l = 0; l < count; ++l)
+    if (acts[l] < OAPB_ACT_LINEAR || acts[l] > OAPB_ACT_SIN) return OAPB_ERR_ARG;
+  for (uint32_t l = 0; l < count; ++l) h->act[l] = acts[l];
+  return OAPB_OK;
+}
+
+int oapb_mlp_get_activations(const oapb_mlp* h, int32_t* acts, uint32_t count) {
+  if (!h || !acts || count != (uint32_t)h->nl) return OAPB_ERR_ARG;
+  for (uint32_t l = 0; l < count; ++l) acts[l] = h->act[l];
+  return OAPB_OK;
+}
+
 uint32_t oapb_mlp_num_layers(const oapb_mlp* h, uint32_t* sizes) {
   if (!h) return 0;
   if (sizes)
@@ -414,7 +469,9 @@ uint32_t oapb_mlp_num_layers(const oapb_mlp* h, uint32_t* sizes) {
 
 // File (the reference's matrix format, matio.cuh): sizes (1 column x
 // nlayers + 1 rows), then per layer its weights (in columns x out rows) and
-// biases (1 column x out rows), FP64 values of the FP32 master weights.
+// biases (1 column x out rows), FP64 values of the FP32 master weights, and
+// last the layers' activations (1 column x nlayers rows, oapb_activation
+// values; a file without it loads with the default activations).
 int oapb_mlp_save(oapb_mlp* h, const char* path) {
   if (!h || !path) return OAPB_ERR_ARG;
   std::vector<float> p((size_t)h->nparam);
@@ -437,6 +494,11 @@ int oapb_mlp_save(oapb_mlp* h, const char* path) {
     matio_append(payload, W);
     matio_append(payload, bv);
   }
+  HostMat acts;
+  acts.columns = 1;
+  acts.rows = (uint32_t)h->nl;
+  for (int a : h->act) acts.re.push_back((double)a);
+  matio_append(payload, acts);
   return matio_write_file(path, payload);
 }
 
@@ -460,8 +522,18 @@ int oapb_mlp_load(oapb_mlp** out, const char* path, uint64_t seed) {
     if (Ws[l].columns != sizes[l] || Ws[l].rows != sizes[l + 1] || bs[l].columns != 1 || bs[l].rows != sizes[l + 1])
       return OAPB_ERR_ARG;
   }
+  std::vector<int32_t> acts;
+  HostMat am;
+  if (off < payload.size()) {
+    if (!matio_parse(payload, off, &am) || am.columns != 1 || am.rows != (uint32_t)nl) return OAPB_ERR_ARG;
+    for (double v : am.re) {
+      if (!(v >= OAPB_ACT_LINEAR && v <= OAPB_ACT_SIN) || v != (double)(int)v) return OAPB_ERR_ARG;
+      acts.push_back((int32_t)v);
+    }
+  }
   oapb_mlp* h = nullptr;
   if ((rc = oapb_mlp_create(&h, sizes.data(), (uint32_t)nl, seed))) return rc;
+  if (!acts.empty()) oapb_mlp_set_activations(h, acts.data(), (uint32_t)nl);
   std::vector<float> p((size_t)h->nparam);
   for (int l = 0; l < nl; ++l) {
     for (size_t e = 0; e < Ws[l].re.size(); ++e) p[h->woff[l] + e] = (float)Ws[l].re[e];

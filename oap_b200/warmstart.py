@@ -95,12 +95,25 @@ def make_targets(fam, theta, wanted=8, nshift=8, chunk=256, hdim=32, tol=1e-10, 
 class Net:
     """oapb_mlp over the C ABI."""
 
-    def __init__(self, sizes, seed=1):
+    def __init__(self, sizes, seed=1, acts=None):
+        """acts: one oapb_activation per layer (len(sizes) - 1), default tanh
+        hidden layers and a linear output."""
         self.sizes = list(sizes)
         self.h = C.c_void_p()
         arr = (C.c_uint32 * len(sizes))(*sizes)
         check(lib().oapb_mlp_create(C.byref(self.h), arr, len(sizes) - 1, seed), "oapb_mlp_create")
         self.nparam = int(lib().oapb_mlp_num_params(self.h))
+        if acts is not None:
+            self.set_activations(acts)
+
+    def set_activations(self, acts):
+        arr = (C.c_int32 * len(acts))(*[int(a) for a in acts])
+        check(lib().oapb_mlp_set_activations(self.h, arr, len(acts)), "oapb_mlp_set_activations")
+
+    def activations(self):
+        arr = (C.c_int32 * (len(self.sizes) - 1))()
+        check(lib().oapb_mlp_get_activations(self.h, arr, len(self.sizes) - 1), "oapb_mlp_get_activations")
+        return list(arr)
 
     def close(self):
         if self.h:

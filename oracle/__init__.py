@@ -216,6 +216,43 @@ def iram_planes(are, aim, k, m, which="LM", tol=1e-10, maxit=300, rho=1.0 / 3.14
             "converged": bool(stats[2]), "dgks": stats[3], "rc": rc}
 
 
+def iram_reference(a, k, m, which="LM", maxit=300, rho=1.0 / 3.14, blimit=1e-5, v0=None, seed=0):
+    """The reference's CuHArnoldi::execute restated as written, for a real
+    operator (see oracle.c: orc_iram_reference): V^T projections over all m
+    basis columns, the 1e-3 triangular gate of the unshifted QR, the
+    reference's shift accumulation and residual-update indices, CHECK_INTERNAL
+    stopping, Krylov-column eigenvectors.
+
+    Returns dict(eigenvalues, vectors (k x n), residuals, restarts, matvecs,
+    stopped (1: CHECK_INTERNAL ended it, 0: maxit), triangular_steps, rc)."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    if v0 is None:
+        v0 = np.random.default_rng(seed).uniform(-1.0, 1.0, n)
+    v0 = np.ascontiguousarray(v0, dtype=np.float64)
+    evr, evi = np.zeros(k), np.zeros(k)
+    x = np.zeros(k * n)
+    res = np.zeros(k)
+    stats = (C.c_int * 4)()
+    rc = lib().orc_iram_reference(n, _p(a), m, k, WHICH[which], maxit, C.c_double(rho), C.c_double(blimit),
+                                  _p(v0), _p(evr), _p(evi), _p(x), _p(res), stats)
+    return {"eigenvalues": evr + 1j * evi, "vectors": x.reshape(k, n), "residuals": res,
+            "restarts": stats[0], "matvecs": stats[1], "stopped": stats[2], "triangular_steps": stats[3],
+            "rc": rc}
+
+
+def qr_givens_reference(a):
+    """The reference's Givens QR as the reference-faithful IRAM restates it
+    (oracle.c: orc_qrgr_ref): rotations only where the input entry is
+    outside (-1e-5, 1e-5), r = sqrtf(c^2 + s^2), the output buffers as the
+    reference's pointer ping-pong leaves them."""
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    n = a.shape[0]
+    q, r = np.zeros((n, n)), np.zeros((n, n))
+    lib().orc_qrgr_ref(_p(a), _p(q), _p(r), n)
+    return q, r
+
+
 def match_eigenvalues(ev, ref):
     """Largest |ev_i - ref_j| / max|ref| over a one-to-one matching of two
     eigenvalue lists (each value of `ev` to the nearest unused one of `ref`,

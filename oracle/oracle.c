@@ -721,3 +721,328 @@ int orc_num_threads(void) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* Reference-faithful IRAM (real operators)                                 */
+/* ------------------------------------------------------------------------ */
+/*
+ * CuHArnoldi::execute as the reference writes it, for documenting how far
+ * its results are from the textbook solve above.  Real operators only: the
+ * reference's complex path scales only the real plane in v = f / B
+ * (CuMultiplicationProcedures.h:28-40) and adds wrongly past one block
+ * (CuAdditionProcedures.h:33-53), so it has no self-consistent complex
+ * result to restate.  Restated, step for step:
+ *   - begin / executeInit (ArnoldiProcedures.cpp:143-180,
+ *     oapGenericArnoldiApi.h:61-71): v = v0 / |v0|; w = A v; V[:,0] = v;
+ *     h = V^T w over ALL m columns of V; f = w - V h; H[0][0] = h[0];
+ *   - executeArnoldiFactorization (ArnoldiProcedures.cpp:407-461) for
+ *     fa = start .. m-2: B = |f| (or the previous |f| when no DGKS pass ran);
+ *     stop when |B| < blimit (1e-5, :39); v = f / B; V[:,fa+1] = v; row
+ *     fa+1 of H zeroed and H[fa+1][fa] = B; w = A v; h = V^T w over all m
+ *     columns (including stale ones); f = w - V h; DGKS when
+ *     |f| < rho |h| (|h| over all m entries): s = V^T f, f -= V s, h += s;
+ *     H[0..fa+1][fa+1] = h[0..fa+1];
+ *   - calculateTriangularHEigens (ArnoldiProcedures.cpp:333-349,
+ *     oapGenericArnoldiApi.h:268-296): unshifted QR iteration T <- R Q
+ *     with the reference's Givens QR until every first-subdiagonal entry
+ *     is within 1e-3 (CuIsUpperTriangularProcedures.h:29-89) or 600 steps;
+ *     Ritz values = diag(T), sorted (std::sort by the ArnUtils order,
+ *     ArnoldiUtils.cpp:24-50), wanted = the first k;
+ *   - executeShiftedQRIteration (ArnoldiProcedures.cpp:509-519,
+ *     oapGenericArnoldiApi.h:186-222): for each of the p = m - k unwanted
+ *     values mu in sort order: (Q1, R) = QRGR(H - mu I); H <- Q1^T H Q1;
+ *     the product Q1 ... accumulates through two buffers whose pointers
+ *     swap every shift, and the member Q receives the full product only for
+ *     odd p (for even p it holds the product of the first p - 1 shifts);
+ *     V <- V Q over all m columns;
+ *   - iram_fVplusfq (oapGenericArnoldiApi.h:73-102): f = V[:,k] H[k+1][k]
+ *     + f Q[m-1][k], FValue = |f|;
+ *   - the triangular form of the shifted H, its sorted diagonal the
+ *     reported eigenvalues; executeChecking CHECK_INTERNAL (:470-507):
+ *     continue while FValue < the previous FValue (initially 200000, :47);
+ *     the next factorization starts at k - 1 (:210);
+ *   - extractOutput (:225-277): eigenvalue q = the q-th sorted diagonal
+ *     entry; eigenvector q = column index(q) of V (a Krylov basis column,
+ *     not a Ritz vector).
+ * The reference's Givens QR (CuQRProcedures_GR.h:80-150) rotates rows
+ * (fa, fb), fb from the bottom up, only where the INPUT entry A[fb][fa] is
+ * outside (-1e-5, 1e-5); r = sqrtf(c^2 + s^2) in single precision; R and Q
+ * ping-pong between the output and auxiliary buffers, so for an even number
+ * of rotations the outputs hold the factors after all rotations but the
+ * last (still Q R = A), and for none they keep their previous contents
+ * (restated as Q = I, R = A).
+ * `maxit` caps the restarts (the reference has no cap under
+ * CHECK_INTERNAL).  Outputs: k eigenvalues, k vectors (vector-contiguous),
+ * the reference's testOutcome residuals (absolute, see the end of the
+ * function), stats[4] = {restarts, matvecs,
+ * stopped by CHECK_INTERNAL (1) or by maxit (0), Schur QR steps of the
+ * last triangularization}.  Returns 0, or 3 on invalid arguments.
+ */
+#define RM(M, r, c, ld) (M)[(size_t)(r) * (ld) + (c)]
+
+/* Q R = A (n x n row-major) by the reference's Givens QR, see above. */
+static void qrgr_ref(const double* A, double* Q, double* R, double* Rw, double* Qw, double* G, int n) {
+  const double tol = 0.00001;
+  double *R1 = Rw, *Rc = R, *Q1 = Qw, *Qc = Q;
+  memcpy(R1, A, sizeof(double) * n * n);
+  int count = 0;
+  for (int fa = 0; fa < n; ++fa) {
+    for (int fb = n - 1; fb > fa; --fb) {
+      double v = RM(A, fb, fa, n);
+      if (-tol < v && v < tol) continue;
+      double c = RM(R1, fa, fa, n), s = RM(R1, fb, fa, n);
+      double r = (double)sqrtf((float)(c * c + s * s));
+      c = c / r;
+      s = s / r;
+      /* Rc = G R1 with G = I except G[fa][fa] = G[fb][fb] = c, G[fa][fb] = s, G[fb][fa] = -s */
+      memcpy(Rc, R1, sizeof(double) * n * n);
+      for (int j = 0; j < n; ++j) {
+        double x = RM(R1, fa, j, n), y = RM(R1, fb, j, n);
+        RM(Rc, fa, j, n) = c * x + s * y;
+        RM(Rc, fb, j, n) = -s * x + c * y;
+      }
+      if (count == 0) {
+        for (int i = 0; i < n * n; ++i) Qc[i] = 0;
+        for (int i = 0; i < n; ++i) RM(Qc, i, i, n) = 1;
+        RM(Qc, fa, fa, n) = c;
+        RM(Qc, fb, fb, n) = c;
+        RM(Qc, fa, fb, n) = -s;
+        RM(Qc, fb, fa, n) = s;
+      } else {
+        /* Qc = Q1 G^T: columns fa, fb */
+        memcpy(Qc, Q1, sizeof(double) * n * n);
+        for (int i = 0; i < n; ++i) {
+          double x = RM(Q1, i, fa, n), y = RM(Q1, i, fb, n);
+          RM(Qc, i, fa, n) = c * x + s * y;
+          RM(Qc, i, fb, n) = -s * x + c * y;
+        }
+      }
+      ++count;
+      double* t = R1; R1 = Rc; Rc = t;
+      t = Q1; Q1 = Qc; Qc = t;
+    }
+  }
+  (void)G;
+  if (count == 0) {
+    /* the reference leaves its outputs untouched; restated as Q = I, R = A */
+    for (int i = 0; i < n * n; ++i) Q[i] = 0;
+    for (int i = 0; i < n; ++i) RM(Q, i, i, n) = 1;
+    memcpy(R, A, sizeof(double) * n * n);
+  }
+  /* odd count: the latest factors are in the output buffers (R1 == R, Q1 ==
+   * Q); even count: the outputs hold the factors of count - 1 rotations */
+}
+
+static int is_upper_ref(const double* T, int n) {
+  for (int c = 0; c + 1 < n; ++c) {
+    double v = RM(T, c + 1, c, n);
+    if (!(-0.001 < v && v < 0.001)) return 0;
+  }
+  return 1;
+}
+
+static void matmul_rm(const double* A, const double* B, double* C_, int n) {
+  for (int i = 0; i < n; ++i)
+    for (int j = 0; j < n; ++j) {
+      double acc = 0;
+      for (int t = 0; t < n; ++t) acc += RM(A, i, t, n) * RM(B, t, j, n);
+      RM(C_, i, j, n) = acc;
+    }
+}
+
+/* unshifted QR iteration to the 1e-3 gate; returns the step count */
+static int triangular_ref(double* T, int n, double* Q, double* R, double* w1, double* w2, double* w3) {
+  int it = 0;
+  while (it < 600 && !is_upper_ref(T, n)) {
+    qrgr_ref(T, Q, R, w1, w2, w3, n);
+    matmul_rm(R, Q, T, n);
+    ++it;
+  }
+  return it;
+}
+
+typedef struct { double re, im; int idx; } ref_pair;
+static int g_ref_which;
+static int ref_pair_cmp(const void* a, const void* b) {
+  const ref_pair* x = a;
+  const ref_pair* y = b;
+  double kx = sort_key(x->re + I * x->im, g_ref_which), ky = sort_key(y->re + I * y->im, g_ref_which);
+  return kx < ky ? -1 : kx > ky ? 1 : 0;
+}
+
+static void sorted_diag(const double* T, int m, int which, ref_pair* out) {
+  for (int i = 0; i < m; ++i) { out[i].re = RM(T, i, i, m); out[i].im = 0; out[i].idx = i; }
+  g_ref_which = which;
+  qsort(out, m, sizeof(ref_pair), ref_pair_cmp);
+}
+
+static double rnorm(const double* x, int n) {
+  double s = 0;
+  for (int i = 0; i < n; ++i) s += x[i] * x[i];
+  return sqrt(s);
+}
+
+static void ref_matvec(const double* A, const double* x, double* y, int n) {
+#pragma omp parallel for schedule(static) if (n >= 512)
+  for (int r = 0; r < n; ++r) {
+    double acc = 0;
+    for (int c = 0; c < n; ++c) acc += A[(size_t)r * n + c] * x[c];
+    y[r] = acc;
+  }
+}
+
+/* h = V^T w over all m columns; vh = V h (V vector-contiguous, m x n) */
+static void ref_project(const double* V, int n, int m, const double* w, double* h, double* vh) {
+  for (int j = 0; j < m; ++j) {
+    double acc = 0;
+    for (int r = 0; r < n; ++r) acc += V[(size_t)j * n + r] * w[r];
+    h[j] = acc;
+  }
+  for (int r = 0; r < n; ++r) {
+    double acc = 0;
+    for (int j = 0; j < m; ++j) acc += V[(size_t)j * n + r] * h[j];
+    vh[r] = acc;
+  }
+}
+
+int orc_iram_reference(int n, const double* A, int m, int k, int which, int maxit, double rho,
+                       double blimit, const double* v0, double* evre, double* evim, double* vecs,
+                       double* resid, int* stats) {
+  if (n <= 0 || m > n || k <= 0 || k + 2 > m || !A || !v0) return 3;
+  const size_t mm = (size_t)m * m;
+  double* V = calloc((size_t)m * n, sizeof(double));
+  double* EV = calloc((size_t)m * n, sizeof(double));
+  double* f = calloc(n, sizeof(double));
+  double* v = calloc(n, sizeof(double));
+  double* w = calloc(n, sizeof(double));
+  double* vh = calloc(n, sizeof(double));
+  double* h = calloc(m, sizeof(double));
+  double* s = calloc(m, sizeof(double));
+  double* H = calloc(mm, sizeof(double));
+  double* T = calloc(mm, sizeof(double));
+  double* Qa = calloc(mm, sizeof(double));  /* member Q (output of the shifts) */
+  double* Qb = calloc(mm, sizeof(double));  /* auxiliary QJ */
+  double* Q1 = calloc(mm, sizeof(double));
+  double* R = calloc(mm, sizeof(double));
+  double* HI = calloc(mm, sizeof(double));
+  double* W1 = calloc(mm, sizeof(double));
+  double* W2 = calloc(mm, sizeof(double));
+  double* W3 = calloc(mm, sizeof(double));
+  ref_pair* pairs = calloc(m, sizeof(ref_pair));
+  int matvecs = 0, restarts = 0, stopped = 0, tri_steps = 0;
+
+  /* begin: v = v0 / |v0| (initVvector_rand), executeInit */
+  double nv = rnorm(v0, n);
+  for (int r = 0; r < n; ++r) v[r] = v0[r] / nv;
+  ref_matvec(A, v, w, n);
+  ++matvecs;
+  memcpy(V, v, sizeof(double) * n);
+  ref_project(V, n, m, w, h, vh);
+  for (int r = 0; r < n; ++r) f[r] = w[r] - vh[r];
+  RM(H, 0, 0, m) = h[0];
+  double prevF = 200000.0, FValue = 0;
+  int start = 0;
+  for (int step = 0;; ++step) {
+    /* executeArnoldiFactorization */
+    double mf = 0;
+    int recalc = 1;
+    for (int fa = start; fa < m - 1; ++fa) {
+      double B = recalc ? rnorm(f, n) : mf;
+      FValue = B;
+      if (fabs(B) < blimit) break;
+      double rB = 1.0 / B;
+      for (int r = 0; r < n; ++r) v[r] = f[r] * rB;
+      memcpy(V + (size_t)(fa + 1) * n, v, sizeof(double) * n);
+      for (int c = 0; c < m; ++c) RM(H, fa + 1, c, m) = 0;
+      RM(H, fa + 1, fa, m) = B;
+      ref_matvec(A, v, w, n);
+      ++matvecs;
+      ref_project(V, n, m, w, h, vh);
+      for (int r = 0; r < n; ++r) f[r] = w[r] - vh[r];
+      mf = rnorm(f, n);
+      double mh = rnorm(h, m);
+      recalc = mf < rho * mh;
+      if (recalc) {
+        ref_project(V, n, m, f, s, vh);
+        for (int r = 0; r < n; ++r) f[r] -= vh[r];
+        for (int j = 0; j < m; ++j) h[j] += s[j];
+      }
+      for (int r = 0; r <= fa + 1; ++r) RM(H, r, fa + 1, m) = h[r];
+    }
+    /* Ritz values of H, wanted / unwanted */
+    memcpy(T, H, sizeof(double) * mm);
+    triangular_ref(T, m, W1, R, W2, W3, HI);
+    sorted_diag(T, m, which, pairs);
+    /* p = m - k exact shifts with the unwanted values */
+    for (int i = 0; i < (int)mm; ++i) { Qa[i] = 0; Qb[i] = 0; }
+    for (int i = 0; i < m; ++i) { RM(Qa, i, i, m) = 1; RM(Qb, i, i, m) = 1; }
+    double *ioQ = Qa, *auxQJ = Qb;
+    for (int q = k; q < m; ++q) {
+      memcpy(HI, H, sizeof(double) * mm);
+      for (int i = 0; i < m; ++i) RM(HI, i, i, m) -= pairs[q].re;
+      qrgr_ref(HI, Q1, R, W1, W2, W3, m);
+      matmul_rm(H, Q1, W1, m);          /* HO = H Q1 */
+      for (int i = 0; i < m; ++i)       /* H = Q1^T HO */
+        for (int j = 0; j < m; ++j) {
+          double acc = 0;
+          for (int t = 0; t < m; ++t) acc += RM(Q1, t, i, m) * RM(W1, t, j, m);
+          RM(H, i, j, m) = acc;
+        }
+      matmul_rm(auxQJ, Q1, ioQ, m);     /* io.Q = QJ Q1 */
+      double* t = ioQ; ioQ = auxQJ; auxQJ = t;
+    }
+    /* the member Q is buffer Qa whatever the parity (see above) */
+    /* V <- V Q over all m columns */
+    memcpy(EV, V, sizeof(double) * m * n);
+    for (int r = 0; r < n; ++r)
+      for (int j = 0; j < m; ++j) {
+        double acc = 0;
+        for (int t = 0; t < m; ++t) acc += EV[(size_t)t * n + r] * RM(Qa, t, j, m);
+        V[(size_t)j * n + r] = acc;
+      }
+    /* iram_fVplusfq with the reference's indices */
+    double qmk = RM(Qa, m - 1, k, m), bmk = RM(H, k + 1, k, m);
+    for (int r = 0; r < n; ++r) f[r] = V[(size_t)k * n + r] * bmk + f[r] * qmk;
+    FValue = rnorm(f, n);
+    /* eigenvalues of the shifted H; CHECK_INTERNAL */
+    memcpy(T, H, sizeof(double) * mm);
+    tri_steps = triangular_ref(T, m, W1, R, W2, W3, HI);
+    sorted_diag(T, m, which, pairs);
+    ++restarts;
+    if (!(FValue < prevF)) { stopped = 1; break; }
+    prevF = FValue;
+    if (restarts >= maxit) break;
+    start = k - 1;
+  }
+  /* outputs: sorted diagonal values; eigenvector q = column index(q) of V
+   * (extractOutput with HOST output, :225-250); residual q = testOutcome
+   * (:521-542, :642-649): ||A x - Re(l) x|| (absolute) for x = column
+   * index(q) of EV, the basis before the last V <- V Q */
+  for (int q = 0; q < k; ++q) {
+    if (evre) evre[q] = pairs[q].re;
+    if (evim) evim[q] = pairs[q].im;
+    if (vecs) memcpy(vecs + (size_t)q * n, V + (size_t)pairs[q].idx * n, sizeof(double) * n);
+    if (resid) {
+      const double* x = EV + (size_t)pairs[q].idx * n;
+      ref_matvec(A, x, w, n);
+      for (int r = 0; r < n; ++r) w[r] -= pairs[q].re * x[r];
+      resid[q] = rnorm(w, n);
+    }
+  }
+  if (stats) { stats[0] = restarts; stats[1] = matvecs; stats[2] = stopped; stats[3] = tri_steps; }
+  free(V); free(EV); free(f); free(v); free(w); free(vh); free(h); free(s); free(H); free(T);
+  free(Qa); free(Qb); free(Q1); free(R); free(HI); free(W1); free(W2); free(W3); free(pairs);
+  return 0;
+}
+
+/* The reference's Givens QR as restated for the reference-faithful IRAM
+ * (real, row-major n x n): single-precision rotation norm, rotations where
+ * the input entry is outside (-1e-5, 1e-5), buffer ping-pong. */
+void orc_qrgr_ref(const double* A, double* Q, double* R, int n) {
+  size_t nn = (size_t)n * n;
+  double* w1 = malloc(nn * sizeof(double));
+  double* w2 = malloc(nn * sizeof(double));
+  qrgr_ref(A, Q, R, w1, w2, NULL, n);
+  free(w1);
+  free(w2);
+}

@@ -46,16 +46,27 @@ static int cpu_tests() {
     threw = e.status() == OAPB_ERR_ARG;
   }
   EXPECT(threw);
-  // Network: only tanh hidden layers and a linear output exist
+  // Network: the reference's four activations are accepted, anything else
+  // (and an empty layer) is an argument error
   oapb::Network net;
   net.createLayer(4);
+  net.createLayer(8, oapb::Activation::SIGMOID);
+  net.createLayer(8, oapb::Activation::SIN);
   threw = false;
   try {
-    net.createLayer(8, oapb::Activation::SIGMOID);
+    net.createLayer(8, static_cast<oapb::Activation>(7));
   } catch (const oapb::Error& e) {
     threw = e.status() == OAPB_ERR_ARG;
   }
   EXPECT(threw);
+  threw = false;
+  try {
+    net.createLayer(0, oapb::Activation::TANH);
+  } catch (const oapb::Error& e) {
+    threw = e.status() == OAPB_ERR_ARG;
+  }
+  EXPECT(threw);
+  EXPECT(net.getLayersCount() == 3);
   return failures;
 }
 

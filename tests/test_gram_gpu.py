@@ -32,9 +32,16 @@ def check_gram(rows, cols, seed, fp64=True):
         assert torch.equal(A64, A.double())
 
 
-@pytest.mark.parametrize("rows,cols", [(256, 256), (128, 64), (300, 1000), (512, 4096)])
+@pytest.mark.parametrize("rows,cols", [(256, 256), (128, 64), (300, 1000), (512, 4096), (1, 5), (129, 31)])
 def test_gram_tensor_cores(rows, cols):
     check_gram(rows, cols, seed=rows + cols)
+
+
+@pytest.mark.parametrize("rows,cols", [(3000, 1000), (4096, 160)])
+def test_gram_stream_k_split_tiles(rows, cols):
+    # more upper-triangle tiles than SMs (156 and 272): the stream-K shares
+    # split tiles between two CTAs, whose partials the finishing kernel adds
+    check_gram(rows, cols, seed=7 * rows + cols)
 
 
 @pytest.mark.gpu

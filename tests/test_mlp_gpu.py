@@ -15,20 +15,26 @@ import oap_b200 as B  # noqa: E402
 from oap_b200 import warmstart as W  # noqa: E402
 
 
-def test_forward_and_gradients_match_oracle():
+@pytest.mark.parametrize("acts", [None, [M.SIGMOID, M.SIN, M.TANH], [M.SIN, M.TANH, M.SIGMOID],
+                                  [M.LINEAR, M.SIGMOID, M.SIN]])
+def test_forward_and_gradients_match_oracle(acts):
+    # every activation of the reference (LINEAR, SIGMOID, TANH, SIN) in hidden
+    # and output layers: forward output and all gradients against the oracle
     sizes = [16, 64, 48, 40]
-    net = W.Net(sizes, seed=3)
+    net = W.Net(sizes, seed=3, acts=acts)
+    if acts is not None:
+        assert net.activations() == acts
     rng = np.random.default_rng(1)
     x = rng.uniform(-1, 1, size=(24, 16)).astype(np.float32)
     t = rng.normal(size=(24, 40)).astype(np.float32)
     xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
     y = net.forward(xd).cpu().numpy()
     p = net.params()
-    hf, _ = M.forward(p, sizes, x)
+    hf, _ = M.forward(p, sizes, x, acts)
     assert np.abs(y - hf[-1]).max() <= 1e-3 * max(1.0, np.abs(hf[-1]).max())
     loss = net.backward(xd, td)
     g = net.grads()
-    lo, go = M.loss_and_grads(p, sizes, x, t)
+    lo, go = M.loss_and_grads(p, sizes, x, t, acts)
     assert abs(loss - lo) <= 1e-4 * lo
     rel = np.linalg.norm(g - go) / np.linalg.norm(go)
     assert rel < 1e-3, rel
@@ -110,3 +116,11 @@ def test_network_save_load_round_trip(tmp_path):
     assert back.sizes == [5, 16, 3]
     assert torch.equal(back.forward(x), y1)
     assert B.mat_read_info(p) == (1, 3, True, False)   # first record: the layer sizes
+    # the activations travel with the file (the last record)
+    net2 = W.Net([5, 16, 16, 3], seed=5, acts=[B.ACT_SIN, B.ACT_SIGMOID, B.ACT_TANH])
+    y2 = net2.forward(x)
+    p2 = tmp_path / "net2.bin"
+    net2.save(p2)
+    back2 = W.Net.load(p2)
+    assert back2.activations() == [B.ACT_SIN, B.ACT_SIGMOID, B.ACT_TANH]
+    assert torch.equal(back2.forward(x), y2)

@@ -33,3 +33,34 @@ def test_bf16_rounding():
     r = M.bf16(x)
     assert r[0] == 1.0 and r[1] == 1.0 and r[2] == np.float32(1.0078125)
     assert abs(r[3] - (-3.140625)) < 1e-6
+
+
+def test_activation_derivatives():
+    # the oracle's activation derivatives (the reference's dsigmoid / dtanh /
+    # dsin / dlinear) against central differences of the activations
+    z = np.linspace(-3, 3, 61)
+    for a in (M.LINEAR, M.SIGMOID, M.TANH, M.SIN):
+        h = M.act(z, a)
+        fd = (M.act(z + 1e-6, a) - M.act(z - 1e-6, a)) / 2e-6
+        assert np.allclose(M.act_grad(z, h, a), fd, atol=1e-8), a
+
+
+def test_oracle_gradient_with_activations_is_consistent():
+    # with every rounding point of the device removed (float64 parameters
+    # that are exact in BF16, no intermediate rounding effects checked), the
+    # output-layer weight gradient of a sigmoid output follows dL/dz = (y - t)
+    # sigmoid'(z) / B
+    rng = np.random.default_rng(3)
+    sizes = [3, 4, 2]
+    npar = 3 * 4 + 4 * 2 + 4 + 2
+    p = (rng.integers(-64, 65, size=npar) / 64.0).astype(np.float32)
+    x = (rng.integers(-64, 65, size=(5, 3)) / 64.0).astype(np.float32)
+    t = rng.normal(size=(5, 2))
+    acts = [M.SIN, M.SIGMOID]
+    loss, g = M.loss_and_grads(p, sizes, x, t, acts)
+    hf, hb, zs = M.forward(p, sizes, x, acts, with_z=True)
+    y = hf[-1].astype(np.float64)
+    dz = M.bf16(((y - t) / 5.0 * y * (1 - y)).astype(np.float32)).astype(np.float64)
+    gW = dz.T @ hb[1]
+    assert np.allclose(g[12:20].reshape(2, 4), gW, rtol=1e-5, atol=1e-7)
+    assert np.isclose(loss, 0.5 * np.sum((y - t) ** 2) / 5.0, rtol=1e-6)
