@@ -300,6 +300,27 @@ OAPB_EXPORT int oapb_arnoldi_set_callback(oapb_arnoldi* handle, oapb_matvec_fn f
 OAPB_EXPORT int oapb_arnoldi_set_gram_operator(oapb_arnoldi* handle, const float* X, uint32_t rows,
                                                uint32_t cols);
 
+/* The implicit Gram operator with X (rows = n samples x cols pixels, FP32,
+ * row-major) in HOST memory, for image sets larger than HBM, as the
+ * reference's application reads its images block by block
+ * (oap2dt3dDevice/MainAPExecutor.cpp:59-100, oapMatrixCuda/RecToSquareApi.cpp:
+ * 71-141): A v = sum_c X_c (X_c^T v) over column blocks X_c of block_cols
+ * pixels (rounded up to a multiple of 4), so one application reads X once.
+ * The first blocks that fit resident_bytes are copied to the device here and
+ * stay; the others are copied host-to-device on every application through
+ * two device buffers, the copy of the next block (on a second stream)
+ * overlapping the passes over the current one; pinned host memory gives the
+ * full copy rate.  X must stay valid while the operator is set.  Real solves,
+ * FP64 path, like oapb_arnoldi_set_gram_operator. */
+OAPB_EXPORT int oapb_arnoldi_set_gram_operator_host(oapb_arnoldi* handle, const float* X, uint32_t rows,
+                                                    uint32_t cols, uint32_t block_cols,
+                                                    uint64_t resident_bytes);
+/* Column blocks of the host-X Gram operator, how many stay resident, and the
+ * host-to-device bytes its applications streamed so far (outputs may be
+ * NULL; OAPB_ERR_ARG when no such operator is set). */
+OAPB_EXPORT int oapb_arnoldi_gram_stream_info(const oapb_arnoldi* handle, uint32_t* blocks,
+                                              uint32_t* resident_blocks, uint64_t* streamed_bytes);
+
 /* Start vector (device planes, n values each; im ignored for real solves). */
 OAPB_EXPORT int oapb_arnoldi_set_start_vector(oapb_arnoldi* handle, const double* re,
                                   const double* im);
@@ -466,6 +487,8 @@ typedef struct oapb_batch_stats {
   uint64_t restarts;
   uint32_t ctas;         /* resident CTAs of the persistent launch */
   double seconds;        /* host wall time of the call */
+  uint32_t variant;      /* launch variant (cfg.autotune: 1 tunes, 2 + v forces v) */
+  uint32_t threads;      /* threads per CTA of that variant */
 } oapb_batch_stats;
 
 /* Solve `count` independent eigenproblems (IEigenCalculator::calculate,
@@ -473,9 +496,13 @@ typedef struct oapb_batch_stats {
  * reference) with one persistent kernel: each CTA takes the next problem
  * from a queue ordered by decreasing n and runs the full restart loop on the
  * device.  cfg: hdim caps the Krylov dimension (m_i = min(n_i, hdim),
- * hdim <= 32), wanted, sort, tolerance, max_restarts, rho, seed; n,
- * is_complex, precision and init are ignored (complex iff im != NULL,
- * FP64, seeded random start).  `problems` is a HOST array.  Host outputs:
+ * hdim <= 32), wanted, sort, tolerance, max_restarts, rho, seed, autotune
+ * (0: the default launch variant, 256 threads per CTA; 1: the variant
+ * (threads per CTA x CTAs per SM the registers are budgeted for: 256 x 1,
+ * 128 x 2, 256 x 2, 128 x 4, 64 x 8) that ran fastest on a sample of the
+ * first batch of a given largest n, hdim, wanted and complexity, cached per
+ * device; 2 + v: variant v, 0..4); n, is_complex, precision and init are
+ * ignored (complex iff im != NULL, FP64, seeded random start).  `problems` is a HOST array.  Host outputs:
  * eig_re / eig_im / residuals (count x wanted, row i = problem i in sort
  * order), status (count, oapb_status per problem).  Synchronises `stream`.
  * Returns OAPB_OK when every problem converged, OAPB_NOT_CONVERGED when some

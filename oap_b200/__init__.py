@@ -76,7 +76,8 @@ class BatchProblem(C.Structure):
 class BatchStats(C.Structure):
     _fields_ = [("problems", C.c_uint32), ("converged", C.c_uint32),
                 ("matvecs", C.c_uint64), ("restarts", C.c_uint64),
-                ("ctas", C.c_uint32), ("seconds", C.c_double)]
+                ("ctas", C.c_uint32), ("seconds", C.c_double),
+                ("variant", C.c_uint32), ("threads", C.c_uint32)]
 
 
 MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,
@@ -116,6 +117,8 @@ def lib():
             "oapb_qr_householder": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_qr_givens_noalloc": [P(Mat), P(Mat), P(Mat), vp],
             "oapb_selftest_bounded_wait": [C.c_uint32, C.c_int32, P(C.c_int32), vp],
+            "oapb_arnoldi_set_gram_operator_host": [vp, vp, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint64],
+            "oapb_arnoldi_gram_stream_info": [vp, P(C.c_uint32), P(C.c_uint32), P(C.c_uint64)],
             "oapb_is_upper_triangular": [P(C.c_int), P(Mat), C.c_double, vp],
             "oapb_calc_triangular_h": [P(Mat), P(Mat), C.c_uint32, P(C.c_uint32), vp],
             "oapb_arnoldi_create": [P(vp), P(Config), vp],
@@ -300,6 +303,30 @@ class Arnoldi:
         check(lib().oapb_arnoldi_set_gram_operator(self.h, C.c_void_p(X.data_ptr()), X.shape[0], X.shape[1]),
               "oapb_arnoldi_set_gram_operator")
 
+    def set_gram_operator_host(self, X, block_cols, resident_bytes=0):
+        """Implicit Gram operator A = X X^T with X (n, pixels) FP32 in HOST
+        memory (a C-contiguous numpy array or a pinned CPU tensor), applied by
+        column blocks of block_cols pixels; the blocks that fit resident_bytes
+        stay on the device, the rest stream on every application."""
+        import numpy as np
+        if hasattr(X, "data_ptr"):
+            assert X.dtype.is_floating_point and X.element_size() == 4 and X.is_contiguous() and not X.is_cuda
+            ptr, rows, cols = X.data_ptr(), X.shape[0], X.shape[1]
+        else:
+            assert X.dtype == np.float32 and X.flags.c_contiguous
+            ptr, rows, cols = X.ctypes.data, X.shape[0], X.shape[1]
+        self._ops = (X,)
+        check(lib().oapb_arnoldi_set_gram_operator_host(self.h, C.c_void_p(ptr), rows, cols, block_cols,
+                                                        int(resident_bytes)),
+              "oapb_arnoldi_set_gram_operator_host")
+
+    def gram_stream_info(self):
+        """(blocks, resident blocks, host-to-device bytes streamed so far)."""
+        nb, nr, by = C.c_uint32(), C.c_uint32(), C.c_uint64()
+        check(lib().oapb_arnoldi_gram_stream_info(self.h, C.byref(nb), C.byref(nr), C.byref(by)),
+              "oapb_arnoldi_gram_stream_info")
+        return nb.value, nr.value, by.value
+
     def save(self, path):
         check(lib().oapb_arnoldi_save(self.h, str(path).encode()), "oapb_arnoldi_save")
 
@@ -390,10 +417,11 @@ def start_vector(n, seed, is_complex=False):
 
 
 def solve_batched(mats, wanted, hdim=24, sort="LM", tolerance=1e-10, max_restarts=300,
-                  rho=1.0 / 3.14, seed=1, vectors=None, stream=None):
+                  rho=1.0 / 3.14, seed=1, vectors=None, stream=None, autotune=True):
     """Batched solve of independent problems.  mats: list of (re, im) device
     tensors (im None for real problems); vectors: optional list of (vre, vim)
-    device tensors of shape (n, wanted).  Returns (eigenvalues [count x
+    device tensors of shape (n, wanted); autotune: True (tune the launch
+    variant once per shape), False (default variant) or 2 + v (variant v).  Returns (eigenvalues [count x
     wanted] complex, residuals, status per problem, stats dict, rc)."""
     import numpy as np
     L = lib()
@@ -402,6 +430,7 @@ def solve_batched(mats, wanted, hdim=24, sort="LM", tolerance=1e-10, max_restart
     cfg.hdim, cfg.wanted = hdim, wanted
     cfg.sort = SORT[sort] if isinstance(sort, str) else int(sort)
     cfg.tolerance, cfg.max_restarts, cfg.rho, cfg.seed = tolerance, max_restarts, rho, seed
+    cfg.autotune = int(autotune)
     cnt = len(mats)
     probs = (BatchProblem * cnt)()
     for i, (re, im) in enumerate(mats):

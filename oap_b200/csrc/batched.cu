@@ -18,6 +18,9 @@
 // slot owned by the CTA (L2-resident).
 #include <algorithm>
 #include <chrono>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -25,8 +28,14 @@
 
 namespace oapb {
 
-constexpr int kBtThreads = 256;
-constexpr int kBtWarps = kBtThreads / 32;
+// launch variants (oapb_batch_stats.variant; the autotuner picks one per
+// (device, largest n, hdim, wanted, complex)): threads per CTA and the
+// resident CTAs per SM the register budget is compiled for (more CTAs per SM
+// keep more problems in flight; fewer registers per thread move the
+// restart's small arrays to local memory)
+constexpr int kBtVariants = 5;
+constexpr int kBtThreadsOf[kBtVariants] = {256, 128, 256, 128, 64};
+constexpr int kBtMinBlocksOf[kBtVariants] = {1, 2, 2, 4, 8};
 constexpr int kBtMaxM = 32;
 constexpr int kBtMaxN = 2048;
 
@@ -111,7 +120,8 @@ __device__ BatchSmem carve(char* base, int nmax, int m) {
   return S;
 }
 
-// Sum of (a, b) over the CTA; every thread gets the result.
+// Sum of (a, b) over the CTA of NT threads; every thread gets the result.
+template <int NT>
 __device__ __forceinline__ cplx cta_sum2(double a, double b, double* red) {
   a = warp_sum(a);
   b = warp_sum(b);
@@ -124,7 +134,7 @@ __device__ __forceinline__ cplx cta_sum2(double a, double b, double* red) {
   __syncthreads();
   double ra = 0, rb = 0;
 #pragma unroll
-  for (int i = 0; i < kBtWarps; ++i) {
+  for (int i = 0; i < NT / 32; ++i) {
     ra += red[i];
     rb += red[32 + i];
   }
@@ -132,11 +142,11 @@ __device__ __forceinline__ cplx cta_sum2(double a, double b, double* red) {
 }
 
 // w = A x  (A row-major n x n; warps over rows, lanes over columns)
-template <bool C>
+template <bool C, int NT>
 __device__ void cta_matvec(const double* __restrict__ Are, const double* __restrict__ Aim, int n, const double* xr,
                            const double* xi, double* wr, double* wi) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  for (int r0 = 2 * w; r0 < n; r0 += 2 * kBtWarps) {
+  for (int r0 = 2 * w; r0 < n; r0 += 2 * (NT / 32)) {
     double sr[2] = {0, 0}, si[2] = {0, 0};
     const int nr = (r0 + 1 < n) ? 2 : 1;
 #pragma unroll 4
@@ -170,11 +180,11 @@ __device__ void cta_matvec(const double* __restrict__ Are, const double* __restr
 }
 
 // coef[i] = sum_r conj(V_i[r]) src[r], i < nvec (warps over vectors)
-template <bool C>
+template <bool C, int NT>
 __device__ void cta_project(const double* Vr, const double* Vi, int n, int nvec, const double* srcr,
                             const double* srci, cplx* coef) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  for (int i = w; i < nvec; i += kBtWarps) {
+  for (int i = w; i < nvec; i += NT / 32) {
     const double* vr = Vr + (long)i * n;
     const double* vi = C ? Vi + (long)i * n : nullptr;
     double a = 0, b = 0;
@@ -195,11 +205,11 @@ __device__ void cta_project(const double* Vr, const double* Vi, int n, int nvec,
 }
 
 // dst = src - V coef; returns ||dst||^2 (CTA-wide)
-template <bool C>
+template <bool C, int NT>
 __device__ double cta_update(const double* Vr, const double* Vi, int n, int nvec, const cplx* coef,
                              const double* srcr, const double* srci, double* dstr, double* dsti, double* red) {
   double s2 = 0;
-  for (int r = threadIdx.x; r < n; r += kBtThreads) {
+  for (int r = threadIdx.x; r < n; r += NT) {
     double a = srcr[r], b = C ? srci[r] : 0.0;
     for (int i = 0; i < nvec; ++i) {
       const double p = Vr[(long)i * n + r];
@@ -215,10 +225,10 @@ __device__ double cta_update(const double* Vr, const double* Vi, int n, int nvec
     if (C) dsti[r] = b;
     s2 += a * a + b * b;
   }
-  return cta_sum2(s2, 0.0, red).re;
+  return cta_sum2<NT>(s2, 0.0, red).re;
 }
 
-template <bool C>
+template <bool C, int NT>
 __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, const BatchSmem& S) {
   const int n = P.n;
   const int m = n < A.mcap ? n : A.mcap;
@@ -233,13 +243,13 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
 
   // start vector
   double s2 = 0;
-  for (int r = tid; r < n; r += kBtThreads) {
+  for (int r = tid; r < n; r += NT) {
     S.fr[r] = uniform_pm1(pseed, r);
     if (C) S.fi[r] = uniform_pm1(pseed ^ 0x5851F42D4C957F2Dull, r);
     s2 += S.fr[r] * S.fr[r] + (C ? S.fi[r] * S.fi[r] : 0.0);
   }
-  double fnorm2 = cta_sum2(s2, 0, S.red).re, hnorm2 = 0;
-  for (int e = tid; e < m * m; e += kBtThreads) S.H[e] = cplx{0, 0};
+  double fnorm2 = cta_sum2<NT>(s2, 0, S.red).re, hnorm2 = 0;
+  for (int e = tid; e < m * m; e += NT) S.H[e] = cplx{0, 0};
   if (tid == 0) {
     S.st->status = 0;
     S.st->converged = 0;
@@ -253,22 +263,22 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
       if (j > 0 && fnorm2 <= 1e-24 * (hnorm2 + fnorm2)) {
         brk = true;
         const uint64_t bs = pseed ^ (0xBF58476D1CE4E5B9ull * (uint64_t)(rs * 64 + j + 1));
-        for (int r = tid; r < n; r += kBtThreads) {
+        for (int r = tid; r < n; r += NT) {
           S.fr[r] = uniform_pm1(bs, r);
           if (C) S.fi[r] = uniform_pm1(bs ^ 0x5851F42D4C957F2Dull, r);
         }
         __syncthreads();
         for (int sweep = 0; sweep < 2; ++sweep) {
-          cta_project<C>(Vr, Vi, n, j, S.fr, S.fi, S.s);
+          cta_project<C, NT>(Vr, Vi, n, j, S.fr, S.fi, S.s);
           __syncthreads();
-          fnorm2 = cta_update<C>(Vr, Vi, n, j, S.s, S.fr, S.fi, S.fr, S.fi, S.red);
+          fnorm2 = cta_update<C, NT>(Vr, Vi, n, j, S.s, S.fr, S.fi, S.fr, S.fi, S.red);
         }
       }
       const double beta = sqrt(fnorm2);
       const double inv = beta > 0 ? 1.0 / beta : 0.0;
       double* vj = Vr + (long)j * n;
       double* vji = Vi + (long)j * n;
-      for (int r = tid; r < n; r += kBtThreads) {
+      for (int r = tid; r < n; r += NT) {
         const double a = S.fr[r] * inv;
         S.xr[r] = a;
         vj[r] = a;
@@ -280,23 +290,23 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
       }
       if (tid == 0 && j > 0) S.H[j + (j - 1) * m] = cplx{brk ? 0.0 : beta, 0};
       __syncthreads();
-      cta_matvec<C>(P.re, P.im, n, S.xr, S.xi, S.wr, S.wi);
+      cta_matvec<C, NT>(P.re, P.im, n, S.xr, S.xi, S.wr, S.wi);
       ++matvecs;
       __syncthreads();
-      cta_project<C>(Vr, Vi, n, j + 1, S.wr, S.wi, S.h);
+      cta_project<C, NT>(Vr, Vi, n, j + 1, S.wr, S.wi, S.h);
       __syncthreads();
-      fnorm2 = cta_update<C>(Vr, Vi, n, j + 1, S.h, S.wr, S.wi, S.fr, S.fi, S.red);
+      fnorm2 = cta_update<C, NT>(Vr, Vi, n, j + 1, S.h, S.wr, S.wi, S.fr, S.fi, S.red);
       double h2 = 0;
       for (int i = 0; i <= j; ++i) h2 += abs2(S.h[i]);
       hnorm2 = h2;
       if (sqrt(fnorm2) < A.rho * sqrt(hnorm2)) {  // DGKS (ArnoldiProcedures.cpp:446-456)
-        cta_project<C>(Vr, Vi, n, j + 1, S.fr, S.fi, S.s);
+        cta_project<C, NT>(Vr, Vi, n, j + 1, S.fr, S.fi, S.s);
         __syncthreads();
-        fnorm2 = cta_update<C>(Vr, Vi, n, j + 1, S.s, S.fr, S.fi, S.fr, S.fi, S.red);
+        fnorm2 = cta_update<C, NT>(Vr, Vi, n, j + 1, S.s, S.fr, S.fi, S.fr, S.fi, S.red);
         if (tid <= j) S.h[tid] = S.h[tid] + S.s[tid];
         __syncthreads();
       }
-      for (int i = tid; i < m; i += kBtThreads) {
+      for (int i = tid; i < m; i += NT) {
         cplx v = i <= j ? S.h[i] : cplx{0, 0};
         if (!C) v.im = 0;
         S.H[i + j * m] = v;
@@ -343,7 +353,7 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
       break;
     }
     // V[0..k] <- V Q[:, 0..k] in place (each thread owns whole rows r)
-    for (int r = tid; r < n; r += kBtThreads) {
+    for (int r = tid; r < n; r += NT) {
       cplx out[kBtMaxM + 1];
       for (int q = 0; q <= k; ++q) out[q] = cplx{0, 0};
       for (int i = 0; i < m; ++i) {
@@ -361,8 +371,8 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
       if (C) S.fi[r] = nf.im;
     }
     double a2 = 0;
-    for (int r = tid; r < n; r += kBtThreads) a2 += S.fr[r] * S.fr[r] + (C ? S.fi[r] * S.fi[r] : 0.0);
-    fnorm2 = cta_sum2(a2, 0, S.red).re;
+    for (int r = tid; r < n; r += NT) a2 += S.fr[r] * S.fr[r] + (C ? S.fi[r] * S.fi[r] : 0.0);
+    fnorm2 = cta_sum2<NT>(a2, 0, S.red).re;
     ++restarts;
     start = k;
   }
@@ -371,7 +381,7 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
   for (int q = 0; q < k; ++q) scale = fmax(scale, cabs_(S.ritz[q]));
   if (scale == 0) scale = 1;
   if (status == OAPB_OK || status == OAPB_NOT_CONVERGED) {
-    for (int r = tid; r < n; r += kBtThreads) {
+    for (int r = tid; r < n; r += NT) {
       cplx out[kBtMaxM];
       for (int q = 0; q < k; ++q) out[q] = cplx{0, 0};
       for (int i = 0; i < m; ++i) {
@@ -388,17 +398,17 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
     for (int q = 0; q < k; ++q) {
       const double* xr = Vr + (long)q * n;
       const double* xi = Vi + (long)q * n;
-      for (int r = tid; r < n; r += kBtThreads) {
+      for (int r = tid; r < n; r += NT) {
         S.xr[r] = xr[r];
         if (C) S.xi[r] = xi[r];
       }
       __syncthreads();
-      cta_matvec<C>(P.re, P.im, n, S.xr, S.xi, S.wr, S.wi);
+      cta_matvec<C, NT>(P.re, P.im, n, S.xr, S.xi, S.wr, S.wi);
       ++matvecs;
       __syncthreads();
       const cplx lam = S.ritz[q];
       double e2 = 0, x2 = 0;
-      for (int r = tid; r < n; r += kBtThreads) {
+      for (int r = tid; r < n; r += NT) {
         const cplx x = {S.xr[r], C ? S.xi[r] : 0.0};
         const cplx w = cplx{S.wr[r], C ? S.wi[r] : 0.0} - lam * x;
         e2 += abs2(w);
@@ -406,7 +416,7 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
         if (P.vre) P.vre[(long)r * k + q] = x.re;
         if (P.vim) P.vim[(long)r * k + q] = x.im;
       }
-      const cplx sums = cta_sum2(e2, x2, S.red);
+      const cplx sums = cta_sum2<NT>(e2, x2, S.red);
       const double rr = sqrt(sums.re) / (scale * (sums.im > 0 ? sqrt(sums.im) : 1.0));
       if (tid == 0) {
         A.ev_re[(long)P.index * k + q] = lam.re;
@@ -425,7 +435,8 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBtThreads) k_batched_iram(BatchArgs A) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_batched_iram(BatchArgs A) {
   extern __shared__ __align__(16) char bsm[];
   __shared__ int next;
   const int mcap = A.mcap;
@@ -443,10 +454,100 @@ __global__ void __launch_bounds__(kBtThreads) k_batched_iram(BatchArgs A) {
     }
     // per-problem hdim: the carve uses mcap; hess_core indexes with m = min(n, mcap)
     if (P.im)
-      solve_one<true>(A, P, blockIdx.x, S);
+      solve_one<true, NT>(A, P, blockIdx.x, S);
     else
-      solve_one<false>(A, P, blockIdx.x, S);
+      solve_one<false, NT>(A, P, blockIdx.x, S);
   }
+}
+
+const void* batched_kernel(int v) {
+  switch (v) {
+    case 1: return (const void*)k_batched_iram<128, 2>;
+    case 2: return (const void*)k_batched_iram<256, 2>;
+    case 3: return (const void*)k_batched_iram<128, 4>;
+    case 4: return (const void*)k_batched_iram<64, 8>;
+    default: return (const void*)k_batched_iram<256, 1>;
+  }
+}
+
+cudaError_t launch_batched(int v, int grid, size_t smem, cudaStream_t s, const BatchArgs& A) {
+  switch (v) {
+    case 1: k_batched_iram<128, 2><<<grid, 128, smem, s>>>(A); break;
+    case 2: k_batched_iram<256, 2><<<grid, 256, smem, s>>>(A); break;
+    case 3: k_batched_iram<128, 4><<<grid, 128, smem, s>>>(A); break;
+    case 4: k_batched_iram<64, 8><<<grid, 64, smem, s>>>(A); break;
+    default: k_batched_iram<256, 1><<<grid, 256, smem, s>>>(A); break;
+  }
+  return cudaGetLastError();
+}
+
+// The autotuner's choice per (device, largest n, hdim, wanted, complex):
+// the variant whose launch on a sample of the batch took the least device
+// time (replaces the fixed launch shapes of utils::mapper::SetThreadsBlocks,
+// oapUtils/ThreadsMapper.cpp:36-74).
+struct BatchKey {
+  int dev, nmax, mcap, k, cplx;
+  bool operator<(const BatchKey& o) const {
+    return std::tie(dev, nmax, mcap, k, cplx) < std::tie(o.dev, o.nmax, o.mcap, o.k, o.cplx);
+  }
+};
+std::mutex g_bt_mutex;
+std::map<BatchKey, int> g_bt_choice;
+
+bool tuned_variant(const BatchKey& key, int* v) {
+  std::lock_guard<std::mutex> lock(g_bt_mutex);
+  auto it = g_bt_choice.find(key);
+  if (it == g_bt_choice.end()) return false;
+  *v = it->second;
+  return true;
+}
+
+void remember_variant(const BatchKey& key, int v) {
+  std::lock_guard<std::mutex> lock(g_bt_mutex);
+  g_bt_choice[key] = v;
+}
+
+// Time every variant on an evenly strided sample of the size-sorted batch
+// (one wave of the default variant's grid) with CUDA events; the sample's
+// outputs land in the batch's output slots and are overwritten by the full
+// launch that follows.  dsample: device room for the sample's descriptors.
+int tune_batched(BatchArgs A, const std::vector<BatchDesc>& d, const int* grids, size_t smem, cudaStream_t s,
+                 char* dsample, int* best) {
+  const int count = (int)d.size();
+  const int ns = std::min(count, grids[0]);
+  std::vector<BatchDesc> sample(ns);
+  for (int i = 0; i < ns; ++i) sample[i] = d[(long)i * count / ns];
+  if (cudaMemcpyAsync(dsample, sample.data(), sizeof(BatchDesc) * ns, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return OAPB_ERR_CUDA;
+  A.desc = (const BatchDesc*)dsample;
+  A.count = ns;
+  cudaEvent_t e0, e1;
+  if (cudaEventCreate(&e0) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (cudaEventCreate(&e1) != cudaSuccess) {
+    cudaEventDestroy(e0);
+    return OAPB_ERR_CUDA;
+  }
+  int rc = OAPB_OK;
+  float best_ms = 0;
+  *best = 0;
+  for (int v = 0; v < kBtVariants && !rc; ++v) {
+    if (cudaMemsetAsync((void*)A.counter, 0, 4 * sizeof(unsigned long long), s) != cudaSuccess ||
+        cudaEventRecord(e0, s) != cudaSuccess ||
+        launch_batched(v, std::min(grids[v], ns), smem, s, A) != cudaSuccess ||
+        cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = OAPB_ERR_CUDA;
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (v == 0 || ms < best_ms) {
+      best_ms = ms;
+      *best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return rc;
 }
 
 }  // namespace oapb
@@ -461,15 +562,18 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
   if (!cfg || !problems || count == 0 || !eig_re || !eig_im || !residuals || !status) return OAPB_ERR_ARG;
   const int mcap = (int)cfg->hdim, k = (int)cfg->wanted;
   if (mcap < 2 || mcap > kBtMaxM || k < 1 || k >= mcap || cfg->sort < 0 || cfg->sort > 5) return OAPB_ERR_ARG;
+  if (cfg->autotune >= 2 && cfg->autotune >= 2 + kBtVariants) return OAPB_ERR_ARG;
   auto t0 = std::chrono::steady_clock::now();
   cudaStream_t s = (cudaStream_t)stream;
   std::vector<BatchDesc> d(count);
   int nmax = 0;
+  bool any_complex = false;
   for (uint32_t i = 0; i < count; ++i) {
     const oapb_batch_problem& p = problems[i];
     if (p.n < 2 || p.n > (uint32_t)kBtMaxN || !p.re || p.n <= (uint32_t)k) return OAPB_ERR_ARG;
     d[i] = BatchDesc{(int)p.n, (int)i, p.re, p.im, p.eigvec_re, p.eigvec_im};
     nmax = std::max(nmax, (int)p.n);
+    any_complex |= p.im != nullptr;
   }
   // largest first: the atomic queue then balances uneven sizes
   std::stable_sort(d.begin(), d.end(), [](const BatchDesc& a, const BatchDesc& b) { return a.n > b.n; });
@@ -479,17 +583,24 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 1024 > (size_t)optin) return OAPB_ERR_ARG;
-  OAPB_CUDA_TRY(cudaFuncSetAttribute(k_batched_iram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int occ = 0;
-  OAPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_batched_iram, kBtThreads, smem));
-  if (occ < 1) return OAPB_ERR_ARG;
-  int grid = kNumSMs * occ;
-  if (grid > (int)count) grid = (int)count;
+  // the persistent grid of every launch variant (resident CTAs x SMs)
+  int grids[kBtVariants];
+  int gmax = 0;
+  for (int v = 0; v < kBtVariants; ++v) {
+    const void* kern = batched_kernel(v);
+    OAPB_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    OAPB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kBtThreadsOf[v], smem));
+    grids[v] = std::min(kNumSMs * occ, (int)count);
+    gmax = std::max(gmax, grids[v]);
+  }
+  if (grids[0] < 1) return OAPB_ERR_ARG;
 
-  // one device allocation for descriptors, counters, outputs and the basis slots
-  const size_t vws = sizeof(double) * 2 * (size_t)(mcap + 1) * nmax * grid;
+  // one device allocation for descriptors (the batch, then a tuning sample),
+  // counters, outputs and the basis slots
+  const size_t vws = sizeof(double) * 2 * (size_t)(mcap + 1) * nmax * gmax;
   const size_t nout = (size_t)count * k;
-  size_t off_desc = 0, off_cnt = align16(off_desc + sizeof(BatchDesc) * count);
+  size_t off_desc = 0, off_cnt = align16(off_desc + sizeof(BatchDesc) * 2 * (size_t)count);
   size_t off_out = align16(off_cnt + 4 * sizeof(unsigned long long));
   size_t off_res = align16(off_out + 2 * sizeof(double) * nout);
   size_t off_st = align16(off_res + sizeof(double) * nout);
@@ -501,10 +612,10 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
     return OAPB_ERR_NOMEM;
   }
   int rc = OAPB_OK;
+  int variant = 0;
   do {
     if (cudaMemcpyAsync(buf + off_desc, d.data(), sizeof(BatchDesc) * count, cudaMemcpyHostToDevice, s) !=
-            cudaSuccess ||
-        cudaMemsetAsync(buf + off_cnt, 0, 4 * sizeof(unsigned long long), s) != cudaSuccess) {
+        cudaSuccess) {
       rc = OAPB_ERR_CUDA;
       break;
     }
@@ -527,8 +638,21 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
     A.ev_im = A.ev_re + nout;
     A.res = (double*)(buf + off_res);
     A.status = (int*)(buf + off_st);
-    k_batched_iram<<<grid, kBtThreads, smem, s>>>(A);
-    if (cudaGetLastError() != cudaSuccess) {
+    // launch variant: forced, cached, or timed on a sample of the batch
+    if (cfg->autotune >= 2) {
+      variant = cfg->autotune - 2;
+    } else if (cfg->autotune == 1) {
+      const BatchKey key{dev, nmax, mcap, k, any_complex ? 1 : 0};
+      if (!tuned_variant(key, &variant)) {
+        rc = tune_batched(A, d, grids, smem, s, buf + off_desc + sizeof(BatchDesc) * count, &variant);
+        if (rc) break;
+        remember_variant(key, variant);
+      }
+    }
+    A.count = (int)count;
+    A.desc = (const BatchDesc*)(buf + off_desc);
+    if (cudaMemsetAsync(buf + off_cnt, 0, 4 * sizeof(unsigned long long), s) != cudaSuccess ||
+        launch_batched(variant, grids[variant], smem, s, A) != cudaSuccess) {
       rc = OAPB_ERR_CUDA;
       break;
     }
@@ -548,8 +672,10 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
       for (uint32_t i = 0; i < count; ++i) stats->converged += status[i] == OAPB_OK;
       stats->matvecs = ctr[1];
       stats->restarts = ctr[2];
-      stats->ctas = (uint32_t)grid;
+      stats->ctas = (uint32_t)grids[variant];
       stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      stats->variant = (uint32_t)variant;
+      stats->threads = (uint32_t)kBtThreadsOf[variant];
     }
   } while (0);
   cudaFreeAsync(buf, s);

@@ -439,6 +439,7 @@ struct oapb_arnoldi {
   const float* gX = nullptr;
   int gcols = 0;
   double* gws = nullptr;
+  GramStream* gS = nullptr;  // the same operator with X in host memory (column blocks)
   // vectors
   double *Vre = nullptr, *Vim = nullptr;
   double *Xre = nullptr, *Xim = nullptr;   // Ritz vectors / restart scratch (m vectors)
@@ -578,6 +579,10 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
   if (a->gX) {
     a->stats.kernel_launches += 3;
     return launch_gram_apply(a->gX, n, a->gcols, xre, yre, a->gws, s);
+  }
+  if (a->gS) {
+    a->stats.kernel_launches += 3 * (uint64_t)gram_stream_blocks(a->gS);
+    return gram_stream_apply(a->gS, xre, yre, s);
   }
   Timed tm{nullptr, nullptr, 0, fp32 ? 1 : 0, 1};
   const bool prof = prof_begin(a, tm);
@@ -756,7 +761,7 @@ int alloc_blocks(oapb_arnoldi* a) {
     a->nsplit = (int)((a->n + ks - 1) / ks);
     rc |= dalloc(&a->Wp, sizeof(double) * 2 * (size_t)kBmMaxB * a->n * a->nsplit);
   }
-  if (!a->cb && !a->gX) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
+  if (!a->cb && !a->gX && !a->gS) {  // stream-K partials of the tensor-core passes (FP64 DMMA and split-BF16)
     size_t need = btc_workspace(a->n, (a->n + 127) / 128 * 128);
     need = std::max(need, i8_workspace(a->n, (a->n + 127) / 128 * 128));
     if (dmma_plan(a->n, &a->dplan)) {
@@ -813,7 +818,7 @@ constexpr double kI8MinTolerance = 1e-12;
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
                 bool fp32 = false, bool bf16 = false, bool coarse = false) {
-  if (a->cb || a->gX) {
+  if (a->cb || a->gX || a->gS) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
                         C ? wi + (long)q * a->n : nullptr, false, OAPB_TYPE_EIGENVECTOR);
@@ -1583,7 +1588,7 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   // and pays off only when the operator pass is HBM-bound: below n = 8192
   // (at most 1 GiB of complex FP64 operator) a pass is a few tens of
   // microseconds and the single-vector FP64 restart loop is faster.
-  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && k <= kBmMaxB && a->mixed_ready &&
+  const bool mixed = a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && !a->gS && k <= kBmMaxB && a->mixed_ready &&
                      a->n >= kMixedMinN;
   if (!resume) a->stats.restarts = 0;  // a resumed solve continues the saved count
   a->stats.matvecs = 0;
@@ -1617,7 +1622,17 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   return a->stats.converged ? OAPB_OK : OAPB_NOT_CONVERGED;
 }
 
+// drop the host-X Gram operator (its copies finish first)
+void drop_gram_stream(oapb_arnoldi* a) {
+  if (a->gS) {
+    cudaStreamSynchronize(a->stream);
+    gram_stream_destroy(a->gS);
+    a->gS = nullptr;
+  }
+}
+
 void free_all(oapb_arnoldi* a) {
+  drop_gram_stream(a);
   void* ps[] = {a->own64re, a->own64im, a->a32re, a->a32im, a->Vre, a->Vim, a->Xre, a->Xim, a->fre,
                 a->fim, a->wre, a->wim, a->x32re, a->x32im, a->v0re, a->v0im, a->H, a->Qs, a->ritz,
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
@@ -1908,6 +1923,7 @@ int oapb_arnoldi_set_dense_operator(oapb_arnoldi* a, const oapb_mat* A) {
   a->a64im = (const double*)A->im;
   a->cb = nullptr;
   a->gX = nullptr;
+  drop_gram_stream(a);
   a->fp32_ready = false;
   a->mixed_ready = false;
   if (a->cfg.precision == OAPB_PREC_MIXED) {
@@ -1922,6 +1938,7 @@ int oapb_arnoldi_set_callback(oapb_arnoldi* a, oapb_matvec_fn fn, void* user) {
   a->cb = fn;
   a->cb_user = user;
   a->gX = nullptr;
+  drop_gram_stream(a);
   return OAPB_OK;
 }
 
@@ -1936,6 +1953,29 @@ int oapb_arnoldi_set_gram_operator(oapb_arnoldi* a, const float* X, uint32_t row
   a->gX = X;
   a->gcols = (int)cols;
   a->cb = nullptr;
+  drop_gram_stream(a);
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_set_gram_operator_host(oapb_arnoldi* a, const float* X, uint32_t rows, uint32_t cols,
+                                        uint32_t block_cols, uint64_t resident_bytes) {
+  if (!a || !X || a->is_c || rows != (uint32_t)a->n || cols < 1 || block_cols < 1) return OAPB_ERR_ARG;
+  drop_gram_stream(a);
+  GramStream* g = nullptr;
+  const int rc = gram_stream_create(X, (int)rows, (int)cols, (int)block_cols, resident_bytes, a->stream, &g);
+  if (rc) return rc;
+  a->gS = g;
+  a->gX = nullptr;
+  a->cb = nullptr;
+  return OAPB_OK;
+}
+
+int oapb_arnoldi_gram_stream_info(const oapb_arnoldi* a, uint32_t* blocks, uint32_t* resident_blocks,
+                                  uint64_t* streamed_bytes) {
+  if (!a || !a->gS) return OAPB_ERR_ARG;
+  if (blocks) *blocks = (uint32_t)gram_stream_blocks(a->gS);
+  if (resident_blocks) *resident_blocks = (uint32_t)gram_stream_resident_blocks(a->gS);
+  if (streamed_bytes) *streamed_bytes = gram_stream_bytes(a->gS);
   return OAPB_OK;
 }
 
@@ -2075,7 +2115,7 @@ int oapb_arnoldi_load(oapb_arnoldi* a, const char* path) {
 static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* residuals, const oapb_mat* evecs,
                        bool resume) {
   if (!a) return OAPB_ERR_ARG;
-  if (!a->cb && !a->gX && !a->a64re) return OAPB_ERR_ARG;
+  if (!a->cb && !a->gX && !a->gS && !a->a64re) return OAPB_ERR_ARG;
   if (evecs && (evecs->columns != (uint32_t)a->k || evecs->rows != (uint32_t)a->n || evecs->dtype != OAPB_F64 ||
                 !evecs->re))
     return OAPB_ERR_ARG;
@@ -2144,6 +2184,7 @@ int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* hi
     a->a64im = a->is_c ? a->own64im : nullptr;
     a->cb = nullptr;
     a->gX = nullptr;
+    drop_gram_stream(a);
     a->fp32_ready = false;
     a->mixed_ready = false;
     // the previous solve's work on the solver stream precedes the copies

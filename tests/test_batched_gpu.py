@@ -88,3 +88,27 @@ def test_batched_rejects_bad_arguments():
         B.solve_batched([planes(A)], 4, hdim=40)     # hdim > 32
     with pytest.raises(B.OapbError):
         B.solve_batched([planes(A)], 8, hdim=8)      # wanted >= hdim
+
+
+def test_batched_launch_variants_agree():
+    # the autotuner's launch variants (threads per CTA x CTAs per SM: 256 x 1,
+    # 128 x 2, 256 x 2, 128 x 4, 64 x 8; forced with autotune = 2 + v) solve
+    # every problem to the default variant's eigenvalues; the tuned call
+    # reports the variant it chose
+    rng = np.random.default_rng(5)
+    sizes = list(rng.integers(24, 300, size=60))
+    As = [complex_problem(int(n), rng) for n in sizes]
+    mats = [planes(A) for A in As]
+    ev0, res0, st0, stats0, rc0 = B.solve_batched(mats, 4, hdim=20, autotune=False)
+    assert rc0 == B.OK and stats0["variant"] == 0 and stats0["threads"] == 256
+    for v, threads in enumerate((256, 128, 256, 128, 64)):
+        ev, res, st, stats, rc = B.solve_batched(mats, 4, hdim=20, autotune=2 + v)
+        assert rc == B.OK and stats["variant"] == v and stats["threads"] == threads
+        assert res.max() <= TOL
+        scale = np.abs(ev0).max(axis=1, keepdims=True)
+        assert (np.abs(ev - ev0) <= 1e-10 * scale).all(), v
+    ev, res, st, stats, rc = B.solve_batched(mats, 4, hdim=20, autotune=True)
+    assert rc == B.OK and 0 <= stats["variant"] < 5 and res.max() <= TOL
+    ev2, _, _, stats2, _ = B.solve_batched(mats, 4, hdim=20, autotune=True)
+    assert stats2["variant"] == stats["variant"]  # cached per shape
+    assert (np.abs(ev2 - ev0) <= 1e-10 * np.abs(ev0).max(axis=1, keepdims=True)).all()

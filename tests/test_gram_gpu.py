@@ -1,7 +1,11 @@
 """Gram build A = X X^T on the tensor cores (split BF16, FP32 accumulation)
-against an FP64 torch reference of the same product."""
+against an FP64 torch reference of the same product; the implicit Gram
+operator (X on the device, or in host memory streamed by column blocks)
+against the CPU oracle's FP64 IRAM on the exact Gram."""
 import numpy as np
 import pytest
+
+import oracle as O
 
 pytestmark = pytest.mark.gpu
 
@@ -44,29 +48,66 @@ def test_gram_stream_k_split_tiles(rows, cols):
     check_gram(rows, cols, seed=7 * rows + cols)
 
 
-@pytest.mark.gpu
-@pytest.mark.parametrize("rows,cols", [(600, 3000), (513, 1027)])
-def test_implicit_gram_operator_matches_explicit(rows, cols):
-    # w = X (X^T v) never forming A; eigenpairs vs the solve on the FP64 Gram
-    # of the same FP32 images (the implicit operator is that Gram exactly)
+def separated_images(rows, cols, seed):
+    """images = 8 separated components + noise: a well-separated top spectrum"""
     g = torch.Generator(device="cuda")
-    g.manual_seed(rows)
-    # images = 8 separated components + noise: well-separated top spectrum
+    g.manual_seed(seed)
     U = torch.randn(rows, 8, generator=g, device="cuda", dtype=torch.float64)
     V = torch.randn(8, cols, generator=g, device="cuda", dtype=torch.float64)
     S = torch.tensor([10.0, 8.0, 6.5, 5.0, 4.0, 3.0, 2.4, 2.0], device="cuda", dtype=torch.float64)
-    X = ((U * S) @ V / cols ** 0.5 + 0.05 * torch.randn(rows, cols, generator=g, device="cuda",
-                                                         dtype=torch.float64)).float().contiguous()
-    A64 = X.double() @ X.double().T
-    ref = B.Arnoldi(rows, 24, 6, seed=3)
-    ref.set_operator(A64.contiguous())
-    ev_ref, res_ref, st = ref.solve()
-    assert st == B.OK
+    return ((U * S) @ V / cols ** 0.5 + 0.05 * torch.randn(rows, cols, generator=g, device="cuda",
+                                                           dtype=torch.float64)).float().contiguous()
+
+
+def oracle_gram_eigenvalues(X, k, m):
+    """The CPU oracle's FP64 IRAM on the exact Gram of the FP32 images."""
+    Xd = X.double().cpu().numpy()
+    A = Xd @ Xd.T
+    o = O.iram(A, k, m, which="LM", tol=1e-12, seed=3)
+    assert o["rc"] == 0
+    return np.sort(o["eigenvalues"].real)[::-1]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("rows,cols", [(600, 3000), (513, 1027)])
+def test_implicit_gram_operator_matches_oracle(rows, cols):
+    # w = X (X^T v) never forming A: the eigenpairs of the exact Gram of the
+    # FP32 images, against the CPU oracle's FP64 IRAM on that Gram
+    X = separated_images(rows, cols, rows)
     imp = B.Arnoldi(rows, 24, 6, seed=3)
     imp.set_gram_operator(X)
     ev, res, st = imp.solve()
     assert st == B.OK and max(res) <= 1e-10
-    assert np.allclose(np.array(ev).real, np.array(ev_ref).real, rtol=1e-11, atol=0)
+    ref = oracle_gram_eigenvalues(X, 6, 24)
+    assert np.allclose(np.sort(np.array(ev).real)[::-1], ref, rtol=1e-11, atol=0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("cols,block_cols,resident", [(3000, 1000, 0), (1027, 256, 2), (2048, 4096, 0),
+                                                      (1027, 100, 10 ** 9)])
+def test_host_streamed_gram_operator_matches_oracle(cols, block_cols, resident):
+    # X in pinned host memory, applied by column blocks (some resident, the
+    # rest streamed on every application, ragged last blocks): the same
+    # eigenvalues as the CPU oracle's FP64 IRAM on the exact Gram, and the
+    # bytes streamed per application equal the non-resident blocks
+    rows = 600
+    X = separated_images(rows, cols, cols + block_cols)
+    Xh = X.cpu().pin_memory()
+    s = B.Arnoldi(rows, 24, 6, seed=3)
+    s.set_gram_operator_host(Xh, block_cols, resident_bytes=resident * 4 * rows * ((block_cols + 3) // 4 * 4))
+    nb, nres, by0 = s.gram_stream_info()
+    bc = min(cols, (block_cols + 3) // 4 * 4)
+    assert nb == -(-cols // bc) and nres == min(nb, resident) and by0 == 0
+    ev, res, st = s.solve()
+    assert st == B.OK and max(res) <= 1e-10
+    ref = oracle_gram_eigenvalues(X, 6, 24)
+    assert np.allclose(np.sort(np.array(ev).real)[::-1], ref, rtol=1e-11, atol=0)
+    nb, nres, by = s.gram_stream_info()
+    per_application = 4 * rows * (cols - min(cols, nres * bc))
+    if per_application == 0:
+        assert by == 0
+    else:  # every application (Arnoldi steps and residual checks) streams the same bytes
+        assert by % per_application == 0 and by // per_application >= s.stats()["matvecs"]
 
 
 @pytest.mark.gpu
