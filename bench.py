@@ -60,6 +60,8 @@ def parse():
                    help="FP32 block passes on CUDA cores instead of the split-BF16 tensor-core pass")
     p.add_argument("--train", type=int, default=20000, help="warm-start training solves")
     p.add_argument("--held-out", type=int, default=48, help="warm-start evaluation solves")
+    p.add_argument("--train-smooth", type=int, default=4096,
+                   help="warm-start training solves of the family with its parameter operators scaled by 0.01")
     p.add_argument("--config", default="single", choices=["single", "batched", "gram", "warmstart"],
                    help="single: the n=16384 complex solve (default line); batched: 2048 uneven "
                         "complex problems n in [32, 512], top-4, hdim=min(n, 24)")
@@ -875,34 +877,30 @@ def run_gram(args, world, rank, local):
         print(json.dumps(out), flush=True)
 
 
-def run_warmstart(args, world, rank, local):
-    """Learned warm start on A(theta) = A0 + sum_i theta_i B_i (n = 2048 real
-    symmetric, 16 parameters): training targets from plain FP64 IRAM solves
-    (batched), network 16 -> 256 -> 256 -> 2048 + 8 trained on the GPU,
-    then held-out solves from the prediction vs from a random start."""
+def warmstart_family(fam, n, k, hdim, n_train, n_test, seed, epochs=40):
+    """Train the network on plain-method solves of A(theta) and compare
+    held-out solves from its prediction with the random start."""
     import numpy as np
     import torch
     import oap_b200 as B
     from oap_b200 import warmstart as W
-    torch.cuda.set_device(local)
-    n, k, hdim = 2048, 8, 24
-    fam = W.ParamFamily(n=n, nparams=16, seed=31 + rank)
     g = torch.Generator(device="cuda")
-    g.manual_seed(77 + rank)
-    th_train = torch.rand(args.train, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
-    th_test = torch.rand(args.held_out, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    g.manual_seed(seed)
+    th_train = torch.rand(n_train, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
+    th_test = torch.rand(n_test, 16, dtype=torch.float64, device="cuda", generator=g) * 2 - 1
     t0 = time.perf_counter()
     T, evs, st = W.make_targets(fam, th_train, wanted=k, nshift=8, chunk=256)
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     net = W.Net([16, 256, 256, n + 8], seed=1)
     t0 = time.perf_counter()
-    losses = net.train(th_train.float().contiguous(), torch.from_numpy(T).cuda(), epochs=40, batch=256, lr=2e-3)
+    losses = net.train(th_train.float().contiguous(), torch.from_numpy(T).cuda(), epochs=epochs, batch=256, lr=2e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     ops = fam.operators(th_test)
     res = {"warm": {"matvecs": 0, "restarts": 0, "seconds": 0.0, "fallbacks": 0, "converged": 0},
            "random": {"matvecs": 0, "restarts": 0, "seconds": 0.0, "converged": 0}}
+    eps = []
     for i in range(th_test.shape[0]):
         A = ops[i].contiguous()
         torch.cuda.synchronize()
@@ -914,6 +912,8 @@ def run_warmstart(args, world, rank, local):
         ev, r2, str_, s_r = W.solve_random(A, n, wanted=k, hdim=hdim)
         torch.cuda.synchronize()
         t3 = time.perf_counter()
+        _, _, _, _, X = W.solve_random(A, n, wanted=k, hdim=hdim, vectors=True)
+        eps.append(W.start_error(pred[:n], X))
         for key, s_, st_, rr, dt in (("warm", s_w, stw, r, t2 - t1), ("random", s_r, str_, r2, t3 - t2)):
             res[key]["matvecs"] += s_["matvecs"]
             res[key]["restarts"] += s_["restarts"]
@@ -924,14 +924,35 @@ def run_warmstart(args, world, rank, local):
     for key in res:
         for f in ("matvecs", "restarts", "seconds"):
             res[key][f + "_per_solve"] = res[key][f] / m
+    return {"training": {"solves": n_train, "data_seconds": t_data, "train_seconds": t_train,
+                         "loss_first": losses[0], "loss_last": losses[-1],
+                         "plain_solves_converged": int((st == B.OK).sum())},
+            "held_out": res, "prediction_eps_median": float(np.median(eps)),
+            "speedup_time": res["random"]["seconds"] / res["warm"]["seconds"] if res["warm"]["seconds"] else None,
+            "matvec_ratio": res["random"]["matvecs"] / max(1, res["warm"]["matvecs"])}
+
+
+def run_warmstart(args, world, rank, local):
+    """Learned warm start on A(theta) = A0 + sum_i theta_i B_i (n = 2048 real
+    symmetric, 16 parameters, top-8): training targets from plain FP64 IRAM
+    solves (batched), network 16 -> 256 -> 256 -> 2048 + 8 trained on the
+    GPU, then held-out solves from the prediction vs from a random start;
+    then the same with the B_i scaled by 0.01, where the wanted subspace is a
+    smooth function of theta."""
+    import torch
+    from oap_b200 import warmstart as W
+    torch.cuda.set_device(local)
+    n, k, hdim = 2048, 8, 24
+    fam = W.ParamFamily(n=n, nparams=16, seed=31 + rank)
+    spec = warmstart_family(fam, n, k, hdim, args.train, args.held_out, 77 + rank)
+    del fam
+    fam = W.ParamFamily(n=n, nparams=16, seed=31 + rank, scale=0.01)
+    smooth = warmstart_family(fam, n, k, hdim, args.train_smooth, args.held_out, 78 + rank)
     out = {"config": {"workload": "A(theta) = A0 + sum theta_i B_i, n=2048 real symmetric, 16 params, top-8 LR, "
                                   "hdim 24; network 16-256-256-2056 BF16",
-                      "training_solves": args.train, "held_out": m},
-           "training": {"data_seconds": t_data, "train_seconds": t_train, "loss_first": losses[0],
-                        "loss_last": losses[-1], "plain_solves_converged": int((st == B.OK).sum())},
-           "held_out": res,
-           "speedup_time": res["random"]["seconds"] / res["warm"]["seconds"] if res["warm"]["seconds"] else None,
-           "matvec_ratio": res["random"]["matvecs"] / max(1, res["warm"]["matvecs"])}
+                      "training_solves": args.train, "held_out": args.held_out},
+           "specified_family": spec,
+           "smooth_family_scale_0.01": smooth}
     if rank == 0:
         print(json.dumps(out), flush=True)
 
