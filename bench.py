@@ -60,6 +60,8 @@ def parse():
                    help="FP32 block passes on CUDA cores instead of the split-BF16 tensor-core pass")
     p.add_argument("--train", type=int, default=20000, help="warm-start training solves")
     p.add_argument("--held-out", type=int, default=48, help="warm-start evaluation solves")
+    p.add_argument("--gram-side", type=int, default=128,
+                   help="image side of the --config gram --quick build (4096 images)")
     p.add_argument("--train-smooth", type=int, default=4096,
                    help="warm-start training solves of the family with its parameter operators scaled by 0.01")
     p.add_argument("--config", default="single", choices=["single", "batched", "gram", "warmstart"],
@@ -817,6 +819,25 @@ def run_gram(args, world, rank, local):
     import oap_b200 as B
     torch.cuda.set_device(local)
     count, side = 4096, 256
+    if args.quick:
+        # profiling run: the build alone on 4096 images of side x side pixels
+        side = args.gram_side
+        X = synthetic_images(count, side, 21 + rank, "cuda")
+        for _ in range(args.warmup):
+            B.gram_build(X)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            B.gram_build(X)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        flops = 2.0 * count * count * side * side
+        if rank == 0:
+            print(json.dumps({"quick": True, "config": "gram build", "images": count, "pixels": side * side,
+                              "build_ms": ms, "tflops_algorithmic": flops / ms / 1e9}), flush=True)
+        return
     X = synthetic_images(count, side, 21 + rank, "cuda")
     torch.cuda.synchronize()
     for _ in range(args.warmup):
