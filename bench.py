@@ -914,8 +914,11 @@ def warmstart_family(fam, n, k, hdim, n_train, n_test, seed, epochs=40):
     torch.cuda.synchronize()
     t_data = time.perf_counter() - t0
     net = W.Net([16, 256, 256, n + 8], seed=1)
+    ok = st == B.OK  # targets from the plain method's converged solves only
+    keep = torch.from_numpy(np.nonzero(ok)[0]).cuda()
     t0 = time.perf_counter()
-    losses = net.train(th_train.float().contiguous(), torch.from_numpy(T).cuda(), epochs=epochs, batch=256, lr=2e-3)
+    losses = net.train(th_train[keep].float().contiguous(), torch.from_numpy(T[ok]).cuda(), epochs=epochs, batch=256,
+                       lr=2e-3)
     torch.cuda.synchronize()
     t_train = time.perf_counter() - t0
     ops = fam.operators(th_test)

@@ -21,11 +21,10 @@
 // Work layout (one warp): T and Z are column-major with an odd leading
 // dimension hess_ld(m), so a lane-per-column access (row rotations) and a
 // lane-per-row access (column rotations) are both free of bank conflicts.
-// A QR sweep costs two warp syncs per rotation: the row rotation runs one
-// lane per column, the column rotation one lane per row, and the lanes that
-// produce the next bulge pair hand it to the warp by shuffle.  Rotations on
-// Z are deferred to the end of the sweep (each lane then applies the whole
-// sequence to its rows).  The eigenvector back substitutions run one lane
+// A QR sweep runs its chain of rotations in registers (the 2 x 2 window and
+// the bulge, one shuffle per rotation) while the lanes apply each row
+// rotation to their columns; the column rotations of the sweep, and those on
+// Z, are applied after the chain (each lane the whole sequence to its rows).  The eigenvector back substitutions run one lane
 // per eigenvector (T read by broadcast).
 //
 // Every loop is bounded (30 m sweeps for the Schur form); hitting the bound
@@ -139,11 +138,36 @@ static __device__ int find_split(const Cx* T, int ld, int h, int lane) {
 }
 
 // One single-shift QR sweep on the active window [l, h] of Hessenberg T,
-// applied to whole rows / columns of T; Z <- Z G_l^H ... G_{h-1}^H at the end
-// of the sweep.  rot: 2 m cplx of scratch.
-template <typename Cx>
-static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot, int lane) {
-  Cx x = TT_(l, l) - mu, y = TT_(l + 1, l);
+// applied to whole rows / columns of T (the final T is G T G^H with G =
+// G_{h-1} ... G_l); Z <- Z G_l^H ... G_{h-1}^H.  rot: 2 m cplx of scratch.
+//
+// The rotations form a dependent chain: rotation k needs the bulge pair
+// left by rotation k - 1.  That chain runs in registers: every lane carries
+// the 2 x 2 window T[k..k+1][k..k+1] and the bulge through the algebra of
+// one rotation on both sides, and the one entry of the window that earlier
+// rotations reach from outside it, T[k][k+1], comes from the lane that owns
+// column k + 1.  The matrix itself is updated off the chain: while the chain
+// runs, lane c applies each row rotation to column c (its row-k entry carried
+// in a register, the row-(k+1) entry read once), and after the chain one
+// lane per row applies all column rotations to its row.  Left and right
+// rotations commute, so the result is G T G^H as in the interleaved sweep;
+// the entries below the subdiagonal that the interleaved sweep never fills
+// come out of this order at rounding level and are set to zero.  Per
+// rotation the chain costs one rotation, one shuffle and a few complex
+// multiply-adds instead of two shared-memory passes and two warp barriers.
+// NT: columns per lane (c = lane + 32 t, t < NT); m <= 32 NT.
+template <typename Cx, int NT>
+static __device__ __forceinline__ void warp_sweep_nt(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot,
+                                                     int lane) {
+  const int nt = (m + 31) >> 5;
+  Cx carry[NT];
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int c = lane + 32 * t;
+    carry[t] = (t < nt && c >= l && c < m) ? TT_(l, c) : Cx{0, 0};
+  }
+  Cx D = TT_(l, l), E = TT_(l, l + 1), F = TT_(l + 1, l), G = TT_(l + 1, l + 1);
+  Cx x = D - mu, y = F;
   for (int k = l; k < h; ++k) {
     Cx p, q;
     givens(x, y, p, q);
@@ -151,32 +175,57 @@ static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx 
       rot[2 * k] = p;
       rot[2 * k + 1] = q;
     }
-    // rows k, k+1 (one lane per column)
-    const int j0 = k > l ? k - 1 : k;
-    for (int j = j0 + lane; j < m; j += 32) {
-      const Cx a = TT_(k, j), b = TT_(k + 1, j);
-      TT_(k, j) = p * a + q * b;
-      TT_(k + 1, j) = (k > l && j == k - 1) ? Cx{0, 0} : (-conj(q)) * a + conj(p) * b;
+    const Cx pc = conj(p), nqc = -conj(q);
+    // row rotation k on the lanes' columns (rows k, k + 1; row k + 1 is
+    // still the sweep's start value there)
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int c = lane + 32 * t;
+      if (t < nt && c >= l && c < m) {
+        const Cx b = TT_(k + 1, c);
+        TT_(k, c) = p * carry[t] + q * b;
+        carry[t] = nqc * carry[t] + pc * b;
+      }
     }
-    __syncwarp();
-    // columns k, k+1 (one lane per row); rows k+1 and k+2 of column k are
-    // the next bulge pair
-    const int ihi = (k + 2 < h) ? k + 2 : h;
-    Cx xn = {0, 0}, yn = {0, 0};
-    for (int i = lane; i <= ihi; i += 32) {
-      const Cx a = TT_(i, k), b = TT_(i, k + 1);
-      const Cx na = a * conj(p) + b * conj(q);
-      TT_(i, k) = na;
-      TT_(i, k + 1) = (-a) * q + b * p;
-      if (i == k + 1) xn = na;
-      if (i == k + 2) yn = na;
-    }
+    // the window through rotation k on both sides, then the next one
     if (k + 1 < h) {
-      x = shfl_c(xn, (k + 1) & 31);
-      y = shfl_c(yn, (k + 2) & 31);
+      const Cx F1 = nqc * D + pc * F, G1 = nqc * E + pc * G;
+      const Cx s = TT_(k + 2, k + 1);  // untouched so far
+      x = F1 * pc + G1 * conj(q);       // T[k+1][k]
+      y = s * conj(q);                  // T[k+2][k], the bulge
+      D = (-F1) * q + G1 * p;           // T[k+1][k+1]
+      F = s * p;                        // T[k+2][k+1]
+      G = TT_(k + 2, k + 2);
+      // T[k+1][k+2] after row rotation k: the carry of column k + 2
+      const int c2 = k + 2;
+      Cx e = carry[0];
+#pragma unroll
+      for (int t = 1; t < NT; ++t)
+        if (t == (c2 >> 5)) e = carry[t];
+      E = shfl_c(e, c2 & 31);
     }
-    __syncwarp();
   }
+#pragma unroll
+  for (int t = 0; t < NT; ++t) {
+    const int c = lane + 32 * t;
+    if (t < nt && c >= l && c < m) TT_(h, c) = carry[t];
+  }
+  __syncwarp();
+  // column rotations l .. h-1 on rows 0 .. h (one lane per row)
+  for (int i = lane; i <= h; i += 32) {
+    Cx c = TT_(i, l);
+    for (int k = l; k < h; ++k) {
+      const Cx p = rot[2 * k], q = rot[2 * k + 1];
+      const Cx nb = TT_(i, k + 1);
+      TT_(i, k) = c * conj(p) + nb * conj(q);
+      c = (-c) * q + nb * p;
+    }
+    TT_(i, h) = c;
+  }
+  __syncwarp();
+  // below the subdiagonal of the window: rounding-level values -> 0
+  for (int i = l + 2 + lane; i <= h; i += 32)
+    for (int c = l; c <= i - 2; ++c) TT_(i, c) = Cx{0, 0};
   if (Z) {
     for (int i = lane; i < m; i += 32) {
       Cx c = ZZ_(i, l);
@@ -188,8 +237,21 @@ static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx 
       }
       ZZ_(i, h) = c;
     }
-    __syncwarp();
   }
+  __syncwarp();
+}
+
+// the carries stay in registers when their count is fixed by m's range
+template <typename Cx>
+static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot, int lane) {
+  if (m <= 32)
+    warp_sweep_nt<Cx, 1>(T, Z, m, ld, l, h, mu, rot, lane);
+  else if (m <= 64)
+    warp_sweep_nt<Cx, 2>(T, Z, m, ld, l, h, mu, rot, lane);
+  else if (m <= 128)
+    warp_sweep_nt<Cx, 4>(T, Z, m, ld, l, h, mu, rot, lane);
+  else
+    warp_sweep_nt<Cx, kMaxM / 32>(T, Z, m, ld, l, h, mu, rot, lane);
 }
 
 // Householder reduction of dense T to Hessenberg form, Z accumulating.
