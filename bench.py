@@ -856,7 +856,7 @@ def run_gram(args, world, rank, local):
     Xd = X.double()
     ref = Xd[idx] @ Xd.T
     rel = ((A64[idx] - ref).abs() / ref.abs().clamp_min(1e-300)).max().item()
-    res = {}
+    res, evs = {}, {}
     for name, prec in (("mixed", B.PREC_MIXED), ("plain_fp64", B.PREC_FP64)):
         s = B.Arnoldi(count, 96, 32, precision=prec, tolerance=TOL, seed=5, profile=True)
         s.set_operator(A64)
@@ -869,6 +869,7 @@ def run_gram(args, world, rank, local):
                      "stats": {k: v for k, v in s.stats().items() if k in ("restarts", "matvecs", "block_matvecs",
                                                                            "refine_iterations")},
                      "top3": [e.real for e in ev[:3]]}
+        evs[name] = ev
         s.close()
     # the implicit operator: A v = X (X^T v), A never formed (two passes over X)
     s = B.Arnoldi(count, 96, 32, tolerance=TOL, seed=5)
@@ -883,6 +884,13 @@ def run_gram(args, world, rank, local):
                             "top3": [e.real for e in ev[:3]],
                             "x_bytes_per_matvec": 2 * 4 * count * side * side}
     s.close()
+    # eigenvalue errors: the split-BF16 built operator's 32 values against the
+    # exact Gram of the FP32 images (implicit operator), and the chosen form
+    # against the plain FP64 solve of the same built operator
+    import oracle as O
+    lm = lambda e: sorted(e, key=lambda z: -abs(z))
+    res["eig_err_built_vs_exact_gram"] = O.match_eigenvalues(lm(evs["plain_fp64"]), lm(ev))
+    res["eig_err_mixed_vs_plain_fp64"] = O.match_eigenvalues(lm(evs["mixed"]), lm(evs["plain_fp64"]))
     peak = 1642.4
     try:
         peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]

@@ -184,8 +184,10 @@ typedef enum oapb_sort {
 typedef enum oapb_precision {
   /* FP64 everywhere: the plain GPU Arnoldi. */
   OAPB_PREC_FP64 = 0,
-  /* The chosen form (dense operators, n >= 8192; below that the FP64 path
-   * is faster and runs): block subspace iteration on an FP32-class copy of
+  /* The chosen form (dense operators, n >= 8192; from 2048 to 8192 the
+   * FP64 restart loop runs, below that - with hdim <= 32 and a random start -
+   * the FP64 restart loop of one problem on one CTA, no launch per step):
+   * block subspace iteration on an FP32-class copy of
    * the operator (split-BF16 tensor-core passes, or FP32 CUDA-core passes
    * with tensor_cores = 0), then FP64-anchored refinement (FP64 residual
    * passes, FP32-class Sylvester corrections) until the residual goal holds
@@ -267,6 +269,9 @@ typedef struct oapb_arnoldi_stats {
                                 triangular projected matrix (the rest: Schur) */
   uint32_t block_i8;         /* FP64-class block passes on the integer tensor
                                 cores (int8 slices of the mixed form's operator) */
+  uint32_t onchip;           /* 1: the last solve ran on one CTA (the chosen
+                                form for dense operators with n <= 2048 and
+                                hdim <= 32, random start) */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

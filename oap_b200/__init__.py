@@ -65,7 +65,7 @@ class Stats(C.Structure):
                 ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32),
                 ("matvec_variant", C.c_uint32), ("block_bf16", C.c_uint32),
                 ("block_bf16_timed", C.c_uint32), ("block_bf16_seconds", C.c_double),
-                ("eig_fast", C.c_uint32), ("block_i8", C.c_uint32)]
+                ("eig_fast", C.c_uint32), ("block_i8", C.c_uint32), ("onchip", C.c_uint32)]
 
 
 class BatchProblem(C.Structure):

@@ -11,13 +11,14 @@
 // both operands K-major).  Only tiles touching the upper triangle are
 // computed; a second kernel writes each (i <= j) element and its mirror.
 //
-// k_gram_tc is persistent and stream-K scheduled: one CTA per SM walks an
-// equal share of the (tile, 32-column K chunk) iterations, so the 272 tiles
-// of a 4096-row Gram do not leave the second wave of SMs a quarter idle.
-// Each CTA's share is at least one tile long, so a tile is split between at
-// most two CTAs: the part that starts at the tile's first chunk goes to
-// slot 0 of the tile's FP32 partials, the rest to slot 1, and k_gram_finish
-// adds the slots in that order (deterministic).  Warps are specialised:
+// k_gram_tc walks (tile, 32-column K chunk) iterations in contiguous CTA
+// shares; it is launched with one CTA per tile (one resident per SM), so the
+// CTAs of a wave read the same K chunks at the same time and the operands
+// come from L2.  With fewer CTAs than tiles (stream-K) each CTA's share is
+// at least one tile long, so a tile is split between at most two CTAs: the
+// part that starts at the tile's first chunk goes to slot 0 of the tile's
+// FP32 partials, the rest to slot 1, and k_gram_finish adds the slots in
+// that order (deterministic).  Warps are specialised:
 //   warp 0      TMA producer: per stage 4 tiled loads (A hi / lo: 128 rows,
 //               B hi / lo: 256 rows, 32 columns = 64 bytes, 64-byte swizzle)
 //               completing on the stage's `full` mbarrier; 4 stages of 48 KB;
@@ -267,10 +268,16 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
     for (int c = 0; c * kGmN < (int)rows; ++c)
       if (r * kGmM <= c * kGmN + kGmN - 1) tiles.push_back(make_int4(r, c, 0, 0));
   const long ntiles = (long)tiles.size();
-  const int ctas = (int)(ntiles < kNumSMs ? ntiles : kNumSMs);
+  // one CTA per tile, resident one per SM, so the CTAs of a wave stream K
+  // in step and read each operand chunk from L2 (a stream-K split over
+  // min(tiles, SMs) CTAs left them at scattered K offsets: 4.7 GB of DRAM
+  // reads for 256 MB of operands at 4096 x 16384); the split machinery below
+  // stays for grids of fewer CTAs than tiles
+  const int ctas = (int)ntiles;
   const long total = ntiles * kch;
   // with at least one tile per CTA a tile meets at most two CTAs: it is
-  // split when the CTA holding its first chunk ends inside it
+  // split when the CTA holding its first chunk ends inside it (never with
+  // one CTA per tile)
   for (long t = 0; t < ntiles; ++t) {
     const long first = t * kch;
     long b = (first * ctas) / total;  // the CTA whose [b total / ctas, (b + 1) total / ctas) holds `first`

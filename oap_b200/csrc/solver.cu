@@ -403,6 +403,16 @@ __global__ void k_to_f32(const double* __restrict__ src, T* dst, long len) {
 }
 
 // row-major (reference layout) n x k matrix from k vector-contiguous vectors
+// the inverse: row-major n x k (column q = vector q) -> vector-major planes
+__global__ void k_rowmajor_to_vectors(const double* __restrict__ ire, const double* __restrict__ iim, int n, int k,
+                                      double* xre, double* xim) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)n * k; t += (long)gridDim.x * blockDim.x) {
+    const long q = t / n, r = t % n;
+    xre[t] = ire[r * k + q];
+    if (xim) xim[t] = iim ? iim[r * k + q] : 0.0;
+  }
+}
+
 __global__ void k_vectors_to_rowmajor(const double* __restrict__ xre, const double* __restrict__ xim, int n, int k,
                                       double* ore, double* oim) {
   for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < (long)n * k; t += (long)gridDim.x * blockDim.x) {
@@ -1060,6 +1070,12 @@ int ensure_side_stream(oapb_arnoldi* a) {
 
 constexpr int kSlow = 100;   // subspace(): convergence too slow for the iteration budget
 constexpr int kMixedMinN = 8192;
+// The chosen form for small dense operators: the whole restart loop of one
+// problem in one CTA (the batched kernel's solver with a batch of one), with
+// no launch or host round trip per Arnoldi step.  Up to n = 2048 and
+// hdim = 32 (the batched kernel's limits).
+constexpr int kOnchipMaxN = 2048;
+constexpr int kOnchipMaxM = 32;
 // BF16 operator passes (tensor cores only).  In the FP32-class subspace
 // iteration: the powers taken while the block is still far from the wanted
 // subspace (before the first check, then while the residual extrapolated
@@ -1581,6 +1597,42 @@ int solve_mixed(oapb_arnoldi* a, double* r) {
   return solve_plain<C>(a, r);
 }
 
+// The chosen form below kMixedMinN: the FP64 restart loop on one CTA
+// (oapb_arnoldi_solve_batched with one problem).  Ritz vectors land in
+// a->Xre (vector-major) like the multi-kernel path's, so the outputs,
+// test_outcome and the host-buffer solve read them the same way.
+template <bool C>
+int solve_onchip(oapb_arnoldi* a, double* r) {
+  const int n = a->n, k = a->k;
+  oapb_arnoldi_config cfg = a->cfg;
+  cfg.hdim = (uint32_t)a->m;
+  oapb_batch_problem p;
+  p.n = (uint32_t)n;
+  p.re = a->a64re;
+  p.im = C ? a->a64im : nullptr;
+  p.eigvec_re = a->Bre[3];  // row-major n x k scratch (a block buffer holds n x 32)
+  p.eigvec_im = C ? a->Bim[3] : nullptr;
+  std::vector<double> er(k), ei(k), rs(k);
+  int32_t st = 0;
+  oapb_batch_stats bs;
+  const int rc = oapb_arnoldi_solve_batched(&cfg, &p, 1, er.data(), ei.data(), rs.data(), &st, &bs, (void*)a->stream);
+  if (rc != OAPB_OK && rc != OAPB_NOT_CONVERGED) return rc;
+  if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
+  a->stats.kernel_launches += 2;
+  k_rowmajor_to_vectors<<<grid_for((long)n * k, 256, kNumSMs * 8), 256, 0, a->stream>>>(
+      a->Bre[3], C ? a->Bim[3] : nullptr, n, k, a->Xre, C ? a->Xim : nullptr);
+  if (cudaGetLastError() != cudaSuccess) return OAPB_ERR_CUDA;
+  a->evals.resize(k);
+  for (int q = 0; q < k; ++q) {
+    a->evals[q] = cplx{er[q], C ? ei[q] : 0.0};
+    r[q] = rs[q];
+  }
+  a->stats.matvecs = (uint32_t)bs.matvecs;
+  a->stats.restarts = (uint32_t)bs.restarts;
+  a->stats.onchip = 1;
+  return st;
+}
+
 template <bool C>
 int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, bool resume = false) {
   const int k = a->k;
@@ -1604,7 +1656,14 @@ int solve_impl(oapb_arnoldi* a, double* eig_re, double* eig_im, double* res, boo
   if (rc) return rc;
   std::vector<double> r(k);
   a->ckpt_ready = false;
-  int st = resume ? resume_plain<C>(a, r.data()) : mixed ? solve_mixed<C>(a, r.data()) : solve_plain<C>(a, r.data());
+  a->stats.onchip = 0;
+  const bool onchip = !resume && !mixed && a->cfg.precision == OAPB_PREC_MIXED && !a->cb && !a->gX && !a->gS &&
+                      a->a64re && a->n <= kOnchipMaxN && a->m <= kOnchipMaxM && a->cfg.init == OAPB_INIT_RANDOM &&
+                      a->start_shifts.empty();
+  int st = resume ? resume_plain<C>(a, r.data())
+           : mixed ? solve_mixed<C>(a, r.data())
+           : onchip ? solve_onchip<C>(a, r.data())
+                    : solve_plain<C>(a, r.data());
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   double mx = 0;
   bool finite = true;

@@ -360,3 +360,27 @@ def test_matvec_autotune_variants(cplx):
         assert 0 <= v < 6 and (autotune is True or v == autotune - 2)
         assert r["res"].max() <= TOL
         assert np.allclose(np.sort_complex(r0["ev"]), np.sort_complex(r["ev"]), rtol=1e-11, atol=0)
+
+
+@pytest.mark.parametrize("cplx,n,k,m", [(False, 256, 5, 32), (True, 300, 6, 24), (True, 2048, 4, 32),
+                                        (False, 64, 4, 12)])
+def test_onchip_chosen_form_small_operators(cplx, n, k, m):
+    # the chosen form below the tensor-core sizes: the whole restart loop of
+    # one problem on one CTA; the same eigenpairs as the multi-kernel FP64
+    # restart loop and the oracle, eigenvectors and test_outcome as usual
+    A = planted_complex(n, seed=n + k, nplant=k) if cplx else planted_symmetric(n, seed=n)[0]
+    r = solve(A, k, m, precision=B.PREC_MIXED, vectors=True)
+    assert r["stats"]["onchip"] == 1 and r["stats"]["converged"] == 1
+    assert r["res"].max() <= TOL
+    p = solve(A, k, m, precision=B.PREC_FP64)
+    assert p["stats"]["onchip"] == 0
+    scale = np.abs(p["ev"]).max()
+    for lam in p["ev"]:
+        assert np.min(np.abs(r["ev"] - lam)) <= 1e-10 * scale
+    o = O.iram(A, k, m, which="LM", tol=TOL, seed=1)
+    for lam in o["eigenvalues"]:
+        assert np.min(np.abs(r["ev"] - lam)) <= 1e-10 * scale
+    X = r["x"]
+    for q in range(k):
+        assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * scale * 1.01
+        assert r["solver"].test_outcome(q) <= TOL

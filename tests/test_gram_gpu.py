@@ -42,9 +42,10 @@ def test_gram_tensor_cores(rows, cols):
 
 
 @pytest.mark.parametrize("rows,cols", [(3000, 1000), (4096, 160)])
-def test_gram_stream_k_split_tiles(rows, cols):
-    # more upper-triangle tiles than SMs (156 and 272): the stream-K shares
-    # split tiles between two CTAs, whose partials the finishing kernel adds
+def test_gram_more_tiles_than_sms(rows, cols):
+    # more upper-triangle tiles than SMs (156 and 272): a second wave of
+    # CTAs, ragged edge tiles, one partial per tile through the finishing
+    # kernel
     check_gram(rows, cols, seed=7 * rows + cols)
 
 
