@@ -715,8 +715,16 @@ def c4_result():
         p.close()
         err = max(err, O.match_eigenvalues(ev[i], pev))
     del mats
+    hbm, kind = peaks()
+    gbs = stats["operator_bytes"] / (ms / 1e3) / 1e9
     return {"workload": "2048 complex problems n~U[32,512], top-4 LM, hdim=min(n,24), one persistent launch",
             "solves_per_s": conv / reps / (ms / 1e3), "launch_ms": ms, "converged_per_launch": conv / reps,
+            "variant": stats["variant"], "threads": stats["threads"], "ctas": stats["ctas"],
+            "matvecs": stats["matvecs"], "restarts": stats["restarts"],
+            "roofline": {"bound": "hbm", "algorithmic_bytes": stats["operator_bytes"], "achieved_GBs": gbs,
+                         "peak": hbm, "frac": gbs / hbm,
+                         "note": "operator bytes of every matvec (16 n^2 each, complex) over the launch time; the "
+                                 "problems in flight exceed L2, so each matvec streams its operator from HBM"},
             "problems": len(sizes), "max_residual": float(res.max()),
             "eig_err_vs_plain_fp64_sample8": err}
 

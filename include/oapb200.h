@@ -459,6 +459,11 @@ OAPB_EXPORT int oapb_mat_read(const char* path, const oapb_mat* dst, void* strea
  * optional device FP64 copy (NULL to skip).  Synchronises `stream`. */
 OAPB_EXPORT int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols,
                                 float* A, double* A64, void* stream);
+/* The build's workspace (BF16 hi / lo planes of X, 4 bytes per element of X,
+ * plus the tile partials) comes from a library-owned stream-ordered pool
+ * that keeps the memory for the next build; this returns it to the driver
+ * (current device; no counterpart in the reference). */
+OAPB_EXPORT int oapb_gram_trim(void);
 
 /* Image ingestion: `count` decoded RGB8 images of `pixels` pixels each
  * (rgb: count x pixels x 3 bytes, on the host when rgb_on_host, else on the
@@ -494,6 +499,9 @@ typedef struct oapb_batch_stats {
   double seconds;        /* host wall time of the call */
   uint32_t variant;      /* launch variant (cfg.autotune: 1 tunes, 2 + v forces v) */
   uint32_t threads;      /* threads per CTA of that variant */
+  uint64_t operator_bytes; /* operator bytes read by all matvecs (8 n^2 real,
+                              16 n^2 complex each): the launch's algorithmic
+                              HBM traffic */
 } oapb_batch_stats;
 
 /* Solve `count` independent eigenproblems (IEigenCalculator::calculate,

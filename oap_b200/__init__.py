@@ -77,7 +77,7 @@ class BatchStats(C.Structure):
     _fields_ = [("problems", C.c_uint32), ("converged", C.c_uint32),
                 ("matvecs", C.c_uint64), ("restarts", C.c_uint64),
                 ("ctas", C.c_uint32), ("seconds", C.c_double),
-                ("variant", C.c_uint32), ("threads", C.c_uint32)]
+                ("variant", C.c_uint32), ("threads", C.c_uint32), ("operator_bytes", C.c_uint64)]
 
 
 MATVEC_FN = C.CFUNCTYPE(C.c_int, C.POINTER(Mat), C.POINTER(Mat), C.c_void_p,
@@ -134,6 +134,7 @@ def lib():
             "oapb_arnoldi_set_profile": [vp, C.c_int32],
             "oapb_arnoldi_test_outcome": [vp, C.c_uint32, P(C.c_double)],
             "oapb_gram_build": [vp, C.c_uint32, C.c_uint32, vp, vp, vp],
+            "oapb_gram_trim": [],
             "oapb_arnoldi_set_start_shifts": [vp, P(C.c_double), C.c_uint32],
             "oapb_arnoldi_apply_block": [vp, vp, vp, C.c_uint32, vp, vp, C.c_int32],
             "oapb_arnoldi_set_gram_operator": [vp, vp, C.c_uint32, C.c_uint32],

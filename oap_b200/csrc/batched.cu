@@ -63,6 +63,7 @@ struct BatchArgs {
   int* status;      // count
   unsigned long long* matvecs;
   unsigned long long* restarts;
+  unsigned long long* op_bytes;  // operator bytes the matvecs read (8 n^2 real, 16 n^2 complex each)
 };
 
 struct BatchSmem {
@@ -431,6 +432,7 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
     A.status[P.index] = status;
     atomicAdd(A.matvecs, matvecs);
     atomicAdd(A.restarts, restarts);
+    atomicAdd(A.op_bytes, matvecs * (unsigned long long)(C ? 16 : 8) * (unsigned long long)n * n);
   }
   __syncthreads();
 }
@@ -625,6 +627,7 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
     A.counter = (int*)(buf + off_cnt);
     A.matvecs = (unsigned long long*)(buf + off_cnt) + 1;
     A.restarts = (unsigned long long*)(buf + off_cnt) + 2;
+    A.op_bytes = (unsigned long long*)(buf + off_cnt) + 3;
     A.mcap = mcap;
     A.k = k;
     A.which = cfg->sort;
@@ -672,6 +675,7 @@ int oapb_arnoldi_solve_batched(const oapb_arnoldi_config* cfg, const oapb_batch_
       for (uint32_t i = 0; i < count; ++i) stats->converged += status[i] == OAPB_OK;
       stats->matvecs = ctr[1];
       stats->restarts = ctr[2];
+      stats->operator_bytes = ctr[3];
       stats->ctas = (uint32_t)grids[variant];
       stats->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
       stats->variant = (uint32_t)variant;

@@ -34,6 +34,7 @@
 // Algorithmic work: 2 rows^2 cols flops (one product, counted once).
 #include <stdio.h>
 
+#include <mutex>
 #include <vector>
 
 #include "common.cuh"
@@ -54,17 +55,65 @@ constexpr uint32_t kGmSmem = kGmStages * kGmStageBytes + 1024;  // + alignment s
 constexpr uint64_t kGmWaitNs = 2000000000ull;                   // 2 s per wait
 constexpr int kGmTileElems = kGmM * kGmN;
 
-// hi / lo split into zero-padded (rows_p x cols_p) BF16 arrays
+// hi / lo split into zero-padded (rows_p x cols_p) BF16 arrays: block row
+// blockIdx.y, four consecutive elements per thread (a 16-byte load when the
+// row allows it, 8-byte stores)
 __global__ void k_split_bf16(const float* __restrict__ X, int rows, int cols, int rows_p, int cols_p,
                              __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-  const long total = (long)rows_p * cols_p;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-    const long r = e / cols_p, c = e % cols_p;
-    const float x = (r < rows && c < cols) ? X[r * cols + c] : 0.0f;
-    const __nv_bfloat16 h = __float2bfloat16_rn(x);
-    hi[e] = h;
-    lo[e] = __float2bfloat16_rn(x - __bfloat162float(h));
+  const bool vec = (cols & 3) == 0 && ((uintptr_t)X & 15) == 0;
+  for (int r = blockIdx.y; r < rows_p; r += gridDim.y) {
+    const float* xr = X + (long)r * cols;
+    __nv_bfloat16* hr = hi + (long)r * cols_p;
+    __nv_bfloat16* lr = lo + (long)r * cols_p;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) * 4; c < cols_p; c += gridDim.x * blockDim.x * 4) {
+      float v[4];
+      if (r < rows && vec && c + 3 < cols) {
+        const float4 x4 = __ldcs(reinterpret_cast<const float4*>(xr + c));
+        v[0] = x4.x, v[1] = x4.y, v[2] = x4.z, v[3] = x4.w;
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) v[j] = (r < rows && c + j < cols) ? xr[c + j] : 0.0f;
+      }
+      __align__(8) __nv_bfloat16 h[4], l[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        h[j] = __float2bfloat16_rn(v[j]);
+        l[j] = __float2bfloat16_rn(v[j] - __bfloat162float(h[j]));
+      }
+      // cols_p is a multiple of 32: the four outputs are in the row and 8-byte aligned
+      *reinterpret_cast<uint2*>(hr + c) = *reinterpret_cast<const uint2*>(h);
+      *reinterpret_cast<uint2*>(lr + c) = *reinterpret_cast<const uint2*>(l);
+    }
   }
+}
+
+// The build's workspace (BF16 planes, partials, tile list) comes from a
+// stream-ordered pool owned by the library, one per device, that keeps freed
+// memory for the next build instead of returning it to the driver at every
+// synchronisation (a 1 GiB workspace mapped anew per call took several
+// milliseconds).  oapb_gram_trim releases what it holds.
+static std::mutex g_gram_pool_mutex;
+static cudaMemPool_t g_gram_pool[64] = {};
+
+static cudaMemPool_t gram_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(g_gram_pool_mutex);
+  if (!g_gram_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_gram_pool[dev] = p;
+  }
+  return g_gram_pool[dev];
 }
 
 struct GramArgs {
@@ -289,7 +338,8 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
   const size_t ws_elems = (size_t)ntiles * 2 * kGmTileElems;
   const size_t bytes = 2 * half * sizeof(__nv_bfloat16) + ws_elems * sizeof(float) + tiles.size() * sizeof(int4) + 256;
   char* buf = nullptr;
-  if (cudaMallocAsync((void**)&buf, bytes, s) != cudaSuccess) {
+  cudaMemPool_t pool = gram_pool();
+  if (!pool || cudaMallocFromPoolAsync((void**)&buf, bytes, pool, s) != cudaSuccess) {
     cudaGetLastError();
     return OAPB_ERR_NOMEM;
   }
@@ -314,7 +364,10 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
       rc = OAPB_ERR_CUDA;
       break;
     }
-    k_split_bf16<<<kNumSMs * 8, 256, 0, s>>>(X, (int)rows, (int)cols, rows_p, cols_p, hi, lo);
+    {
+      const int bx = (int)std::min<long>((cols_p / 4 + 255) / 256, 16);
+      k_split_bf16<<<dim3(bx, std::min(rows_p, 65535)), 256, 0, s>>>(X, (int)rows, (int)cols, rows_p, cols_p, hi, lo);
+    }
     if (cudaFuncSetAttribute(k_gram_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGmSmem) !=
         cudaSuccess) {
       rc = OAPB_ERR_CUDA;
@@ -342,6 +395,14 @@ int oapb_gram_build(const float* X, uint32_t rows, uint32_t cols, float* A, doub
   } while (0);
   cudaFreeAsync(buf, s);
   return rc;
+}
+
+int oapb_gram_trim(void) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OAPB_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(g_gram_pool_mutex);
+  if (g_gram_pool[dev] && cudaMemPoolTrimTo(g_gram_pool[dev], 0) != cudaSuccess) return OAPB_ERR_CUDA;
+  return OAPB_OK;
 }
 
 }  // extern "C"

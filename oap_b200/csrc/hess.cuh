@@ -160,15 +160,42 @@ template <typename Cx, int NT>
 static __device__ __forceinline__ void warp_sweep_nt(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot,
                                                      int lane) {
   const int nt = (m + 31) >> 5;
-  Cx carry[NT];
+  const Cx zero = {0, 0};
+  Cx carry[NT], b[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int c = lane + 32 * t;
-    carry[t] = (t < nt && c >= l && c < m) ? TT_(l, c) : Cx{0, 0};
+    const bool own = t < nt && c >= l && c < m;
+    carry[t] = own ? TT_(l, c) : zero;
+    b[t] = own ? TT_(l + 1, c) : zero;
   }
   Cx D = TT_(l, l), E = TT_(l, l + 1), F = TT_(l + 1, l), G = TT_(l + 1, l + 1);
   Cx x = D - mu, y = F;
+  // start values the window needs at the next rotation, loaded one rotation
+  // ahead (rows below k + 1 are not written before rotation k + 1)
+  Cx s2 = l + 2 <= h ? TT_(l + 2, l + 1) : zero, g2 = l + 2 <= h ? TT_(l + 2, l + 2) : zero;
+  Cx t2 = l + 2 <= h ? TT_(l + 1, l + 2) : zero;
   for (int k = l; k < h; ++k) {
+    // prefetch for rotation k + 1
+    Cx bn[NT];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) {
+      const int c = lane + 32 * t;
+      bn[t] = (k + 2 <= h && t < nt && c >= l && c < m) ? TT_(k + 2, c) : zero;
+    }
+    const bool more = k + 3 <= h;
+    const Cx sn = more ? TT_(k + 3, k + 2) : zero, gn = more ? TT_(k + 3, k + 3) : zero;
+    const Cx tn = more ? TT_(k + 2, k + 3) : zero;
+    // row k's entry of column k + 2 before this rotation (off the chain)
+    Cx epre = zero;
+    if (k + 1 < h) {
+      const int c2 = k + 2;
+      Cx e = carry[0];
+#pragma unroll
+      for (int t = 1; t < NT; ++t)
+        if (t == (c2 >> 5)) e = carry[t];
+      epre = shfl_c(e, c2 & 31);
+    }
     Cx p, q;
     givens(x, y, p, q);
     if (lane == 0) {
@@ -176,34 +203,29 @@ static __device__ __forceinline__ void warp_sweep_nt(Cx* T, Cx* Z, int m, int ld
       rot[2 * k + 1] = q;
     }
     const Cx pc = conj(p), nqc = -conj(q);
-    // row rotation k on the lanes' columns (rows k, k + 1; row k + 1 is
-    // still the sweep's start value there)
+    // the window through rotation k on both sides, then the next one
+    if (k + 1 < h) {
+      const Cx F1 = nqc * D + pc * F, G1 = nqc * E + pc * G;
+      x = F1 * pc + G1 * conj(q);  // T[k+1][k]
+      y = s2 * conj(q);            // T[k+2][k], the bulge
+      D = (-F1) * q + G1 * p;      // T[k+1][k+1]
+      F = s2 * p;                  // T[k+2][k+1]
+      G = g2;                      // T[k+2][k+2]
+      E = nqc * epre + pc * t2;    // T[k+1][k+2] after row rotation k
+    }
+    // row rotation k on the lanes' columns (rows k, k + 1)
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
       const int c = lane + 32 * t;
       if (t < nt && c >= l && c < m) {
-        const Cx b = TT_(k + 1, c);
-        TT_(k, c) = p * carry[t] + q * b;
-        carry[t] = nqc * carry[t] + pc * b;
+        TT_(k, c) = p * carry[t] + q * b[t];
+        carry[t] = nqc * carry[t] + pc * b[t];
       }
+      b[t] = bn[t];
     }
-    // the window through rotation k on both sides, then the next one
-    if (k + 1 < h) {
-      const Cx F1 = nqc * D + pc * F, G1 = nqc * E + pc * G;
-      const Cx s = TT_(k + 2, k + 1);  // untouched so far
-      x = F1 * pc + G1 * conj(q);       // T[k+1][k]
-      y = s * conj(q);                  // T[k+2][k], the bulge
-      D = (-F1) * q + G1 * p;           // T[k+1][k+1]
-      F = s * p;                        // T[k+2][k+1]
-      G = TT_(k + 2, k + 2);
-      // T[k+1][k+2] after row rotation k: the carry of column k + 2
-      const int c2 = k + 2;
-      Cx e = carry[0];
-#pragma unroll
-      for (int t = 1; t < NT; ++t)
-        if (t == (c2 >> 5)) e = carry[t];
-      E = shfl_c(e, c2 & 31);
-    }
+    s2 = sn;
+    g2 = gn;
+    t2 = tn;
   }
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
@@ -211,32 +233,31 @@ static __device__ __forceinline__ void warp_sweep_nt(Cx* T, Cx* Z, int m, int ld
     if (t < nt && c >= l && c < m) TT_(h, c) = carry[t];
   }
   __syncwarp();
-  // column rotations l .. h-1 on rows 0 .. h (one lane per row)
-  for (int i = lane; i <= h; i += 32) {
-    Cx c = TT_(i, l);
+  // column rotations l .. h-1 on rows 0 .. h of T and on every row of Z (one
+  // lane per row); then the rounding-level entries the interleaved sweep
+  // never fills, below the subdiagonal of the window, are set to zero
+  for (int i = lane; i < m; i += 32) {
+    const bool trow = i <= h;
+    Cx c = trow ? TT_(i, l) : zero;
+    Cx cz = Z ? ZZ_(i, l) : zero;
     for (int k = l; k < h; ++k) {
-      const Cx p = rot[2 * k], q = rot[2 * k + 1];
-      const Cx nb = TT_(i, k + 1);
-      TT_(i, k) = c * conj(p) + nb * conj(q);
-      c = (-c) * q + nb * p;
-    }
-    TT_(i, h) = c;
-  }
-  __syncwarp();
-  // below the subdiagonal of the window: rounding-level values -> 0
-  for (int i = l + 2 + lane; i <= h; i += 32)
-    for (int c = l; c <= i - 2; ++c) TT_(i, c) = Cx{0, 0};
-  if (Z) {
-    for (int i = lane; i < m; i += 32) {
-      Cx c = ZZ_(i, l);
-      for (int k = l; k < h; ++k) {
-        const Cx p = rot[2 * k], q = rot[2 * k + 1];
-        const Cx z1 = ZZ_(i, k + 1);
-        ZZ_(i, k) = c * conj(p) + z1 * conj(q);
-        c = (-c) * q + z1 * p;
+      const Cx p = rot[2 * k], q = rot[2 * k + 1], pc = conj(p), qc = conj(q);
+      if (trow) {
+        const Cx nb = TT_(i, k + 1);
+        TT_(i, k) = c * pc + nb * qc;
+        c = (-c) * q + nb * p;
       }
-      ZZ_(i, h) = c;
+      if (Z) {
+        const Cx z1 = ZZ_(i, k + 1);
+        ZZ_(i, k) = cz * pc + z1 * qc;
+        cz = (-cz) * q + z1 * p;
+      }
     }
+    if (trow) {
+      TT_(i, h) = c;
+      for (int cc = l; cc <= i - 2; ++cc) TT_(i, cc) = zero;
+    }
+    if (Z) ZZ_(i, h) = cz;
   }
   __syncwarp();
 }

@@ -41,6 +41,21 @@ def test_gram_tensor_cores(rows, cols):
     check_gram(rows, cols, seed=rows + cols)
 
 
+def test_gram_workspace_pool_reuse_and_trim():
+    # the build's workspace comes from a library-owned pool that keeps it for
+    # the next build: repeated builds give identical results; trimming the
+    # pool returns its memory and the next build still runs
+    g = torch.Generator(device="cuda")
+    g.manual_seed(3)
+    X = torch.rand(700, 2500, dtype=torch.float32, device="cuda", generator=g)
+    A1, _ = B.gram_build(X)
+    A2, _ = B.gram_build(X)
+    assert torch.equal(A1, A2)
+    assert B.lib().oapb_gram_trim() == B.OK
+    A3, _ = B.gram_build(X)
+    assert torch.equal(A1, A3)
+
+
 @pytest.mark.parametrize("rows,cols", [(3000, 1000), (4096, 160)])
 def test_gram_more_tiles_than_sms(rows, cols):
     # more upper-triangle tiles than SMs (156 and 272): a second wave of
