@@ -354,56 +354,51 @@ __device__ void warp_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, Cho
 __device__ __forceinline__ void chol_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
 
 // The same with nthr threads of a block (whole warps, tid = 0 .. nthr - 1,
-// all calling): per step k one thread takes the pivot, then every trailing
-// entry R[i][j] (k < i <= j) has a thread of its own; the inverse X = R^-1
-// goes up the rows, X[i][j] for all j > i in parallel.  A barrier (chol_bar)
-// per phase.
+// all calling), by symmetric Gaussian elimination on [G | I]: step k takes
+// the pivot d_k = M[k][k] and, for every row i > k, subtracts
+// conj(M[k][i]) / d_k times row k from the upper-triangular part of row i
+// and from the entries of the augmented part left of the diagonal (the
+// multiplier M[i][k] of the Hermitian trailing matrix is conj(M[k][i])).
+// Row k is read and rows below it are written, so one barrier per step
+// suffices; every updated entry has a thread of its own when nthr >= (b - 1)
+// b.  At the end the augmented part holds L^-1 of G = L D L^H (unit lower
+// triangular), so R = D^1/2 L^H and Rinv = L^-H D^-1/2:
+// Rinv[r][c] = conj(L^-1[c][r]) / sqrt(d_c), r <= c.
 __device__ void block_chol_inv(const cplx* G, int b, cplx* Rinv, int* status, CholSmem& sm, int tid, int nthr) {
   constexpr int LD = kCholLD;
-  cplx* R = sm.R;
-  cplx* X = sm.X;
+  cplx* M = sm.R;  // left part: M[i + c LD], upper triangle in use
+  cplx* L = sm.X;  // augmented part: L[i + c LD] = L^-1[i][c]
   double* rd = sm.rd;
   for (int e = tid; e < b * b; e += nthr) {  // L2 loads: G may come from other blocks of the caller
     const double* gp = reinterpret_cast<const double*>(G + e);
-    R[e % b + (e / b) * LD] = cplx{__ldcg(gp), __ldcg(gp + 1)};
+    const int r = e % b, c = e / b;
+    M[r + c * LD] = cplx{__ldcg(gp), __ldcg(gp + 1)};
+    L[r + c * LD] = cplx{r == c ? 1.0 : 0.0, 0.0};
   }
   chol_bar(nthr);
-  for (int k = 0; k < b; ++k) {
-    if (tid == 0) {
-      const double piv = R[k + k * LD].re;
-      const double rkk = piv > 0 ? sqrt(piv) : 1e-300;
-      if (!(piv > 0)) atomicOr(status, 4);
-      rd[k] = 1.0 / rkk;
-      R[k + k * LD] = cplx{rkk, 0};
-    }
-    chol_bar(nthr);
-    for (int j = k + 1 + tid; j < b; j += nthr) R[k + j * LD] = rd[k] * R[k + j * LD];
-    chol_bar(nthr);
+  for (int k = 0; k + 1 < b; ++k) {
+    const double piv = M[k + k * LD].re;
+    const double inv = 1.0 / (piv > 0 ? piv : 1e-300);
     const int t = b - k - 1;
-    for (int e = tid; e < t * t; e += nthr) {
-      const int i = k + 1 + e / t, j = k + 1 + e % t;
-      if (i <= j) R[i + j * LD] = R[i + j * LD] - conj(R[k + i * LD]) * R[k + j * LD];
+    for (int e = tid; e < t * b; e += nthr) {
+      const int i = k + 1 + e / b, c = e % b;
+      const cplx mi = inv * conj(M[k + i * LD]);  // M[i][k] / d_k
+      if (c >= i)
+        M[i + c * LD] = M[i + c * LD] - mi * M[k + c * LD];
+      else if (c <= k)
+        L[i + c * LD] = L[i + c * LD] - mi * L[k + c * LD];
     }
     chol_bar(nthr);
   }
-  for (int j = tid; j < b; j += nthr) X[j + j * LD] = cplx{rd[j], 0};
+  for (int j = tid; j < b; j += nthr) {
+    const double piv = M[j + j * LD].re;
+    if (!(piv > 0)) atomicOr(status, 4);
+    rd[j] = rsqrt(piv > 0 ? piv : 1e-300);
+  }
   chol_bar(nthr);
-  for (int i = b - 2; i >= 0; --i) {
-    for (int j = i + 1 + tid; j < b; j += nthr) {
-      cplx a0 = {0, 0}, a1 = {0, 0};
-      int p = i + 1;
-      for (; p + 1 <= j; p += 2) {
-        a0 = a0 + R[i + p * LD] * X[p + j * LD];
-        a1 = a1 + R[i + (p + 1) * LD] * X[p + 1 + j * LD];
-      }
-      if (p <= j) a0 = a0 + R[i + p * LD] * X[p + j * LD];
-      X[i + j * LD] = (-rd[i]) * (a0 + a1);
-    }
-    chol_bar(nthr);
-  }
   for (int e = tid; e < b * b; e += nthr) {
     const int r = e % b, c = e / b;
-    Rinv[e] = r <= c ? X[r + c * LD] : cplx{0, 0};
+    Rinv[e] = r <= c ? rd[c] * conj(L[c + r * LD]) : cplx{0, 0};
   }
 }
 
@@ -527,11 +522,11 @@ __global__ void __launch_bounds__(1024) k_block_reduce(const cplx* __restrict__ 
   __syncthreads();
   if (!last) return;
   __threadfence();
-  // the factor and its inverse on 8 warps (a barrier per phase costs less
-  // with fewer warps; the trailing updates have at most 31 x 31 entries)
-  constexpr int kCholThreads = 256;
-  if (ty * 32 + tx >= kCholThreads) return;
-  block_chol_inv(G, b, Rinv, status, sm.chol, ty * 32 + tx, kCholThreads);
+  // the factor and its inverse on the warps that give every entry of a
+  // step's update a thread of its own ((b - 1) b of them)
+  const int nthr = ((b - 1) * b + 31) / 32 * 32 < 32 ? 32 : ((b - 1) * b + 31) / 32 * 32;
+  if (ty * 32 + tx >= nthr) return;
+  block_chol_inv(G, b, Rinv, status, sm.chol, ty * 32 + tx, nthr);
   if (tx == 0 && ty == 0) *done = 0;
 }
 

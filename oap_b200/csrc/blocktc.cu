@@ -444,21 +444,27 @@ int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_
 }
 
 // stream-K grid over (tile, stage) iterations of kh K chunks each
-static SkGrid btc_grid(int n, int kp, int kh) {
-  return sk_grid((n + kBtcM - 1) / kBtcM, kp / (kBtcK * kh), kNumSMs);
+static SkGrid btc_grid(int n, int kp, int kh, int ctas = kNumSMs) {
+  return sk_grid((n + kBtcM - 1) / kBtcM, kp / (kBtcK * kh), ctas);
 }
 
 size_t btc_workspace(int n, int kp) {
-  const size_t a = sk_workspace(btc_grid(n, kp, 1)), b = sk_workspace(btc_grid(n, kp, 2));
-  return a > b ? a : b;
+  size_t w = 0;
+  for (int kh = 1; kh <= 2; ++kh)
+    for (int c = kNumSMs - 1; c <= kNumSMs; ++c) {
+      const size_t x = sk_workspace(btc_grid(n, kp, kh, c));
+      w = x > w ? x : w;
+    }
+  return w;
 }
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only, bool x_hi_only) {
+                           cudaStream_t s, bool bf16_only, bool x_hi_only, int ctas) {
   const bool cplx = op.aih != nullptr;
   const int kh = bf16_only ? 2 : 1;
   if (b < 1 || b > 32 || op.kp % (kBtcK * kh) != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
+  if (ctas < kNumSMs - 1 || ctas > kNumSMs) return OAPB_ERR_ARG;  // the workspace covers these grids
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
@@ -472,7 +478,7 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   if (!make_tmap(&g.tm[4], xbh, op.kp, N, N) || !make_tmap(&g.tm[5], xbl, op.kp, N, N)) return OAPB_ERR_CUDA;
   g.ws = ws;
   g.err = err;
-  g.grid = btc_grid(op.n, op.kp, kh);
+  g.grid = btc_grid(op.n, op.kp, kh, ctas);
   g.n = op.n;
   g.b = b;
   g.QB = QB;

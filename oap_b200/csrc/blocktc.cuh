@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stddef.h>
 
+#include "common.cuh"
+
 namespace oapb {
 
 // Operator stored as BF16 hi / lo planes, n x kp (kp = n rounded up to 128,
@@ -19,7 +21,8 @@ struct BtcOperator {
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
                         long row0 = 0, long rows = -1, double* err2 = nullptr);
 
-// Doubles of stream-K partial workspace for an n x n operator (b <= 32).
+// Doubles of stream-K partial workspace for an n x n operator (b <= 32),
+// for a grid of any CTA count from kNumSMs - 1 to kNumSMs.
 size_t btc_workspace(int n, int kp);
 
 // W (planes wr / wi, vector q at offset q n) = A X for b <= 32 vectors (X
@@ -27,8 +30,10 @@ size_t btc_workspace(int n, int kp);
 // block); ws: btc_workspace() doubles; *err receives timeout bits.
 // bf16_only: the operator's hi planes only (half the bytes, BF16 accuracy);
 // x_hi_only (with bf16_only): X rounded to BF16 as well (its lo part unused).
+// ctas: stream-K CTAs (kNumSMs - 1 leaves one SM to kernels of another
+// stream; every CTA holds most of its SM's shared memory).
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only = false, bool x_hi_only = false);
+                           cudaStream_t s, bool bf16_only = false, bool x_hi_only = false, int ctas = kNumSMs);
 
 }  // namespace oapb

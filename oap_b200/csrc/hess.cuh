@@ -83,11 +83,61 @@ struct HessK;
 template <>
 struct HessK<double> {
   static constexpr double eps = 2.220446049250313e-16, tiny = 1e-300, big = 1e150, unbig = 1e-150;
+  static constexpr double tiny2 = 1e-280;  // |x|^2 + |y|^2 of a negligible pair (prescaled matrix)
 };
 template <>
 struct HessK<float> {
   static constexpr float eps = 1.1920929e-7f, tiny = 1e-37f, big = 1e30f, unbig = 1e-30f;
+  static constexpr float tiny2 = 1e-36f;
 };
+
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float rsqrt_t(float a) { return rsqrtf(a); }
+__device__ __forceinline__ double rsqrt_t(double a) { return rsqrt(a); }
+__device__ __forceinline__ float sqrt_t(float a) { return sqrtf(a); }
+__device__ __forceinline__ float abs_t(float a) { return fabsf(a); }
+__device__ __forceinline__ double abs_t(double a) { return fabs(a); }
+__device__ __forceinline__ double sqrt_t(double a) { return sqrt(a); }
+
+// a b + c with fused multiply-adds
+template <typename Cx>
+__device__ __forceinline__ Cx cfma(Cx a, Cx b, Cx c) {
+  return {fma_t(a.re, b.re, fma_t(-a.im, b.im, c.re)), fma_t(a.re, b.im, fma_t(a.im, b.re, c.im))};
+}
+// a b + c d
+template <typename Cx>
+__device__ __forceinline__ Cx cfma2(Cx a, Cx b, Cx c, Cx d) {
+  return cfma(a, b, c * d);
+}
+
+// The rotation of givens() (p x + q y = sqrt(|x|^2 + |y|^2), p = conj(x) / r,
+// q = conj(y) / r) for entries of a matrix that hess_core has scaled to a
+// largest entry in [1, 2): the sum of squares cannot overflow, and a pair
+// whose squares sum below tiny2 (far below the working precision relative
+// to the matrix) gives the identity.  No branch: the sweep's rotation chain
+// stays one straight block of instructions.
+template <typename Cx>
+__device__ __forceinline__ void givens_s(Cx x, Cx y, Cx& p, Cx& q) {
+  using R = decltype(Cx::re);
+  const R r2 = fma_t(x.re, x.re, fma_t(x.im, x.im, fma_t(y.re, y.re, y.im * y.im)));
+  const bool ok = r2 > HessK<R>::tiny2;
+  const R ir = rsqrt_t(ok ? r2 : R(1));
+  p = ok ? Cx{x.re * ir, -x.im * ir} : Cx{1, 0};
+  q = ok ? Cx{y.re * ir, -y.im * ir} : Cx{0, 0};
+}
+
+// principal square root of z (prescaled entries: |z| stays far inside the
+// range), re >= 0
+template <typename Cx>
+__device__ __forceinline__ Cx csqrt_s(Cx z) {
+  using R = decltype(Cx::re);
+  const R r = sqrt_t(abs2(z));
+  const R u = R(0.5) * (r + abs_t(z.re));
+  const R iu = rsqrt_t(u > 0 ? u : R(1));
+  const R t = u > 0 ? u * iu : R(0), hh = u > 0 ? R(0.5) * z.im * iu : R(0);  // sqrt(u), im / (2 sqrt(u))
+  return z.re >= 0 ? Cx{t, hh} : Cx{abs_t(hh), z.im >= 0 ? t : -t};
+}
 
 __device__ __forceinline__ double warp_sum_t(double v) { return warp_sum(v); }
 __device__ __forceinline__ float warp_sum_t(float v) { return warp_sumf(v); }
@@ -140,6 +190,7 @@ static __device__ int find_split(const Cx* T, int ld, int h, int lane) {
 // One single-shift QR sweep on the active window [l, h] of Hessenberg T,
 // applied to whole rows / columns of T (the final T is G T G^H with G =
 // G_{h-1} ... G_l); Z <- Z G_l^H ... G_{h-1}^H.  rot: 2 m cplx of scratch.
+// T must be prescaled (hess_core): the rotations come from givens_s.
 //
 // The rotations form a dependent chain: rotation k needs the bulge pair
 // left by rotation k - 1.  That chain runs in registers: every lane carries
@@ -149,130 +200,127 @@ static __device__ int find_split(const Cx* T, int ld, int h, int lane) {
 // column k + 1.  The matrix itself is updated off the chain: while the chain
 // runs, lane c applies each row rotation to column c (its row-k entry carried
 // in a register, the row-(k+1) entry read once), and after the chain one
-// lane per row applies all column rotations to its row.  Left and right
-// rotations commute, so the result is G T G^H as in the interleaved sweep;
-// the entries below the subdiagonal that the interleaved sweep never fills
-// come out of this order at rounding level and are set to zero.  Per
-// rotation the chain costs one rotation, one shuffle and a few complex
-// multiply-adds instead of two shared-memory passes and two warp barriers.
-// NT: columns per lane (c = lane + 32 t, t < NT); m <= 32 NT.
-template <typename Cx, int NT>
+// lane per row applies all column rotations to its row of T and of Z.  Left
+// and right rotations commute, so the result is G T G^H as in the
+// interleaved sweep; the entries below the subdiagonal that the interleaved
+// sweep never fills come out of this order at rounding level and are set
+// to zero.  The loop over rotations l .. h-2 has no branch (the last
+// rotation, which has no next window, is peeled): a single warp issues it
+// as one straight block, so the row updates fill the chain's latency.
+// NT: columns per lane (c = lane + 32 t, t < NT); m <= 32 NT.  WZ: Z is
+// updated (Z non-null).
+template <typename Cx, int NT, bool WZ>
 static __device__ __forceinline__ void warp_sweep_nt(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot,
                                                      int lane) {
   const int nt = (m + 31) >> 5;
   const Cx zero = {0, 0};
   Cx carry[NT], b[NT];
+  bool own[NT];
 #pragma unroll
   for (int t = 0; t < NT; ++t) {
     const int c = lane + 32 * t;
-    const bool own = t < nt && c >= l && c < m;
-    carry[t] = own ? TT_(l, c) : zero;
-    b[t] = own ? TT_(l + 1, c) : zero;
+    own[t] = t < nt && c >= l && c < m;
+    carry[t] = own[t] ? TT_(l, c) : zero;
+    b[t] = own[t] ? TT_(l + 1, c) : zero;
   }
   Cx D = TT_(l, l), E = TT_(l, l + 1), F = TT_(l + 1, l), G = TT_(l + 1, l + 1);
   Cx x = D - mu, y = F;
-  // start values the window needs at the next rotation, loaded one rotation
-  // ahead (rows below k + 1 are not written before rotation k + 1)
-  Cx s2 = l + 2 <= h ? TT_(l + 2, l + 1) : zero, g2 = l + 2 <= h ? TT_(l + 2, l + 2) : zero;
-  Cx t2 = l + 2 <= h ? TT_(l + 1, l + 2) : zero;
-  for (int k = l; k < h; ++k) {
-    // prefetch for rotation k + 1
+  int k = l;
+  for (; k + 1 < h; ++k) {
+    // inputs of this step from rows k + 1, k + 2 (not written before it)
     Cx bn[NT];
 #pragma unroll
-    for (int t = 0; t < NT; ++t) {
-      const int c = lane + 32 * t;
-      bn[t] = (k + 2 <= h && t < nt && c >= l && c < m) ? TT_(k + 2, c) : zero;
-    }
-    const bool more = k + 3 <= h;
-    const Cx sn = more ? TT_(k + 3, k + 2) : zero, gn = more ? TT_(k + 3, k + 3) : zero;
-    const Cx tn = more ? TT_(k + 2, k + 3) : zero;
-    // row k's entry of column k + 2 before this rotation (off the chain)
-    Cx epre = zero;
-    if (k + 1 < h) {
-      const int c2 = k + 2;
-      Cx e = carry[0];
+    for (int t = 0; t < NT; ++t) bn[t] = own[t] ? TT_(k + 2, lane + 32 * t) : zero;
+    const Cx s2 = TT_(k + 2, k + 1), g2 = TT_(k + 2, k + 2), t2 = TT_(k + 1, k + 2);
+    // row k's entry of column k + 2 before this rotation
+    const int c2 = k + 2;
+    Cx e = carry[0];
 #pragma unroll
-      for (int t = 1; t < NT; ++t)
-        if (t == (c2 >> 5)) e = carry[t];
-      epre = shfl_c(e, c2 & 31);
-    }
+    for (int t = 1; t < NT; ++t)
+      if (t == (c2 >> 5)) e = carry[t];
+    const Cx epre = shfl_c(e, c2 & 31);
     Cx p, q;
-    givens(x, y, p, q);
-    if (lane == 0) {
-      rot[2 * k] = p;
-      rot[2 * k + 1] = q;
-    }
-    const Cx pc = conj(p), nqc = -conj(q);
+    givens_s(x, y, p, q);
+    rot[2 * k] = p;  // every lane stores the same values
+    rot[2 * k + 1] = q;
+    const Cx pc = conj(p), qc = conj(q), nqc = -qc;
     // the window through rotation k on both sides, then the next one
-    if (k + 1 < h) {
-      const Cx F1 = nqc * D + pc * F, G1 = nqc * E + pc * G;
-      x = F1 * pc + G1 * conj(q);  // T[k+1][k]
-      y = s2 * conj(q);            // T[k+2][k], the bulge
-      D = (-F1) * q + G1 * p;      // T[k+1][k+1]
-      F = s2 * p;                  // T[k+2][k+1]
-      G = g2;                      // T[k+2][k+2]
-      E = nqc * epre + pc * t2;    // T[k+1][k+2] after row rotation k
-    }
+    const Cx F1 = cfma2(nqc, D, pc, F), G1 = cfma2(nqc, E, pc, G);
+    x = cfma2(F1, pc, G1, qc);   // T[k+1][k]
+    y = s2 * qc;                 // T[k+2][k], the bulge
+    D = cfma2(-F1, q, G1, p);    // T[k+1][k+1]
+    F = s2 * p;                  // T[k+2][k+1]
+    G = g2;                      // T[k+2][k+2]
+    E = cfma2(nqc, epre, pc, t2);  // T[k+1][k+2] after row rotation k
     // row rotation k on the lanes' columns (rows k, k + 1)
 #pragma unroll
     for (int t = 0; t < NT; ++t) {
-      const int c = lane + 32 * t;
-      if (t < nt && c >= l && c < m) {
-        TT_(k, c) = p * carry[t] + q * b[t];
-        carry[t] = nqc * carry[t] + pc * b[t];
+      if (own[t]) {
+        TT_(k, lane + 32 * t) = cfma2(p, carry[t], q, b[t]);
+        carry[t] = cfma2(nqc, carry[t], pc, b[t]);
       }
       b[t] = bn[t];
     }
-    s2 = sn;
-    g2 = gn;
-    t2 = tn;
   }
+  {  // rotation h - 1
+    Cx p, q;
+    givens_s(x, y, p, q);
+    rot[2 * k] = p;
+    rot[2 * k + 1] = q;
+    const Cx pc = conj(p), nqc = -conj(q);
 #pragma unroll
-  for (int t = 0; t < NT; ++t) {
-    const int c = lane + 32 * t;
-    if (t < nt && c >= l && c < m) TT_(h, c) = carry[t];
+    for (int t = 0; t < NT; ++t) {
+      if (own[t]) {
+        TT_(k, lane + 32 * t) = cfma2(p, carry[t], q, b[t]);
+        TT_(h, lane + 32 * t) = cfma2(nqc, carry[t], pc, b[t]);
+      }
+    }
   }
   __syncwarp();
   // column rotations l .. h-1 on rows 0 .. h of T and on every row of Z (one
-  // lane per row); then the rounding-level entries the interleaved sweep
-  // never fills, below the subdiagonal of the window, are set to zero
+  // lane per row); the entries below the subdiagonal of the window (rows
+  // i >= k + 2 of column k) are set to zero.  Rows below h hold zeros in
+  // these columns: their T stores are skipped.
   for (int i = lane; i < m; i += 32) {
     const bool trow = i <= h;
-    Cx c = trow ? TT_(i, l) : zero;
-    Cx cz = Z ? ZZ_(i, l) : zero;
-    for (int k = l; k < h; ++k) {
-      const Cx p = rot[2 * k], q = rot[2 * k + 1], pc = conj(p), qc = conj(q);
-      if (trow) {
-        const Cx nb = TT_(i, k + 1);
-        TT_(i, k) = c * pc + nb * qc;
-        c = (-c) * q + nb * p;
-      }
-      if (Z) {
-        const Cx z1 = ZZ_(i, k + 1);
-        ZZ_(i, k) = cz * pc + z1 * qc;
-        cz = (-cz) * q + z1 * p;
+    Cx c = TT_(i, l);
+    Cx cz = WZ ? ZZ_(i, l) : zero;
+    for (int kk = l; kk < h; ++kk) {
+      const Cx p = rot[2 * kk], q = rot[2 * kk + 1], pc = conj(p), qc = conj(q);
+      const Cx nb = TT_(i, kk + 1);
+      const Cx tk = cfma2(c, pc, nb, qc);
+      if (trow) TT_(i, kk) = kk + 2 <= i ? zero : tk;
+      c = cfma2(-c, q, nb, p);
+      if (WZ) {
+        const Cx z1 = ZZ_(i, kk + 1);
+        ZZ_(i, kk) = cfma2(cz, pc, z1, qc);
+        cz = cfma2(-cz, q, z1, p);
       }
     }
-    if (trow) {
-      TT_(i, h) = c;
-      for (int cc = l; cc <= i - 2; ++cc) TT_(i, cc) = zero;
-    }
-    if (Z) ZZ_(i, h) = cz;
+    if (trow) TT_(i, h) = c;
+    if (WZ) ZZ_(i, h) = cz;
   }
   __syncwarp();
 }
 
 // the carries stay in registers when their count is fixed by m's range
+template <typename Cx, bool WZ>
+static __device__ void warp_sweep_z(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot, int lane) {
+  if (m <= 32)
+    warp_sweep_nt<Cx, 1, WZ>(T, Z, m, ld, l, h, mu, rot, lane);
+  else if (m <= 64)
+    warp_sweep_nt<Cx, 2, WZ>(T, Z, m, ld, l, h, mu, rot, lane);
+  else if (m <= 128)
+    warp_sweep_nt<Cx, 4, WZ>(T, Z, m, ld, l, h, mu, rot, lane);
+  else
+    warp_sweep_nt<Cx, kMaxM / 32, WZ>(T, Z, m, ld, l, h, mu, rot, lane);
+}
 template <typename Cx>
 static __device__ void warp_sweep(Cx* T, Cx* Z, int m, int ld, int l, int h, Cx mu, Cx* rot, int lane) {
-  if (m <= 32)
-    warp_sweep_nt<Cx, 1>(T, Z, m, ld, l, h, mu, rot, lane);
-  else if (m <= 64)
-    warp_sweep_nt<Cx, 2>(T, Z, m, ld, l, h, mu, rot, lane);
-  else if (m <= 128)
-    warp_sweep_nt<Cx, 4>(T, Z, m, ld, l, h, mu, rot, lane);
+  if (Z)
+    warp_sweep_z<Cx, true>(T, Z, m, ld, l, h, mu, rot, lane);
   else
-    warp_sweep_nt<Cx, kMaxM / 32>(T, Z, m, ld, l, h, mu, rot, lane);
+    warp_sweep_z<Cx, false>(T, Z, m, ld, l, h, mu, rot, lane);
 }
 
 // Householder reduction of dense T to Hessenberg form, Z accumulating.
@@ -335,6 +383,94 @@ static __device__ void warp_hessenberg(Cx* T, Cx* Z, Cx* v, int m, int ld, int l
   }
 }
 
+// The same reduction for FP32 and m <= 32 with the work in registers: lane
+// j holds column j of T while the reflector acts from the left (P T), the
+// matrix goes through shared memory once per step so that lane i takes row
+// i of T and of Z for the right-hand side (T P, Z P), and comes back as
+// columns.  Every loop runs over the 32 possible rows / columns unrolled,
+// the entries outside the m x m matrix being zero in registers (and never
+// stored), so a step is one straight block of independent loads and
+// multiply-adds.  v (32 entries of scratch, zero outside rows k+1 .. m-1)
+// carries the reflector; |v|^2 = 2 a (a + |x0|) needs no second reduction.
+static __device__ void warp_hessenberg_r32(cplxf* T, cplxf* Z, cplxf* v, int m, int ld, int lane) {
+  constexpr int W = 32;
+  const cplxf zero = {0.f, 0.f};
+  const bool lc = lane < m;
+  cplxf col[W];
+#pragma unroll
+  for (int i = 0; i < W; ++i) col[i] = (lc && i < m) ? TT_(i, lane) : zero;
+  for (int k = 0; k + 2 < m; ++k) {
+    __syncwarp();  // the previous step's reads of v are done
+    if (lane == k) {
+#pragma unroll
+      for (int i = 0; i < W; ++i) v[i] = i > k ? col[i] : zero;
+    }
+    __syncwarp();
+    const float s = warp_sumf(abs2(v[lane]));
+    if (s == 0) continue;  // (warp-uniform) column k is reduced already
+    const cplxf x0 = v[k + 1];
+    const float a = sqrtf(s), ax0 = sqrtf(abs2(x0));
+    const cplxf ph = ax0 > 0 ? cplxf{x0.re / ax0, x0.im / ax0} : cplxf{1.f, 0.f};
+    const float f = 1.f / (a * (a + ax0));  // 2 / |v|^2
+    __syncwarp();
+    if (lane == 0) v[k + 1] = x0 + a * ph;
+    __syncwarp();
+    // P T: lane j, w = f v^H T(:, j), T(:, j) -= v w (columns left of k
+    // have zeros where v is non-zero: w = 0 there)
+    cplxf w0 = zero, w1 = zero, w2 = zero, w3 = zero;
+#pragma unroll
+    for (int i = 0; i < W; i += 4) {
+      w0 = cfma(conj(v[i]), col[i], w0);
+      w1 = cfma(conj(v[i + 1]), col[i + 1], w1);
+      w2 = cfma(conj(v[i + 2]), col[i + 2], w2);
+      w3 = cfma(conj(v[i + 3]), col[i + 3], w3);
+    }
+    const cplxf w = f * ((w0 + w1) + (w2 + w3));
+#pragma unroll
+    for (int i = 0; i < W; ++i) col[i] = cfma(-v[i], w, col[i]);
+    if (lane == k) {  // below the subdiagonal of column k: exact zeros
+#pragma unroll
+      for (int i = 0; i < W; ++i)
+        if (i >= k + 2) col[i] = zero;
+    }
+#pragma unroll
+    for (int i = 0; i < W; ++i)
+      if (lc && i < m) TT_(i, lane) = col[i];
+    __syncwarp();
+    // T P and Z P: lane i, y = f T(i, :) v, T(i, :) -= y v^H (same for Z)
+    if (lc) {
+      cplxf r[W];
+      cplxf y0 = zero, y1 = zero;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        r[j] = j < m ? TT_(lane, j) : zero;
+        if (j & 1) y1 = cfma(r[j], v[j], y1);
+        else y0 = cfma(r[j], v[j], y0);
+      }
+      const cplxf y = f * (y0 + y1);
+#pragma unroll
+      for (int j = 0; j < W; ++j)
+        if (j < m) TT_(lane, j) = cfma(-y, conj(v[j]), r[j]);
+      y0 = zero;
+      y1 = zero;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        r[j] = j < m ? ZZ_(lane, j) : zero;
+        if (j & 1) y1 = cfma(r[j], v[j], y1);
+        else y0 = cfma(r[j], v[j], y0);
+      }
+      const cplxf yz = f * (y0 + y1);
+#pragma unroll
+      for (int j = 0; j < W; ++j)
+        if (j < m) ZZ_(lane, j) = cfma(-yz, conj(v[j]), r[j]);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < W; ++i) col[i] = (lc && i < m) ? TT_(i, lane) : zero;
+  }
+  __syncwarp();
+}
+
 // Complex Schur form in place; returns false when the sweep budget ran out.
 template <typename Cx>
 static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane) {
@@ -350,17 +486,15 @@ static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane
       continue;
     }
     if (++total > 30 * m) return false;
-    Cx a = TT_(h - 1, h - 1), b = TT_(h - 1, h), c = TT_(h, h - 1), d = TT_(h, h);
-    Cx mu;
-    if (its > 0 && its % 10 == 0) {
-      mu = d + Cx{cabs_(c), 0};
-    } else {
-      Cx tr2 = R(0.5) * (a + d);
-      Cx amd = R(0.5) * (a - d);
-      Cx disc = csqrt_(amd * amd + b * c);
-      Cx m1 = tr2 + disc, m2 = tr2 - disc;
-      mu = cabs_(m1 - d) < cabs_(m2 - d) ? m1 : m2;
-    }
+    // Wilkinson shift: the eigenvalue of the trailing 2 x 2 nearer d
+    // (prescaled entries: squared moduli stay in range); every tenth sweep
+    // of a window an exceptional shift d + |c|
+    const Cx a = TT_(h - 1, h - 1), b = TT_(h - 1, h), c = TT_(h, h - 1), d = TT_(h, h);
+    const Cx tr2 = R(0.5) * (a + d), amd = R(0.5) * (a - d);
+    const Cx disc = csqrt_s(cfma(amd, amd, b * c));
+    const Cx m1 = tr2 + disc, m2 = tr2 - disc;
+    Cx mu = abs2(m1 - d) < abs2(m2 - d) ? m1 : m2;
+    if (its > 0 && its % 10 == 0) mu = d + Cx{sqrt_t(abs2(c)), 0};
     warp_sweep(T, Z, m, ld, l, h, mu, rot, lane);
     ++its;
   }
@@ -465,13 +599,34 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   Cx* rot = scratch;           // 2 m
   Cx* U = scratch + 2 * m + 2; // m x 32
 
+  // T = sig H with sig a power of two that puts the largest |re| or |im| of
+  // H in [1, 2): exact, and the Schur sweeps' rotations and shifts then need
+  // no overflow / underflow branches (givens_s, csqrt_s).  Values leave
+  // hess_core unscaled (times isig).
+  double mx = 0;
+  for (long i = lane; i < mm; i += 32) mx = fmax(mx, fmax(fabs(a.Hin[i].re), fabs(a.Hin[i].im)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  int ex = 0;
+  if (mx > 0 && mx <= 1.7e308) frexp(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
+  ex = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
+  const double sig = ldexp(1.0, 1 - ex), isig = ldexp(1.0, ex - 1);
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    TT_(r, c) = cx_from<Cx>(a.Hin[i]);
+    TT_(r, c) = cx_from<Cx>(sig * a.Hin[i]);
     ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
   __syncwarp();
-  if (a.dense) warp_hessenberg(T, Z, u, m, ld, lane);
+  if (a.dense) {
+    if constexpr (sizeof(Cx) == sizeof(cplxf)) {
+      if (m <= 32)
+        warp_hessenberg_r32(T, Z, u, m, ld, lane);
+      else
+        warp_hessenberg(T, Z, u, m, ld, lane);
+    } else {
+      warp_hessenberg(T, Z, u, m, ld, lane);
+    }
+  }
   if (!warp_schur(T, Z, m, ld, rot, lane)) {
     if (lane == 0) { st->status |= 2; st->converged = 0; }
     return;
@@ -490,10 +645,11 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   __syncwarp();
   for (int q = lane; q < m; q += 32) {
     a.order[q] = ord[q];
-    a.ritz[q] = cx_to(TT_(ord[q], ord[q]));
+    a.ritz[q] = isig * cx_to(TT_(ord[q], ord[q]));
   }
-  double scale = 0;
+  double scale = 0;  // max |theta| over the wanted set, unscaled
   for (int q = 0; q < k; ++q) scale = fmax(scale, (double)cabs_(TT_(ord[q], ord[q])));
+  scale *= isig;
   if (scale == 0) scale = 1;
   double tnorm = 0;
   for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, (double)cabs_(TT_(i, i)));
@@ -521,7 +677,7 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   __syncwarp();
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    TT_(r, c) = cx_from<Cx>(a.Hin[i]);
+    TT_(r, c) = cx_from<Cx>(sig * a.Hin[i]);
     ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
   __syncwarp();
@@ -539,12 +695,12 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   }
   __syncwarp();
   if (lane == 0) {
-    st->beta_hat = cx_to(TT_(k, k - 1));
+    st->beta_hat = isig * cx_to(TT_(k, k - 1));
     st->sigma = cx_to(ZZ_(m - 1, k - 1));
   }
   for (long i = lane; i < mm; i += 32) {
     const int r = (int)(i % m), c = (int)(i / m);
-    a.Hout[i] = (r < k && c < k) ? cx_to(TT_(r, c)) : cplx{0, 0};
+    a.Hout[i] = (r < k && c < k) ? isig * cx_to(TT_(r, c)) : cplx{0, 0};
     a.Qout[i] = cx_to(ZZ_(r, c));
   }
 }

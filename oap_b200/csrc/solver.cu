@@ -32,6 +32,7 @@
 #include <tuple>
 #include <new>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 #include <vector>
 
@@ -485,6 +486,10 @@ struct oapb_arnoldi {
   // the main stream takes the next power: own Gram scratch, pinned outputs
   cudaStream_t s2 = nullptr;
   cudaEvent_t ev_w = nullptr, ev_chk = nullptr;
+  // a check is in flight on s2: the tensor-core passes leave one SM to it
+  // (their CTAs hold most of an SM's shared memory, so a check kernel that
+  // holds an SM would otherwise hold back one CTA of the pass)
+  bool side_busy = false;
   cplx* bpart2 = nullptr;
   unsigned* bdone2 = nullptr;
   unsigned char* hpin = nullptr;  // pinned: norm partials, Ritz values, DevState, tcerr
@@ -825,6 +830,16 @@ void block_gram(oapb_arnoldi* a, const double* xr, const double* xi, int b1, con
 // smallest residual goal the FP64-class int8-slice pass serves
 constexpr double kI8MinTolerance = 1e-12;
 
+// OAPB_SIDE_SM_RESERVE=0 turns the SM left to an overlapped check off (for
+// A/B timing); on by default
+static bool side_sm_reserve() {
+  static const int v = [] {
+    const char* e = getenv("OAPB_SIDE_SM_RESERVE");
+    return (e && e[0] == '0') ? 0 : 1;
+  }();
+  return v != 0;
+}
+
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
                 bool fp32 = false, bool bf16 = false, bool coarse = false) {
@@ -849,8 +864,9 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   if (tcp) {
     BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
                    C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
+    const int ctas = (a->side_busy && side_sm_reserve()) ? kNumSMs - 1 : kNumSMs;
     int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
-                                    a->tcerr, a->stream, bf16, bf16 && coarse);
+                                    a->tcerr, a->stream, bf16, bf16 && coarse, ctas);
     if (bf16) a->stats.block_bf16++;
     if (prof) prof_end(a, tm);
     if (rc) return rc;
@@ -1029,6 +1045,7 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
   if (near_tri && b <= 32 &&
       cudaMemcpyAsync(hp + pin_nt_off(a), a->ntflag, sizeof(int), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
     return OAPB_ERR_CUDA;
+  a->side_busy = side;
   *(double*)(hp + pin_e2_off(a)) = -1;  // the BF16 rounding energy rides along until known
   if (a->bf16_err < 0 && a->bf16err2 &&
       cudaMemcpyAsync(hp + pin_e2_off(a), a->bf16err2, sizeof(double), cudaMemcpyDeviceToHost, cs) != cudaSuccess)
@@ -1038,6 +1055,7 @@ int check_enqueue(oapb_arnoldi* a, cudaStream_t cs, const double* X, const doubl
 
 // wait for the enqueued check: Ritz values (b) and residual norms ||E_q|| (kk)
 int check_collect(oapb_arnoldi* a, int b, int kk, cplx* th, double* norms) {
+  a->side_busy = false;
   if (cudaEventSynchronize(a->ev_chk) != cudaSuccess) return OAPB_ERR_CUDA;
   const unsigned char* hp = a->hpin;
   const double* part = (const double*)(hp + pin_norm_off(a));
