@@ -87,7 +87,7 @@ struct HessK<double> {
 };
 template <>
 struct HessK<float> {
-  static constexpr float eps = 1.1920929e-7f, tiny = 1e-37f, big = 1e30f, unbig = 1e-30f;
+  static constexpr float eps = 1.1920929e-7f, tiny = 1e-37f, big = 1e15f, unbig = 1e-15f;  // big^2 stays finite
   static constexpr float tiny2 = 1e-36f;
 };
 
@@ -471,6 +471,102 @@ static __device__ void warp_hessenberg_r32(cplxf* T, cplxf* Z, cplxf* v, int m, 
   __syncwarp();
 }
 
+// barrier of the NW warps of a multi-warp small eigensolver (named barrier
+// 1: the rest of a block may use barrier 0)
+__device__ __forceinline__ void hess_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
+
+// The Householder reduction on NW warps (m <= 32, all NW warps calling;
+// warp 0 forms each reflector): per step, P T has one lane per column and
+// the rows split over the warps (partial sums v^H T summed through shared
+// memory), T P and Z P one lane per row and the columns split over the
+// warps.  part: 2 NW x 32 entries of shared scratch; v: 32; fs: 1.
+template <typename Cx, int NW>
+static __device__ void block_hessenberg32(Cx* T, Cx* Z, Cx* v, Cx* part, decltype(Cx::re)* fs, int m, int ld,
+                                          int warp, int lane) {
+  using R = decltype(Cx::re);
+  constexpr int nthr = NW * 32;
+  const Cx zero = {0, 0};
+  Cx* pa = part;            // NW x 32: P T partials, then T P partials
+  Cx* pz = part + NW * 32;  // NW x 32: Z P partials
+  for (int k = 0; k + 2 < m; ++k) {
+    hess_bar(nthr);  // the previous step's updates are in place
+    if (warp == 0) {
+      const Cx xi = (lane > k && lane < m) ? TT_(lane, k) : zero;
+      const R s = warp_sum_t(abs2(xi));
+      const Cx x0 = shfl_c(xi, k + 1);
+      R f = 0;
+      Cx vi = xi;
+      if (s > 0) {
+        const R a = sqrt_t(s), ax0 = sqrt_t(abs2(x0));
+        const Cx ph = ax0 > 0 ? Cx{x0.re / ax0, x0.im / ax0} : Cx{1, 0};
+        if (lane == k + 1) vi = xi + a * ph;
+        f = R(1) / (a * (a + ax0));  // 2 / |v|^2
+      }
+      v[lane] = vi;  // zero outside rows k + 1 .. m - 1
+      if (lane == 0) *fs = f;
+    }
+    hess_bar(nthr);
+    const R f = *fs;
+    if (f == 0) continue;  // column k is reduced already (the same for every warp)
+    // P T: lane j = column (j >= k), this warp's rows of k + 1 .. m - 1
+    const int nr = m - k - 1, cr = (nr + NW - 1) / NW;
+    const int i0 = k + 1 + warp * cr, i1 = i0 + cr < m ? i0 + cr : m;
+    const bool colj = lane >= k && lane < m;
+    {
+      Cx w0 = zero, w1 = zero;
+      if (colj) {
+        int i = i0;
+        for (; i + 1 < i1; i += 2) {
+          w0 = cfma(conj(v[i]), TT_(i, lane), w0);
+          w1 = cfma(conj(v[i + 1]), TT_(i + 1, lane), w1);
+        }
+        if (i < i1) w0 = cfma(conj(v[i]), TT_(i, lane), w0);
+      }
+      pa[warp * 32 + lane] = w0 + w1;
+    }
+    hess_bar(nthr);
+    {
+      Cx w = pa[lane];
+#pragma unroll
+      for (int u = 1; u < NW; ++u) w = w + pa[u * 32 + lane];
+      w = f * w;
+      if (colj)
+        for (int i = i0; i < i1; ++i) TT_(i, lane) = (lane == k && i >= k + 2) ? zero : cfma(-v[i], w, TT_(i, lane));
+    }
+    hess_bar(nthr);
+    // T P, Z P: lane i = row, this warp's columns of k + 1 .. m - 1
+    const int j0 = k + 1 + warp * cr, j1 = j0 + cr < m ? j0 + cr : m;
+    const bool rowi = lane < m;
+    {
+      Cx y0 = zero, y1 = zero;
+      if (rowi)
+        for (int j = j0; j < j1; ++j) {
+          y0 = cfma(TT_(lane, j), v[j], y0);
+          y1 = cfma(ZZ_(lane, j), v[j], y1);
+        }
+      pa[warp * 32 + lane] = y0;
+      pz[warp * 32 + lane] = y1;
+    }
+    hess_bar(nthr);
+    {
+      Cx y = pa[lane], yz = pz[lane];
+#pragma unroll
+      for (int u = 1; u < NW; ++u) {
+        y = y + pa[u * 32 + lane];
+        yz = yz + pz[u * 32 + lane];
+      }
+      y = f * y;
+      yz = f * yz;
+      if (rowi)
+        for (int j = j0; j < j1; ++j) {
+          TT_(lane, j) = cfma(-y, conj(v[j]), TT_(lane, j));
+          ZZ_(lane, j) = cfma(-yz, conj(v[j]), ZZ_(lane, j));
+        }
+    }
+  }
+  hess_bar(nthr);
+}
+
 // Complex Schur form in place; returns false when the sweep budget ran out.
 template <typename Cx>
 static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane) {
@@ -504,95 +600,162 @@ static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane
 
 // Eigenvectors y_q = Z u_q (q < nvec) of the upper triangular T for the
 // diagonal entries ord[q]: u by back substitution, one lane per eigenvector
-// (columns of U in the scratch, stride min(32, nvec)); Y = Z U one lane per
-// row.  Returns max over q < k of the relative estimates beta |y_q[m-1]| /
-// (scale ||y_q||).
+// (columns of U in the scratch, stride min(32, nvec)), then Y = Z U one
+// lane per row.  The back substitution divides through |den|^2 (one real
+// reciprocal per step; T is prescaled, so |den|^2 >= small^2 stays in
+// range).  warp_backsub: one warp, the U columns of eigenvectors
+// q0 .. q0 + 31.
 template <typename Cx>
-static __device__ double warp_eigvecs(const Cx* T, const Cx* Z, int m, int ld, const int* ord, int nvec, int k,
-                                      double small_d, double beta, double scale, Cx* U, cplx* Y, double* est,
-                                      int lane) {
+static __device__ void warp_backsub(const Cx* T, int m, int ld, const int* ord, int nvec, int q0, double small_d,
+                                    Cx* U, int lane) {
   using R = decltype(Cx::re);
-  const R small = (R)small_d;
-  double maxest = 0;
+  const R small = (R)small_d, small2 = small * small;
+  const Cx zero = {0, 0};
   const int W = nvec < 32 ? nvec : 32;
-  for (int q0 = 0; q0 < nvec; q0 += 32) {
-    const int q = q0 + lane;
-    const bool act = lane < W && q < nvec;
-    const int idx = act ? ord[q] : 0;
-    const Cx lam = TT_(idx, idx);
-    if (lane < W)
-      for (int i = 0; i < m; ++i) U[i * W + lane] = (act && i == idx) ? Cx{1, 0} : Cx{0, 0};
-    for (int i = m - 2; i >= 0; --i) {
-      Cx a0 = {0, 0}, a1 = {0, 0};
-      if (lane < W) {
-        int j = i + 1;
+  const int q = q0 + lane;
+  const bool act = lane < W && q < nvec;
+  const int idx = act ? ord[q] : 0;
+  const Cx lam = TT_(idx, idx);
+  if (lane < W)
+    for (int i = 0; i < m; ++i) U[i * W + lane] = (act && i == idx) ? Cx{1, 0} : zero;
+  for (int i = m - 2; i >= 0; --i) {
+    Cx a0 = zero, a1 = zero;
+    if (lane < W) {
+      int j = i + 1;
+      for (; j + 1 < m; j += 2) {
+        a0 = cfma(TT_(i, j), U[j * W + lane], a0);
+        a1 = cfma(TT_(i, j + 1), U[(j + 1) * W + lane], a1);
+      }
+      if (j < m) a0 = cfma(TT_(i, j), U[j * W + lane], a0);
+    }
+    if (act && i < idx) {
+      Cx den = TT_(i, i) - lam;
+      R d2 = abs2(den);
+      if (d2 < small2) {
+        den = Cx{small, 0};
+        d2 = small2;
+      }
+      const Cx ui = (-R(1) / d2) * ((a0 + a1) * conj(den));
+      U[i * W + lane] = ui;
+      if (cabs1(ui) > HessK<R>::big)  // rescale this column to avoid overflow
+        for (int j = i; j <= idx; ++j) U[j * W + lane] = HessK<R>::unbig * U[j * W + lane];
+    }
+  }
+}
+
+// Y[:, q] = Z U[:, q - q0] normalised, and the estimates beta |y_q[m-1]| /
+// (scale ||y_q||), for the eigenvectors q0 + c with c < nq in this warp's
+// share: for m <= 32, chunks of eight columns c0 = 8 (part + nparts t), one
+// lane per row, their norms summed by interleaved butterflies.  Returns the
+// largest estimate over q < k of the share.
+template <typename Cx>
+static __device__ double warp_zu(const Cx* Z, int m, int ld, const Cx* U, int W, int q0, int nq, int k, double beta,
+                                 double scale, cplx* Y, double* est, int part, int nparts, int lane) {
+  using R = decltype(Cx::re);
+  const Cx zero = {0, 0};
+  double maxest = 0;
+  if (m <= 32) {
+    constexpr int CH = 8;
+    const bool rin = lane < m;
+    for (int c0 = CH * part; c0 < nq; c0 += CH * nparts) {
+      Cx y[CH];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) y[c] = zero;
+      for (int j = 0; j < m; ++j) {
+        const Cx z = rin ? ZZ_(lane, j) : zero;
+#pragma unroll
+        for (int c = 0; c < CH; ++c) y[c] = cfma(z, U[j * W + (c0 + c < nq ? c0 + c : c0)], y[c]);
+      }
+      R n2[CH];
+      Cx yl[CH];
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        n2[c] = abs2(y[c]);
+        yl[c] = shfl_c(y[c], m - 1);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int c = 0; c < CH; ++c) n2[c] += __shfl_xor_sync(0xffffffffu, n2[c], o);
+#pragma unroll
+      for (int c = 0; c < CH; ++c) {
+        const int qq = q0 + c0 + c;
+        if (c0 + c < nq) {
+          const R nrm = sqrt_t(n2[c]);
+          const R inv = nrm > 0 ? R(1) / nrm : R(0);
+          if (rin) Y[(long)qq * m + lane] = cx_to(inv * y[c]);
+          const double e = beta * (double)sqrt_t(abs2(yl[c])) * (double)inv / scale;
+          if (lane == 0) est[qq] = e;
+          if (qq < k) maxest = fmax(maxest, e);
+        }
+      }
+    }
+    return maxest;
+  }
+  for (int c = part; c < nq; c += nparts) {
+    const int qq = q0 + c;
+    Cx yv[kMaxM / 32];
+    R nrm = 0;
+    Cx ylast = zero;
+#pragma unroll
+    for (int t = 0; t < kMaxM / 32; ++t) {
+      const int r = lane + 32 * t;
+      yv[t] = zero;
+      if (r < m) {
+        Cx s0 = zero, s1 = zero;
+        int j = 0;
         for (; j + 1 < m; j += 2) {
-          a0 = a0 + TT_(i, j) * U[j * W + lane];
-          a1 = a1 + TT_(i, j + 1) * U[(j + 1) * W + lane];
+          s0 = cfma(ZZ_(r, j), U[j * W + c], s0);
+          s1 = cfma(ZZ_(r, j + 1), U[(j + 1) * W + c], s1);
         }
-        if (j < m) a0 = a0 + TT_(i, j) * U[j * W + lane];
-      }
-      if (act && i < idx) {
-        Cx den = TT_(i, i) - lam;
-        if (cabs_(den) < small) den = Cx{small, 0};
-        const Cx ui = -cdiv(a0 + a1, den);
-        U[i * W + lane] = ui;
-        if (cabs_(ui) > HessK<R>::big)  // rescale this column to avoid overflow
-          for (int j = i; j <= idx; ++j) U[j * W + lane] = HessK<R>::unbig * U[j * W + lane];
+        if (j < m) s0 = cfma(ZZ_(r, j), U[j * W + c], s0);
+        yv[t] = s0 + s1;
+        nrm += abs2(yv[t]);
+        if (r == m - 1) ylast = yv[t];
       }
     }
-    __syncwarp();
-    // Y[:, q] = Z U[:, q], one lane per row; normalise; estimate
-    const int nq = (nvec - q0) < W ? (nvec - q0) : W;
-    for (int c = 0; c < nq; ++c) {
-      const int qq = q0 + c;
-      Cx yv[kMaxM / 32];
-      R nrm = 0;
-      Cx ylast = {0, 0};
+    nrm = sqrt(warp_sum_t(nrm));
+    ylast.re = warp_sum_t(ylast.re);
+    ylast.im = warp_sum_t(ylast.im);
+    const R inv = nrm > 0 ? R(1) / nrm : R(0);
 #pragma unroll
-      for (int t = 0; t < kMaxM / 32; ++t) {
-        const int r = lane + 32 * t;
-        yv[t] = Cx{0, 0};
-        if (r < m) {
-          Cx s0 = {0, 0}, s1 = {0, 0};
-          int j = 0;
-          for (; j + 1 < m; j += 2) {
-            s0 = s0 + ZZ_(r, j) * U[j * W + c];
-            s1 = s1 + ZZ_(r, j + 1) * U[(j + 1) * W + c];
-          }
-          if (j < m) s0 = s0 + ZZ_(r, j) * U[j * W + c];
-          yv[t] = s0 + s1;
-          nrm += abs2(yv[t]);
-          if (r == m - 1) ylast = yv[t];
-        }
-      }
-      nrm = sqrt(warp_sum_t(nrm));
-      ylast.re = warp_sum_t(ylast.re);
-      ylast.im = warp_sum_t(ylast.im);
-      const R inv = nrm > 0 ? R(1) / nrm : R(0);
-#pragma unroll
-      for (int t = 0; t < kMaxM / 32; ++t) {
-        const int r = lane + 32 * t;
-        if (r < m) Y[(long)qq * m + r] = cx_to(inv * yv[t]);
-      }
-      const double e = beta * (double)cabs_(ylast) * (double)inv / scale;
-      if (lane == 0) est[qq] = e;
-      if (qq < k) maxest = fmax(maxest, e);
+    for (int t = 0; t < kMaxM / 32; ++t) {
+      const int r = lane + 32 * t;
+      if (r < m) Y[(long)qq * m + r] = cx_to(inv * yv[t]);
     }
-    __syncwarp();
+    const double e = beta * (double)cabs_(ylast) * (double)inv / scale;
+    if (lane == 0) est[qq] = e;
+    if (qq < k) maxest = fmax(maxest, e);
   }
   return maxest;
 }
 
-// The body of k_hess for one warp (lane = 0..31 of the calling warp), with
-// its workspaces passed in: T, Z (leading dimension hess_ld(m), m columns
-// each), u (m), key (m), ord (m), scratch (hess_scratch_cplx(m)).  Callable
-// from any kernel by one full warp; the outputs in `a` may point to shared
-// or global memory.
-template <typename Cx>
+// Shared scratch of the multi-warp (NW > 1) hess_core beyond its workspaces.
+template <typename Cx, int NW>
+struct HessShared {
+  Cx v[32];
+  Cx part[2 * NW * 32];
+  decltype(Cx::re) f;
+  double mx[NW];
+  double scale;
+  int ok;
+};
+
+// The body of k_hess on NW warps (tid = 0 .. 32 NW - 1 of the calling
+// threads), with its workspaces passed in: T, Z (leading dimension
+// hess_ld(m), m columns each), u (m), key (m), ord (m), scratch
+// (hess_scratch_cplx(m)); hs (NW > 1 only): shared scratch.  Callable from
+// any kernel by one full warp (NW = 1) or by NW full warps when m <= 32; the
+// outputs in `a` may point to shared or global memory.  With NW > 1 the
+// Householder reduction and the product Y = Z U run on all warps, the Schur
+// sweeps, the sort and the back substitutions on warp 0; the other warps
+// return before the exact shifts.
+template <typename Cx, int NW = 1>
 static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double* key, int* ord, Cx* scratch,
-                                 int lane) {
+                                 int tid, HessShared<Cx, NW>* hs = nullptr) {
   using R = decltype(Cx::re);
+  constexpr int nthr = NW * 32;
+  const int lane = tid & 31, warp = tid >> 5;
   const int m = a.m, k = a.k, ld = hess_ld(m);
   const long mm = (long)m * m;
   DevState* st = a.st;
@@ -602,7 +765,7 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   // T = sig H with sig a power of two that puts the largest |re| or |im| of
   // H in [1, 2): exact, and the Schur sweeps' rotations and shifts then need
   // no overflow / underflow branches (givens_s, csqrt_s).  Values leave
-  // hess_core unscaled (times isig).
+  // hess_core unscaled (times isig).  (Every warp finds the same maximum.)
   double mx = 0;
   for (long i = lane; i < mm; i += 32) mx = fmax(mx, fmax(fabs(a.Hin[i].re), fabs(a.Hin[i].im)));
 #pragma unroll
@@ -611,57 +774,97 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   if (mx > 0 && mx <= 1.7e308) frexp(mx, &ex);  // mx = f 2^ex, f in [0.5, 1)
   ex = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
   const double sig = ldexp(1.0, 1 - ex), isig = ldexp(1.0, ex - 1);
-  for (long i = lane; i < mm; i += 32) {
+  for (long i = tid; i < mm; i += nthr) {
     const int r = (int)(i % m), c = (int)(i / m);
     TT_(r, c) = cx_from<Cx>(sig * a.Hin[i]);
     ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
-  __syncwarp();
-  if (a.dense) {
-    if constexpr (sizeof(Cx) == sizeof(cplxf)) {
-      if (m <= 32)
-        warp_hessenberg_r32(T, Z, u, m, ld, lane);
-      else
+  if constexpr (NW > 1) {
+    hess_bar(nthr);
+    if (a.dense) block_hessenberg32<Cx, NW>(T, Z, hs->v, hs->part, &hs->f, m, ld, warp, lane);
+  } else {
+    __syncwarp();
+    if (a.dense) {
+      if constexpr (sizeof(Cx) == sizeof(cplxf)) {
+        if (m <= 32)
+          warp_hessenberg_r32(T, Z, u, m, ld, lane);
+        else
+          warp_hessenberg(T, Z, u, m, ld, lane);
+      } else {
         warp_hessenberg(T, Z, u, m, ld, lane);
-    } else {
-      warp_hessenberg(T, Z, u, m, ld, lane);
+      }
     }
   }
-  if (!warp_schur(T, Z, m, ld, rot, lane)) {
-    if (lane == 0) { st->status |= 2; st->converged = 0; }
-    return;
-  }
-  // sort order of diag(T)
-  for (int i = lane; i < m; i += 32) {
-    double kv = sort_key(cx_to(TT_(i, i)), a.which);
-    key[i] = (kv != kv) ? INFINITY : kv;  // NaN sorts last; ranks stay a permutation
-  }
-  __syncwarp();
-  for (int i = lane; i < m; i += 32) {
-    int r = 0;
-    for (int j = 0; j < m; ++j) r += (key[j] < key[i]) || (key[j] == key[i] && j < i);
-    ord[r] = i;
-  }
-  __syncwarp();
-  for (int q = lane; q < m; q += 32) {
-    a.order[q] = ord[q];
-    a.ritz[q] = isig * cx_to(TT_(ord[q], ord[q]));
-  }
-  double scale = 0;  // max |theta| over the wanted set, unscaled
-  for (int q = 0; q < k; ++q) scale = fmax(scale, (double)cabs_(TT_(ord[q], ord[q])));
-  scale *= isig;
-  if (scale == 0) scale = 1;
-  double tnorm = 0;
-  for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, (double)cabs_(TT_(i, i)));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
-  const double small = (double)HessK<R>::eps * (tnorm > 0 ? tnorm : 1.0);
-  const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
-
-  // eigenvectors of the first nvec Ritz values (the wanted k and optional
-  // guard vectors) and the estimates of the wanted ones
   const int nvec = a.nvec > k ? (a.nvec < m ? a.nvec : m) : k;
-  const double maxest = warp_eigvecs(T, Z, m, ld, ord, nvec, k, small, beta, scale, U, a.Y, a.est, lane);
+  const int W = nvec < 32 ? nvec : 32;
+  double scale = 0, small = 0;
+  const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
+  if (warp == 0) {
+    const bool ok = warp_schur(T, Z, m, ld, rot, lane);
+    if (!ok && lane == 0) {
+      st->status |= 2;
+      st->converged = 0;
+    }
+    if constexpr (NW > 1) {
+      if (lane == 0) hs->ok = ok;
+    }
+    if (ok) {
+      // sort order of diag(T)
+      for (int i = lane; i < m; i += 32) {
+        double kv = sort_key(cx_to(TT_(i, i)), a.which);
+        key[i] = (kv != kv) ? INFINITY : kv;  // NaN sorts last; ranks stay a permutation
+      }
+      __syncwarp();
+      for (int i = lane; i < m; i += 32) {
+        int r = 0;
+        for (int j = 0; j < m; ++j) r += (key[j] < key[i]) || (key[j] == key[i] && j < i);
+        ord[r] = i;
+      }
+      __syncwarp();
+      for (int q = lane; q < m; q += 32) {
+        a.order[q] = ord[q];
+        a.ritz[q] = isig * cx_to(TT_(ord[q], ord[q]));
+      }
+      // max |theta| over the wanted set, unscaled
+      for (int q = 0; q < k; ++q) scale = fmax(scale, (double)cabs_(TT_(ord[q], ord[q])));
+      scale *= isig;
+      if (scale == 0) scale = 1;
+      double tnorm = 0;
+      for (int i = lane; i < m; i += 32) tnorm = fmax(tnorm, (double)cabs_(TT_(i, i)));
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) tnorm = fmax(tnorm, __shfl_xor_sync(0xffffffffu, tnorm, o));
+      small = (double)HessK<R>::eps * (tnorm > 0 ? tnorm : 1.0);
+      warp_backsub(T, m, ld, ord, nvec, 0, small, U, lane);
+      if constexpr (NW > 1) {
+        if (lane == 0) hs->scale = scale;
+      }
+    }
+    __syncwarp();
+  }
+  double maxest = 0;
+  if constexpr (NW > 1) {
+    // eigenvectors of the first nvec Ritz values (the wanted k and optional
+    // guard vectors; nvec <= m <= 32) on all warps
+    hess_bar(nthr);
+    if (!hs->ok) return;
+    scale = hs->scale;
+    const double me = warp_zu(Z, m, ld, U, W, 0, nvec, k, beta, scale, a.Y, a.est, warp, NW, lane);
+    if (lane == 0) hs->mx[warp] = me;
+    hess_bar(nthr);
+    if (warp != 0) return;
+    for (int w = 0; w < NW; ++w) maxest = fmax(maxest, hs->mx[w]);
+  } else {
+    if (scale == 0) return;  // the Schur sweeps ran out (status set)
+    for (int q0 = 0; q0 < nvec; q0 += 32) {
+      if (q0 > 0) {
+        warp_backsub(T, m, ld, ord, nvec, q0, small, U, lane);
+        __syncwarp();
+      }
+      const int nq = (nvec - q0) < W ? (nvec - q0) : W;
+      maxest = fmax(maxest, warp_zu(Z, m, ld, U, W, q0, nq, k, beta, scale, a.Y, a.est, 0, 1, lane));
+      __syncwarp();
+    }
+  }
   const int conv = maxest <= a.tol;
   if (lane == 0) {
     st->converged = conv;
@@ -705,19 +908,28 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   }
 }
 
-// dynamic shared memory (or a.gws): T, Z, scratch of the working type Cx
+// warps of k_hess / k_hess_f32 for m <= 32 (one warp above)
+constexpr int kHessWarps = 4;
+__host__ __device__ inline int hess_threads(int m) { return m <= 32 ? 32 * kHessWarps : 32; }
+
+// dynamic shared memory (or a.gws): T, Z, scratch of the working type Cx;
+// launched with hess_threads(m) threads
 template <typename Cx>
 static __device__ void hess_kernel_body(const HessArgs& a, unsigned char* dyn) {
   __shared__ Cx u[kMaxM];
   __shared__ double key[kMaxM];
   __shared__ int ord[kMaxM];
+  __shared__ HessShared<Cx, kHessWarps> hs;
   Cx* T = a.gws ? reinterpret_cast<Cx*>(a.gws) : reinterpret_cast<Cx*>(dyn);
   const size_t tz = (size_t)hess_ld(a.m) * a.m;
-  hess_core<Cx>(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x);
+  if (blockDim.x == 32 * kHessWarps && a.m <= 32)
+    hess_core<Cx, kHessWarps>(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x, &hs);
+  else if (threadIdx.x < 32)
+    hess_core<Cx, 1>(a, T, T + tz, u, key, ord, T + 2 * tz, threadIdx.x);
 }
 
 // FP64 working arithmetic (the restart loop and the refinement)
-static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
+static __global__ void __launch_bounds__(32 * kHessWarps) k_hess(HessArgs a) {
   extern __shared__ __align__(16) unsigned char hess_dyn[];
   asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   if (a.skip && *(volatile const int*)a.skip) return;
@@ -727,7 +939,7 @@ static __global__ void __launch_bounds__(32) k_hess(HessArgs a) {
 // FP32 working arithmetic, FP64 inputs and outputs: the Rayleigh-Ritz checks
 // of the FP32-class phase (whose Ritz vectors are FP32-accurate at best);
 // dynamic shared memory hess_ws_cplx(m) * sizeof(cplxf)
-static __global__ void __launch_bounds__(32) k_hess_f32(HessArgs a) {
+static __global__ void __launch_bounds__(32 * kHessWarps) k_hess_f32(HessArgs a) {
   extern __shared__ __align__(16) unsigned char hess_dyn[];
   asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   hess_kernel_body<cplxf>(a, hess_dyn);

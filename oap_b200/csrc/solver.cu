@@ -678,7 +678,7 @@ int hess(oapb_arnoldi* a, int do_shift, double tol) {
   h.tol = tol;
   h.beta = 0;
   ++a->stats.kernel_launches;
-  launch_dependent(k_hess, dim3(1), dim3(32), a->hess_smem, a->stream, h);
+  launch_dependent(k_hess, dim3(1), dim3(hess_threads(h.m)), a->hess_smem, a->stream, h);
   return launch_check();
 }
 
@@ -991,9 +991,9 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
     h.skip = a->ntflag;
   }
   if (fp32)
-    launch_dependent(k_hess_f32, dim3(1), dim3(32), sizeof(cplxf) * hess_ws_cplx(b), a->stream, h);
+    launch_dependent(k_hess_f32, dim3(1), dim3(hess_threads(b)), sizeof(cplxf) * hess_ws_cplx(b), a->stream, h);
   else
-    launch_dependent(k_hess, dim3(1), dim3(32), sizeof(cplx) * hess_ws_cplx(b), a->stream, h);
+    launch_dependent(k_hess, dim3(1), dim3(hess_threads(b)), sizeof(cplx) * hess_ws_cplx(b), a->stream, h);
   return launch_check();
 }
 
@@ -1851,7 +1851,8 @@ int oapb_arnoldi_create(oapb_arnoldi** out, const oapb_arnoldi_config* cfg, void
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const size_t static_smem = kMaxM * (sizeof(cplx) + sizeof(double) + sizeof(int)) + 1024;
+  const size_t static_smem =
+      kMaxM * (sizeof(cplx) + sizeof(double) + sizeof(int)) + sizeof(HessShared<cplx, kHessWarps>) + 1024;
   if (hb + static_smem <= (size_t)optin) {
     a->hess_smem = hb;
   } else {
