@@ -383,94 +383,6 @@ static __device__ void warp_hessenberg(Cx* T, Cx* Z, Cx* v, int m, int ld, int l
   }
 }
 
-// The same reduction for FP32 and m <= 32 with the work in registers: lane
-// j holds column j of T while the reflector acts from the left (P T), the
-// matrix goes through shared memory once per step so that lane i takes row
-// i of T and of Z for the right-hand side (T P, Z P), and comes back as
-// columns.  Every loop runs over the 32 possible rows / columns unrolled,
-// the entries outside the m x m matrix being zero in registers (and never
-// stored), so a step is one straight block of independent loads and
-// multiply-adds.  v (32 entries of scratch, zero outside rows k+1 .. m-1)
-// carries the reflector; |v|^2 = 2 a (a + |x0|) needs no second reduction.
-static __device__ void warp_hessenberg_r32(cplxf* T, cplxf* Z, cplxf* v, int m, int ld, int lane) {
-  constexpr int W = 32;
-  const cplxf zero = {0.f, 0.f};
-  const bool lc = lane < m;
-  cplxf col[W];
-#pragma unroll
-  for (int i = 0; i < W; ++i) col[i] = (lc && i < m) ? TT_(i, lane) : zero;
-  for (int k = 0; k + 2 < m; ++k) {
-    __syncwarp();  // the previous step's reads of v are done
-    if (lane == k) {
-#pragma unroll
-      for (int i = 0; i < W; ++i) v[i] = i > k ? col[i] : zero;
-    }
-    __syncwarp();
-    const float s = warp_sumf(abs2(v[lane]));
-    if (s == 0) continue;  // (warp-uniform) column k is reduced already
-    const cplxf x0 = v[k + 1];
-    const float a = sqrtf(s), ax0 = sqrtf(abs2(x0));
-    const cplxf ph = ax0 > 0 ? cplxf{x0.re / ax0, x0.im / ax0} : cplxf{1.f, 0.f};
-    const float f = 1.f / (a * (a + ax0));  // 2 / |v|^2
-    __syncwarp();
-    if (lane == 0) v[k + 1] = x0 + a * ph;
-    __syncwarp();
-    // P T: lane j, w = f v^H T(:, j), T(:, j) -= v w (columns left of k
-    // have zeros where v is non-zero: w = 0 there)
-    cplxf w0 = zero, w1 = zero, w2 = zero, w3 = zero;
-#pragma unroll
-    for (int i = 0; i < W; i += 4) {
-      w0 = cfma(conj(v[i]), col[i], w0);
-      w1 = cfma(conj(v[i + 1]), col[i + 1], w1);
-      w2 = cfma(conj(v[i + 2]), col[i + 2], w2);
-      w3 = cfma(conj(v[i + 3]), col[i + 3], w3);
-    }
-    const cplxf w = f * ((w0 + w1) + (w2 + w3));
-#pragma unroll
-    for (int i = 0; i < W; ++i) col[i] = cfma(-v[i], w, col[i]);
-    if (lane == k) {  // below the subdiagonal of column k: exact zeros
-#pragma unroll
-      for (int i = 0; i < W; ++i)
-        if (i >= k + 2) col[i] = zero;
-    }
-#pragma unroll
-    for (int i = 0; i < W; ++i)
-      if (lc && i < m) TT_(i, lane) = col[i];
-    __syncwarp();
-    // T P and Z P: lane i, y = f T(i, :) v, T(i, :) -= y v^H (same for Z)
-    if (lc) {
-      cplxf r[W];
-      cplxf y0 = zero, y1 = zero;
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-        r[j] = j < m ? TT_(lane, j) : zero;
-        if (j & 1) y1 = cfma(r[j], v[j], y1);
-        else y0 = cfma(r[j], v[j], y0);
-      }
-      const cplxf y = f * (y0 + y1);
-#pragma unroll
-      for (int j = 0; j < W; ++j)
-        if (j < m) TT_(lane, j) = cfma(-y, conj(v[j]), r[j]);
-      y0 = zero;
-      y1 = zero;
-#pragma unroll
-      for (int j = 0; j < W; ++j) {
-        r[j] = j < m ? ZZ_(lane, j) : zero;
-        if (j & 1) y1 = cfma(r[j], v[j], y1);
-        else y0 = cfma(r[j], v[j], y0);
-      }
-      const cplxf yz = f * (y0 + y1);
-#pragma unroll
-      for (int j = 0; j < W; ++j)
-        if (j < m) ZZ_(lane, j) = cfma(-yz, conj(v[j]), r[j]);
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < W; ++i) col[i] = (lc && i < m) ? TT_(i, lane) : zero;
-  }
-  __syncwarp();
-}
-
 // barrier of the NW warps of a multi-warp small eigensolver (named barrier
 // 1: the rest of a block may use barrier 0)
 __device__ __forceinline__ void hess_bar(int nthr) { asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory"); }
@@ -784,16 +696,7 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
     if (a.dense) block_hessenberg32<Cx, NW>(T, Z, hs->v, hs->part, &hs->f, m, ld, warp, lane);
   } else {
     __syncwarp();
-    if (a.dense) {
-      if constexpr (sizeof(Cx) == sizeof(cplxf)) {
-        if (m <= 32)
-          warp_hessenberg_r32(T, Z, u, m, ld, lane);
-        else
-          warp_hessenberg(T, Z, u, m, ld, lane);
-      } else {
-        warp_hessenberg(T, Z, u, m, ld, lane);
-      }
-    }
+    if (a.dense) warp_hessenberg(T, Z, u, m, ld, lane);
   }
   const int nvec = a.nvec > k ? (a.nvec < m ? a.nvec : m) : k;
   const int W = nvec < 32 ? nvec : 32;
