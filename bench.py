@@ -364,7 +364,8 @@ def run_ours(args, world, rank, local):
         launches0 = s.stats()["kernel_launches"]
         prof = {"matvec_seconds": 0.0, "matvec_timed": 0, "block_seconds": 0.0, "block_timed": 0,
                 "block_fp32_seconds": 0.0, "block_fp32_timed": 0, "block_fp32_width": 0,
-                "block_bf16_seconds": 0.0, "block_bf16_timed": 0}
+                "block_bf16_seconds": 0.0, "block_bf16_timed": 0,
+                "pass_kernel_seconds": [0.0, 0.0, 0.0], "pass_kernel_timed": [0, 0, 0]}
         conv = 0
         # per-launch CUDA events (the roofline's kernel times) on the last
         # third of the timed solves: an event pair around a pass also breaks
@@ -378,7 +379,12 @@ def run_ours(args, world, rank, local):
             ev, res, st = s.solve(allow_not_converged=True)
             stt = s.stats()
             for key in prof:
-                prof[key] = stt[key] if key == "block_fp32_width" else prof[key] + stt[key]
+                if key == "block_fp32_width":
+                    prof[key] = stt[key]
+                elif isinstance(prof[key], list):
+                    prof[key] = [x + y for x, y in zip(prof[key], stt[key])]
+                else:
+                    prof[key] += stt[key]
             conv += int(st == B.OK and max(res) <= TOL)
         e1.record()
         torch.cuda.synchronize()
@@ -490,17 +496,32 @@ def run_ours(args, world, rank, local):
                  else "k_block_matvec_dmma<complex> (FP64 DMMA block pass)" if not args.no_tc
                  else "k_block_matvec<double,complex> (FP64 CUDA-core block pass)")
     fp64_bytes = (12.0 * n * kp if i8 else 16.0 * n * n) + 32.0 * bw * n
+    # the tensor-core passes are timed by events right around their kernel
+    # (pass_kernel_*: [0] FP64-class, [1] split, [2] BF16); the unit times
+    # (block_*_seconds) also hold the vector split and the stream-K reduction
+    pk_s, pk_n = prof["pass_kernel_seconds"], prof["pass_kernel_timed"]
+    tc_fp32 = (not args.no_tc) and pk_n[1] > 0
+    tc_fp64 = (not args.no_tc) and pk_n[0] > 0
     kernels = {
         "k_matvec<float,complex> (FP32 complex matvec)":
             (prof["matvec_seconds"], prof["matvec_timed"], 8.0 * n * n + 16.0 * n, 8.0 * n * n),
         fp32_name:
-            (prof["block_fp32_seconds"], prof["block_fp32_timed"], 8.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
+            ((pk_s[1], pk_n[1]) if tc_fp32 else (prof["block_fp32_seconds"], prof["block_fp32_timed"])) +
+            (8.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n),
         fp64_name:
-            (prof["block_seconds"], prof["block_timed"], fp64_bytes, 8.0 * bw * n * n),
+            ((pk_s[0], pk_n[0]) if tc_fp64 else (prof["block_seconds"], prof["block_timed"])) +
+            (fp64_bytes, 8.0 * bw * n * n),
     }
     if not args.no_tc:
         kernels["k_block_matvec_tc<complex, BF16> (BF16 hi-plane tcgen05 block pass)"] = (
-            prof["block_bf16_seconds"], prof["block_bf16_timed"], 4.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n)
+            pk_s[2], pk_n[2], 4.0 * n * n + 32.0 * bw * n, 8.0 * bw * n * n)
+    # the same passes with their vector split and stream-K reduction (what a
+    # pass costs the solve)
+    units = {fp32_name: (prof["block_fp32_seconds"], prof["block_fp32_timed"]),
+             fp64_name: (prof["block_seconds"], prof["block_timed"])}
+    if not args.no_tc:
+        units["k_block_matvec_tc<complex, BF16> (BF16 hi-plane tcgen05 block pass)"] = (
+            prof["block_bf16_seconds"], prof["block_bf16_timed"])
     name, (tot, cnt, alg_bytes, flops) = max(kernels.items(), key=lambda kv: kv[1][0])
     per_launch = tot / max(1, cnt)
     achieved = alg_bytes / per_launch / 1e9 if per_launch > 0 else 0.0
@@ -511,8 +532,12 @@ def run_ours(args, world, rank, local):
             "traffic": (traffic or {}).get(name.split(" (")[0], {}).get("bytes_per_launch") if traffic else None,
             "launch_ms": per_launch * 1e3, "launches_timed": cnt, "algorithmic_bytes_per_launch": alg_bytes,
             "tflops": flops / per_launch / 1e12 if per_launch > 0 else 0.0,
+            "timing": "CUDA events recorded right before and after the pass kernel's launch on its stream",
             # the kernel's device time per profiled solve over the time per solve
             "share_of_step": (tot / prof["profiled_solves"]) / (secs / args.steps) if secs > 0 else None,
+            "with_split_and_reduce": {k: {"launches": v[1], "ms_per_launch": v[0] / v[1] * 1e3 if v[1] else None,
+                                          "frac": (kernels[k][2] / (v[0] / v[1]) / 1e9 / hbm) if v[1] else None}
+                                      for k, v in units.items()},
             "all_kernels": {k: {"launches": v[1], "total_ms": v[0] * 1e3,
                                 "GBs": (v[2] / (v[0] / v[1]) / 1e9) if v[1] else None,
                                 "frac": (v[2] / (v[0] / v[1]) / 1e9 / hbm) if v[1] else None,

@@ -272,6 +272,13 @@ typedef struct oapb_arnoldi_stats {
   uint32_t onchip;           /* 1: the last solve ran on one CTA (the chosen
                                 form for dense operators with n <= 2048 and
                                 hdim <= 32, random start) */
+  /* device time of the tensor-core pass kernels alone (profile), between
+   * events recorded right before and after each launch: [0] FP64-class
+   * (int8-slice) pass, [1] split-BF16 pass, [2] BF16 hi-plane pass; the
+   * block_*_seconds fields above also cover the vector split and the
+   * stream-K reduction around each pass */
+  double pass_kernel_seconds[3];
+  uint32_t pass_kernel_timed[3];
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

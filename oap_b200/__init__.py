@@ -65,7 +65,8 @@ class Stats(C.Structure):
                 ("block_fp32_width", C.c_uint32), ("fallbacks", C.c_uint32),
                 ("matvec_variant", C.c_uint32), ("block_bf16", C.c_uint32),
                 ("block_bf16_timed", C.c_uint32), ("block_bf16_seconds", C.c_double),
-                ("eig_fast", C.c_uint32), ("block_i8", C.c_uint32), ("onchip", C.c_uint32)]
+                ("eig_fast", C.c_uint32), ("block_i8", C.c_uint32), ("onchip", C.c_uint32),
+                ("pass_kernel_seconds", C.c_double * 3), ("pass_kernel_timed", C.c_uint32 * 3)]
 
 
 class BatchProblem(C.Structure):
@@ -378,7 +379,8 @@ class Arnoldi:
     def stats(self):
         s = Stats()
         check(lib().oapb_arnoldi_get_stats(self.h, C.byref(s)), "oapb_arnoldi_get_stats")
-        return {f: getattr(s, f) for f, _ in Stats._fields_}
+        return {f: (list(getattr(s, f)) if isinstance(getattr(s, f), C.Array) else getattr(s, f))
+                for f, _ in Stats._fields_}
 
     def test_outcome(self, index):
         out = C.c_double()

@@ -221,7 +221,7 @@ constexpr int kDotChunk = 32;
 constexpr int kDotBlocks = 2 * kNumSMs;
 
 // part[blk][i + j * b1] = sum over the block's row chunks of conj(X_i[r]) Y_j[r]
-// (chunks blk, blk + gridDim.x, ...; every thread owns up to 4 entries)
+// (chunks blk, blk + gridDim.x, ...; every thread owns a 2 x 2 tile of entries)
 template <bool CPLX>
 __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xre, const double* __restrict__ Xim,
                                                    int b1, const double* __restrict__ Yre,
@@ -231,6 +231,11 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
   if (blockDim.x != 256) return;  // the staging below assumes 256 threads
   pdl_wait();
   const int cnt = b1 * b2;
+  // 2 x 2 tiles over (b1 rounded up to even) x (b2 rounded up to even):
+  // at most 16 x 16 = 256 tiles for b <= 32
+  const int tb1 = (b1 + 1) / 2, tb2 = (b2 + 1) / 2;
+  const bool tile = (int)threadIdx.x < tb1 * tb2;
+  const int i0 = tile ? 2 * ((int)threadIdx.x % tb1) : 0, j0 = tile ? 2 * ((int)threadIdx.x / tb1) : 0;
   double ar[4] = {0, 0, 0, 0}, ai[4] = {0, 0, 0, 0};
   const long nchunks = (n + kDotChunk - 1) / kDotChunk;
   // 256 threads: each stages kDotPer elements of every plane, loaded into
@@ -261,27 +266,37 @@ __global__ void __launch_bounds__(256) k_block_dot(const double* __restrict__ Xr
       yi[q][rr] = vyi[u];
     }
     __syncthreads();
+    // thread = 2 x 2 tile of entries (rows i0, i0 + 1 of X, j0, j0 + 1 of Y):
+    // each staged value feeds two products; per entry the chunk's rows are
+    // summed in order and the chunk sum added to the running sum
+    if (tile) {
+      double sr[4] = {0, 0, 0, 0}, si[4] = {0, 0, 0, 0};
+#pragma unroll 4
+      for (int rr = 0; rr < kDotChunk; ++rr) {
+        const double a0 = xr[i0][rr], b0 = xi[i0][rr], a1 = xr[i0 + 1][rr], b1v = xi[i0 + 1][rr];
+        const double c0 = yr[j0][rr], d0 = yi[j0][rr], c1 = yr[j0 + 1][rr], d1 = yi[j0 + 1][rr];
+        sr[0] += a0 * c0 + b0 * d0;
+        si[0] += a0 * d0 - b0 * c0;
+        sr[1] += a1 * c0 + b1v * d0;
+        si[1] += a1 * d0 - b1v * c0;
+        sr[2] += a0 * c1 + b0 * d1;
+        si[2] += a0 * d1 - b0 * c1;
+        sr[3] += a1 * c1 + b1v * d1;
+        si[3] += a1 * d1 - b1v * c1;
+      }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int p = threadIdx.x + u * 256;
-      if (p < cnt) {
-        const int i = p % b1, j = p / b1;
-        double sr = 0, si = 0;
-#pragma unroll 8
-        for (int rr = 0; rr < kDotChunk; ++rr) {
-          const double a = xr[i][rr], bb = xi[i][rr], c = yr[j][rr], d = yi[j][rr];
-          sr += a * c + bb * d;
-          si += a * d - bb * c;
-        }
-        ar[u] += sr;
-        ai[u] += si;
+      for (int u = 0; u < 4; ++u) {
+        ar[u] += sr[u];
+        ai[u] += si[u];
       }
     }
   }
+  if (tile) {
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    const int p = threadIdx.x + u * 256;
-    if (p < cnt) part[(long)blockIdx.x * cnt + p] = cplx{ar[u], ai[u]};
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + (u & 1), j = j0 + (u >> 1);
+      if (i < b1 && j < b2) part[(long)blockIdx.x * cnt + i + j * b1] = cplx{ar[u], ai[u]};
+    }
   }
 }
 
@@ -578,14 +593,30 @@ __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__
     __syncthreads();
     const long r = r0 + rr;
     if (r < n) {
-      for (int j = g; j < b2; j += kUpGroups) {
-        cplx acc = {0, 0};
-        for (int i = 0; i < b1; ++i) acc = acc + cplx{xs_r[i][rr], CPLX ? xs_i[i][rr] : 0.0} * cs[i + j * b1];
-        cplx o;
-        if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc;
-        else o = negate ? -acc : acc;
-        Ore[(long)j * n + r] = o.re;
-        if (CPLX) Oim[(long)j * n + r] = o.im;
+      // outputs j = g + 4 t of this row: each staged x_i is read once and
+      // feeds every accumulator (the coefficients are broadcast reads)
+      constexpr int kT = kBmMaxB / kUpGroups;
+      cplx acc[kT];
+#pragma unroll
+      for (int t = 0; t < kT; ++t) acc[t] = cplx{0, 0};
+      for (int i = 0; i < b1; ++i) {
+        const cplx x = {xs_r[i][rr], CPLX ? xs_i[i][rr] : 0.0};
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+          const int j = g + kUpGroups * t;
+          if (j < b2) acc[t] = acc[t] + x * cs[i + j * b1];
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < kT; ++t) {
+        const int j = g + kUpGroups * t;
+        if (j < b2) {
+          cplx o;
+          if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc[t];
+          else o = negate ? -acc[t] : acc[t];
+          Ore[(long)j * n + r] = o.re;
+          if (CPLX) Oim[(long)j * n + r] = o.im;
+        }
       }
     }
   }

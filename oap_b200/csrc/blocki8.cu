@@ -554,7 +554,7 @@ int split_operator_i8(const double* are, const double* aim, int n, int kp, int8_
 size_t i8_workspace(int n, int kp) { return sk_workspace(i8_grid(n, kp)); }
 
 int launch_block_matvec_i8(const I8Operator& op, const double* xr, const double* xi, int b, double* wr, double* wi,
-                           int8_t* xs, double* xscale, double* ws, int* err, cudaStream_t s) {
+                           int8_t* xs, double* xscale, double* ws, int* err, cudaStream_t s, const cudaEvent_t* kev) {
   const bool cplx = op.cplx;
   if (b < 1 || b > i8_max_vectors(cplx) || op.kp % 128 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
   const int QB = (b + 7) / 8 * 8;
@@ -596,7 +596,9 @@ int launch_block_matvec_i8(const I8Operator& op, const double* xr, const double*
   auto kern = cplx ? k_block_matvec_i8<true> : k_block_matvec_i8<false>;
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return OAPB_ERR_CUDA;
+  if (kev) cudaEventRecord(kev[0], s);
   if (launch_dependent(kern, dim3(g.grid.grid), dim3(kI8Threads), smem, s, g) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (kev) cudaEventRecord(kev[1], s);
   if (cplx)
     launch_sk_reduce<true>(ws, g.grid, op.n, b, wr, wi, s);
   else

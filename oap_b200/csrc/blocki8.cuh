@@ -46,8 +46,11 @@ size_t i8_workspace(int n, int kp);
 // W (planes wr / wi, vector q at offset q n) = A X for b <= i8_max_vectors
 // vectors (X vector-contiguous FP64).  xs: i8_block_bytes(kp) bytes, xscale:
 // kI8ScaleDoubles doubles, ws: i8_workspace() doubles; *err receives
-// timeout bits.
+// timeout bits.  kev (optional, two events): recorded right before and after
+// the pass kernel alone (profiling; breaks the dependent-launch overlap with
+// the kernels around it).
 int launch_block_matvec_i8(const I8Operator& op, const double* xr, const double* xi, int b, double* wr, double* wi,
-                           int8_t* xs, double* xscale, double* ws, int* err, cudaStream_t s);
+                           int8_t* xs, double* xscale, double* ws, int* err, cudaStream_t s,
+                           const cudaEvent_t* kev = nullptr);
 
 }  // namespace oapb

@@ -460,7 +460,7 @@ size_t btc_workspace(int n, int kp) {
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only, bool x_hi_only, int ctas) {
+                           cudaStream_t s, bool bf16_only, bool x_hi_only, int ctas, const cudaEvent_t* kev) {
   const bool cplx = op.aih != nullptr;
   const int kh = bf16_only ? 2 : 1;
   if (b < 1 || b > 32 || op.kp % (kBtcK * kh) != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
@@ -495,7 +495,9 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
                         : (cplx ? k_block_matvec_tc<true, true, true> : k_block_matvec_tc<false, true, true>);
   if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return OAPB_ERR_CUDA;
+  if (kev) cudaEventRecord(kev[0], s);
   if (launch_dependent(kern, dim3(g.grid.grid), dim3(kBtcThreads), smem, s, g) != cudaSuccess) return OAPB_ERR_CUDA;
+  if (kev) cudaEventRecord(kev[1], s);
   if (cplx)
     launch_sk_reduce<true>(ws, g.grid, op.n, b, wr, wi, s);
   else

@@ -31,9 +31,12 @@ size_t btc_workspace(int n, int kp);
 // bf16_only: the operator's hi planes only (half the bytes, BF16 accuracy);
 // x_hi_only (with bf16_only): X rounded to BF16 as well (its lo part unused).
 // ctas: stream-K CTAs (kNumSMs - 1 leaves one SM to kernels of another
-// stream; every CTA holds most of its SM's shared memory).
+// stream; every CTA holds most of its SM's shared memory).  kev (optional,
+// two events): recorded right before and after the pass kernel alone
+// (profiling; breaks the dependent-launch overlap with the kernels around it).
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only = false, bool x_hi_only = false, int ctas = kNumSMs);
+                           cudaStream_t s, bool bf16_only = false, bool x_hi_only = false, int ctas = kNumSMs,
+                           const cudaEvent_t* kev = nullptr);
 
 }  // namespace oapb

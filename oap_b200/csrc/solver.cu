@@ -569,6 +569,21 @@ bool prof_begin(oapb_arnoldi* a, Timed& t) {
   return true;
 }
 void prof_end(oapb_arnoldi* a, Timed& t) { cudaEventRecord(t.e1, a->stream); }
+// a pair of events for a pass kernel alone (kind 6 + pass: 0 FP64-class,
+// 1 split, 2 BF16), recorded by the launch function; nullptr without profile
+const cudaEvent_t* prof_kernel_pair(oapb_arnoldi* a, int pass) {
+  if (!a->cfg.profile) return nullptr;
+  while (a->ev_pool.size() < a->ev_used + 2) {
+    cudaEvent_t ev;
+    if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+    a->ev_pool.push_back(ev);
+  }
+  const cudaEvent_t* e = &a->ev_pool[a->ev_used];
+  a->ev_used += 2;
+  a->ev_kind.push_back(6 + pass);
+  a->ev_b.push_back(0);
+  return e;
+}
 
 // f <- ||f||^2 into st->fnorm2
 int set_fnorm(oapb_arnoldi* a) {
@@ -865,8 +880,9 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     BtcOperator op{a->abf, a->abf + (size_t)a->n * a->kp, C ? a->abf + 2 * (size_t)a->n * a->kp : nullptr,
                    C ? a->abf + 3 * (size_t)a->n * a->kp : nullptr, a->n, a->kp};
     const int ctas = (a->side_busy && side_sm_reserve()) ? kNumSMs - 1 : kNumSMs;
+    const cudaEvent_t* kev = prof ? prof_kernel_pair(a, bf16 ? 2 : 1) : nullptr;
     int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
-                                    a->tcerr, a->stream, bf16, bf16 && coarse, ctas);
+                                    a->tcerr, a->stream, bf16, bf16 && coarse, ctas, kev);
     if (bf16) a->stats.block_bf16++;
     if (prof) prof_end(a, tm);
     if (rc) return rc;
@@ -878,7 +894,8 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
   if (!fp32 && a->have_i8 && a->mixed_ready && a->cfg.tensor_cores && b <= i8_max_vectors(C) &&
       a->cfg.tolerance >= kI8MinTolerance) {
     const I8Operator op{a->ai8, a->ai8s, a->n, a->kp, C};
-    int rc = launch_block_matvec_i8(op, xr, xi, b, wr, wi, a->xi8, a->xi8s, a->wdm, a->tcerr, a->stream);
+    const cudaEvent_t* kev = prof ? prof_kernel_pair(a, 0) : nullptr;
+    int rc = launch_block_matvec_i8(op, xr, xi, b, wr, wi, a->xi8, a->xi8s, a->wdm, a->tcerr, a->stream, kev);
     if (prof) prof_end(a, tm);
     if (rc) return rc;
     a->stats.block_matvecs++;
@@ -2219,13 +2236,20 @@ static int solve_entry(oapb_arnoldi* a, double* eig_re, double* eig_im, double* 
   a->stats.block_fp32_timed = 0;
   a->stats.block_bf16_seconds = 0;
   a->stats.block_bf16_timed = 0;
+  for (int p = 0; p < 3; ++p) {
+    a->stats.pass_kernel_seconds[p] = 0;
+    a->stats.pass_kernel_timed[p] = 0;
+  }
   if (a->ev_used) {
     cudaStreamSynchronize(a->stream);
     for (size_t i = 0; i + 1 < a->ev_used; i += 2) {
       float ms = 0;
       if (cudaEventElapsedTime(&ms, a->ev_pool[i], a->ev_pool[i + 1]) != cudaSuccess) continue;
       const int kind = a->ev_kind[i / 2];
-      if (kind == 0 || kind == 2) {
+      if (kind >= 6) {
+        a->stats.pass_kernel_seconds[kind - 6] += ms * 1e-3;
+        a->stats.pass_kernel_timed[kind - 6]++;
+      } else if (kind == 0 || kind == 2) {
         a->stats.matvec_seconds += ms * 1e-3;
         a->stats.matvec_timed++;
       } else if (kind == 1) {
