@@ -128,11 +128,9 @@ OAPB_EXPORT int oapb_qr_givens(const oapb_mat* Q, const oapb_mat* R, const oapb_
  * reference: it exists for callers that cannot allocate (a stream capture
  * that forbids allocations, allocator hooks, fixed memory budgets).  Same
  * results as oapb_qr_givens; the workspace is a static 512 KiB device array
- * of the library, so n <= 128 (OAPB_ERR_ARG beyond).  The first call on a
- * device resolves the array's address and should precede any stream
- * capture; the address stays cached, so the entry point must not be used
- * on a device after cudaDeviceReset; calls that overlap on the GPU share
- * the array and race. */
+ * of the library, so n <= 128 (OAPB_ERR_ARG beyond).  The first call in a
+ * context loads the array's module and should precede any stream capture;
+ * calls that overlap on the GPU share the array and race. */
 OAPB_EXPORT int oapb_qr_givens_noalloc(const oapb_mat* Q, const oapb_mat* R,
                                        const oapb_mat* A, void* stream);
 

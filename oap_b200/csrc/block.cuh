@@ -593,30 +593,14 @@ __global__ void __launch_bounds__(256) k_block_update(const double* __restrict__
     __syncthreads();
     const long r = r0 + rr;
     if (r < n) {
-      // outputs j = g + 4 t of this row: each staged x_i is read once and
-      // feeds every accumulator (the coefficients are broadcast reads)
-      constexpr int kT = kBmMaxB / kUpGroups;
-      cplx acc[kT];
-#pragma unroll
-      for (int t = 0; t < kT; ++t) acc[t] = cplx{0, 0};
-      for (int i = 0; i < b1; ++i) {
-        const cplx x = {xs_r[i][rr], CPLX ? xs_i[i][rr] : 0.0};
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-          const int j = g + kUpGroups * t;
-          if (j < b2) acc[t] = acc[t] + x * cs[i + j * b1];
-        }
-      }
-#pragma unroll
-      for (int t = 0; t < kT; ++t) {
-        const int j = g + kUpGroups * t;
-        if (j < b2) {
-          cplx o;
-          if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc[t];
-          else o = negate ? -acc[t] : acc[t];
-          Ore[(long)j * n + r] = o.re;
-          if (CPLX) Oim[(long)j * n + r] = o.im;
-        }
+      for (int j = g; j < b2; j += kUpGroups) {
+        cplx acc = {0, 0};
+        for (int i = 0; i < b1; ++i) acc = acc + cplx{xs_r[i][rr], CPLX ? xs_i[i][rr] : 0.0} * cs[i + j * b1];
+        cplx o;
+        if (Bre) o = cplx{Bre[(long)j * n + r], CPLX ? Bim[(long)j * n + r] : 0.0} - acc;
+        else o = negate ? -acc : acc;
+        Ore[(long)j * n + r] = o.re;
+        if (CPLX) Oim[(long)j * n + r] = o.im;
       }
     }
   }

@@ -63,23 +63,31 @@ constexpr size_t kBtcSmemBudget = 220 * 1024;
 constexpr int kBtcSub = 32;
 
 // X (FP64 planes, b vectors of n) -> B operand hi / lo (rows: q for re,
-// QB + q for im; K = n padded to kp), zero rows / columns beyond b / n
+// QB + q for im; K = n padded to kp), zero rows / columns beyond b / n.
+// Grid (column blocks, nrows): row blockIdx.y, four consecutive columns per
+// thread, stored as 8-byte packs (kp is a multiple of 128).
 __global__ void k_split_block_bf16(const double* __restrict__ xr, const double* __restrict__ xi, int b, int QB,
                                    int nrows, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo) {
   // launched as a dependent of whatever wrote X (or last read hi / lo)
   tc::griddep_wait();
-  const long total = (long)nrows * kp;
-  for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-    const int row = (int)(e / kp);
-    const long c = e % kp;
-    float v = 0.f;
-    if (c < n) {
-      if (row < b) v = (float)xr[(long)row * n + c];
-      else if (xi && row >= QB && row < QB + b) v = (float)xi[(long)(row - QB) * n + c];
+  const int row = blockIdx.y;
+  if (row >= nrows) return;
+  const double* src = row < b ? xr + (long)row * n
+                              : ((xi && row >= QB && row < QB + b) ? xi + (long)(row - QB) * n : nullptr);
+  __nv_bfloat16* hrow = hi + (long)row * kp;
+  __nv_bfloat16* lrow = lo + (long)row * kp;
+  for (long c0 = ((long)blockIdx.x * blockDim.x + threadIdx.x) * 4; c0 < kp;
+       c0 += (long)gridDim.x * blockDim.x * 4) {
+    __align__(8) __nv_bfloat16 h[4], l[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const long c = c0 + u;
+      const float v = (src && c < n) ? (float)src[c] : 0.f;
+      h[u] = __float2bfloat16_rn(v);
+      l[u] = __float2bfloat16_rn(v - __bfloat162float(h[u]));
     }
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    hi[e] = h;
-    lo[e] = __float2bfloat16_rn(v - __bfloat162float(h));
+    *reinterpret_cast<uint2*>(hrow + c0) = *reinterpret_cast<const uint2*>(h);
+    *reinterpret_cast<uint2*>(lrow + c0) = *reinterpret_cast<const uint2*>(l);
   }
 }
 
@@ -468,8 +476,8 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
-  if (launch_dependent(k_split_block_bf16, dim3(kNumSMs * 4), dim3(256), 0, s, xr, cplx ? xi : nullptr, b, QB, N, op.n,
-                       op.kp, xbh, xbl) != cudaSuccess)
+  if (launch_dependent(k_split_block_bf16, dim3((op.kp + 1023) / 1024, N), dim3(256), 0, s, xr, cplx ? xi : nullptr, b,
+                       QB, N, op.n, op.kp, xbh, xbl) != cudaSuccess)
     return OAPB_ERR_CUDA;
   BtcArgs g;
   const __nv_bfloat16* planes[4] = {op.arh, op.arl, cplx ? op.aih : op.arh, cplx ? op.ail : op.arl};

@@ -20,7 +20,6 @@
 // host threads on one device) race on it and must be serialised by the
 // caller.  The kernel overwrites the whole workspace it uses before reading
 // it, so nothing has to be cleared between calls.
-#include <mutex>
 
 #include "common.cuh"
 
@@ -37,21 +36,13 @@ __global__ void k_qr_givens(const double* __restrict__ are, const double* __rest
                             double* qim, double* rre, double* rim, int n, cplx* gws);
 
 namespace {
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of g_qr_scratch on the current device (looked up once).
+// Device address of g_qr_scratch in the current context, looked up on every
+// call (the lookup allocates nothing, and a cached address would not survive
+// a reset of the context).
 int scratch_address(void** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return OAPB_ERR_CUDA;
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_qr_scratch) != cudaSuccess || !p) return OAPB_ERR_CUDA;
-    g_scratch_addr[dev] = p;
-  }
-  *out = g_scratch_addr[dev];
+  void* p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_qr_scratch) != cudaSuccess || !p) return OAPB_ERR_CUDA;
+  *out = p;
   return OAPB_OK;
 }
 }  // namespace
