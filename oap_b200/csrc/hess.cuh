@@ -854,54 +854,40 @@ static __global__ void __launch_bounds__(32 * kHessWarps) k_hess_f32(HessArgs a)
 // Eigenpairs of a nearly upper-triangular T (m x m complex, column-major,
 // m <= 32): the Rayleigh quotient of an orthonormalised basis of Ritz vectors
 // ordered like their values, whose strictly lower part is of the size of the
-// Ritz vectors' errors.  Warp w of nw takes pairs q = w, w + nw, ...:
-// Rayleigh quotient iteration from v = e_q, sigma = T(q,q) (LU with partial
-// pivoting of T - sigma I, a zero pivot replaced by eps ||T||_F; v <- (T -
-// sigma I)^-1 v normalised; sigma <- v^H T v), at most kNtIters steps, until
-// ||T v - sigma v|| <= 16 eps ||T||_F.  Accepted when every such residual is
-// <= 64 eps ||T||_F and the values are pairwise apart by more than 1e-9
-// max |theta|:
-// then ritz / Y / order are written in the ArnUtils order of `which` (as
-// k_hess writes them, Y column q at Y + q m, unit 2-norm) and *delivered = 1;
-// otherwise *delivered = 0 and nothing else is written (k_hess follows with
-// skip = delivered).  Launch nt_warps(m) warps, dynamic shared memory
-// nt_smem_bytes(m, nt_warps(m)).
-constexpr int kNtWarpsMax = 16;
+// Ritz vectors' errors.  k_eig_near_tri: one CTA of one warp per pair q
+// (grid m, each pair on its own SM): Rayleigh quotient iteration from v =
+// e_q, sigma = T(q,q) (LU with partial pivoting of T - sigma I, a zero pivot
+// replaced by eps ||T||_F; v <- (T - sigma I)^-1 v normalised; sigma <- v^H
+// T v), at most kNtIters steps, until ||T v - sigma v|| <= 16 eps ||T||_F;
+// the pair goes to the scratch (V column q at V + q m, th[q]) and ok[0] is
+// cleared when its residual is above 64 eps ||T||_F.  k_eig_near_tri_finish
+// (one warp, after it): accepted when ok[0] is set and the values are
+// pairwise apart by more than 1e-9 max |theta|; then ritz / Y / order are
+// written in the ArnUtils order of `which` (as k_hess writes them, Y column
+// q at Y + q m, unit 2-norm) and *delivered = 1; otherwise *delivered = 0
+// and nothing else is written (k_hess follows with skip = delivered).
+// ok[0] is set again for the next call (it must hold 1 before the first).
 constexpr int kNtIters = 4;
 __host__ __device__ inline int nt_ld(int m) { return m + 1; }
-__host__ __device__ inline size_t nt_smem_bytes(int m, int nw) {
-  return sizeof(cplx) * ((size_t)(nw + 1) * m * nt_ld(m) + (size_t)2 * nw * m + (size_t)m * m + m) +
-         sizeof(double) * 2 * m + sizeof(int) * (nw * m + m + 1);
-}
-// warps for m: one per pair while the workspace stays within 200 KB
-inline int nt_warps(int m) {
-  int nw = m < kNtWarpsMax ? m : kNtWarpsMax;
-  while (nw > 1 && nt_smem_bytes(m, nw) > 200 * 1024) --nw;
-  return nw;
+// dynamic shared memory of k_eig_near_tri: T, M (m x LD), x, t (m), pivots
+__host__ __device__ inline size_t nt_smem_bytes(int m) {
+  return sizeof(cplx) * (2 * (size_t)m * nt_ld(m) + 2 * (size_t)m) + sizeof(int) * (size_t)m;
 }
 
-static __global__ void __launch_bounds__(kNtWarpsMax * 32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, int which,
-                                                                cplx* ritz, cplx* Y, int* order, int* delivered) {
+static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, cplx* V, cplx* th,
+                                                            int* ok) {
   extern __shared__ __align__(16) unsigned char nt_dyn[];
   asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
   const int LD = nt_ld(m);
-  cplx* T = reinterpret_cast<cplx*>(nt_dyn);                 // m x LD
-  const int nw = blockDim.x >> 5;
-  cplx* Mw = T + (size_t)m * LD;                             // nw x (m x LD)
-  cplx* xw = Mw + (size_t)nw * m * LD;                       // nw x m
-  cplx* tw = xw + (size_t)nw * m;                            // nw x m
-  cplx* V = tw + (size_t)nw * m;                             // m x m eigenvectors (column q)
-  cplx* th = V + (size_t)m * m;                              // m
-  double* res = reinterpret_cast<double*>(th + m);           // m
-  double* key = res + m;                                     // m
-  int* piv = reinterpret_cast<int*>(key + m);                // nw x m
-  int* ord = piv + nw * m;                                   // m
-  int* ok = ord + m;                                         // 1
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (m < 1 || m > 32) return;
-  for (int e = tid; e < m * m; e += blockDim.x) T[(e % m) + (e / m) * LD] = Tin[e];
-  if (tid == 0) *ok = 1;
-  __syncthreads();
+  cplx* T = reinterpret_cast<cplx*>(nt_dyn);  // m x LD
+  cplx* M = T + (size_t)m * LD;               // m x LD
+  cplx* x = M + (size_t)m * LD;               // m
+  cplx* t = x + m;                            // m
+  int* pv = reinterpret_cast<int*>(t + m);    // m
+  const int lane = threadIdx.x, q = blockIdx.x;
+  if (m < 1 || m > 32 || q >= m) return;
+  for (int e = lane; e < m * m; e += 32) T[(e % m) + (e / m) * LD] = Tin[e];
+  __syncwarp();
   double fro = 0;
   for (int e = lane; e < m * m; e += 32) fro += abs2(T[(e % m) + (e / m) * LD]);
 #pragma unroll
@@ -909,11 +895,7 @@ static __global__ void __launch_bounds__(kNtWarpsMax * 32) k_eig_near_tri(const 
   fro = sqrt(fro);
   const double eps = 2.220446049250313e-16;
   const double tiny = eps * (fro > 0 ? fro : 1.0);
-  cplx* M = Mw + (size_t)warp * m * LD;
-  cplx* x = xw + (size_t)warp * m;
-  cplx* t = tw + (size_t)warp * m;
-  int* pv = piv + warp * m;
-  for (int q = warp; q < m; q += nw) {
+  {
     cplx sigma = T[q + q * LD], thq = {0, 0};
     double rq = 1e300;
     for (int i = lane; i < m; i += 32) x[i] = cplx{i == q ? 1.0 : 0.0, 0.0};
@@ -1026,45 +1008,53 @@ static __global__ void __launch_bounds__(kNtWarpsMax * 32) k_eig_near_tri(const 
     for (int i = lane; i < m; i += 32) V[i + (size_t)q * m] = x[i];
     if (lane == 0) {
       th[q] = thq;
-      res[q] = rq;
-      if (!(rq <= 64 * eps * fro)) *ok = 0;
+      if (!(rq <= 64 * eps * fro)) ok[0] = 0;
     }
-    __syncwarp();
   }
-  __syncthreads();
+}
+
+static __global__ void __launch_bounds__(32) k_eig_near_tri_finish(int m, int which, const cplx* __restrict__ V,
+                                                                   const cplx* __restrict__ th, int* ok, cplx* ritz,
+                                                                   cplx* Y, int* order, int* delivered) {
+  __shared__ double key[32];
+  __shared__ int ord[32];
+  asm volatile("griddepcontrol.wait;" ::: "memory");  // dependent launch
+  const int lane = threadIdx.x;
+  if (m < 1 || m > 32) return;
   // distinct values, then the ArnUtils order
-  if (warp == 0) {
-    double tmax = 0;
-    for (int q = lane; q < m; q += 32) tmax = fmax(tmax, cabs_(th[q]));
+  double tmax = 0;
+  for (int q = lane; q < m; q += 32) tmax = fmax(tmax, cabs_(th[q]));
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
-    int bad = 0;
-    for (int e = lane; e < m * m; e += 32) {
-      const int q = e % m, r = e / m;
-      if (q < r && !(cabs_(th[q] - th[r]) > 1e-9 * tmax)) bad = 1;
-    }
-    bad = __any_sync(0xffffffffu, bad);
-    if (lane == 0 && bad) *ok = 0;
-    for (int i = lane; i < m; i += 32) {
-      const double kv = sort_key(th[i], which);
-      key[i] = (kv != kv) ? INFINITY : kv;
-    }
-    __syncwarp();
-    for (int i = lane; i < m; i += 32) {
-      int r = 0;
-      for (int j = 0; j < m; ++j) r += (key[j] < key[i]) || (key[j] == key[i] && j < i);
-      ord[r] = i;
-    }
+  for (int o = 16; o > 0; o >>= 1) tmax = fmax(tmax, __shfl_xor_sync(0xffffffffu, tmax, o));
+  int bad = 0;
+  for (int e = lane; e < m * m; e += 32) {
+    const int q = e % m, r = e / m;
+    if (q < r && !(cabs_(th[q] - th[r]) > 1e-9 * tmax)) bad = 1;
   }
-  __syncthreads();
-  const int good = *ok;
-  if (tid == 0) *delivered = good;
+  bad = __any_sync(0xffffffffu, bad);
+  for (int i = lane; i < m; i += 32) {
+    const double kv = sort_key(th[i], which);
+    key[i] = (kv != kv) ? INFINITY : kv;
+  }
+  __syncwarp();
+  for (int i = lane; i < m; i += 32) {
+    int r = 0;
+    for (int j = 0; j < m; ++j) r += (key[j] < key[i]) || (key[j] == key[i] && j < i);
+    ord[r] = i;
+  }
+  __syncwarp();
+  const int good = ok[0] && !bad;
+  __syncwarp();
+  if (lane == 0) {
+    *delivered = good;
+    ok[0] = 1;
+  }
   if (!good) return;
-  for (int q = tid; q < m; q += blockDim.x) {
+  for (int q = lane; q < m; q += 32) {
     ritz[q] = th[ord[q]];
     order[q] = ord[q];
   }
-  for (int e = tid; e < m * m; e += blockDim.x) {
+  for (int e = lane; e < m * m; e += 32) {
     const int i = e % m, q = e / m;
     Y[i + (size_t)q * m] = V[i + (size_t)ord[q] * m];
   }

@@ -473,7 +473,7 @@ struct oapb_arnoldi {
   static constexpr int kBlocks = 6;
   double *Bre[kBlocks] = {}, *Bim[kBlocks] = {};
   cplx* Tinv = nullptr;   // T^-1 of the refinement's projected operator (kBmMaxB^2)
-  int* ntflag = nullptr;  // the near-triangular eigensolver delivered (device word)
+  int* ntflag = nullptr;  // [0] the near-triangular eigensolver delivered, [1] its pairs' acceptance (device words)
   std::vector<oapb_trace_rec> trace;  // convergence checks of the last solve
   cplx *bpart = nullptr, *G = nullptr, *G2 = nullptr, *Rinv = nullptr, *bY = nullptr, *bQ = nullptr, *bH = nullptr;
   cplx *britz = nullptr;
@@ -813,7 +813,11 @@ int alloc_blocks(oapb_arnoldi* a) {
   rc |= dalloc(&a->bH, bb);
   rc |= dalloc(&a->britz, sizeof(cplx) * kBmMaxB);
   rc |= dalloc(&a->Tinv, bb);
-  rc |= dalloc(&a->ntflag, sizeof(int));
+  rc |= dalloc(&a->ntflag, 2 * sizeof(int));
+  if (a->ntflag) {  // delivered = 0, ok = 1 (k_eig_near_tri_finish sets ok again after each use)
+    const int init[2] = {0, 1};
+    if (cudaMemcpy(a->ntflag, init, sizeof(init), cudaMemcpyHostToDevice) != cudaSuccess) rc |= OAPB_ERR_CUDA;
+  }
   rc |= dalloc(&a->best, sizeof(double) * kBmMaxB);
   rc |= dalloc(&a->bnorm, sizeof(double) * kBmMaxB * (size_t)a->nnorm);
   rc |= dalloc(&a->border, sizeof(int) * kBmMaxB);
@@ -997,14 +1001,13 @@ int small_eig(oapb_arnoldi* a, const cplx* G, int b, int kk, int nv, bool fp32 =
   h.beta = 0;
   ++a->stats.kernel_launches;
   if (near_tri && !fp32 && b <= 32 && a->ntflag) {
-    // the opt-in above 48 KB of dynamic shared memory (per device)
-    const int nw = nt_warps(b);
-    const size_t nsm = nt_smem_bytes(b, nw);
-    if (cudaFuncSetAttribute(k_eig_near_tri, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)nsm) != cudaSuccess)
-      return OAPB_ERR_CUDA;
-    ++a->stats.kernel_launches;
-    launch_dependent(k_eig_near_tri, dim3(1), dim3(nw * 32), nsm, a->stream, (const cplx*)G, b, (int)a->cfg.sort, a->britz,
-                     a->bY, a->border, a->ntflag);
+    // one CTA per pair (V, th in the unused bQ / bH scratch), then the
+    // acceptance and ordering; ntflag[0] = delivered, ntflag[1] = ok
+    a->stats.kernel_launches += 2;
+    launch_dependent(k_eig_near_tri, dim3(b), dim3(32), nt_smem_bytes(b), a->stream, (const cplx*)G, b, a->bQ,
+                     a->bH, a->ntflag + 1);
+    launch_dependent(k_eig_near_tri_finish, dim3(1), dim3(32), 0, a->stream, b, (int)a->cfg.sort,
+                     (const cplx*)a->bQ, (const cplx*)a->bH, a->ntflag + 1, a->britz, a->bY, a->border, a->ntflag);
     h.skip = a->ntflag;
   }
   if (fp32)
