@@ -510,6 +510,146 @@ static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane
   return true;
 }
 
+// Real symmetric tridiagonal path (the restart loop of a real symmetric
+// operator, whose Hessenberg matrix is symmetric tridiagonal to rounding):
+// d (m) and e (m - 1) real in shared memory; the implicit QR step with
+// shift mu on the window [l, h] (Golub & Van Loan, Matrix Computations,
+// Alg. 8.3.2) runs its rotation chain on lane 0 and records the rotations
+// (c, s) in cs; every lane then applies them to one row of Z (Z <- Z G^T).
+// The rotation of the pair (x, y) is c = x / r, s = y / r (the entries are
+// prescaled, so r^2 stays in range; a pair below tiny2 gives the identity).
+
+// true when T (prescaled: largest entry in [1, 2), m x m) is real and
+// symmetric to rtol: the Arnoldi matrix of a real symmetric operator, whose
+// entries beyond the tridiagonal band and whose asymmetry come from the
+// basis's loss of orthogonality (about 4e-13 of max |H| for an n = 256
+// operator with eigenvalues over three decades); they are dropped, which
+// moves the Ritz values by as much, so rtol is a tenth of the residual goal
+// (every result is verified against the operator)
+template <typename Cx>
+static __device__ bool warp_is_real_symmetric(const Cx* T, int m, int ld, double rtol, int lane) {
+  using R = decltype(Cx::re);
+  const R tol = (R)rtol;
+  int bad = 0;
+  for (int e = lane; e < m * m; e += 32) {
+    const int r = e % m, c = e / m;
+    const Cx a = TT_(r, c), b = TT_(c, r);
+    if (!(abs_t(a.im) <= tol && abs_t(a.re - b.re) <= tol)) bad = 1;
+  }
+  return !__any_sync(0xffffffffu, bad);
+}
+
+template <typename R>
+static __device__ void symtri_step(R* d, R* e, R* cs, int l, int h, R mu) {  // one lane
+  R x = d[l] - mu, y = e[l];
+  for (int k = l; k < h; ++k) {
+    const R r2 = x * x + y * y;
+    const bool ok = r2 > HessK<R>::tiny2;
+    const R ir = rsqrt_t(ok ? r2 : R(1));
+    const R c = ok ? x * ir : R(1), s = ok ? y * ir : R(0);
+    if (k > l) e[k - 1] = ok ? r2 * ir : x;
+    const R dk = d[k], dk1 = d[k + 1], ek = e[k];
+    const R t1 = c * dk + s * ek, t2 = c * ek + s * dk1;
+    const R t3 = c * ek - s * dk, t4 = c * dk1 - s * ek;
+    d[k] = c * t1 + s * t2;
+    e[k] = c * t2 - s * t1;
+    d[k + 1] = c * t4 - s * t3;
+    cs[2 * k] = c;
+    cs[2 * k + 1] = s;
+    if (k + 1 < h) {  // the bulge at (k + 2, k)
+      x = e[k];
+      y = s * e[k + 1];
+      e[k + 1] = c * e[k + 1];
+    }
+  }
+}
+
+// Z <- Z G_l^T ... G_{h-1}^T, one lane per row
+template <typename Cx>
+static __device__ void symtri_apply_z(Cx* Z, const decltype(Cx::re)* cs, int m, int ld, int l, int h, int lane) {
+  for (int i = lane; i < m; i += 32) {
+    Cx zc = ZZ_(i, l);
+    for (int k = l; k < h; ++k) {
+      const auto c = cs[2 * k], s = cs[2 * k + 1];
+      const Cx z1 = ZZ_(i, k + 1);
+      ZZ_(i, k) = Cx{c * zc.re + s * z1.re, c * zc.im + s * z1.im};
+      zc = Cx{c * z1.re - s * zc.re, c * z1.im - s * zc.im};
+    }
+    ZZ_(i, h) = zc;
+  }
+}
+
+// the largest l in [1, h] with e[l-1] negligible, else 0 (all lanes)
+template <typename R>
+static __device__ int symtri_split(const R* d, const R* e, int h, int lane) {
+  for (int base = h; base >= 1; base -= 32) {
+    const int l = base - lane;
+    const bool f = l >= 1 && abs_t(e[l - 1]) <= HessK<R>::eps * (abs_t(d[l - 1]) + abs_t(d[l]));
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (bal) return base - (__ffs(bal) - 1);
+  }
+  return 0;
+}
+
+// T (m x m) <-> d, e
+template <typename Cx>
+static __device__ void symtri_load(const Cx* T, int m, int ld, decltype(Cx::re)* d, decltype(Cx::re)* e, int lane) {
+  for (int i = lane; i < m; i += 32) {
+    d[i] = TT_(i, i).re;
+    if (i + 1 < m) e[i] = TT_(i + 1, i).re;
+  }
+  __syncwarp();
+}
+template <typename Cx>
+static __device__ void symtri_store(Cx* T, int m, int ld, const decltype(Cx::re)* d, const decltype(Cx::re)* e,
+                                    int lane) {
+  __syncwarp();
+  for (int x = lane; x < m * m; x += 32) {
+    const int r = x % m, c = x / m;
+    using R = decltype(Cx::re);
+    const R v = r == c ? d[r] : (r == c + 1 ? e[c] : (c == r + 1 ? e[r] : R(0)));
+    TT_(r, c) = Cx{v, 0};
+  }
+  __syncwarp();
+}
+
+// Eigen-decomposition of the symmetric tridiagonal (d, e): d becomes the
+// eigenvalues, Z accumulates the rotations; false when the sweep budget ran
+// out.
+template <typename Cx>
+static __device__ bool warp_symtri_eig(decltype(Cx::re)* d, decltype(Cx::re)* e, decltype(Cx::re)* cs, Cx* Z, int m,
+                                       int ld, int lane) {
+  using R = decltype(Cx::re);
+  int h = m - 1, its = 0, total = 0;
+  while (h > 0) {
+    const int l = symtri_split(d, e, h, lane);
+    __syncwarp();
+    if (l > 0 && lane == 0) e[l - 1] = 0;
+    __syncwarp();
+    if (l == h) {
+      --h;
+      its = 0;
+      continue;
+    }
+    if (++total > 30 * m) return false;
+    if (lane == 0) {
+      // Wilkinson shift: the eigenvalue of the trailing 2 x 2 nearer d[h];
+      // every tenth step of a window an exceptional shift d[h] + |e[h-1]|
+      const R a = d[h - 1], c = d[h], b = e[h - 1];
+      const R del = R(0.5) * (a - c);
+      const R den = del + (del >= 0 ? R(1) : R(-1)) * sqrt_t(del * del + b * b);
+      R mu = den != 0 ? c - b * b / den : c;
+      if (its > 0 && its % 10 == 0) mu = c + abs_t(b);
+      symtri_step(d, e, cs, l, h, mu);
+    }
+    __syncwarp();
+    symtri_apply_z(Z, cs, m, ld, l, h, lane);
+    __syncwarp();
+    ++its;
+  }
+  return true;
+}
+
 // Eigenvectors y_q = Z u_q (q < nvec) of the upper triangular T for the
 // diagonal entries ord[q]: u by back substitution, one lane per eigenvector
 // (columns of U in the scratch, stride min(32, nvec)), then Y = Z U one
@@ -702,8 +842,25 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   const int W = nvec < 32 ? nvec : 32;
   double scale = 0, small = 0;
   const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
+  // real symmetric Hessenberg input: the tridiagonal path (d, e in the
+  // eigenvector scratch, the rotations in rot)
+  R* sd = reinterpret_cast<R*>(U);
+  R* se = sd + m;
+  R* scs = reinterpret_cast<R*>(rot);
+  bool sym = false;
   if (warp == 0) {
-    const bool ok = warp_schur(T, Z, m, ld, rot, lane);
+    sym = !a.dense && a.tol > 0 && warp_is_real_symmetric(T, m, ld, 0.1 * a.tol, lane);
+    bool ok;
+    if (sym) {
+      symtri_load(T, m, ld, sd, se, lane);
+      ok = warp_symtri_eig(sd, se, scs, Z, m, ld, lane);
+      if (ok) {
+        for (int i = lane; i + 1 < m; i += 32) se[i] = 0;
+        symtri_store(T, m, ld, sd, se, lane);
+      }
+    } else {
+      ok = warp_schur(T, Z, m, ld, rot, lane);
+    }
     if (!ok && lane == 0) {
       st->status |= 2;
       st->converged = 0;
@@ -787,16 +944,38 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
     ZZ_(r, c) = (r == c) ? Cx{1, 0} : Cx{0, 0};
   }
   __syncwarp();
-  for (int q = k; q < m; ++q) {
-    Cx mu = u[q];
-    if (a.real_shifts) mu.im = 0;
-    int hb = m - 1;
-    while (hb > 0) {
-      const int l = find_split(T, ld, hb, lane);
-      if (l > 0 && lane == 0) TT_(l, l - 1) = Cx{0, 0};
-      __syncwarp();
-      if (l < hb) warp_sweep(T, Z, m, ld, l, hb, mu, rot, lane);
-      hb = l - 1;
+  if (sym) {  // the same exact shifts as implicit symmetric tridiagonal steps
+    symtri_load(T, m, ld, sd, se, lane);
+    for (int q = k; q < m; ++q) {
+      const R mu = u[q].re;
+      int hb = m - 1;
+      while (hb > 0) {
+        const int l = symtri_split(sd, se, hb, lane);
+        __syncwarp();
+        if (l > 0 && lane == 0) se[l - 1] = 0;
+        __syncwarp();
+        if (l < hb) {
+          if (lane == 0) symtri_step(sd, se, scs, l, hb, mu);
+          __syncwarp();
+          symtri_apply_z(Z, scs, m, ld, l, hb, lane);
+          __syncwarp();
+        }
+        hb = l - 1;
+      }
+    }
+    symtri_store(T, m, ld, sd, se, lane);
+  } else {
+    for (int q = k; q < m; ++q) {
+      Cx mu = u[q];
+      if (a.real_shifts) mu.im = 0;
+      int hb = m - 1;
+      while (hb > 0) {
+        const int l = find_split(T, ld, hb, lane);
+        if (l > 0 && lane == 0) TT_(l, l - 1) = Cx{0, 0};
+        __syncwarp();
+        if (l < hb) warp_sweep(T, Z, m, ld, l, hb, mu, rot, lane);
+        hb = l - 1;
+      }
     }
   }
   __syncwarp();
