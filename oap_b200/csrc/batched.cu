@@ -143,18 +143,26 @@ __device__ __forceinline__ cplx cta_sum2(double a, double b, double* red) {
 }
 
 // w = A x  (A row-major n x n; warps over rows, lanes over columns)
+// w = A x for one problem (A row-major split planes in global memory, x in
+// shared memory): warp w takes kMvRows rows at a time, the lanes stride the
+// columns; the loads of all its rows are issued together (the operator
+// streams from HBM, so the bytes a CTA keeps in flight set its rate), each
+// row summed per lane in column order and then across the warp.
+constexpr int kMvRows = 4;
 template <bool C, int NT>
 __device__ void cta_matvec(const double* __restrict__ Are, const double* __restrict__ Aim, int n, const double* xr,
                            const double* xi, double* wr, double* wi) {
   const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  for (int r0 = 2 * w; r0 < n; r0 += 2 * (NT / 32)) {
-    double sr[2] = {0, 0}, si[2] = {0, 0};
-    const int nr = (r0 + 1 < n) ? 2 : 1;
+  for (int r0 = kMvRows * w; r0 < n; r0 += kMvRows * (NT / 32)) {
+    double sr[kMvRows], si[kMvRows];
+#pragma unroll
+    for (int q = 0; q < kMvRows; ++q) sr[q] = si[q] = 0.0;
+    const int nr = (n - r0) < kMvRows ? (n - r0) : kMvRows;
 #pragma unroll 4
     for (int c = l; c < n; c += 32) {
       const double x0 = xr[c], x1 = C ? xi[c] : 0.0;
 #pragma unroll
-      for (int q = 0; q < 2; ++q) {
+      for (int q = 0; q < kMvRows; ++q) {
         if (q < nr) {
           const long idx = (long)(r0 + q) * n + c;
           const double a = __ldcs(Are + idx);
@@ -169,7 +177,7 @@ __device__ void cta_matvec(const double* __restrict__ Are, const double* __restr
       }
     }
 #pragma unroll
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kMvRows; ++q) {
       const double a = warp_sum(sr[q]);
       const double b = C ? warp_sum(si[q]) : 0.0;
       if (l == 0 && q < nr) {
