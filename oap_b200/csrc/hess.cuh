@@ -1,4 +1,5 @@
-// Small dense kernels of the restart loop, one warp, FP64 complex.
+// Small dense kernels of the restart loop and of the block methods' checks,
+// FP64 complex (FP32 working arithmetic in k_hess_f32).
 //
 // k_hess works on the m x m upper Hessenberg H of the Arnoldi factorization
 // (column-major, m <= kMaxM):
@@ -6,7 +7,9 @@
 //      bulge chasing, Wilkinson shifts, deflation at
 //      |T[i][i-1]| <= eps (|T[i-1][i-1]| + |T[i][i]|)), the restatement of
 //      calculateTriangularHEigens (ArnoldiProcedures.cpp:341-349) with a
-//      shifted, deflating iteration instead of the reference's unshifted one;
+//      shifted, deflating iteration instead of the reference's unshifted
+//      one; for a real symmetric H (a real symmetric operator) the implicit
+//      symmetric tridiagonal QR instead;
 //   2. Ritz values = diag(T), sorted by the ArnUtils order
 //      (ArnoldiUtils.cpp:24-50); wanted = first k (getWanted,
 //      ArnoldiProcedures.cpp:381-398);
@@ -16,16 +19,21 @@
 //      (iram_shiftedQRIterations, oapGenericArnoldiApi.h:186-222) on H,
 //      Q accumulating the rotations, H compressed to its leading k x k block.
 // With `dense` set the input is a general matrix, first reduced to
-// Hessenberg form by Householder reflectors accumulated into Z.
+// Hessenberg form by Householder reflectors accumulated into Z.  The input
+// is scaled by a power of two (exact) so that the rotations need no
+// overflow branches.
 //
-// Work layout (one warp): T and Z are column-major with an odd leading
-// dimension hess_ld(m), so a lane-per-column access (row rotations) and a
+// Work layout: T and Z are column-major with an odd leading dimension
+// hess_ld(m), so a lane-per-column access (row rotations) and a
 // lane-per-row access (column rotations) are both free of bank conflicts.
 // A QR sweep runs its chain of rotations in registers (the 2 x 2 window and
 // the bulge, one shuffle per rotation) while the lanes apply each row
 // rotation to their columns; the column rotations of the sweep, and those on
-// Z, are applied after the chain (each lane the whole sequence to its rows).  The eigenvector back substitutions run one lane
-// per eigenvector (T read by broadcast).
+// Z, are applied after the chain (each lane the whole sequence to its
+// rows).  The eigenvector back substitutions run one lane per eigenvector
+// (T read by broadcast).  The sweeps run on one warp; for m <= 32 the kernel
+// has four warps, which share the Householder reduction and the product
+// Y = Z U.
 //
 // Every loop is bounded (30 m sweeps for the Schur form); hitting the bound
 // sets bit 1 of DevState::status and the kernel returns.
