@@ -1056,9 +1056,10 @@ static __global__ void __launch_bounds__(32 * kHessWarps) k_hess_f32(HessArgs a)
 // ok[0] is set again for the next call (it must hold 1 before the first).
 constexpr int kNtIters = 4;
 __host__ __device__ inline int nt_ld(int m) { return m + 1; }
-// dynamic shared memory of k_eig_near_tri: T, M (m x LD), x, t (m), pivots
+// dynamic shared memory of k_eig_near_tri: T, M (m x LD), x, t, the pivots'
+// reciprocals (m each), pivot rows
 __host__ __device__ inline size_t nt_smem_bytes(int m) {
-  return sizeof(cplx) * (2 * (size_t)m * nt_ld(m) + 2 * (size_t)m) + sizeof(int) * (size_t)m;
+  return sizeof(cplx) * (2 * (size_t)m * nt_ld(m) + 3 * (size_t)m) + sizeof(int) * (size_t)m;
 }
 
 static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restrict__ Tin, int m, cplx* V, cplx* th,
@@ -1070,7 +1071,8 @@ static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restri
   cplx* M = T + (size_t)m * LD;               // m x LD
   cplx* x = M + (size_t)m * LD;               // m
   cplx* t = x + m;                            // m
-  int* pv = reinterpret_cast<int*>(t + m);    // m
+  cplx* dinv = t + m;                         // m: reciprocals of U's diagonal
+  int* pv = reinterpret_cast<int*>(dinv + m); // m
   const int lane = threadIdx.x, q = blockIdx.x;
   if (m < 1 || m > 32 || q >= m) return;
   for (int e = lane; e < m * m; e += 32) T[(e % m) + (e / m) * LD] = Tin[e];
@@ -1120,9 +1122,20 @@ static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restri
           M[bi + c * LD] = tmp;
         }
         __syncwarp();
-        if (lane == 0 && cabs_(M[k + k * LD]) < tiny) M[k + k * LD] = cplx{tiny, 0};
+        // the pivot (a zero one replaced by tiny) and its reciprocal
+        // conj(p) / |p|^2, kept for the back substitution
+        cplx pk = M[k + k * LD];
+        double p2 = abs2(pk);
+        if (!(p2 >= tiny * tiny)) {
+          pk = cplx{tiny, 0};
+          p2 = tiny * tiny;
+        }
+        const cplx inv = (1.0 / p2) * conj(pk);
         __syncwarp();
-        const cplx inv = cdiv(cplx{1, 0}, M[k + k * LD]);
+        if (lane == 0) {
+          M[k + k * LD] = pk;
+          dinv[k] = inv;
+        }
         for (int i = k + 1 + lane; i < m; i += 32) M[i + k * LD] = M[i + k * LD] * inv;  // multipliers
         __syncwarp();
         for (int c = k + 1 + lane; c < m; c += 32) {
@@ -1131,45 +1144,31 @@ static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restri
         }
         __syncwarp();
       }
-      // x <- (T - sigma I)^-1 x, normalised
-      if (lane == 0) {
-        for (int k = 0; k < m; ++k) {  // P b
-          const int r = pv[k];
-          const cplx tmp = x[k];
-          x[k] = x[r];
-          x[r] = tmp;
-        }
+      // x <- (T - sigma I)^-1 x, normalised: lane i holds x_i; the row
+      // swaps, then L y = P b and U x = y column by column (one shuffle of
+      // the finished entry per column)
+      cplx xv = lane < m ? x[lane] : cplx{0, 0};
+      for (int k = 0; k < m; ++k) {
+        const int r = pv[k];
+        const cplx xk = shfl_c(xv, k), xr = shfl_c(xv, r);
+        if (lane == k) xv = xr;
+        else if (lane == r) xv = xk;
       }
-      __syncwarp();
-      for (int i = 1; i < m; ++i) {  // L y = P b (unit lower)
-        cplx acc = {0, 0};
-        for (int j = lane; j < i; j += 32) acc = acc + M[i + j * LD] * x[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
-          acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
-        }
-        if (lane == 0) x[i] = x[i] - acc;
-        __syncwarp();
+      for (int j = 0; j + 1 < m; ++j) {
+        const cplx xj = shfl_c(xv, j);
+        if (lane > j && lane < m) xv = xv - M[lane + j * LD] * xj;
       }
-      for (int i = m - 1; i >= 0; --i) {  // U x = y
-        cplx acc = {0, 0};
-        for (int j = i + 1 + lane; j < m; j += 32) acc = acc + M[i + j * LD] * x[j];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
-          acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
-        }
-        if (lane == 0) x[i] = cdiv(x[i] - acc, M[i + i * LD]);
-        __syncwarp();
+      for (int i = m - 1; i >= 0; --i) {
+        if (lane == i) xv = xv * dinv[i];
+        const cplx xi = shfl_c(xv, i);
+        if (lane < i) xv = xv - M[lane + i * LD] * xi;
       }
-      double nrm = 0;
-      for (int i = lane; i < m; i += 32) nrm += abs2(x[i]);
+      double nrm = abs2(xv);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) nrm += __shfl_xor_sync(0xffffffffu, nrm, o);
       nrm = sqrt(nrm);
       const double sc = nrm > 0 ? 1.0 / nrm : 0.0;
-      for (int i = lane; i < m; i += 32) x[i] = sc * x[i];
+      if (lane < m) x[lane] = sc * xv;
       __syncwarp();
       // Rayleigh quotient (the next shift) and residual ||T x - theta x||
       for (int i = lane; i < m; i += 32) {
