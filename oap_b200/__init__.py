@@ -66,7 +66,8 @@ class Stats(C.Structure):
                 ("matvec_variant", C.c_uint32), ("block_bf16", C.c_uint32),
                 ("block_bf16_timed", C.c_uint32), ("block_bf16_seconds", C.c_double),
                 ("eig_fast", C.c_uint32), ("block_i8", C.c_uint32), ("onchip", C.c_uint32),
-                ("pass_kernel_seconds", C.c_double * 3), ("pass_kernel_timed", C.c_uint32 * 3)]
+                ("pass_kernel_seconds", C.c_double * 3), ("pass_kernel_timed", C.c_uint32 * 3),
+                ("symtri", C.c_uint32)]
 
 
 class BatchProblem(C.Structure):

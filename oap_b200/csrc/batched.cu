@@ -262,6 +262,7 @@ __device__ void solve_one(const BatchArgs& A, const BatchDesc& P, int slot, cons
   if (tid == 0) {
     S.st->status = 0;
     S.st->converged = 0;
+    S.st->symtri = 0;
   }
   __syncthreads();
   int start = 0;

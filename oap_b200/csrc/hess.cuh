@@ -58,6 +58,7 @@ struct DevState {
   double maxest;    // max relative Ritz estimate of the wanted set
   cplx beta_hat;    // H[k][k-1] after the shifts
   cplx sigma;       // Q[m-1][k-1]
+  int symtri;       // eigensolves that took the real symmetric tridiagonal path
 };
 
 struct HessArgs {
@@ -858,6 +859,7 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   bool sym = false;
   if (warp == 0) {
     sym = !a.dense && a.tol > 0 && warp_is_real_symmetric(T, m, ld, 0.1 * a.tol, lane);
+    if (sym && lane == 0) st->symtri += 1;
     bool ok;
     if (sym) {
       symtri_load(T, m, ld, sd, se, lane);

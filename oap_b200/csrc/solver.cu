@@ -742,6 +742,7 @@ int iram(oapb_arnoldi* a, bool fp32, double tol, unsigned max_restarts, int star
     if (hs.status & 1) return OAPB_ERR_BREAKDOWN;
     if (hs.status & 2) return OAPB_ERR_TIMEOUT;
     a->stats.dgks_passes = hs.dgks_count;
+    a->stats.symtri = (uint32_t)hs.symtri;
     if (hs.converged) return OAPB_OK;
     if (!do_shift) return OAPB_NOT_CONVERGED;
     if ((rc = restart<C>(a))) return rc;
