@@ -30,7 +30,7 @@ namespace oapb {
 constexpr int kGxThreads = 256;
 constexpr int kGxCols = kGxThreads * 4;  // pixels per block
 
-__global__ void __launch_bounds__(kGxThreads) k_gram_xt(const float* __restrict__ X, int rows, int cols, long ldx,
+__global__ void __launch_bounds__(kGxThreads) k_gram_xt(const float* __restrict__ X, int rows, int cols,
                                                        const double* __restrict__ v, int rows_per_split,
                                                        double* __restrict__ part) {
   const long c = ((long)blockIdx.x * kGxThreads + threadIdx.x) * 4;
@@ -38,9 +38,9 @@ __global__ void __launch_bounds__(kGxThreads) k_gram_xt(const float* __restrict_
   const int r1 = min(rows, r0 + rows_per_split);
   double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
   if (c < cols) {
-    if ((cols & 3) == 0 && (ldx & 3) == 0) {
+    if ((cols & 3) == 0) {
       for (int r = r0; r < r1; ++r) {
-        const float4 x = __ldcg(reinterpret_cast<const float4*>(X + (long)r * ldx + c));
+        const float4 x = __ldcs(reinterpret_cast<const float4*>(X + (long)r * cols + c));
         const double vr = v[r];
         a0 = fma((double)x.x, vr, a0);
         a1 = fma((double)x.y, vr, a1);
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(kGxThreads) k_gram_xt(const float* __restrict_
       }
     } else {
       for (int r = r0; r < r1; ++r) {
-        const float* xr = X + (long)r * ldx;
+        const float* xr = X + (long)r * cols;
         const double vr = v[r];
         a0 = fma((double)xr[c], vr, a0);
         if (c + 1 < cols) a1 = fma((double)xr[c + 1], vr, a1);
@@ -74,15 +74,15 @@ __global__ void k_gram_reduce(const double* __restrict__ part, int nsplit, int c
   }
 }
 
-__global__ void __launch_bounds__(256) k_gram_x(const float* __restrict__ X, int rows, int cols, long ldx,
+__global__ void __launch_bounds__(256) k_gram_x(const float* __restrict__ X, int rows, int cols,
                                                const double* __restrict__ t, double* __restrict__ w,
                                                int accumulate) {
   const int lane = threadIdx.x & 31;
   const long warps = (long)gridDim.x * (blockDim.x >> 5);
   for (long r = (long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < rows; r += warps) {
-    const float* xr = X + r * ldx;
+    const float* xr = X + r * cols;
     double a0 = 0, a1 = 0;
-    if ((cols & 3) == 0 && (ldx & 3) == 0) {
+    if ((cols & 3) == 0) {
       for (int q = lane; q < cols / 4; q += 32) {
         const float4 x = __ldcs(reinterpret_cast<const float4*>(xr) + q);
         const double2 t0 = *reinterpret_cast<const double2*>(t + 4 * q);
@@ -111,38 +111,16 @@ int gram_op_splits(int rows, int cols) {
 size_t gram_op_workspace(int rows, int cols) { return ((size_t)gram_op_splits(rows, cols) + 1) * cols; }
 
 int launch_gram_apply(const float* X, int rows, int cols, const double* v, double* w, double* ws, cudaStream_t s,
-                      bool accumulate, long ldx) {
-  if (ldx <= 0) ldx = cols;
-  if (!X || !v || !w || !ws || rows < 1 || cols < 1 || ldx < cols) return OAPB_ERR_ARG;
-  if ((cols & 3) == 0 && (ldx & 3) == 0 && ((uintptr_t)X & 15)) return OAPB_ERR_ARG;
+                      bool accumulate) {
+  if (!X || !v || !w || !ws || rows < 1 || cols < 1) return OAPB_ERR_ARG;
+  if ((cols & 3) == 0 && ((uintptr_t)X & 15)) return OAPB_ERR_ARG;
   const int ns = gram_op_splits(rows, cols);
   const int rps = (rows + ns - 1) / ns;
   double* t = ws + (size_t)ns * cols;
-  k_gram_xt<<<dim3((cols + kGxCols - 1) / kGxCols, ns), kGxThreads, 0, s>>>(X, rows, cols, ldx, v, rps, ws);
+  k_gram_xt<<<dim3((cols + kGxCols - 1) / kGxCols, ns), kGxThreads, 0, s>>>(X, rows, cols, v, rps, ws);
   k_gram_reduce<<<grid_for(cols, 256, kNumSMs * 4), 256, 0, s>>>(ws, ns, cols, t);
-  k_gram_x<<<grid_for((long)rows * 32, 256, kNumSMs * 8), 256, 0, s>>>(X, rows, cols, ldx, t, w,
-                                                                       accumulate ? 1 : 0);
+  k_gram_x<<<grid_for((long)rows * 32, 256, kNumSMs * 8), 256, 0, s>>>(X, rows, cols, t, w, accumulate ? 1 : 0);
   return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
-}
-
-int gram_l2_block_cols(int rows, int cols) {
-  // pixels per block whose rows x block FP32 fit kGramL2Block bytes (a
-  // multiple of 4 for the 16-byte loads)
-  long bc = (long)(kGramL2Block / (sizeof(float) * (size_t)(rows > 0 ? rows : 1))) / 4 * 4;
-  if (bc < 4) bc = 4;
-  return bc >= cols ? cols : (int)bc;
-}
-
-int launch_gram_apply_blocked(const float* X, int rows, int cols, const double* v, double* w, double* ws,
-                              cudaStream_t s) {
-  const int bc = gram_l2_block_cols(rows, cols);
-  if (bc >= cols || (cols & 3) || ((uintptr_t)X & 15)) return launch_gram_apply(X, rows, cols, v, w, ws, s);
-  for (int c0 = 0; c0 < cols; c0 += bc) {
-    const int wdt = cols - c0 < bc ? cols - c0 : bc;
-    const int rc = launch_gram_apply(X + c0, rows, wdt, v, w, ws, s, c0 > 0, cols);
-    if (rc) return rc;
-  }
-  return OAPB_OK;
 }
 
 // ------------------------------------------------------------ host X --

@@ -3,7 +3,6 @@
 #pragma once
 
 #include <cuda_runtime.h>
-#include <stddef.h>
 
 namespace oapb {
 
@@ -12,19 +11,9 @@ int gram_op_splits(int rows, int cols);
 size_t gram_op_workspace(int rows, int cols);
 
 // w = X (X^T v) (accumulate: w += X (X^T v)); v, w: rows FP64 values; ws:
-// gram_op_workspace() doubles; ldx: the row stride of X in floats (0: cols)
+// gram_op_workspace() doubles
 int launch_gram_apply(const float* X, int rows, int cols, const double* v, double* w, double* ws, cudaStream_t s,
-                      bool accumulate = false, long ldx = 0);
-
-// Device-resident X larger than about half of L2: the same product by column
-// blocks of gram_l2_block_cols(rows, cols) pixels, w = sum_c X_c (X_c^T v),
-// so that the second pass over a block (X_c t_c) reads it from L2 and an
-// application reads X from HBM about once; ws: gram_op_workspace(rows,
-// gram_l2_block_cols(rows, cols)) doubles
-constexpr size_t kGramL2Block = 48ull << 20;
-int gram_l2_block_cols(int rows, int cols);
-int launch_gram_apply_blocked(const float* X, int rows, int cols, const double* v, double* w, double* ws,
-                              cudaStream_t s);
+                      bool accumulate = false);
 
 // X in host memory, applied by column blocks of block_cols pixels: the
 // blocks that fit resident_bytes are copied to the device once, the others

@@ -607,9 +607,8 @@ int apply_op(oapb_arnoldi* a, const double* xre, const double* xim, double* yre,
     return rc == 0 ? OAPB_OK : OAPB_ERR_CALLBACK;
   }
   if (a->gX) {
-    const int bc = gram_l2_block_cols(n, a->gcols);
-    a->stats.kernel_launches += 3 * (uint64_t)((a->gcols + bc - 1) / bc);
-    return launch_gram_apply_blocked(a->gX, n, a->gcols, xre, yre, a->gws, s);
+    a->stats.kernel_launches += 3;
+    return launch_gram_apply(a->gX, n, a->gcols, xre, yre, a->gws, s);
   }
   if (a->gS) {
     a->stats.kernel_launches += 3 * (uint64_t)gram_stream_blocks(a->gS);
@@ -2049,12 +2048,7 @@ int oapb_arnoldi_set_gram_operator(oapb_arnoldi* a, const float* X, uint32_t row
     cudaFree(a->gws);
     a->gws = nullptr;
   }
-  if (!a->gws) {
-    // the whole-X passes or the L2-sized column blocks, whichever needs more
-    const size_t w0 = gram_op_workspace(a->n, (int)cols),
-                 w1 = gram_op_workspace(a->n, gram_l2_block_cols(a->n, (int)cols));
-    if (dalloc(&a->gws, sizeof(double) * (w0 > w1 ? w0 : w1))) return OAPB_ERR_NOMEM;
-  }
+  if (!a->gws && dalloc(&a->gws, sizeof(double) * gram_op_workspace(a->n, (int)cols))) return OAPB_ERR_NOMEM;
   a->gX = X;
   a->gcols = (int)cols;
   a->cb = nullptr;

@@ -85,11 +85,10 @@ def oracle_gram_eigenvalues(X, k, m):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("rows,cols", [(600, 3000), (513, 1027), (1024, 16384)])
+@pytest.mark.parametrize("rows,cols", [(600, 3000), (513, 1027)])
 def test_implicit_gram_operator_matches_oracle(rows, cols):
     # w = X (X^T v) never forming A: the eigenpairs of the exact Gram of the
-    # FP32 images, against the CPU oracle's FP64 IRAM on that Gram (1024 x
-    # 16384: 64 MB of X, applied by two L2-sized column blocks)
+    # FP32 images, against the CPU oracle's FP64 IRAM on that Gram
     X = separated_images(rows, cols, rows)
     imp = B.Arnoldi(rows, 24, 6, seed=3)
     imp.set_gram_operator(X)
