@@ -442,97 +442,6 @@ static size_t btc_stage_bytes(int N, bool cplx, bool lo, bool xlo) {
   return ((size_t)(NA * kBtcM * 128 + (xlo ? 2 : 1) * KH * N * 128) + 1023) & ~(size_t)1023;
 }
 
-// A refinement sweep's step after its pass, in one kernel: the stream-K
-// partials of W = A X summed per row (in CTA order, as k_sk_reduce does),
-// D = (W + R) Tinv (Tinv b x b column-major, summed over j in order, as
-// k_block_update does) written as FP64 planes, and D's BF16 hi / lo rows
-// (q for re, QB + q for im, zero rows and K columns beyond b / n) as the
-// next pass's B operand, as k_split_block_bf16 writes them.  One block per
-// 128-row tile (tiles x 128 = kp), one thread per row; b <= kFuseB.
-template <bool CPLX>
-__global__ void __launch_bounds__(kSkRows) k_sk_reduce_update(const double* __restrict__ ws, SkGrid p, int n, int b,
-                                                              int QB, int N, int kp, const double* __restrict__ Rr,
-                                                              const double* __restrict__ Ri,
-                                                              const cplx* __restrict__ Tinv, double* Dr, double* Di,
-                                                              __nv_bfloat16* hi, __nv_bfloat16* lo) {
-  __shared__ cplx ts[kFuseB * kFuseB];
-  tc::griddep_wait();  // the pass wrote the partials
-  for (int e = threadIdx.x; e < b * b; e += kSkRows) ts[e] = Tinv[e];
-  __syncthreads();
-  const long tile = blockIdx.x;
-  const long row = tile * kSkRows + threadIdx.x;
-  const __nv_bfloat16 z = __float2bfloat16_rn(0.f);
-  if (row >= kp) return;
-  if (row >= n) {  // a padding column of K: zero in every B row
-    for (int q = 0; q < N; ++q) {
-      hi[(long)q * kp + row] = z;
-      lo[(long)q * kp + row] = z;
-    }
-    return;
-  }
-  constexpr int NP = CPLX ? 2 : 1;
-  const int npq = NP * b;
-  const long ilo = tile * p.kchunks;
-  const long ihi = min(p.total, ilo + p.kchunks) - 1;
-  const long c0 = sk_owner(ilo, p.total, p.grid), c1 = sk_owner(ihi, p.total, p.grid);
-  double xr[kFuseB], xi[kFuseB];
-#pragma unroll
-  for (int q = 0; q < kFuseB; ++q) xr[q] = xi[q] = 0.0;
-  for (long c = c0; c <= c1; ++c) {
-    const long slot = tile - sk_begin(c, p.total, p.grid) / p.kchunks;
-    const double* src = ws + ((size_t)c * p.slots + slot) * npq * kSkRows + threadIdx.x;
-#pragma unroll
-    for (int q = 0; q < kFuseB; ++q)
-      if (q < b) {
-        xr[q] += src[(size_t)q * kSkRows];
-        if (CPLX) xi[q] += src[(size_t)(b + q) * kSkRows];
-      }
-  }
-#pragma unroll
-  for (int q = 0; q < kFuseB; ++q)
-    if (q < b) {
-      xr[q] = xr[q] + Rr[(long)q * n + row];
-      if (CPLX) xi[q] = xi[q] + Ri[(long)q * n + row];
-    }
-  for (int q = 0; q < b; ++q) {
-    cplx acc = {0, 0};
-#pragma unroll
-    for (int j = 0; j < kFuseB; ++j)
-      if (j < b) acc = acc + cplx{xr[j], CPLX ? xi[j] : 0.0} * ts[j + q * b];
-    Dr[(long)q * n + row] = acc.re;
-    if (CPLX) Di[(long)q * n + row] = acc.im;
-    const float vr = (float)acc.re;
-    const __nv_bfloat16 hr = __float2bfloat16_rn(vr);
-    hi[(long)q * kp + row] = hr;
-    lo[(long)q * kp + row] = __float2bfloat16_rn(vr - __bfloat162float(hr));
-    if (CPLX) {
-      const float vi = (float)acc.im;
-      const __nv_bfloat16 h2 = __float2bfloat16_rn(vi);
-      hi[(long)(QB + q) * kp + row] = h2;
-      lo[(long)(QB + q) * kp + row] = __float2bfloat16_rn(vi - __bfloat162float(h2));
-    }
-  }
-  for (int q = b; q < N; ++q) {
-    if (CPLX && q >= QB && q < QB + b) continue;
-    hi[(long)q * kp + row] = z;
-    lo[(long)q * kp + row] = z;
-  }
-}
-
-int launch_sk_reduce_update(const double* ws, const SkGrid& p, int n, int kp, int b, bool is_c, const double* Rr,
-                            const double* Ri, const cplx* Tinv, double* Dr, double* Di, __nv_bfloat16* xbh,
-                            __nv_bfloat16* xbl, cudaStream_t s) {
-  if (b < 1 || b > kFuseB || p.tiles * kSkRows != kp || (is_c && (!Ri || !Di))) return OAPB_ERR_ARG;
-  const int QB = (b + 7) / 8 * 8;
-  int N = is_c ? 2 * QB : QB;
-  if (N % 16) N += 8;
-  cudaError_t e = is_c ? launch_dependent(k_sk_reduce_update<true>, dim3((unsigned)p.tiles), dim3(kSkRows), 0, s, ws,
-                                          p, n, b, QB, N, kp, Rr, Ri, Tinv, Dr, Di, xbh, xbl)
-                       : launch_dependent(k_sk_reduce_update<false>, dim3((unsigned)p.tiles), dim3(kSkRows), 0, s, ws,
-                                          p, n, b, QB, N, kp, Rr, Ri, Tinv, Dr, Di, xbh, xbl);
-  return e == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
-}
-
 int split_operator_bf16(const double* a, int n, int kp, __nv_bfloat16* hi, __nv_bfloat16* lo, cudaStream_t s,
                         long row0, long rows, double* err2) {
   if (rows < 0) rows = n - row0;
@@ -559,8 +468,7 @@ size_t btc_workspace(int n, int kp) {
 
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
-                           cudaStream_t s, bool bf16_only, bool x_hi_only, int ctas, const cudaEvent_t* kev,
-                           bool b_ready, SkGrid* defer) {
+                           cudaStream_t s, bool bf16_only, bool x_hi_only, int ctas, const cudaEvent_t* kev) {
   const bool cplx = op.aih != nullptr;
   const int kh = bf16_only ? 2 : 1;
   if (b < 1 || b > 32 || op.kp % (kBtcK * kh) != 0 || (cplx && (!xi || !wi))) return OAPB_ERR_ARG;
@@ -568,8 +476,8 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   const int QB = (b + 7) / 8 * 8;
   int N = cplx ? 2 * QB : QB;
   if (N % 16) N += 8;  // M = 128 needs N % 16 == 0
-  if (!b_ready && launch_dependent(k_split_block_bf16, dim3((op.kp + 1023) / 1024, N), dim3(256), 0, s, xr,
-                                   cplx ? xi : nullptr, b, QB, N, op.n, op.kp, xbh, xbl) != cudaSuccess)
+  if (launch_dependent(k_split_block_bf16, dim3((op.kp + 1023) / 1024, N), dim3(256), 0, s, xr, cplx ? xi : nullptr, b,
+                       QB, N, op.n, op.kp, xbh, xbl) != cudaSuccess)
     return OAPB_ERR_CUDA;
   BtcArgs g;
   const __nv_bfloat16* planes[4] = {op.arh, op.arl, cplx ? op.aih : op.arh, cplx ? op.ail : op.arl};
@@ -598,10 +506,6 @@ int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double
   if (kev) cudaEventRecord(kev[0], s);
   if (launch_dependent(kern, dim3(g.grid.grid), dim3(kBtcThreads), smem, s, g) != cudaSuccess) return OAPB_ERR_CUDA;
   if (kev) cudaEventRecord(kev[1], s);
-  if (defer) {  // the caller reduces the partials (k_sk_reduce_update)
-    *defer = g.grid;
-    return cudaGetLastError() == cudaSuccess ? OAPB_OK : OAPB_ERR_CUDA;
-  }
   if (cplx)
     launch_sk_reduce<true>(ws, g.grid, op.n, b, wr, wi, s);
   else

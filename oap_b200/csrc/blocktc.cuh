@@ -6,7 +6,6 @@
 #include <stddef.h>
 
 #include "common.cuh"
-#include "streamk.cuh"
 
 namespace oapb {
 
@@ -35,20 +34,9 @@ size_t btc_workspace(int n, int kp);
 // stream; every CTA holds most of its SM's shared memory).  kev (optional,
 // two events): recorded right before and after the pass kernel alone
 // (profiling; breaks the dependent-launch overlap with the kernels around it).
-// b_ready: xbh / xbl already hold X's split (k_sk_reduce_update wrote it);
-// defer: the stream-K reduction is left to the caller, which receives the
-// grid (W is then not written).
 int launch_block_matvec_tc(const BtcOperator& op, const double* xr, const double* xi, int b, double* wr,
                            double* wi, __nv_bfloat16* xbh, __nv_bfloat16* xbl, double* ws, int* err,
                            cudaStream_t s, bool bf16_only = false, bool x_hi_only = false, int ctas = kNumSMs,
-                           const cudaEvent_t* kev = nullptr, bool b_ready = false, SkGrid* defer = nullptr);
-
-// After a pass launched with `defer`: D = (W + R) Tinv from the pass's
-// partials (W never written), D as FP64 planes and as the next pass's B
-// operand in xbh / xbl (b <= 16; kp = the operator's padded columns).
-constexpr int kFuseB = 16;
-int launch_sk_reduce_update(const double* ws, const SkGrid& p, int n, int kp, int b, bool is_c, const double* Rr,
-                            const double* Ri, const cplx* Tinv, double* Dr, double* Di, __nv_bfloat16* xbh,
-                            __nv_bfloat16* xbl, cudaStream_t s);
+                           const cudaEvent_t* kev = nullptr);
 
 }  // namespace oapb

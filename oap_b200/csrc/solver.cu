@@ -860,13 +860,9 @@ static bool side_sm_reserve() {
   return v != 0;
 }
 
-// b_ready / defer (tensor-core FP32-class passes only, fused_sweep_ok()):
-// X's B-operand split is already in a->xbf / the stream-K reduction is left
-// to the caller (launch_sk_reduce_update), W is then not written.
 template <bool C>
 int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, double* wr, double* wi,
-                bool fp32 = false, bool bf16 = false, bool coarse = false, bool b_ready = false,
-                SkGrid* defer = nullptr) {
+                bool fp32 = false, bool bf16 = false, bool coarse = false) {
   if (a->cb || a->gX || a->gS) {
     for (int q = 0; q < b; ++q) {
       int rc = apply_op(a, xr + (long)q * a->n, C ? xi + (long)q * a->n : nullptr, wr + (long)q * a->n,
@@ -883,7 +879,6 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     const int rc = ensure_fp32_copy(a);
     if (rc) return rc;
   }
-  if ((b_ready || defer) && !tcp) return OAPB_ERR_ARG;  // only the tensor-core FP32-class pass defers
   Timed tm{nullptr, nullptr, 1, fp32 ? (tcp && bf16 ? 2 : 1) : 0, b};
   const bool prof = prof_begin(a, tm);
   if (tcp) {
@@ -892,7 +887,7 @@ int block_apply(oapb_arnoldi* a, const double* xr, const double* xi, int b, doub
     const int ctas = (a->side_busy && side_sm_reserve()) ? kNumSMs - 1 : kNumSMs;
     const cudaEvent_t* kev = prof ? prof_kernel_pair(a, bf16 ? 2 : 1) : nullptr;
     int rc = launch_block_matvec_tc(op, xr, xi, b, wr, wi, a->xbf, a->xbf + 64 * (size_t)a->kp, a->wdm,
-                                    a->tcerr, a->stream, bf16, bf16 && coarse, ctas, kev, b_ready, defer);
+                                    a->tcerr, a->stream, bf16, bf16 && coarse, ctas, kev);
     if (bf16) a->stats.block_bf16++;
     if (prof) prof_end(a, tm);
     if (rc) return rc;
@@ -1439,27 +1434,12 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
     const double spread = tmin > 0 ? tmax / tmin : 1e300;
     int every = spread > 1.0 + 1e-12 ? (int)floor(log(4.0) / log(spread)) : J;
     if (every < 1) every = 1;
-    // a sweep without a projection ends in one kernel: the pass's stream-K
-    // partials, D = (W + R) T^-1 and D's split for the next pass
-    const bool fuse = a->have_tc && a->cfg.tensor_cores && p <= kFuseB;
-    bool dsplit = false;  // a->xbf holds D's split
     for (int j = 0; j < J; ++j) {
-      const bool proj = (j + 1) % every == 0 || j + 1 == J;
-      SkGrid sg{};
       // BF16 sweeps before the last one also round D to BF16 (coarse): an
       // error a sweep leaves is damped by every later sweep, so only the last
       // BF16 sweep's, contracted by the Jf that follow, reaches the result
-      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true, j < Jb, j + 1 < Jb, dsplit, fuse && !proj ? &sg : nullptr)))
-        return rc;
-      if (fuse && !proj) {  // D = (P A D + R) T^-1, P A D = A D here
-        a->stats.kernel_launches++;
-        if ((rc = launch_sk_reduce_update(a->wdm, sg, n, a->kp, p, C, R, Ri, a->Tinv, D, Di, a->xbf,
-                                          a->xbf + 64 * (size_t)a->kp, a->stream)))
-          return rc;
-        dsplit = true;
-        continue;
-      }
-      if (proj) {
+      if ((rc = block_apply<C>(a, D, Di, p, W, Wi, true, j < Jb, j + 1 < Jb))) return rc;
+      if ((j + 1) % every == 0 || j + 1 == J) {
         block_gram<C>(a, X, Xi, p, W, Wi, p, a->G2);
         a->stats.kernel_launches++;
         launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, X, Xi, p, a->G2, p, p, W, Wi, 1, n, W, Wi, nullptr, nullptr);
@@ -1467,7 +1447,6 @@ int refine(oapb_arnoldi* a, double tol, double rho, double res0, const std::vect
       // D = (P A D + R) T^-1
       a->stats.kernel_launches++;
       launch_dependent(k_block_update<C>, dim3(grid_up(n)), dim3(256), 0, a->stream, W, Wi, p, a->Tinv, p, p, nullptr, nullptr, 0, n, D, Di, R, Ri);
-      dsplit = false;
     }
     // X <- orth(X + D): X is orthonormal and D orthogonal to it, so X + D is
     // conditioned like 1 + ||D|| and one CholeskyQR pass is orthonormal to
