@@ -51,12 +51,13 @@ def test_planted_symmetric_n256():
     assert np.allclose(np.sort(o["eigenvalues"].real), np.sort(r["ev"].real), rtol=1e-12)
 
 
-def test_real_symmetric_takes_tridiagonal_path():
+@pytest.mark.parametrize("m", [24, 40])
+def test_real_symmetric_takes_tridiagonal_path(m):
     # a real symmetric operator: the restart loop's small eigensolves take the
-    # symmetric tridiagonal QR; eigenpairs against the known spectrum and the
-    # host FP64 residuals
+    # symmetric tridiagonal QR (four warps for m <= 32, one above); eigenpairs
+    # against the known spectrum and the host FP64 residuals
     A, lam = planted_symmetric(512, seed=4)
-    r = solve(A, 6, 24, vectors=True)
+    r = solve(A, 6, m, vectors=True)
     assert r["stats"]["symtri"] > 0
     assert np.allclose(np.sort(r["ev"].real)[::-1], lam[:6], rtol=1e-10, atol=0)
     assert r["res"].max() <= TOL
@@ -67,7 +68,7 @@ def test_real_symmetric_takes_tridiagonal_path():
     # both agree on the perturbed operator's eigenvalues (numpy as the judge)
     rng = np.random.default_rng(9)
     P = A + 1e-6 * rng.normal(size=A.shape) / np.sqrt(512)
-    rp = solve(P, 6, 24)
+    rp = solve(P, 6, m)
     assert rp["stats"]["symtri"] == 0
     ref = np.linalg.eigvals(P)
     ref = ref[np.argsort(-np.abs(ref))][:6]
