@@ -65,7 +65,7 @@ def test_real_symmetric_takes_tridiagonal_path(m):
     for q in range(6):
         assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * lam[0]
     # a small non-symmetric perturbation keeps the general Schur path, and
-    # both agree on the perturbed operator's eigenvalues (numpy as the judge)
+    # its eigenvalues agree with numpy's for the perturbed operator
     rng = np.random.default_rng(9)
     P = A + 1e-6 * rng.normal(size=A.shape) / np.sqrt(512)
     rp = solve(P, 6, m)
