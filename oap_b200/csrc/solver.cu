@@ -438,6 +438,8 @@ struct oapb_arnoldi {
   const double* a64im = nullptr;
   double* own64re = nullptr;   // library-owned FP64 copy (host-input solves)
   double* own64im = nullptr;
+  double* hvre = nullptr;      // row-major eigenvectors staged for the host (n x k each)
+  double* hvim = nullptr;
   float* a32re = nullptr;
   float* a32im = nullptr;
   bool fp32_ready = false;   // a32 holds the current operator (built on first use)
@@ -1731,7 +1733,7 @@ void drop_gram_stream(oapb_arnoldi* a) {
 
 void free_all(oapb_arnoldi* a) {
   drop_gram_stream(a);
-  void* ps[] = {a->own64re, a->own64im, a->a32re, a->a32im, a->Vre, a->Vim, a->Xre, a->Xim, a->fre,
+  void* ps[] = {a->own64re, a->own64im, a->hvre, a->hvim, a->a32re, a->a32im, a->Vre, a->Vim, a->Xre, a->Xim, a->fre,
                 a->fim, a->wre, a->wim, a->x32re, a->x32im, a->v0re, a->v0im, a->H, a->Qs, a->ritz,
                 a->Y, a->h, a->s, a->part, a->hws, a->est, a->fpart, a->order, a->st};
   for (void* p : ps)
@@ -2322,22 +2324,20 @@ int oapb_arnoldi_solve_host(oapb_arnoldi* a, const double* hre, const double* hi
   int st = oapb_arnoldi_solve(a, eig_re, eig_im, residuals, nullptr);
   if (st != OAPB_OK && st != OAPB_NOT_CONVERGED) return st;
   if (vre || vim) {
-    double *dre = nullptr, *dim = nullptr;
+    // staging buffers kept with the handle (a free would synchronise the
+    // device on every call)
     const long nk = (long)a->n * a->k;
-    if (dalloc(&dre, sizeof(double) * nk)) return OAPB_ERR_NOMEM;
-    if (a->is_c && dalloc(&dim, sizeof(double) * nk)) {
-      cudaFree(dre);
-      return OAPB_ERR_NOMEM;
-    }
+    if (!a->hvre && dalloc(&a->hvre, sizeof(double) * nk)) return OAPB_ERR_NOMEM;
+    if (a->is_c && !a->hvim && dalloc(&a->hvim, sizeof(double) * nk)) return OAPB_ERR_NOMEM;
     ++a->stats.kernel_launches;
-    k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(a->Xre, a->is_c ? a->Xim : nullptr,
-                                                                                  a->n, a->k, dre, dim);
-    if (vre) cudaMemcpyAsync(vre, dre, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream);
-    if (vim && dim) cudaMemcpyAsync(vim, dim, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream);
-    cudaError_t e = cudaStreamSynchronize(a->stream);
-    cudaFree(dre);
-    if (dim) cudaFree(dim);
-    if (e != cudaSuccess) return OAPB_ERR_CUDA;
+    k_vectors_to_rowmajor<<<grid_for(nk, 256, kNumSMs * 8), 256, 0, a->stream>>>(
+        a->Xre, a->is_c ? a->Xim : nullptr, a->n, a->k, a->hvre, a->is_c ? a->hvim : nullptr);
+    if (vre && cudaMemcpyAsync(vre, a->hvre, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    if (vim && a->is_c &&
+        cudaMemcpyAsync(vim, a->hvim, sizeof(double) * nk, cudaMemcpyDeviceToHost, a->stream) != cudaSuccess)
+      return OAPB_ERR_CUDA;
+    if (cudaStreamSynchronize(a->stream) != cudaSuccess) return OAPB_ERR_CUDA;
   }
   return st;
 }
