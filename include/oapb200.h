@@ -278,8 +278,8 @@ typedef struct oapb_arnoldi_stats {
   double pass_kernel_seconds[3];
   uint32_t pass_kernel_timed[3];
   uint32_t symtri;           /* restart-loop eigensolves of the last plain solve
-                                that took the real symmetric tridiagonal path
-                                (real symmetric operators) */
+                                that took the Hermitian tridiagonal path
+                                (Hermitian or real symmetric operators) */
 } oapb_arnoldi_stats;
 
 typedef struct oapb_arnoldi oapb_arnoldi;   /* opaque solver handle */

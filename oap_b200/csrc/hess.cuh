@@ -8,8 +8,8 @@
 //      |T[i][i-1]| <= eps (|T[i-1][i-1]| + |T[i][i]|)), the restatement of
 //      calculateTriangularHEigens (ArnoldiProcedures.cpp:341-349) with a
 //      shifted, deflating iteration instead of the reference's unshifted
-//      one; for a real symmetric H (a real symmetric operator) the implicit
-//      symmetric tridiagonal QR instead;
+//      one; for a Hermitian H (a Hermitian or real symmetric operator) the
+//      implicit symmetric tridiagonal QR instead;
 //   2. Ritz values = diag(T), sorted by the ArnUtils order
 //      (ArnoldiUtils.cpp:24-50); wanted = first k (getWanted,
 //      ArnoldiProcedures.cpp:381-398);
@@ -58,7 +58,7 @@ struct DevState {
   double maxest;    // max relative Ritz estimate of the wanted set
   cplx beta_hat;    // H[k][k-1] after the shifts
   cplx sigma;       // Q[m-1][k-1]
-  int symtri;       // eigensolves that took the real symmetric tridiagonal path
+  int symtri;       // eigensolves that took the Hermitian tridiagonal path
 };
 
 struct HessArgs {
@@ -519,31 +519,37 @@ static __device__ bool warp_schur(Cx* T, Cx* Z, int m, int ld, Cx* rot, int lane
   return true;
 }
 
-// Real symmetric tridiagonal path (the restart loop of a real symmetric
-// operator, whose Hessenberg matrix is symmetric tridiagonal to rounding):
-// d (m) and e (m - 1) real in shared memory; the implicit QR step with
-// shift mu on the window [l, h] (Golub & Van Loan, Matrix Computations,
-// Alg. 8.3.2) runs its rotation chain on lane 0 and records the rotations
-// (c, s) in cs; every lane then applies them to one row of Z (Z <- Z G^T).
-// The rotation of the pair (x, y) is c = x / r, s = y / r (the entries are
-// prescaled, so r^2 stays in range; a pair below tiny2 gives the identity).
+// Hermitian tridiagonal path (the restart loop of a Hermitian operator,
+// real symmetric included, whose Hessenberg matrix is Hermitian tridiagonal
+// to rounding): with the diagonal unitary D of phases D_0 = 1, D_{i+1} =
+// D_i e_i / |e_i| (e_i = H[i+1][i]), H = D T' D^H where T' is real
+// symmetric tridiagonal with diagonal Re H[i][i] and off-diagonal |e_i|.
+// d (m) and e (m - 1) of T' are real in shared memory; Z starts as D and
+// accumulates the real rotations, so Z = D Q' holds the eigenvectors of H
+// (and the exact shifts' Q for the restart, with T' after the shifts as the
+// new H).  The implicit QR step with shift mu on the window [l, h] (Golub &
+// Van Loan, Matrix Computations, Alg. 8.3.2) runs its rotation chain on
+// lane 0 and records the rotations (c, s) in cs; every lane then applies
+// them to one row of Z (Z <- Z G^T).  The rotation of the pair (x, y) is
+// c = x / r, s = y / r (the entries are prescaled, so r^2 stays in range; a
+// pair below tiny2 gives the identity).
 
-// true when T (prescaled: largest entry in [1, 2), m x m) is real and
-// symmetric to rtol: the Arnoldi matrix of a real symmetric operator, whose
-// entries beyond the tridiagonal band and whose asymmetry come from the
-// basis's loss of orthogonality (about 4e-13 of max |H| for an n = 256
+// true when T (prescaled: largest entry in [1, 2), m x m) is Hermitian to
+// rtol: the Arnoldi matrix of a Hermitian operator, whose entries beyond the
+// tridiagonal band and whose departure from Hermitian symmetry come from the
+// basis's loss of orthogonality (about 4e-13 of max |H| for a real n = 256
 // operator with eigenvalues over three decades); they are dropped, which
 // moves the Ritz values by as much, so rtol is a tenth of the residual goal
 // (every result is verified against the operator)
 template <typename Cx>
-static __device__ bool warp_is_real_symmetric(const Cx* T, int m, int ld, double rtol, int lane) {
+static __device__ bool warp_is_hermitian(const Cx* T, int m, int ld, double rtol, int lane) {
   using R = decltype(Cx::re);
   const R tol = (R)rtol;
   int bad = 0;
   for (int e = lane; e < m * m; e += 32) {
     const int r = e % m, c = e / m;
     const Cx a = TT_(r, c), b = TT_(c, r);
-    if (!(abs_t(a.im) <= tol && abs_t(a.re - b.re) <= tol)) bad = 1;
+    if (!(abs_t(a.re - b.re) <= tol && abs_t(a.im + b.im) <= tol)) bad = 1;
   }
   return !__any_sync(0xffffffffu, bad);
 }
@@ -600,12 +606,25 @@ static __device__ int symtri_split(const R* d, const R* e, int h, int lane) {
   return 0;
 }
 
-// T (m x m) <-> d, e
+// T (m x m, Hermitian tridiagonal) -> d, e of T'; Z (the identity on
+// entry) <- D, the phases
 template <typename Cx>
-static __device__ void symtri_load(const Cx* T, int m, int ld, decltype(Cx::re)* d, decltype(Cx::re)* e, int lane) {
+static __device__ void symtri_load(const Cx* T, Cx* Z, int m, int ld, decltype(Cx::re)* d, decltype(Cx::re)* e,
+                                   int lane) {
+  using R = decltype(Cx::re);
   for (int i = lane; i < m; i += 32) {
     d[i] = TT_(i, i).re;
-    if (i + 1 < m) e[i] = TT_(i + 1, i).re;
+    if (i + 1 < m) e[i] = sqrt_t(abs2(TT_(i + 1, i)));
+  }
+  __syncwarp();
+  if (lane == 0) {
+    Cx ph = {1, 0};
+    for (int i = 0; i + 1 < m; ++i) {
+      const Cx sub = TT_(i + 1, i);
+      const R a = e[i];
+      if (a > 0) ph = ph * Cx{sub.re / a, sub.im / a};
+      ZZ_(i + 1, i + 1) = ph;
+    }
   }
   __syncwarp();
 }
@@ -851,18 +870,18 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   const int W = nvec < 32 ? nvec : 32;
   double scale = 0, small = 0;
   const double beta = a.use_beta ? sqrt(st->fnorm2) : a.beta;
-  // real symmetric Hessenberg input: the tridiagonal path (d, e in the
+  // Hermitian Hessenberg input: the tridiagonal path (d, e in the
   // eigenvector scratch, the rotations in rot)
   R* sd = reinterpret_cast<R*>(U);
   R* se = sd + m;
   R* scs = reinterpret_cast<R*>(rot);
   bool sym = false;
   if (warp == 0) {
-    sym = !a.dense && a.tol > 0 && warp_is_real_symmetric(T, m, ld, 0.1 * a.tol, lane);
+    sym = !a.dense && a.tol > 0 && warp_is_hermitian(T, m, ld, 0.1 * a.tol, lane);
     if (sym && lane == 0) st->symtri += 1;
     bool ok;
     if (sym) {
-      symtri_load(T, m, ld, sd, se, lane);
+      symtri_load(T, Z, m, ld, sd, se, lane);
       ok = warp_symtri_eig(sd, se, scs, Z, m, ld, lane);
       if (ok) {
         for (int i = lane; i + 1 < m; i += 32) se[i] = 0;
@@ -955,7 +974,7 @@ static __device__ void hess_core(const HessArgs& a, Cx* T, Cx* Z, Cx* u, double*
   }
   __syncwarp();
   if (sym) {  // the same exact shifts as implicit symmetric tridiagonal steps
-    symtri_load(T, m, ld, sd, se, lane);
+    symtri_load(T, Z, m, ld, sd, se, lane);
     for (int q = k; q < m; ++q) {
       const R mu = u[q].re;
       int hb = m - 1;

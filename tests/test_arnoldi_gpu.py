@@ -76,6 +76,26 @@ def test_real_symmetric_takes_tridiagonal_path(m):
     assert rp["res"].max() <= TOL
 
 
+def test_complex_hermitian_takes_tridiagonal_path():
+    # A = Q diag(lambda) Q^H with a complex unitary Q: the Arnoldi matrix is
+    # Hermitian tridiagonal to rounding, reduced to a real symmetric one by
+    # phases; eigenvalues against the known spectrum, host FP64 residuals
+    n, k, m = 400, 6, 24
+    rng = np.random.default_rng(21)
+    Q, _ = np.linalg.qr(rng.normal(size=(n, n)) + 1j * rng.normal(size=(n, n)))
+    lam = 10.0 ** (-2.0 * np.arange(n) / (n - 1))
+    A = (Q * lam) @ Q.conj().T
+    A = (A + A.conj().T) / 2
+    r = solve(A, k, m, vectors=True)
+    assert r["stats"]["symtri"] > 0
+    assert np.allclose(np.sort(r["ev"].real)[::-1], lam[:k], rtol=1e-10, atol=0)
+    assert np.abs(r["ev"].imag).max() <= 1e-12
+    assert r["res"].max() <= TOL
+    X = r["x"]
+    for q in range(k):
+        assert np.linalg.norm(A @ X[:, q] - r["ev"][q] * X[:, q]) <= TOL * lam[0]
+
+
 @pytest.mark.parametrize("idx", range(4))
 def test_reference_known_spectrum(golden, idx):
     # oapArnoldiPackageMatricesTests.cpp:244-266 (SortLargestReValues)
