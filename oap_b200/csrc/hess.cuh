@@ -1096,7 +1096,18 @@ static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restri
   int* pv = reinterpret_cast<int*>(dinv + m); // m
   const int lane = threadIdx.x, q = blockIdx.x;
   if (m < 1 || m > 32 || q >= m) return;
-  for (int e = lane; e < m * m; e += 32) T[(e % m) + (e / m) * LD] = Tin[e];
+  // T scaled by the power of two that puts its largest |re| or |im| in
+  // [1, 2) (exact): the pivots' squared moduli below stay in range; the
+  // value is unscaled on output
+  double mx = 0;
+  for (int e = lane; e < m * m; e += 32) mx = fmax(mx, fmax(fabs(Tin[e].re), fabs(Tin[e].im)));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  int ex = 0;
+  if (mx > 0 && mx <= 1.7e308) frexp(mx, &ex);
+  ex = ex > 1000 ? 1000 : (ex < -1000 ? -1000 : ex);
+  const double sig = ldexp(1.0, 1 - ex), isig = ldexp(1.0, ex - 1);
+  for (int e = lane; e < m * m; e += 32) T[(e % m) + (e / m) * LD] = sig * Tin[e];
   __syncwarp();
   double fro = 0;
   for (int e = lane; e < m * m; e += 32) fro += abs2(T[(e % m) + (e / m) * LD]);
@@ -1214,7 +1225,7 @@ static __global__ void __launch_bounds__(32) k_eig_near_tri(const cplx* __restri
     }
     for (int i = lane; i < m; i += 32) V[i + (size_t)q * m] = x[i];
     if (lane == 0) {
-      th[q] = thq;
+      th[q] = isig * thq;
       if (!(rq <= 64 * eps * fro)) ok[0] = 0;
     }
   }
